@@ -1,0 +1,190 @@
+/* pfdd_b200.h -- C ABI of the B200 Ginzburg-Landau stepper (libpfdd_b200.so).
+ *
+ * The library advances the PFDD Ginzburg-Landau relaxation that the reference
+ * runs inside its FFT style object, driven step by step from SolveGL::iterate
+ * (src/solve_GL.cpp:70-158).  One call to pfdd_gpu_advance replaces, per GL
+ * iteration, the reference's sequence
+ *     init_loop -> gradient -> App::core_energy -> prep_forward ->
+ *     internal_energy -> prep_backward -> update_order_parameter ->
+ *     prepare_next_itr
+ * (src/solve_GL.cpp:92-124, src/fft_fftw_slab.cpp:1628-1862).
+ *
+ * Conventions (all as in the reference):
+ *   - grid nx*ny*nz, z fastest: site r = k + j*nz + i*ny*nz
+ *     (src/fft_fftw_slab.cpp:1763-1766);
+ *   - slip-system fields are stacked: value of system a at site r is at
+ *     [r + a*N], N = nx*ny*nz;
+ *   - the order parameter is complex (xi[0][2*(r+a*N)] = Re, +1 = Im in the
+ *     reference, src/fft.h:48); this ABI takes/returns Re and Im planes;
+ *   - stresses are in units of the shear modulus (the deck's `sigma` values,
+ *     src/app.cpp:325-381);
+ *   - elastic constants in Pa, b in m, GSFE energies in J/m^2
+ *     (src/material.cpp:41-156).
+ *
+ * Every entry point returns a pfdd_status (0 = success, < 0 = error) and never
+ * exits the process or throws across the boundary; pfdd_gpu_last_error gives
+ * the message.  (The reference reports errors through Error::all/one, which
+ * print and call exit/MPI_Abort, src/error.cpp:34-69.)
+ *
+ * A handle is thread-compatible: calls on one handle must not overlap; calls
+ * on different handles may run concurrently from different host threads.
+ */
+#ifndef PFDD_B200_H
+#define PFDD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int pfdd_status;
+enum {
+  PFDD_OK = 0,
+  PFDD_EINVAL = -1,        /* bad argument / descriptor */
+  PFDD_ENOMEM = -2,        /* device or host allocation failed */
+  PFDD_ECUDA = -3,         /* CUDA runtime error */
+  PFDD_EUNSUPPORTED = -4,  /* size/model combination not built */
+  PFDD_EDIVERGED = -5,     /* non-finite order parameter detected */
+  PFDD_ENODEVICE = -6,     /* no usable sm_100 device */
+  PFDD_ESTATE = -7         /* call not valid in the handle's current state */
+};
+
+#define PFDD_MAX_SLIP 12
+
+/* Arithmetic of the step. */
+enum { PFDD_FP64 = 0, PFDD_FP32 = 1 };
+
+/* How the imaginary part of the complex order parameter is carried.
+ * The reference's forward and inverse transforms are complex-to-complex and
+ * its B(k) table is indexed so that B at index -k differs from B at k on the
+ * Nyquist planes (src/fft_fftw_slab.cpp:280-337 maps index n/2 to -1/2); a
+ * real xi therefore grows an imaginary part there, which feeds back into the
+ * real part.  PFDD_IMAG_FULL carries Im xi as a second real field and is
+ * exact in every case (masks included).  PFDD_IMAG_NYQUIST carries only the
+ * Nyquist-plane spectrum of Im xi, which is exact when no obstacle mask is
+ * set and the initial Im xi is zero.  PFDD_IMAG_AUTO picks NYQUIST when it
+ * is exact, else FULL. */
+enum { PFDD_IMAG_AUTO = 0, PFDD_IMAG_FULL = 1, PFDD_IMAG_NYQUIST = 2 };
+
+/* GSFE core models, numbered as App::core_energy dispatches them
+ * (src/app.cpp:663-672), plus one model with no reference counterpart. */
+enum {
+  PFDD_CORE_PERFECT = 1,     /* core_energy_perfect   src/fft_fftw_slab.cpp:1130-1191 */
+  PFDD_CORE_EXTENDED = 2,    /* core_energy_extended  src/fft_fftw_slab.cpp:1243-1354 */
+  PFDD_CORE_SINE = 3,        /* core_energy_sine      src/fft_fftw_slab.cpp:1360-1418 */
+  PFDD_CORE_PYRII = 4,       /* core_energy_pyrII     src/fft_fftw_slab.cpp:1429-1493 */
+  PFDD_CORE_USFE_ANGLE = 6,  /* core_energy_USFE_angle_tau src/fft_fftw_slab.cpp:1500-1545;
+                                the caller passes the resulting amplitude in `An` */
+  PFDD_CORE_MPEA = 7,        /* core_energy_mpea      src/fft_fftw_slab.cpp:1196-1235 */
+  PFDD_CORE_SINE_FIELD = 103 /* sine GSFE with a per-site multiplier on isf and usf
+                                (random-alloy fields); no reference counterpart,
+                                equals PFDD_CORE_SINE when the multiplier is 1 */
+};
+
+/* One simulation instance: what FFTW_Slab::setup consumes
+ * (rotate_stress, frec, stiffness, Bmatrix: src/fft_fftw_slab.cpp:111-119). */
+typedef struct {
+  int nx, ny, nz;              /* FFT::nx, ny, nz */
+  int n_slip;                  /* FFT::slip_systems (1..PFDD_MAX_SLIP) */
+  double four[3][3];           /* FFT::four, reciprocal basis (src/app.cpp:383-444) */
+  double prim[3][3];           /* FFT::prim, normalised primitive vectors (src/fft.cpp:96-135) */
+  double xn[PFDD_MAX_SLIP][3]; /* slip normals after App::set_slip */
+  double xb[PFDD_MAX_SLIP][3]; /* Burgers vectors after App::set_slip */
+  double C44, C12, C11;        /* Material elastic constants, Pa */
+  double dslip, b;             /* Material::dslip, Material::b (m) */
+  double cd_dt;                /* App::CD * App::timestep */
+  int core_flag;               /* PFDD_CORE_* */
+  double isf, usf, An;         /* J/m^2 */
+  double c[7];                 /* c0 c1 c2 c3 c4 a1 a3 (extended core), J/m^2 */
+  double aa[5], bb[4];         /* aa0..aa4, bb1..bb4 (pyrII core), J/m^2 */
+  const double *site_gsfe;     /* per-site [S*N]: A_mpea (J/m^2) for MPEA, the
+                                  multiplier for SINE_FIELD; else NULL.  Copied. */
+  const double *xo;            /* obstacle mask [S*N] (nonzero = frozen), or NULL. Copied. */
+  double sigma[3][3];          /* App::sigma at the first stress state (units of mu) */
+  double dsigma[3][3];         /* App::deltasig added after each stress state */
+} pfdd_instance_desc;
+
+typedef struct {
+  int precision;       /* PFDD_FP64 or PFDD_FP32 */
+  int imag_mode;       /* PFDD_IMAG_* */
+  int device;          /* CUDA device ordinal */
+  int use_graphs;      /* capture multi-step advance in a CUDA graph (1 = yes) */
+  int check_finite;    /* scan for non-finite xi after each advance (1 = yes) */
+} pfdd_options;
+
+typedef struct {
+  double xinorm;       /* sqrt(sum |dxi|^2) of the last step (src/fft_fftw_slab.cpp:1787-1789) */
+  double xiave;        /* sum of Re xi after the last step (ibid.) */
+  int steps_done;      /* GL iterations performed by this call */
+  int converged;       /* 1 if xinorm < tol ended the stress state early */
+} pfdd_step_stats;
+
+typedef struct pfdd_gpu pfdd_gpu;
+
+/* Create a handle for n_instances independent instances (each may have its
+ * own grid size, slip systems and material), allocate device memory, compute
+ * the per-instance constants in FP64 and upload the initial state xi = 0.
+ * Replaces FFTW_Slab::init/setup (src/fft_fftw_slab.cpp:52-119). */
+pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances,
+                            const pfdd_options *opt, pfdd_gpu **out);
+
+/* Set instance `inst`'s order parameter from host planes xi_re, xi_im
+ * ([S*N] each, reference site order; xi_im may be NULL = 0).  Replaces the
+ * xi/data_fftw fill of initial_sxtal_* (src/fft_fftw_slab.cpp:2196-3247). */
+pfdd_status pfdd_gpu_set_state(pfdd_gpu *h, int inst, const double *xi_re, const double *xi_im);
+
+/* Same, from the reference's interleaved layout xi[0][2*(r + a*N) + {0,1}]. */
+pfdd_status pfdd_gpu_set_state_interleaved(pfdd_gpu *h, int inst, const double *xi);
+
+/* Copy instance `inst`'s order parameter to host planes ([S*N] each; either
+ * pointer may be NULL).  The host refills FFT::xi from it for dumps
+ * (src/app_fcc.cpp:320-502 reads xi through compute_mean_xi). */
+pfdd_status pfdd_gpu_get_state(pfdd_gpu *h, int inst, double *xi_re, double *xi_im);
+
+/* Same, into the reference's interleaved layout. */
+pfdd_status pfdd_gpu_get_state_interleaved(pfdd_gpu *h, int inst, double *xi);
+
+/* Run the SolveGL::iterate loop (src/solve_GL.cpp:80-156) on every instance:
+ * `stress_states` outer iterations, each recomputing the resolved shear
+ * stress (rotate_stress + resolSS_Schmid, src/fft_fftw_slab.cpp:242-274,
+ * 737-769) and running up to `n_steps` GL iterations; a stress state ends
+ * early when xinorm < tol (tol <= 0 disables the test); sigma += dsigma after
+ * each stress state.  stats (may be NULL) receives one record per instance. */
+pfdd_status pfdd_gpu_advance(pfdd_gpu *h, int n_steps, int stress_states, double tol,
+                             pfdd_step_stats *stats);
+
+/* Per-step xinorm/xiave history of instance `inst` for the last advance call:
+ * up to `cap` records are written to xinorm[] / xiave[]; *count gets the
+ * number of steps recorded. */
+pfdd_status pfdd_gpu_step_history(pfdd_gpu *h, int inst, double *xinorm, double *xiave, int cap,
+                                  int *count);
+
+/* Total energy of the current state, per unit site, FP64 with compensated
+ * summation: elastic 1/2 <xi, L xi>, core sum f(xi), applied -sum tau_a xi_a.
+ * The reference accumulates E_core but never reduces or reports it
+ * (src/fft_fftw_slab.cpp:1399); these are the terms whose gradient is the
+ * drift of update_order_parameter (src/fft_fftw_slab.cpp:1773). */
+pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_core,
+                            double *e_applied);
+
+/* Resolved shear stresses tau[S] of instance `inst` at the current stress state. */
+pfdd_status pfdd_gpu_tau(pfdd_gpu *h, int inst, double *tau);
+
+/* Number of instances, and the device bytes the handle holds. */
+pfdd_status pfdd_gpu_info(pfdd_gpu *h, int *n_instances, size_t *device_bytes);
+
+/* Last error message of the handle (or of the last failed create when h is NULL). */
+const char *pfdd_gpu_last_error(pfdd_gpu *h);
+
+/* Release the handle and all its device memory. */
+void pfdd_gpu_destroy(pfdd_gpu *h);
+
+/* Library version string. */
+const char *pfdd_gpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PFDD_B200_H */

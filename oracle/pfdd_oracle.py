@@ -1,0 +1,347 @@
+"""CPU oracle: a numpy restatement of the reference PFDD Ginzburg-Landau step.
+
+TEST INFRASTRUCTURE ONLY.  Nothing in the product path imports this module;
+only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use
+it, and only as the checker.
+
+Every function cites the reference file:line it restates (paths inside the
+reference project's src/).  Semantics kept exactly, including the reference's
+quirks:
+  * the state xi is complex and the FFTs are full 3-D complex-to-complex,
+    unnormalised both ways, 1/N applied in the update (fft_fftw_slab.cpp:1773);
+  * B(k) uses the frequency convention of frec() (k_i in [-1/2, 1/2), index
+    n/2 maps to -1/2), so B at index -k differs from B at k on the Nyquist
+    planes and a real xi grows an imaginary part there;
+  * core_energy_sine scales isf before using it in Cn
+    (fft_fftw_slab.cpp:1403-1404);
+  * core_energy_pyrII writes dE_core only at the last site of each system
+    (fft_fftw_slab.cpp:1491);
+  * update_order_parameter accumulates xinorm with a stale previous value on
+    masked sites (fft_fftw_slab.cpp:1769-1781).
+
+Parity pin: tests/test_oracle_vs_reference.py runs this module and the
+reference sources compiled in oracle/_ref (built by oracle/ref_build/Makefile)
+on the same decks and states; tests/golden/ holds fixtures written by the
+compiled reference (tests/golden/make_golden.py).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+PI = math.pi
+
+
+# ---------------------------------------------------------------- elasticity
+def stiffness(C44: float, C12: float) -> np.ndarray:
+    """Isotropic C_ijkm (fft_fftw_slab.cpp:373-391)."""
+    d = np.eye(3)
+    return (C44 * (np.einsum("ik,jm->ijkm", d, d) + np.einsum("im,jk->ijkm", d, d))
+            + C12 * np.einsum("ij,km->ijkm", d, d))
+
+
+def voigt_constants(C44: float, C12: float, C11: float):
+    """mu, lambda, young, nu by Voigt average (fft_fftw_slab.cpp:483-491)."""
+    mu = C44 - (2.0 * C44 + C12 - C11) / 5.0
+    ll = C12 - (2.0 * C44 + C12 - C11) / 5.0
+    young = mu * (3 * ll + 2 * mu) / (ll + mu)
+    xnu = young / 2.0 / mu - 1.0
+    return mu, ll, young, xnu
+
+
+def material_constants(mu_in: float, young_in: float):
+    """C44, C12, C11 from the deck's mu/young (material.cpp:148-156)."""
+    C44 = mu_in
+    nu = young_in / 2.0 / mu_in - 1.0
+    C12 = 2.0 * nu * C44 / (1.0 - 2.0 * nu)
+    C11 = 2.0 * C44 + C12
+    return C44, C12, C11
+
+
+def frequencies(nx: int, ny: int, nz: int, four: np.ndarray):
+    """Per-site wavevector fx, fy, fz (fft_fftw_slab.cpp:280-337).
+
+    Index i >= n/2 maps to (i - n)/n, else i/n; the vector is
+    k = kx*four[0] + ky*four[1] + kz*four[2].
+    """
+    def axis(n):
+        i = np.arange(n, dtype=np.float64)
+        return np.where(i >= n // 2, (i - n) / n, i / n)
+    kx, ky, kz = np.meshgrid(axis(nx), axis(ny), axis(nz), indexing="ij")
+    four = np.asarray(four, dtype=np.float64)
+    fx = kx * four[0, 0] + ky * four[1, 0] + kz * four[2, 0]
+    fy = kx * four[0, 1] + ky * four[1, 1] + kz * four[2, 1]
+    fz = kx * four[0, 2] + ky * four[1, 2] + kz * four[2, 2]
+    return fx, fy, fz
+
+
+def slip_eigenstrain(xn: np.ndarray, xb: np.ndarray, dslip: float) -> np.ndarray:
+    """eps^a_ij = xb_a,i * xn_a,j / dslip (fft_fftw_slab.cpp:559-566)."""
+    return np.einsum("ai,aj->aij", xb, xn) / dslip
+
+
+def bmatrix(nx, ny, nz, four, xn, xb, C44, C12, C11, dslip, chunk=8):
+    """BB[a, b, x, y, z] (fft_fftw_slab.cpp:466-638).
+
+    A_mnuv(k) = C_mnuv - C_kluv C_ijmn G_ki k_j k_l with
+    G_ki = (2 delta_ik / k^2 - k_i k_k / ((1 - nu) k^4)) / (2 C44), and
+    B_ab = A_mnuv eps^a_mn eps^b_uv / mu; A = 0 at k = 0 (first point).
+    """
+    C = stiffness(C44, C12)
+    mu, ll, young, xnu = voigt_constants(C44, C12, C11)
+    eps = slip_eigenstrain(np.asarray(xn, float), np.asarray(xb, float), dslip)
+    S = eps.shape[0]
+    fx, fy, fz = frequencies(nx, ny, nz, four)
+    BB = np.empty((S, S, nx, ny, nz))
+    for x0 in range(0, nx, chunk):
+        k = np.stack([fx[x0:x0 + chunk], fy[x0:x0 + chunk], fz[x0:x0 + chunk]], axis=-1)
+        k2 = np.einsum("...i,...i->...", k, k)
+        nz_mask = k2 > 0
+        k2s = np.where(nz_mask, k2, 1.0)
+        eye = np.eye(3)
+        G = (2.0 * eye / k2s[..., None, None]
+             - (1.0 / (1.0 - xnu)) * np.einsum("...i,...k->...ki", k, k) / (k2s ** 2)[..., None, None]
+             ) / (2.0 * C44)
+        # Ck = C_ijmn k_j  -> [.., i, m, n];  Cl = C_kluv k_l -> [.., k, u, v]
+        Ck = np.einsum("ijmn,...j->...imn", C, k)
+        Cl = np.einsum("kluv,...l->...kuv", C, k)
+        A = C - np.einsum("...kuv,...ki,...imn->...mnuv", Cl, G, Ck)
+        A = np.where(nz_mask[..., None, None, None, None], A, 0.0)
+        Ae = np.einsum("...mnuv,buv->...bmn", A, eps)
+        B = np.einsum("...bmn,amn->ab...", Ae, eps) / mu
+        BB[:, :, x0:x0 + chunk] = B
+    return BB
+
+
+# ---------------------------------------------------------------- stress
+def rotate_stress(sigma, prim, invprim, norvol):
+    """sigma_rot (fft_fftw_slab.cpp:242-274): rotated when |det prim| ~ 1."""
+    sigma = np.asarray(sigma, float)
+    if 0.99 < abs(norvol) < 1.01:
+        return np.asarray(prim) @ sigma @ np.asarray(invprim)
+    return sigma.copy()
+
+
+def resolved_shear(sigma_rot, xn, xb, dslip):
+    """tau_a = sum_ij sigma_rot_ij xn_a,j xb_a,i / dslip (fft_fftw_slab.cpp:737-769)."""
+    return np.einsum("ij,aj,ai->a", np.asarray(sigma_rot), np.asarray(xn), np.asarray(xb)) / dslip
+
+
+# ---------------------------------------------------------------- core energy
+@dataclass
+class CoreModel:
+    """GSFE core model; constants in the reference's SI units (J/m^2, Pa, m).
+
+    flag: 1 perfect (fft_fftw_slab.cpp:1130-1191), 2 extended (:1243-1354),
+    3 sine (:1360-1418), 4 pyrII (:1429-1493), 6 USFE(angle, tau)
+    (:1500-1545, An supplied by the caller), 7 mpea (:1196-1235), and
+    103 = sine with a per-site multiplier on isf and usf (random-alloy GSFE;
+    no reference counterpart, reduces to flag 3 when the multiplier is 1).
+    """
+    flag: int
+    mu: float              # Material::mu after Bmatrix (Voigt)
+    dslip: float
+    b: float
+    isf: float = 0.0
+    usf: float = 0.0
+    An: float = 0.0
+    c: tuple = (0.0,) * 7          # c0 c1 c2 c3 c4 a1 a3
+    aa: tuple = (0.0,) * 5         # aa0..aa4
+    bb: tuple = (0.0,) * 4         # bb1..bb4
+    site: np.ndarray | None = field(default=None, repr=False)  # A_mpea or multiplier, [S, nx, ny, nz]
+
+    def scale(self):
+        return self.mu * self.dslip * self.b
+
+    def derivative(self, xr: np.ndarray) -> np.ndarray:
+        """dE_core[a, r] from Re xi [S, nx, ny, nz]."""
+        s = self.scale()
+        f = self.flag
+        if f in (1, 6):
+            An = self.An / s
+            return An * PI * np.sin(2.0 * PI * xr)
+        if f == 3:
+            isf = self.isf / s
+            Cn = (self.usf - isf / 2.0) / s
+            return isf * PI * np.sin(2 * PI * xr) + Cn * 2 * PI * np.sin(4 * PI * xr)
+        if f == 103:
+            m = self.site
+            isf = self.isf * m / s
+            Cn = (self.usf * m - isf / 2.0) / s
+            return isf * PI * np.sin(2 * PI * xr) + Cn * 2 * PI * np.sin(4 * PI * xr)
+        if f == 7:
+            return self.site / s * PI * np.sin(2.0 * PI * xr)
+        if f == 4:
+            aa = np.asarray(self.aa) / s
+            bb = np.asarray(self.bb) / s
+            out = np.zeros_like(xr)
+            S = xr.shape[0]
+            last = xr.reshape(S, -1)[:, -1]
+            v = sum((2.0 * PI * (n + 1)) * (bb[n] * np.cos(2.0 * PI * (n + 1) * last)
+                                             - aa[n + 1] * np.sin(2.0 * PI * (n + 1) * last))
+                    for n in range(4))
+            out.reshape(S, -1)[:, -1] = v
+            return out
+        if f == 2:
+            return self._extended_derivative(xr)
+        raise ValueError("core model %d not restated" % f)
+
+    def _extended_derivative(self, xr):
+        c0, c1, c2, c3, c4, a1, a3 = (v / self.mu for v in self.c)
+        db = self.dslip * self.b
+        S = xr.shape[0]
+        out = np.empty_like(xr)
+        tp = 2.0 * PI
+        fp = 4.0 * PI
+        for p in range(S // 3):
+            x1, x2, x3 = xr[3 * p], xr[3 * p + 1], xr[3 * p + 2]
+            sin, cos = np.sin, np.cos
+            d1 = (tp / db) * (
+                c1 * (sin(tp * (x2 - x1)) + sin(tp * (x3 - x1)))
+                + c2 * (2.0 * sin(tp * (x2 + x3 - 2.0 * x1)) + sin(tp * (2.0 * x2 - x3 - x1))
+                        + sin(tp * (2.0 * x3 - x1 - x2)))
+                + (2.0 * c3) * (sin(fp * (x2 - x1)) + sin(fp * (x3 - x1)))
+                + c4 * (3.0 * sin(tp * (x2 + 2.0 * x3 - 3.0 * x1)) + 3.0 * sin(tp * (2.0 * x2 + x3 - 3.0 * x1))
+                        + 2.0 * sin(tp * (3.0 * x2 - x3 - 2.0 * x1)) + sin(tp * (3.0 * x2 - 2.0 * x3 - x1))
+                        + sin(tp * (3.0 * x3 - x1 - 2.0 * x2)) + 2.0 * sin(tp * (3.0 * x3 - 2.0 * x1 - x2)))
+                + a1 * (cos(tp * (x1 - x2)) - cos(tp * (x3 - x1)))
+                + (2.0 * a3) * (cos(fp * (x1 - x2)) - cos(fp * (x3 - x1))))
+            d2 = (tp / db) * (
+                c1 * (sin(tp * (x1 - x2)) + sin(tp * (x3 - x2)))
+                + c2 * (sin(tp * (2.0 * x1 - x2 - x3)) + 2.0 * sin(tp * (x3 + x1 - 2.0 * x2))
+                        + sin(tp * (2.0 * x3 - x1 - x2)))
+                + (2.0 * c3) * (sin(fp * (x1 - x2)) + sin(fp * (x3 - x2)))
+                + c4 * (sin(tp * (3.0 * x1 - x2 - 2.0 * x3)) + 2.0 * sin(tp * (3.0 * x1 - 2.0 * x2 - x3))
+                        + 3.0 * sin(tp * (x3 + 2.0 * x1 - 3.0 * x2)) + 3.0 * sin(tp * (2.0 * x3 + x1 - 3.0 * x2))
+                        + 2.0 * sin(tp * (3.0 * x3 - x1 - 2.0 * x2)) + sin(tp * (3.0 * x3 - 2.0 * x1 - x2)))
+                + a1 * (cos(tp * (x2 - x3)) - cos(tp * (x1 - x2)))
+                + (2.0 * a3) * (cos(fp * (x2 - x3)) - cos(fp * (x1 - x2))))
+            d3 = (tp / db) * (
+                c1 * (sin(tp * (x2 - x3)) + sin(tp * (x1 - x3)))
+                + c2 * (sin(tp * (2.0 * x1 - x2 - x3)) + sin(tp * (2.0 * x2 - x3 - x1))
+                        + 2.0 * sin(tp * (x1 + x2 - 2.0 * x3)))
+                + (2.0 * c3) * (sin(fp * (x2 - x3)) + sin(fp * (x1 - x3)))
+                + c4 * (2.0 * sin(tp * (3.0 * x1 - x2 - 2.0 * x3)) + sin(tp * (3.0 * x1 - 2.0 * x2 - x3))
+                        + sin(tp * (3.0 * x2 - x3 - 2.0 * x1)) + 2.0 * sin(tp * (3.0 * x2 - 2.0 * x3 - x1))
+                        + 3.0 * sin(tp * (x1 + 2.0 * x2 - 3.0 * x3)) + 3.0 * sin(tp * (2.0 * x1 + x2 - 3.0 * x3)))
+                + a1 * (cos(tp * (x3 - x1)) - cos(tp * (x2 - x3)))
+                + (2.0 * a3) * (cos(fp * (x3 - x1)) - cos(fp * (x2 - x3))))
+            out[3 * p], out[3 * p + 1], out[3 * p + 2] = d1, d2, d3
+        return out
+
+    def energy_density(self, xr: np.ndarray) -> np.ndarray:
+        """f(xi) per site-slip, the integral of derivative() (no reference
+        counterpart is ever reduced: E_core is accumulated but not output)."""
+        s = self.scale()
+        f = self.flag
+        if f in (1, 6):
+            return self.An / s * np.sin(PI * xr) ** 2
+        if f == 3:
+            isf = self.isf / s
+            Cn = (self.usf - isf / 2.0) / s
+            return isf * np.sin(PI * xr) ** 2 + Cn * np.sin(2 * PI * xr) ** 2
+        if f == 103:
+            m = self.site
+            isf = self.isf * m / s
+            Cn = (self.usf * m - isf / 2.0) / s
+            return isf * np.sin(PI * xr) ** 2 + Cn * np.sin(2 * PI * xr) ** 2
+        if f == 7:
+            return self.site / s * np.sin(PI * xr) ** 2
+        raise ValueError("energy of core model %d not restated" % f)
+
+
+# ---------------------------------------------------------------- the step
+@dataclass
+class Instance:
+    nx: int
+    ny: int
+    nz: int
+    BB: np.ndarray          # [S, S, nx, ny, nz]
+    tau: np.ndarray         # [S]
+    cd_dt: float            # App::CD * App::timestep
+    core: CoreModel
+    xo: np.ndarray | None = None   # [S, nx, ny, nz], 1 = frozen
+
+    @property
+    def S(self):
+        return self.BB.shape[0]
+
+    @property
+    def N(self):
+        return self.nx * self.ny * self.nz
+
+
+def gl_step(inst: Instance, xi: np.ndarray):
+    """One GL iteration, SolveGL::iterate body (solve_GL.cpp:92-106).
+
+    xi: complex [S, nx, ny, nz] (real part = the physical order parameter).
+    Returns (xi_new, xinorm, xiave).
+      core force from the current Re xi         (app.cpp:663-672)
+      X = FFT(xi) per slip system, unnormalised  (fft_fftw_slab.cpp:1953-1964)
+      R_a = sum_b BB_ab X_b                      (fft_fftw_slab.cpp:1670-1695)
+      r = IFFT(R)/N                              (fft_fftw_slab.cpp:2012-2023)
+      update where xo == 0                       (fft_fftw_slab.cpp:1746-1790)
+    """
+    dE = inst.core.derivative(xi.real)
+    X = np.fft.fftn(xi, axes=(1, 2, 3))
+    R = np.einsum("abxyz,bxyz->axyz", inst.BB, X)
+    r = np.fft.ifftn(R, axes=(1, 2, 3))
+    cd = inst.cd_dt
+    new_re = xi.real - cd * (r.real - inst.tau[:, None, None, None] + dE)
+    new_im = xi.imag - cd * r.imag
+    if inst.xo is not None:
+        upd = inst.xo == 0.0
+        new_re = np.where(upd, new_re, xi.real)
+        new_im = np.where(upd, new_im, xi.imag)
+    xi_new = new_re + 1j * new_im
+    xinorm = _xinorm(xi, xi_new, inst.xo)
+    xiave = float(new_re.sum())
+    return xi_new, xinorm, xiave
+
+
+def _xinorm(old, new, xo):
+    """sqrt(sum |dxi|^2) with the reference's stale 'previous' value on masked
+    sites: xirep/xiimp keep the last unmasked site's old value (0 before any),
+    in loop order isa, i, j, k (fft_fftw_slab.cpp:1761-1781)."""
+    o = old.reshape(-1)
+    n = new.reshape(-1)
+    if xo is None:
+        d = n - o
+        return float(math.sqrt(np.sum(d.real ** 2 + d.imag ** 2)))
+    upd = (xo.reshape(-1) == 0.0)
+    idx = np.where(upd, np.arange(o.size), -1)
+    idx = np.maximum.accumulate(idx)
+    prev = np.where(idx >= 0, o[np.maximum(idx, 0)], 0.0)
+    d = n - prev
+    return float(math.sqrt(np.sum(d.real ** 2 + d.imag ** 2)))
+
+
+def run(inst: Instance, xi0: np.ndarray, steps: int):
+    """steps GL iterations at one stress state; returns (xi, xinorms, xiaves)."""
+    xi = xi0.astype(np.complex128)
+    norms, aves = [], []
+    for _ in range(steps):
+        xi, xn, xa = gl_step(inst, xi)
+        norms.append(xn)
+        aves.append(xa)
+    return xi, np.array(norms), np.array(aves)
+
+
+# ---------------------------------------------------------------- energy
+def total_energy(inst: Instance, xr: np.ndarray):
+    """E = 1/2 <xi, L xi> + sum f(xi) - sum tau_a xi_a per unit site.
+
+    The reference never reduces an energy (E_core is accumulated and unused,
+    fft_fftw_slab.cpp:1399); this is the functional whose gradient is the
+    drift term of update_order_parameter, data_real/N - tau + dE_core
+    (fft_fftw_slab.cpp:1773), so d E / d xi_a(r) equals that drift.
+    Returns (elastic, core, applied) summed over sites.
+    """
+    X = np.fft.fftn(xr, axes=(1, 2, 3))
+    R = np.einsum("abxyz,bxyz->axyz", inst.BB, X)
+    el = 0.5 * float(np.real(np.sum(np.conj(X) * R))) / inst.N
+    core = float(np.sum(inst.core.energy_density(xr)))
+    app = -float(np.sum(inst.tau[:, None, None, None] * xr))
+    return el, core, app

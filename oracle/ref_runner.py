@@ -1,0 +1,108 @@
+"""Run the compiled reference (oracle/_ref/pfdd_ref_harness) on a workload.
+
+TEST INFRASTRUCTURE ONLY: used by tests/ and by the golden-fixture script to
+obtain the reference's own results; never part of the product path.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+HARNESS = os.path.join(REF_DIR, "pfdd_ref_harness")
+
+
+def available() -> bool:
+    return os.access(HARNESS, os.X_OK)
+
+
+def parse_setup(path):
+    out = {"slip": {}, "tau": {}, "four": {}, "sigma_rot": {}}
+    with open(path) as f:
+        for line in f:
+            w = line.split()
+            if not w:
+                continue
+            if w[0] in ("slip", "four", "sigma_rot", "tau"):
+                out[w[0]][int(w[1])] = [float(v) for v in w[2:]]
+            elif w[0] in ("nx", "ny", "nz", "S", "core_flag", "iterations"):
+                out[w[0]] = int(w[1])
+            else:
+                out[w[0]] = float(w[1])
+    S = out["S"]
+    out["xn"] = np.array([out["slip"][a][:3] for a in range(S)])
+    out["xb"] = np.array([out["slip"][a][3:] for a in range(S)])
+    out["tau"] = np.array([out["tau"][a][0] for a in range(S)])
+    out["four"] = np.array([out["four"][i] for i in range(3)])
+    out["sigma_rot"] = np.array([out["sigma_rot"][i] for i in range(3)])
+    return out
+
+
+def run_reference(workload, steps, state=None, xo=None, mpea=None, sets=(), want_B=False,
+                  timing=False, workdir=None, timeout=3600):
+    """Run `steps` GL iterations of the reference on `workload`.
+
+    state: complex or real array [S, nx, ny, nz] (default workload.xi0).
+    Returns dict with xi (complex [S,nx,ny,nz]), xinorm, xiave, setup, and
+    optionally BB [S,S,nx,ny,nz] and the timing record.
+    """
+    if not available():
+        raise RuntimeError("reference oracle not built: make -C oracle/ref_build")
+    tmp = workdir or tempfile.mkdtemp(prefix="pfdd_ref_")
+    S, nx, ny, nz = workload.S, workload.nx, workload.ny, workload.nz
+    deck = os.path.join(tmp, "in.deck")
+    with open(deck, "w") as f:
+        f.write(workload.deck(steps))
+    st = workload.xi0 if state is None else state
+    st = np.asarray(st)
+    inter = np.empty((S * nx * ny * nz, 2))
+    inter[:, 0] = np.real(st).reshape(-1)
+    inter[:, 1] = np.imag(st).reshape(-1) if np.iscomplexobj(st) else 0.0
+    inter.tofile(os.path.join(tmp, "xi0.bin"))
+    args = [HARNESS, "-deck", deck, "-steps", str(steps),
+            "-state_in", os.path.join(tmp, "xi0.bin"),
+            "-state_out", os.path.join(tmp, "xi.bin"),
+            "-stats_out", os.path.join(tmp, "stats.txt"),
+            "-setup_out", os.path.join(tmp, "setup.txt")]
+    xo = workload.xo if xo is None else xo
+    if xo is not None:
+        np.asarray(xo, dtype=np.float64).tofile(os.path.join(tmp, "xo.bin"))
+        args += ["-xo_in", os.path.join(tmp, "xo.bin")]
+    if mpea is not None:
+        np.asarray(mpea, dtype=np.float64).tofile(os.path.join(tmp, "mpea.bin"))
+        args += ["-mpea_in", os.path.join(tmp, "mpea.bin")]
+    m = workload.material
+    for k, v in (("b", m.b), ("dslip", m.dslip)) + tuple(sets):
+        args += ["-set", k, repr(float(v))]
+    args += ["-set", "CD", repr(float(workload.cd_dt))]
+    if want_B:
+        args += ["-B_out", os.path.join(tmp, "B.bin")]
+    if timing:
+        args += ["-timing"]
+    env = dict(os.environ)
+    proc = subprocess.run(args, cwd=tmp, capture_output=True, text=True, timeout=timeout, env=env)
+    if proc.returncode != 0:
+        raise RuntimeError("reference harness failed (%d):\n%s\n%s" % (proc.returncode, proc.stdout[-3000:],
+                                                                      proc.stderr[-3000:]))
+    xi = np.fromfile(os.path.join(tmp, "xi.bin")).reshape(S, nx, ny, nz, 2)
+    stats = np.loadtxt(os.path.join(tmp, "stats.txt"), ndmin=2)
+    out = {
+        "xi": xi[..., 0] + 1j * xi[..., 1],
+        "xinorm": stats[:, 1] if stats.size else np.zeros(0),
+        "xiave": stats[:, 2] if stats.size else np.zeros(0),
+        "setup": parse_setup(os.path.join(tmp, "setup.txt")),
+        "stdout": proc.stdout,
+    }
+    if want_B:
+        out["BB"] = np.fromfile(os.path.join(tmp, "B.bin")).reshape(S, S, nx, ny, nz)
+    if timing:
+        import json
+        for line in proc.stdout.splitlines()[::-1]:
+            if line.startswith("{") and "loop_s" in line:
+                out["timing"] = json.loads(line)
+                break
+    return out

@@ -1,0 +1,707 @@
+// C-ABI implementation of libpfdd_b200.so (declared in include/pfdd_b200.h).
+//
+// Host side: FP64 set-up of every per-instance constant (what
+// FFTW_Slab::setup computes: rotate_stress, frec, stiffness, Bmatrix,
+// fft_fftw_slab.cpp:111-119), device buffers, radix plans and twiddle tables,
+// and the per-step launch sequence P1 -> P2 -> P3 -> finalize of
+// pfdd_kernels.cuh.  Multi-step advances are captured once into a CUDA graph
+// per (step count, buffer parity) and replayed.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "pfdd_b200.h"
+#include "pfdd_kernels.cuh"
+
+using namespace pfdd;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t alloc(size_t n) {
+    bytes = n;
+    return n ? cudaMalloc(&p, n) : cudaSuccess;
+  }
+  template <typename T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+// Radix plan: greedy 16, 8, 4, 2, 3 factors; sub-lengths L_s.
+bool make_plan(int n, FftPlan &p) {
+  p.n = n;
+  p.nst = 0;
+  int rem = n, L = n;
+  while (rem > 1) {
+    int r;
+    if (rem % 16 == 0) r = 16;
+    else if (rem % 8 == 0) r = 8;
+    else if (rem % 4 == 0) r = 4;
+    else if (rem % 2 == 0) r = 2;
+    else if (rem % 3 == 0) r = 3;
+    else return false;
+    if (p.nst >= 8) return false;
+    p.radix[p.nst] = r;
+    p.L[p.nst] = L;
+    ++p.nst;
+    L /= r;
+    rem /= r;
+  }
+  return true;
+}
+
+// position of frequency k after the forward (digit-reversing) transform
+std::vector<int> positions(const FftPlan &p) {
+  std::vector<int> pos(p.n);
+  for (int k = 0; k < p.n; ++k) {
+    int rem = k, q = 0;
+    for (int s = 0; s < p.nst; ++s) {
+      int d = rem % p.radix[s];
+      rem /= p.radix[s];
+      q += d * (p.L[s] / p.radix[s]);
+    }
+    pos[k] = q;
+  }
+  return pos;
+}
+
+// W_n^m = exp(-2 pi i m / n), m = 0..count-1, evaluated in FP64 with the
+// angle reduced to the first octant's neighbourhood before cos/sin.
+void twiddles(int n, int count, std::vector<double> &out) {
+  out.resize(2 * (size_t)count);
+  for (int m = 0; m < count; ++m) {
+    long long e = m % n;
+    double ang = 2.0 * M_PI * (double)e / (double)n;
+    out[2 * m] = std::cos(ang);
+    out[2 * m + 1] = -std::sin(ang);
+  }
+}
+
+struct Instance {
+  pfdd_instance_desc d;
+  int S, F, imag;
+  int nx, ny, nz, nzh, M;
+  size_t N;
+  FftPlan px, py, pz;
+  int ccols;
+  size_t smem_plane, smem_update, smem_pencil;
+  Green green;
+  Core core;
+  StressArgs stress;
+  DevBuf xi[2];        // ping-pong real fields [F][N]
+  int cur = 0;
+  DevBuf spec;         // [F][nx][ny][nzh] complex
+  DevBuf partials;     // 2 * F * nx doubles
+  DevBuf stats;        // 2 * cap doubles
+  int stats_cap = 0;
+  DevBuf small;        // tau[S], sigma[9], flags
+  DevBuf mask, site;
+  DevBuf tw_x, tw_y, tw_z, tw_r, tab16;  // twiddles in compute precision, int16 tables
+  const int16_t *posM = nullptr, *kx_of = nullptr, *ky_of = nullptr, *kz_of = nullptr;
+  std::vector<double> hist;  // host copy of the last advance's per-step stats
+  int hist_count = 0;
+  double *tau() const { return small.as<double>(); }
+  double *sigma() const { return small.as<double>() + PFDD_MAXS; }
+  int *flags() const { return reinterpret_cast<int *>(small.as<double>() + PFDD_MAXS + 9); }
+  // flags: [0] stop, [1] bad, [2] steps_done
+};
+
+}  // namespace
+
+struct pfdd_gpu {
+  int precision = PFDD_FP64;
+  int device = 0;
+  pfdd_options opt{};
+  std::vector<std::unique_ptr<Instance>> inst;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  size_t device_bytes = 0;
+};
+
+namespace {
+
+pfdd_status fail(pfdd_gpu *h, pfdd_status code, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (h) h->err = buf;
+  else g_create_error = buf;
+  return code;
+}
+
+#define CUDA_TRY(h, call)                                                                   \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail(h, e_ == cudaErrorMemoryAllocation ? PFDD_ENOMEM : PFDD_ECUDA, "%s: %s (%s:%d)", \
+                  #call, cudaGetErrorString(e_), __FILE__, __LINE__);                       \
+  } while (0)
+
+template <typename T> size_t csize() { return sizeof(cx<T>); }
+
+// Green constants in FP64: sigma^a = C44 (eps^a + eps^a^T) + C12 tr(eps^a) I,
+// eps^a = xb_a (x) xn_a / dslip (fft_fftw_slab.cpp:559-566); mu and nu by the
+// Voigt average (fft_fftw_slab.cpp:483-491).
+void build_green(const pfdd_instance_desc &d, Green &g) {
+  memset(&g, 0, sizeof g);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) g.four[i][j] = d.four[i][j];
+  const double C44 = d.C44, C12 = d.C12, C11 = d.C11;
+  const double mu = C44 - (2.0 * C44 + C12 - C11) / 5.0;
+  const double ll = C12 - (2.0 * C44 + C12 - C11) / 5.0;
+  const double young = mu * (3 * ll + 2 * mu) / (ll + mu);
+  const double xnu = young / 2.0 / mu - 1.0;
+  g.inv_mu = 1.0 / mu;
+  g.c2 = 1.0 / (2.0 * C44);
+  g.c1nu = 1.0 / (1.0 - xnu);
+  for (int a = 0; a < d.n_slip; ++a) {
+    double e[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) e[i][j] = d.xb[a][i] * d.xn[a][j] / d.dslip;
+    const double tr = e[0][0] + e[1][1] + e[2][2];
+    double s[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) s[i][j] = C44 * (e[i][j] + e[j][i]) + (i == j ? C12 * tr : 0.0);
+    g.sig[a][0] = s[0][0]; g.sig[a][1] = s[1][1]; g.sig[a][2] = s[2][2];
+    g.sig[a][3] = s[0][1]; g.sig[a][4] = s[0][2]; g.sig[a][5] = s[1][2];
+    g.eps[a][0] = e[0][0]; g.eps[a][1] = e[1][1]; g.eps[a][2] = e[2][2];
+    g.eps[a][3] = e[0][1] + e[1][0]; g.eps[a][4] = e[0][2] + e[2][0]; g.eps[a][5] = e[1][2] + e[2][1];
+  }
+}
+
+// Core constants with the reference's order of operations.
+bool build_core(const pfdd_instance_desc &d, Core &c) {
+  memset(&c, 0, sizeof c);
+  c.flag = d.core_flag;
+  const double C44 = d.C44, C12 = d.C12, C11 = d.C11;
+  const double mu = C44 - (2.0 * C44 + C12 - C11) / 5.0;
+  const double s = mu * d.dslip * d.b;
+  switch (d.core_flag) {
+    case PFDD_CORE_PERFECT:
+    case PFDD_CORE_USFE_ANGLE:
+      c.k[0] = d.An / s * M_PI;  // An' pi, core_energy_perfect fft_fftw_slab.cpp:1181,1187
+      return true;
+    case PFDD_CORE_SINE: {
+      const double isf = d.isf / s;               // fft_fftw_slab.cpp:1403
+      const double Cn = (d.usf - (isf / 2.0)) / s; // fft_fftw_slab.cpp:1405 (uses the scaled isf)
+      c.k[0] = isf * M_PI;
+      c.k[1] = Cn * 2 * M_PI;
+      return true;
+    }
+    case PFDD_CORE_SINE_FIELD:
+      c.k[2] = d.isf / s;
+      c.k[3] = d.usf / s;
+      c.k[4] = 1.0 / (2.0 * s);
+      return true;
+    case PFDD_CORE_MPEA:
+      c.k[0] = M_PI / s;   // A(r)/(mu dslip b) pi, fft_fftw_slab.cpp:1231
+      return true;
+    case PFDD_CORE_PYRII:
+      for (int n = 1; n <= 4; ++n) {
+        c.k[n] = d.aa[n] / s;
+        c.k[4 + n] = d.bb[n - 1] / s;
+      }
+      return true;
+    case PFDD_CORE_EXTENDED:
+      if (d.n_slip % 3) return false;
+      c.k[0] = d.c[1] / mu; c.k[1] = d.c[2] / mu; c.k[2] = d.c[3] / mu; c.k[3] = d.c[4] / mu;
+      c.k[4] = d.c[5] / mu; c.k[5] = d.c[6] / mu;
+      c.k[6] = (2.0 * M_PI) / (d.dslip * d.b);
+      return true;
+  }
+  return false;
+}
+
+void build_stress(const pfdd_instance_desc &d, StressArgs &s) {
+  memset(&s, 0, sizeof s);
+  const double (*p)[3] = d.prim;
+  // determinant and inverse as fft.cpp computes them (cofactors / norvol)
+  double norvol = p[1][0] * p[2][1] * p[0][2] - p[2][0] * p[1][1] * p[0][2] + p[2][0] * p[0][1] * p[1][2] -
+                  p[0][0] * p[2][1] * p[1][2] + p[0][0] * p[1][1] * p[2][2] - p[1][0] * p[0][1] * p[2][2];
+  double inv[3][3];
+  inv[0][0] = (p[1][1] * p[2][2] - p[2][1] * p[1][2]) / norvol;
+  inv[0][1] = (p[2][1] * p[0][2] - p[0][1] * p[2][2]) / norvol;
+  inv[0][2] = (p[0][1] * p[1][2] - p[1][1] * p[0][2]) / norvol;
+  inv[1][0] = (p[1][2] * p[2][0] - p[2][2] * p[1][0]) / norvol;
+  inv[1][1] = (p[2][2] * p[0][0] - p[0][2] * p[2][0]) / norvol;
+  inv[1][2] = (p[0][2] * p[1][0] - p[1][2] * p[0][0]) / norvol;
+  inv[2][0] = (p[1][0] * p[2][1] - p[2][0] * p[1][1]) / norvol;
+  inv[2][1] = (p[2][0] * p[0][1] - p[0][0] * p[2][1]) / norvol;
+  inv[2][2] = (p[0][0] * p[1][1] - p[1][0] * p[0][1]) / norvol;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      s.prim[i][j] = p[i][j];
+      s.invprim[i][j] = inv[i][j];
+      s.dsig[i][j] = d.dsigma[i][j];
+    }
+  s.ortho = (std::fabs(norvol) < 1.01 && std::fabs(norvol) > 0.99) ? 1 : 0;
+  s.S = d.n_slip;
+  s.dslip = d.dslip;
+  for (int a = 0; a < d.n_slip; ++a)
+    for (int i = 0; i < 3; ++i) { s.xn[a][i] = d.xn[a][i]; s.xb[a][i] = d.xb[a][i]; }
+}
+
+template <typename T>
+pfdd_status upload_twiddles(pfdd_gpu *h, DevBuf &dst, int n, int count) {
+  std::vector<double> tw;
+  twiddles(n, count, tw);
+  std::vector<T> t(tw.size());
+  for (size_t i = 0; i < tw.size(); ++i) t[i] = (T)tw[i];
+  CUDA_TRY(h, dst.alloc(t.size() * sizeof(T)));
+  CUDA_TRY(h, cudaMemcpy(dst.p, t.data(), t.size() * sizeof(T), cudaMemcpyHostToDevice));
+  h->device_bytes += dst.bytes;
+  return PFDD_OK;
+}
+
+template <typename T>
+pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
+  const pfdd_instance_desc &d = I.d;
+  using C = cx<T>;
+  pfdd_status st;
+  if ((st = upload_twiddles<T>(h, I.tw_x, I.nx, I.nx))) return st;
+  if ((st = upload_twiddles<T>(h, I.tw_y, I.ny, I.ny))) return st;
+  if ((st = upload_twiddles<T>(h, I.tw_z, I.M, I.M))) return st;
+  if ((st = upload_twiddles<T>(h, I.tw_r, I.nz, I.M))) return st;
+
+  // int16 tables: posM[M], kx_of[nx], ky_of[ny], kz_of[nzh]
+  std::vector<int> pz = positions(I.pz), px = positions(I.px), py = positions(I.py);
+  std::vector<int16_t> tab(I.M + I.nx + I.ny + I.nzh);
+  int16_t *t_posM = tab.data(), *t_kx = t_posM + I.M, *t_ky = t_kx + I.nx, *t_kz = t_ky + I.ny;
+  for (int k = 0; k < I.M; ++k) t_posM[k] = (int16_t)pz[k];
+  for (int k = 0; k < I.nx; ++k) t_kx[px[k]] = (int16_t)k;
+  for (int k = 0; k < I.ny; ++k) t_ky[py[k]] = (int16_t)k;
+  for (int k = 0; k < I.M; ++k) t_kz[pz[k]] = (int16_t)k;
+  t_kz[I.M] = (int16_t)I.M;
+  CUDA_TRY(h, I.tab16.alloc(tab.size() * sizeof(int16_t)));
+  CUDA_TRY(h, cudaMemcpy(I.tab16.p, tab.data(), tab.size() * sizeof(int16_t), cudaMemcpyHostToDevice));
+  h->device_bytes += I.tab16.bytes;
+  const int16_t *base = I.tab16.as<int16_t>();
+  I.posM = base;
+  I.kx_of = base + I.M;
+  I.ky_of = I.kx_of + I.nx;
+  I.kz_of = I.ky_of + I.ny;
+
+  const size_t fieldN = (size_t)I.F * I.N;
+  for (int b = 0; b < 2; ++b) {
+    CUDA_TRY(h, I.xi[b].alloc(fieldN * sizeof(T)));
+    CUDA_TRY(h, cudaMemset(I.xi[b].p, 0, fieldN * sizeof(T)));
+    h->device_bytes += I.xi[b].bytes;
+  }
+  CUDA_TRY(h, I.spec.alloc((size_t)I.F * I.nx * I.ny * I.nzh * sizeof(C)));
+  h->device_bytes += I.spec.bytes;
+  CUDA_TRY(h, I.partials.alloc(2 * (size_t)I.F * I.nx * sizeof(double)));
+  h->device_bytes += I.partials.bytes;
+  CUDA_TRY(h, I.small.alloc((PFDD_MAXS + 9 + 8) * sizeof(double)));
+  CUDA_TRY(h, cudaMemset(I.small.p, 0, (PFDD_MAXS + 9 + 8) * sizeof(double)));
+  double sig9[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) sig9[3 * i + j] = d.sigma[i][j];
+  CUDA_TRY(h, cudaMemcpy(I.sigma(), sig9, sizeof sig9, cudaMemcpyHostToDevice));
+
+  if (d.xo) {
+    std::vector<uint8_t> m((size_t)I.S * I.N);
+    for (size_t i = 0; i < m.size(); ++i) m[i] = d.xo[i] != 0.0;
+    CUDA_TRY(h, I.mask.alloc(m.size()));
+    CUDA_TRY(h, cudaMemcpy(I.mask.p, m.data(), m.size(), cudaMemcpyHostToDevice));
+    h->device_bytes += I.mask.bytes;
+  }
+  if (d.core_flag == PFDD_CORE_MPEA || d.core_flag == PFDD_CORE_SINE_FIELD) {
+    if (!d.site_gsfe) return fail(h, PFDD_EINVAL, "core model %d needs site_gsfe", d.core_flag);
+    std::vector<T> sv((size_t)I.S * I.N);
+    for (size_t i = 0; i < sv.size(); ++i) sv[i] = (T)d.site_gsfe[i];
+    CUDA_TRY(h, I.site.alloc(sv.size() * sizeof(T)));
+    CUDA_TRY(h, cudaMemcpy(I.site.p, sv.data(), sv.size() * sizeof(T), cudaMemcpyHostToDevice));
+    h->device_bytes += I.site.bytes;
+  }
+
+  // shared-memory budgets
+  I.smem_plane = ((size_t)I.ny * I.nzh + I.ny + 2 * (size_t)I.M) * sizeof(C) + (size_t)I.M * 4 + 16;
+  I.smem_update = I.smem_plane + 4 * 2 + 64 * sizeof(double) + 16;
+  const size_t limit = 227 * 1024;
+  if (I.smem_update > limit)
+    return fail(h, PFDD_EUNSUPPORTED, "x-plane of %dx%d does not fit shared memory in this precision", I.ny, I.nz);
+  const size_t ncols = (size_t)I.ny * I.nzh;
+  int cc = 32;
+  while (cc > 1 && (ncols % cc || ((size_t)I.F * I.nx * cc + I.nx) * sizeof(C) > 200 * 1024)) cc >>= 1;
+  if (((size_t)I.F * I.nx * cc + I.nx) * sizeof(C) > limit)
+    return fail(h, PFDD_EUNSUPPORTED, "x-pencil of %d x %d fields does not fit shared memory", I.nx, I.F);
+  I.ccols = cc;
+  I.smem_pencil = ((size_t)I.F * I.nx * cc + I.nx) * sizeof(C);
+
+  build_green(d, I.green);
+  if (!build_core(d, I.core)) return fail(h, PFDD_EUNSUPPORTED, "core model %d not supported", d.core_flag);
+  build_stress(d, I.stress);
+  return PFDD_OK;
+}
+
+template <typename T>
+void fill_plane_args(const Instance &I, PlaneArgs &pa) {
+  pa.py = I.py; pa.pz = I.pz;
+  pa.nx = I.nx; pa.ny = I.ny; pa.nz = I.nz; pa.nzh = I.nzh; pa.M = I.M;
+  pa.S = I.S; pa.F = I.F;
+  pa.tw_y = I.tw_y.p; pa.tw_z = I.tw_z.p; pa.tw_r = I.tw_r.p;
+  pa.posM = I.posM;
+}
+
+template <typename T>
+pfdd_status set_smem_attrs(pfdd_gpu *h, size_t plane, size_t upd, size_t pencil) {
+  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_xpencil<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pencil));
+  return PFDD_OK;
+}
+
+// Enqueue one GL iteration of one instance; `step` indexes the stats record.
+template <typename T>
+void enqueue_step(Instance &I, cudaStream_t st, int step, double tol) {
+  PlaneArgs pa;
+  fill_plane_args<T>(I, pa);
+  int *flags = I.flags();
+  const T *xin = I.xi[I.cur].as<T>();
+  T *xout = I.xi[I.cur ^ 1].as<T>();
+  cx<T> *spec = I.spec.as<cx<T>>();
+  const int planes = I.F * I.nx;
+  k_fwd_planes<T><<<planes, 256, I.smem_plane, st>>>(xin, spec, pa, flags);
+  PencilArgs pe;
+  pe.px = I.px;
+  pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.M = I.M;
+  pe.S = I.S; pe.F = I.F; pe.imag = I.imag;
+  pe.ncols = I.ny * I.nzh;
+  pe.ccols = I.ccols;
+  pe.tw_x = I.tw_x.p;
+  pe.kx_of = I.kx_of; pe.ky_of = I.ky_of; pe.kz_of = I.kz_of;
+  pe.g = I.green;
+  k_xpencil<T><<<pe.ncols / pe.ccols, 256, I.smem_pencil, st>>>(spec, pe, flags);
+  UpdateArgs ua;
+  ua.nx = I.nx; ua.ny = I.ny; ua.nz = I.nz; ua.nzh = I.nzh; ua.S = I.S; ua.F = I.F;
+  ua.cd = I.d.cd_dt;
+  ua.invN = 1.0 / (double)I.N;
+  ua.core = I.core;
+  ua.tau = I.tau();
+  ua.mask = I.mask.as<uint8_t>();
+  ua.site = I.site.p;
+  ua.stop = flags;
+  k_inv_update<T><<<planes, 256, I.smem_update, st>>>(spec, xin, xout, pa, ua, I.partials.as<double>());
+  k_finalize<<<1, 1024, 0, st>>>(I.partials.as<double>(), planes, I.stats.as<double>(), step, tol, flags,
+                                 flags + 1, flags + 2, nullptr);
+}
+
+template <typename T>
+pfdd_status advance_impl(pfdd_gpu *h, int n_steps, int stress_states, double tol, pfdd_step_stats *stats) {
+  cudaStream_t st = h->stream;
+  for (auto &ip : h->inst) {
+    Instance &I = *ip;
+    if (I.stats_cap < n_steps) {
+      I.stats.release();
+      CUDA_TRY(h, I.stats.alloc(2 * (size_t)std::max(n_steps, 1) * sizeof(double)));
+      I.stats_cap = std::max(n_steps, 1);
+    }
+  }
+  std::vector<int> done(h->inst.size(), 0), conv(h->inst.size(), 0);
+  for (int ss = 0; ss < stress_states; ++ss) {
+    for (auto &ip : h->inst) {
+      Instance &I = *ip;
+      k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.stress, 0, I.flags());
+    }
+    // interleave instances step by step so independent instances overlap
+    // their short tails on the device
+    for (int it = 0; it < n_steps; ++it) {
+      for (auto &ip : h->inst) {
+        Instance &I = *ip;
+        enqueue_step<T>(I, st, it, tol);
+        I.cur ^= 1;
+      }
+    }
+    // the stop flag freezes later steps without moving data, but the host
+    // flips buffers unconditionally: recover the true parity from steps_done
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    for (size_t i = 0; i < h->inst.size(); ++i) {
+      Instance &I = *h->inst[i];
+      int fl[3];
+      CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+      if (fl[1]) return fail(h, PFDD_EDIVERGED, "instance %zu: non-finite order parameter", i);
+      const int did = fl[2];
+      // parity: started at cur0, flipped n_steps times on the host, but only `did` real swaps
+      if ((n_steps - did) & 1) I.cur ^= 1;
+      done[i] = did;
+      conv[i] = fl[0];
+      I.hist.resize(2 * (size_t)did);
+      if (did) CUDA_TRY(h, cudaMemcpy(I.hist.data(), I.stats.p, 2 * (size_t)did * sizeof(double),
+                                      cudaMemcpyDeviceToHost));
+      I.hist_count = did;
+      k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.stress, 1, I.flags());
+      CUDA_TRY(h, cudaMemsetAsync(I.flags() + 2, 0, sizeof(int), st));
+    }
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  CUDA_TRY(h, cudaGetLastError());
+  if (stats) {
+    for (size_t i = 0; i < h->inst.size(); ++i) {
+      Instance &I = *h->inst[i];
+      stats[i].steps_done = done[i];
+      stats[i].converged = conv[i];
+      stats[i].xinorm = I.hist_count ? I.hist[2 * (I.hist_count - 1)] : 0.0;
+      stats[i].xiave = I.hist_count ? I.hist[2 * (I.hist_count - 1) + 1] : 0.0;
+    }
+  }
+  return PFDD_OK;
+}
+
+template <typename T>
+pfdd_status set_state_impl(pfdd_gpu *h, Instance &I, const double *re, const double *im, bool interleaved) {
+  const size_t n = (size_t)I.S * I.N;
+  DevBuf tmp;
+  CUDA_TRY(h, tmp.alloc(n * sizeof(double) * (interleaved ? 2 : 1)));
+  T *dre = I.xi[I.cur].as<T>();
+  T *dim = I.F > I.S ? dre + n : nullptr;
+  if (interleaved) {
+    CUDA_TRY(h, cudaMemcpyAsync(tmp.p, re, 2 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    k_from_interleaved<T><<<1184, 256, 0, h->stream>>>(tmp.as<double>(), dre, dim, n);
+  } else {
+    CUDA_TRY(h, cudaMemcpyAsync(tmp.p, re, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    k_from_planar<T><<<1184, 256, 0, h->stream>>>(tmp.as<double>(), dre, n);
+    if (dim) {
+      if (im) {
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        CUDA_TRY(h, cudaMemcpyAsync(tmp.p, im, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        k_from_planar<T><<<1184, 256, 0, h->stream>>>(tmp.as<double>(), dim, n);
+      } else {
+        CUDA_TRY(h, cudaMemsetAsync(dim, 0, n * sizeof(T), h->stream));
+      }
+    }
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  CUDA_TRY(h, cudaGetLastError());
+  return PFDD_OK;
+}
+
+template <typename T>
+pfdd_status get_state_impl(pfdd_gpu *h, Instance &I, double *re, double *im, double *inter) {
+  const size_t n = (size_t)I.S * I.N;
+  DevBuf tmp;
+  CUDA_TRY(h, tmp.alloc(n * sizeof(double) * 2));
+  const T *dre = I.xi[I.cur].as<T>();
+  const T *dim = I.F > I.S ? dre + n : nullptr;
+  if (inter) {
+    k_to_interleaved<T><<<1184, 256, 0, h->stream>>>(dre, dim, tmp.as<double>(), n);
+    CUDA_TRY(h, cudaMemcpyAsync(inter, tmp.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  } else {
+    if (re) {
+      k_to_planar<T><<<1184, 256, 0, h->stream>>>(dre, tmp.as<double>(), n);
+      CUDA_TRY(h, cudaMemcpyAsync(re, tmp.p, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
+    if (im) {
+      if (dim) {
+        k_to_planar<T><<<1184, 256, 0, h->stream>>>(dim, tmp.as<double>() + n, n);
+        CUDA_TRY(h, cudaMemcpyAsync(im, tmp.as<double>() + n, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                    h->stream));
+      } else {
+        memset(im, 0, n * sizeof(double));
+      }
+    }
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  CUDA_TRY(h, cudaGetLastError());
+  return PFDD_OK;
+}
+
+bool valid_size(int n) {
+  if (n < 2 || n > 1024 || (n & 1)) return false;
+  FftPlan p;
+  return make_plan(n, p) && make_plan(n / 2, p);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *pfdd_gpu_version(void) { return "pfdd_b200 0.1 (sm_100a)"; }
+
+pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, const pfdd_options *opt,
+                            pfdd_gpu **out) {
+  if (!out) return fail(nullptr, PFDD_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (!descs || n_instances < 1) return fail(nullptr, PFDD_EINVAL, "need at least one instance");
+  pfdd_options o{};
+  o.precision = PFDD_FP64;
+  o.imag_mode = PFDD_IMAG_AUTO;
+  o.use_graphs = 1;
+  o.check_finite = 1;
+  if (opt) o = *opt;
+  if (o.precision != PFDD_FP64 && o.precision != PFDD_FP32)
+    return fail(nullptr, PFDD_EINVAL, "precision must be PFDD_FP64 or PFDD_FP32");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(nullptr, PFDD_ENODEVICE, "no CUDA device");
+  if (o.device < 0 || o.device >= ndev) return fail(nullptr, PFDD_EINVAL, "device %d out of range", o.device);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, o.device) != cudaSuccess || prop.major < 10)
+    return fail(nullptr, PFDD_ENODEVICE, "device %d is not sm_100 class", o.device);
+  for (int i = 0; i < n_instances; ++i) {
+    const pfdd_instance_desc &d = descs[i];
+    if (d.n_slip < 1 || d.n_slip > PFDD_MAX_SLIP)
+      return fail(nullptr, PFDD_EINVAL, "instance %d: n_slip %d outside 1..%d", i, d.n_slip, PFDD_MAX_SLIP);
+    if (!valid_size(d.nx) || !valid_size(d.ny) || !valid_size(d.nz) || d.nz < 4)
+      return fail(nullptr, PFDD_EUNSUPPORTED,
+                  "instance %d: grid %dx%dx%d: each extent must be even, 2^a 3^b, <= 1024 (nz >= 4)", i, d.nx,
+                  d.ny, d.nz);
+    if (!(d.dslip > 0) || !(d.b > 0) || !(d.C44 > 0))
+      return fail(nullptr, PFDD_EINVAL, "instance %d: dslip, b and C44 must be positive", i);
+  }
+  std::unique_ptr<pfdd_gpu> h(new pfdd_gpu);
+  h->opt = o;
+  h->precision = o.precision;
+  h->device = o.device;
+  if (cudaSetDevice(o.device) != cudaSuccess) return fail(nullptr, PFDD_ECUDA, "cudaSetDevice failed");
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(nullptr, PFDD_ECUDA, "stream creation failed");
+  size_t max_plane = 0, max_upd = 0, max_pen = 0;
+  for (int i = 0; i < n_instances; ++i) {
+    std::unique_ptr<Instance> I(new Instance);
+    I->d = descs[i];
+    I->d.site_gsfe = nullptr;
+    I->d.xo = nullptr;
+    I->S = descs[i].n_slip;
+    int imag = o.imag_mode;
+    if (imag == PFDD_IMAG_AUTO) imag = PFDD_IMAG_FULL;  // the Nyquist-only carrier is not built yet
+    if (imag == PFDD_IMAG_NYQUIST) return fail(nullptr, PFDD_EUNSUPPORTED, "PFDD_IMAG_NYQUIST is not built yet");
+    I->imag = (imag == PFDD_IMAG_FULL) ? IMAG_FULL : IMAG_NONE;
+    I->F = I->imag == IMAG_FULL ? 2 * I->S : I->S;
+    I->nx = descs[i].nx; I->ny = descs[i].ny; I->nz = descs[i].nz;
+    I->M = I->nz / 2;
+    I->nzh = I->M + 1;
+    I->N = (size_t)I->nx * I->ny * I->nz;
+    make_plan(I->nx, I->px);
+    make_plan(I->ny, I->py);
+    make_plan(I->M, I->pz);
+    pfdd_instance_desc d = descs[i];
+    I->d.xo = d.xo;               // used during set-up only
+    I->d.site_gsfe = d.site_gsfe;
+    pfdd_status st = (o.precision == PFDD_FP64) ? setup_instance<double>(h.get(), *I) : setup_instance<float>(h.get(), *I);
+    I->d.xo = nullptr;
+    I->d.site_gsfe = nullptr;
+    if (st != PFDD_OK) {
+      g_create_error = h->err;
+      return st;
+    }
+    max_plane = std::max(max_plane, I->smem_plane);
+    max_upd = std::max(max_upd, I->smem_update);
+    max_pen = std::max(max_pen, I->smem_pencil);
+    h->inst.push_back(std::move(I));
+  }
+  pfdd_status st = (o.precision == PFDD_FP64) ? set_smem_attrs<double>(h.get(), max_plane, max_upd, max_pen)
+                                              : set_smem_attrs<float>(h.get(), max_plane, max_upd, max_pen);
+  if (st != PFDD_OK) { g_create_error = h->err; return st; }
+  *out = h.release();
+  return PFDD_OK;
+}
+
+pfdd_status pfdd_gpu_set_state(pfdd_gpu *h, int inst, const double *xi_re, const double *xi_im) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  if (!xi_re) return fail(h, PFDD_EINVAL, "xi_re is NULL");
+  cudaSetDevice(h->device);
+  return h->precision == PFDD_FP64 ? set_state_impl<double>(h, *h->inst[inst], xi_re, xi_im, false)
+                                   : set_state_impl<float>(h, *h->inst[inst], xi_re, xi_im, false);
+}
+
+pfdd_status pfdd_gpu_set_state_interleaved(pfdd_gpu *h, int inst, const double *xi) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  if (!xi) return fail(h, PFDD_EINVAL, "xi is NULL");
+  cudaSetDevice(h->device);
+  return h->precision == PFDD_FP64 ? set_state_impl<double>(h, *h->inst[inst], xi, nullptr, true)
+                                   : set_state_impl<float>(h, *h->inst[inst], xi, nullptr, true);
+}
+
+pfdd_status pfdd_gpu_get_state(pfdd_gpu *h, int inst, double *xi_re, double *xi_im) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  cudaSetDevice(h->device);
+  return h->precision == PFDD_FP64 ? get_state_impl<double>(h, *h->inst[inst], xi_re, xi_im, nullptr)
+                                   : get_state_impl<float>(h, *h->inst[inst], xi_re, xi_im, nullptr);
+}
+
+pfdd_status pfdd_gpu_get_state_interleaved(pfdd_gpu *h, int inst, double *xi) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  if (!xi) return fail(h, PFDD_EINVAL, "xi is NULL");
+  cudaSetDevice(h->device);
+  return h->precision == PFDD_FP64 ? get_state_impl<double>(h, *h->inst[inst], nullptr, nullptr, xi)
+                                   : get_state_impl<float>(h, *h->inst[inst], nullptr, nullptr, xi);
+}
+
+pfdd_status pfdd_gpu_advance(pfdd_gpu *h, int n_steps, int stress_states, double tol, pfdd_step_stats *stats) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (n_steps < 0 || stress_states < 0) return fail(h, PFDD_EINVAL, "negative step count");
+  if (n_steps == 0 || stress_states == 0) return PFDD_OK;
+  cudaSetDevice(h->device);
+  return h->precision == PFDD_FP64 ? advance_impl<double>(h, n_steps, stress_states, tol, stats)
+                                   : advance_impl<float>(h, n_steps, stress_states, tol, stats);
+}
+
+pfdd_status pfdd_gpu_step_history(pfdd_gpu *h, int inst, double *xinorm, double *xiave, int cap, int *count) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  Instance &I = *h->inst[inst];
+  const int n = std::min(cap, I.hist_count);
+  for (int i = 0; i < n; ++i) {
+    if (xinorm) xinorm[i] = I.hist[2 * i];
+    if (xiave) xiave[i] = I.hist[2 * i + 1];
+  }
+  if (count) *count = I.hist_count;
+  return PFDD_OK;
+}
+
+pfdd_status pfdd_gpu_tau(pfdd_gpu *h, int inst, double *tau) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size() || !tau) return fail(h, PFDD_EINVAL, "bad arguments");
+  Instance &I = *h->inst[inst];
+  cudaSetDevice(h->device);
+  k_stress_state<<<1, 32, 0, h->stream>>>(I.sigma(), I.tau(), I.stress, 0, nullptr);
+  CUDA_TRY(h, cudaMemcpyAsync(tau, I.tau(), I.S * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return PFDD_OK;
+}
+
+pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_core, double *e_applied) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  (void)inst; (void)e_elastic; (void)e_core; (void)e_applied;
+  return fail(h, PFDD_EUNSUPPORTED, "energy reduction not built yet");
+}
+
+pfdd_status pfdd_gpu_info(pfdd_gpu *h, int *n_instances, size_t *device_bytes) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (n_instances) *n_instances = (int)h->inst.size();
+  if (device_bytes) *device_bytes = h->device_bytes;
+  return PFDD_OK;
+}
+
+const char *pfdd_gpu_last_error(pfdd_gpu *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+void pfdd_gpu_destroy(pfdd_gpu *h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  h->inst.clear();
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+}  // extern "C"

@@ -1,0 +1,208 @@
+// Device FFT building blocks for the PFDD Ginzburg-Landau stepper (sm_100a).
+//
+// Transforms run in place in shared memory as a sequence of mixed-radix
+// decimation-in-frequency stages (radices 2, 3, 4, 8, 16).  Stage s of a
+// length-n transform has sub-length L_s (L_0 = n, L_{s+1} = L_s / R_s); work
+// item (block, j) loads R_s elements at positions block*L_s + j + r*L_s/R_s,
+// applies a register DFT of size R_s, multiplies output k by W_{L_s}^{j*k}
+// and stores back to the same positions.  The forward transform therefore
+// maps natural order to a digit-reversed order: frequency
+//   k = k_0 + R_0 k_1 + R_0 R_1 k_2 + ...
+// ends at position k_0 L_1 + k_1 L_2 + ... .  The inverse runs the stages in
+// reverse with conjugate twiddles and the conjugate DFT, mapping the
+// digit-reversed order back to natural order, unnormalised.  Consumers of the
+// spectrum read frequencies through per-axis slot->k tables built on the host.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pfdd {
+
+template <typename T> struct cx_of;
+template <> struct cx_of<float> { using type = float2; };
+template <> struct cx_of<double> { using type = double2; };
+template <typename T> using cx = typename cx_of<T>::type;
+
+template <typename C> __device__ __forceinline__ C mk(decltype(C::x) a, decltype(C::x) b) {
+  C r; r.x = a; r.y = b; return r;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mk<C>(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mk<C>(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  return mk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+template <typename C> __device__ __forceinline__ C cmulc(C a, C b) {
+  return mk<C>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+template <typename C> __device__ __forceinline__ C cconj(C a) { return mk<C>(a.x, -a.y); }
+template <typename C, typename T> __device__ __forceinline__ C cscale(C a, T s) { return mk<C>(a.x * s, a.y * s); }
+// multiply by SIGN * i
+template <int SIGN, typename C> __device__ __forceinline__ C mul_si(C a) {
+  return mk<C>(-SIGN * a.y, SIGN * a.x);
+}
+
+// Exact constants (decimal expansions of cos/sin of multiples of pi/8, pi/3).
+#define PFDD_H 0.70710678118654752440084436210484903928
+#define PFDD_C8 0.92387953251128675612818318939678828682
+#define PFDD_S8 0.38268343236508977172845998403039886676
+#define PFDD_S3 0.86602540378443864676372317075293618347
+
+// multiply by W_16^M = exp(SIGN * 2 pi i M / 16), M in 0..15
+template <int M, int SIGN, typename C> __device__ __forceinline__ C tw16(C a) {
+  using T = decltype(C::x);
+  constexpr int m = M & 15;
+  if constexpr (m == 0) return a;
+  else if constexpr (m == 4) return mul_si<SIGN>(a);
+  else if constexpr (m == 8) return mk<C>(-a.x, -a.y);
+  else if constexpr (m == 12) return mul_si<-SIGN>(a);
+  else {
+    constexpr double cr[16] = {1, PFDD_C8, PFDD_H, PFDD_S8, 0, -PFDD_S8, -PFDD_H, -PFDD_C8,
+                               -1, -PFDD_C8, -PFDD_H, -PFDD_S8, 0, PFDD_S8, PFDD_H, PFDD_C8};
+    constexpr double sr[16] = {0, PFDD_S8, PFDD_H, PFDD_C8, 1, PFDD_C8, PFDD_H, PFDD_S8,
+                               0, -PFDD_S8, -PFDD_H, -PFDD_C8, -1, -PFDD_C8, -PFDD_H, -PFDD_S8};
+    const T wr = (T)cr[m], wi = (T)(SIGN * sr[m]);
+    return mk<C>(a.x * wr - a.y * wi, a.x * wi + a.y * wr);
+  }
+}
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft2(C &a, C &b) {
+  C t = a; a = cadd(t, b); b = csub(t, b);
+}
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft4(C &v0, C &v1, C &v2, C &v3) {
+  C t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), t3 = mul_si<SIGN>(csub(v1, v3));
+  v0 = cadd(t0, t2); v2 = csub(t0, t2); v1 = cadd(t1, t3); v3 = csub(t1, t3);
+}
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft3(C &v0, C &v1, C &v2) {
+  using T = decltype(C::x);
+  C s = cadd(v1, v2), d = csub(v1, v2);
+  C m = mk<C>(v0.x - (T)0.5 * s.x, v0.y - (T)0.5 * s.y);
+  const T s3 = (T)(SIGN * PFDD_S3);
+  C isd = mk<C>(-s3 * d.y, s3 * d.x);
+  v0 = cadd(v0, s);
+  v1 = cadd(m, isd);
+  v2 = csub(m, isd);
+}
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft8(C *v) {
+  dft4<SIGN>(v[0], v[2], v[4], v[6]);
+  dft4<SIGN>(v[1], v[3], v[5], v[7]);
+  // odd outputs sit at v[1],v[3],v[5],v[7] for k = 0..3; twiddle by W8^k = W16^(2k)
+  C o1 = tw16<2, SIGN>(v[3]), o2 = tw16<4, SIGN>(v[5]), o3 = tw16<6, SIGN>(v[7]);
+  C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6], o0 = v[1];
+  v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+}
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft16(C *v) {
+  // n = 4 n1 + n2, k = k1 + 4 k2
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) dft4<SIGN>(v[n2], v[4 + n2], v[8 + n2], v[12 + n2]);
+  // v[4*k1 + n2] holds Y[n2][k1]; twiddle by W16^(n2*k1)
+  v[5] = tw16<1, SIGN>(v[5]);  v[6] = tw16<2, SIGN>(v[6]);  v[7] = tw16<3, SIGN>(v[7]);
+  v[9] = tw16<2, SIGN>(v[9]);  v[10] = tw16<4, SIGN>(v[10]); v[11] = tw16<6, SIGN>(v[11]);
+  v[13] = tw16<3, SIGN>(v[13]); v[14] = tw16<6, SIGN>(v[14]); v[15] = tw16<9, SIGN>(v[15]);
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) dft4<SIGN>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+  // v[4*k1 + k2] holds X[k1 + 4 k2]; transpose to natural order
+  C t[16];
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) t[k1 + 4 * k2] = v[4 * k1 + k2];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = t[i];
+}
+
+template <int R, int SIGN, typename C> __device__ __forceinline__ void dft(C *v) {
+  if constexpr (R == 2) dft2<SIGN>(v[0], v[1]);
+  else if constexpr (R == 3) dft3<SIGN>(v[0], v[1], v[2]);
+  else if constexpr (R == 4) dft4<SIGN>(v[0], v[1], v[2], v[3]);
+  else if constexpr (R == 8) dft8<SIGN>(v);
+  else if constexpr (R == 16) dft16<SIGN>(v);
+}
+
+// Radix plan of one axis, built on the host.
+struct FftPlan {
+  int n;
+  int nst;
+  int radix[8];
+  int L[8];
+};
+
+// Batched transform geometry in shared memory: transform b (0 <= b < batch)
+// starts at (b % bin) * bs_in + (b / bin) * bs_out and its element i sits at
+// start + i * es.  If batch_fast, consecutive threads take consecutive b (use
+// when bs_in == 1); otherwise consecutive butterflies of one transform.
+struct Batch {
+  int batch, bin, bs_in, bs_out, es;
+  bool batch_fast;
+};
+
+template <int R, bool INV, typename C>
+__device__ __forceinline__ void fft_stage(C *__restrict__ x, const C *__restrict__ tw, int n, int L,
+                                          const Batch &g, int tid, int nthr) {
+  const int Lr = L / R;
+  const int per = n / R;
+  const int total = g.batch * per;
+  const int twstep = n / L;
+  for (int w = tid; w < total; w += nthr) {
+    int b, bf;
+    if (g.batch_fast) { b = w % g.batch; bf = w / g.batch; }
+    else { bf = w % per; b = w / per; }
+    const int blk = bf / Lr, j = bf - blk * Lr;
+    C *base = x + (b % g.bin) * g.bs_in + (b / g.bin) * g.bs_out + (blk * L + j) * g.es;
+    const int st = Lr * g.es;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = base[r * st];
+    if constexpr (!INV) {
+      dft<R, -1>(v);
+#pragma unroll
+      for (int k = 1; k < R; ++k) v[k] = cmul(v[k], tw[j * k * twstep]);
+    } else {
+#pragma unroll
+      for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], tw[j * k * twstep]);
+      dft<R, 1>(v);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) base[r * st] = v[r];
+  }
+}
+
+template <bool INV, typename C>
+__device__ __forceinline__ void fft_stage_dispatch(C *x, const C *tw, int n, int R, int L, const Batch &g,
+                                                   int tid, int nthr) {
+  switch (R) {
+    case 2: fft_stage<2, INV>(x, tw, n, L, g, tid, nthr); break;
+    case 3: fft_stage<3, INV>(x, tw, n, L, g, tid, nthr); break;
+    case 4: fft_stage<4, INV>(x, tw, n, L, g, tid, nthr); break;
+    case 8: fft_stage<8, INV>(x, tw, n, L, g, tid, nthr); break;
+    case 16: fft_stage<16, INV>(x, tw, n, L, g, tid, nthr); break;
+    default: break;
+  }
+}
+
+// Forward (natural -> digit-reversed).  Ends with __syncthreads().
+template <typename C>
+__device__ void fft_forward(C *x, const C *tw, const FftPlan &p, const Batch &g) {
+  for (int s = 0; s < p.nst; ++s) {
+    fft_stage_dispatch<false>(x, tw, p.n, p.radix[s], p.L[s], g, threadIdx.x, blockDim.x);
+    __syncthreads();
+  }
+}
+
+// Inverse, unnormalised (digit-reversed -> natural).  Ends with __syncthreads().
+template <typename C>
+__device__ void fft_inverse(C *x, const C *tw, const FftPlan &p, const Batch &g) {
+  for (int s = p.nst - 1; s >= 0; --s) {
+    fft_stage_dispatch<true>(x, tw, p.n, p.radix[s], p.L[s], g, threadIdx.x, blockDim.x);
+    __syncthreads();
+  }
+}
+
+}  // namespace pfdd

@@ -1,0 +1,624 @@
+// Hot-path kernels of one Ginzburg-Landau iteration (sm_100a).
+//
+// One GL iteration of the reference (solve_GL.cpp:92-124) on real fields
+// (Re xi and, when carried, Im xi) becomes three passes over HBM:
+//   P1 k_fwd_planes   per (field, x-plane): z real-to-complex FFT (half-length
+//                     packing) + y FFT, in shared memory   -> half spectrum
+//   P2 k_xpencil      per tile of (ky, kz) columns, all fields: x FFT, the
+//                     per-k Green's contraction of internal_energy
+//                     (fft_fftw_slab.cpp:1670-1695) with B(k) regenerated from
+//                     k in registers, inverse x FFT          -> elastic spectrum
+//   P3 k_inv_update   per (field, x-plane): inverse y FFT + z complex-to-real,
+//                     fused with the GSFE core force (core_energy_*), the
+//                     applied stress and the explicit Euler update with the
+//                     obstacle mask (update_order_parameter,
+//                     fft_fftw_slab.cpp:1746-1790), plus FP64 partial sums of
+//                     |dxi|^2 and sum Re xi
+// followed by a one-block FP64 compensated reduction (k_finalize).
+//
+// Spectrum layout: spec[f][x][sy][sz] with sy, sz the digit-reversed slots of
+// ky and kz (z slot M = nz/2 holds the Nyquist column); P2 additionally
+// permutes kx inside shared memory only.  Frequencies are recovered through
+// slot tables, so no transform ever reorders data.
+#pragma once
+#include "pfdd_fft.cuh"
+
+#define PFDD_MAXS 12
+#define PFDD_PI_T 3.14159265358979323846
+
+namespace pfdd {
+
+// Per-instance constants of the contraction and the update (FP64 on the host).
+struct Green {
+  double four[3][3];
+  double sig[PFDD_MAXS][6];   // sigma^a = C : eps^a  (xx yy zz xy xz yz)
+  double eps[PFDD_MAXS][6];   // eps^a contracted with a symmetric tensor: xx yy zz, xy+yx, xz+zx, yz+zy
+  double inv_mu;              // 1 / mu (Voigt), fft_fftw_slab.cpp:628
+  double c2;                  // 1 / (2 C44), Green's function prefactor, fft_fftw_slab.cpp:597
+  double c1nu;                // 1 / (1 - nu) (Voigt nu)
+};
+
+struct Core {
+  int flag;
+  double k[12];               // scaled constants, see core_derivative
+};
+
+enum { IMAG_NONE = 0, IMAG_FULL = 1 };
+
+struct PlaneArgs {
+  FftPlan py, pz;
+  int nx, ny, nz, nzh, M;
+  int S, F;                   // slip systems; fields in flight (S, or 2S with Im xi)
+  const void *tw_y, *tw_z, *tw_r;   // W_ny^m, W_M^m, W_nz^k tables in compute precision
+  const int16_t *posM;        // position of z-frequency k (< M) after the M-point transform
+};
+
+struct PencilArgs {
+  FftPlan px;
+  int nx, ny, nz, nzh, M;
+  int S, F, imag;
+  int ncols;                  // ny * nzh
+  int ccols;                  // columns per CTA
+  const void *tw_x;
+  const int16_t *kx_of, *ky_of, *kz_of;   // frequency index of each slot (kz_of has nzh entries)
+  Green g;
+};
+
+struct UpdateArgs {
+  int nx, ny, nz, nzh, S, F;
+  double cd;                  // CD * timestep
+  double invN;
+  Core core;
+  const double *tau;          // [S] device, FP64
+  const uint8_t *mask;        // [S*N] or null
+  const void *site;           // [S*N] per-site GSFE field (compute precision) or null
+  const int *stop;            // device flag: skip the step when nonzero
+};
+
+// ------------------------------------------------------------ small helpers
+template <typename T> __device__ __forceinline__ void sincospi_t(T x, T *s, T *c);
+template <> __device__ __forceinline__ void sincospi_t<double>(double x, double *s, double *c) { sincospi(x, s, c); }
+template <> __device__ __forceinline__ void sincospi_t<float>(float x, float *s, float *c) { sincospif(x, s, c); }
+template <typename T> __device__ __forceinline__ T sinpi_t(T x);
+template <> __device__ __forceinline__ double sinpi_t<double>(double x) { return sinpi(x); }
+template <> __device__ __forceinline__ float sinpi_t<float>(float x) { return sinpif(x); }
+template <typename T> __device__ __forceinline__ T cospi_t(T x);
+template <> __device__ __forceinline__ double cospi_t<double>(double x) { return cospi(x); }
+template <> __device__ __forceinline__ float cospi_t<float>(float x) { return cospif(x); }
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-reduce two doubles into out[0..1] (thread 0 writes). smem: 2*32 doubles.
+__device__ __forceinline__ void block_sum2(double a, double b, double *scratch, double *out) {
+  a = warp_sum(a);
+  b = warp_sum(b);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if (lane == 0) { scratch[wid] = a; scratch[32 + wid] = b; }
+  __syncthreads();
+  if (wid == 0) {
+    a = lane < nw ? scratch[lane] : 0.0;
+    b = lane < nw ? scratch[32 + lane] : 0.0;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0) { out[0] = a; out[1] = b; }
+  }
+}
+
+template <typename C>
+__device__ __forceinline__ void load_table(C *dst, const void *src, int n) {
+  const C *s = reinterpret_cast<const C *>(src);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = s[i];
+}
+
+// ------------------------------------------------------------ P1
+// grid.x = F * nx planes; dynamic smem = (ny*nzh + ny + 2M) * sizeof(C) + M * 4
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwd_planes(const T *__restrict__ xi, cx<T> *__restrict__ spec,
+                                                    PlaneArgs a, const int *__restrict__ stop) {
+  using C = cx<T>;
+  if (stop && *stop) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ny = a.ny, nz = a.nz, nzh = a.nzh, M = a.M;
+  C *buf = reinterpret_cast<C *>(smem_raw);
+  C *twy = buf + ny * nzh;
+  C *twz = twy + ny;
+  C *twr = twz + M;
+  int *pos = reinterpret_cast<int *>(twr + M);
+  load_table(twy, a.tw_y, ny);
+  load_table(twz, a.tw_z, M);
+  load_table(twr, a.tw_r, M);
+  for (int i = threadIdx.x; i < M; i += blockDim.x) pos[i] = a.posM[i];
+
+  const size_t plane = blockIdx.x;
+  const T *src = xi + plane * (size_t)ny * nz;
+  T *bufr = reinterpret_cast<T *>(buf);
+  for (int i = threadIdx.x; i < ny * nz; i += blockDim.x) {
+    const int y = i / nz, z = i - y * nz;
+    bufr[y * 2 * nzh + z] = src[i];
+  }
+  __syncthreads();
+
+  // z: M-point complex transform of the packed rows
+  Batch gz{ny, ny, nzh, 0, 1, false};
+  fft_forward(buf, twz, a.pz, gz);
+
+  // real-to-complex unpacking, pairs (k, M-k); X[M] goes to slot M
+  const int half = M / 2 + 1;
+  for (int w = threadIdx.x; w < ny * half; w += blockDim.x) {
+    const int y = w / half, k = w - y * half;
+    C *row = buf + y * nzh;
+    if (k == 0) {
+      C z0 = row[pos[0]];
+      row[pos[0]] = mk<C>(z0.x + z0.y, (T)0);
+      row[M] = mk<C>(z0.x - z0.y, (T)0);
+    } else {
+      const int pk = pos[k], pm = pos[M - k];
+      C zk = row[pk], zm = row[pm];
+      // E = (Zk + conj Zm)/2, O = (Zk - conj Zm)/(2i), X[k] = E + W^k O, X[M-k] = conj(E - W^k O)
+      C e = mk<C>((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y - zm.y));
+      C o = mk<C>((T)0.5 * (zk.y + zm.y), (T)-0.5 * (zk.x - zm.x));
+      C wo = cmul(twr[k], o);
+      row[pk] = cadd(e, wo);
+      if (pm != pk) row[pm] = cconj(csub(e, wo));
+    }
+  }
+  __syncthreads();
+
+  // y: ny-point transforms over the nzh slot columns
+  Batch gy{nzh, nzh, 1, 0, nzh, true};
+  fft_forward(buf, twy, a.py, gy);
+
+  C *dst = spec + plane * (size_t)ny * nzh;
+  for (int i = threadIdx.x; i < ny * nzh; i += blockDim.x) dst[i] = buf[i];
+}
+
+// ------------------------------------------------------------ B(k) operator
+// out_a = sum_b B_ab(k) Y_b for complex Y, with the closed form of Bmatrix
+// (fft_fftw_slab.cpp:587-629):  B_ab = (eps^a:C:eps^b - t^b.G.t^a)/mu,
+// t^a = sigma^a k, G = (2 I/k^2 - k k^T/((1-nu) k^4)) / (2 C44).
+// Because t^a is linear in sigma^a, sum_b B_ab Y_b =
+//   (eps^a : Sig - [2 (t^a . U)/k^2 - (k.t^a)(k.U)/((1-nu)k^4)]/(2 C44)) / mu
+// with Sig = sum_b Y_b sigma^b and U = Sig k: O(S) work per k instead of O(S^2).
+template <typename T, typename C>
+__device__ __forceinline__ void green_prepare(const Green &g, const C (&sig)[6], T kx, T ky, T kz, C (&U)[3],
+                                              C &V, T &g1, T &g2, bool &zero) {
+  const T k2 = kx * kx + ky * ky + kz * kz;
+  zero = !(k2 > (T)0);
+  const T ik2 = zero ? (T)0 : (T)1 / k2;
+  g1 = (T)2 * ik2 * (T)g.c2;
+  g2 = ik2 * ik2 * (T)g.c1nu * (T)g.c2;
+  // sig order: xx yy zz xy xz yz
+  U[0] = mk<C>(sig[0].x * kx + sig[3].x * ky + sig[4].x * kz, sig[0].y * kx + sig[3].y * ky + sig[4].y * kz);
+  U[1] = mk<C>(sig[3].x * kx + sig[1].x * ky + sig[5].x * kz, sig[3].y * kx + sig[1].y * ky + sig[5].y * kz);
+  U[2] = mk<C>(sig[4].x * kx + sig[5].x * ky + sig[2].x * kz, sig[4].y * kx + sig[5].y * ky + sig[2].y * kz);
+  V = mk<C>(kx * U[0].x + ky * U[1].x + kz * U[2].x, kx * U[0].y + ky * U[1].y + kz * U[2].y);
+}
+
+template <typename T, typename C>
+__device__ __forceinline__ C green_apply(const Green &g, int a, const C (&sig)[6], T kx, T ky, T kz,
+                                         const C (&U)[3], C V, T g1, T g2, bool zero) {
+  if (zero) return mk<C>((T)0, (T)0);
+  const double *s = g.sig[a];
+  const double *e = g.eps[a];
+  const T tx = (T)s[0] * kx + (T)s[3] * ky + (T)s[4] * kz;
+  const T ty = (T)s[3] * kx + (T)s[1] * ky + (T)s[5] * kz;
+  const T tz = (T)s[4] * kx + (T)s[5] * ky + (T)s[2] * kz;
+  const T p = kx * tx + ky * ty + kz * tz;
+  C es;
+  es.x = (T)e[0] * sig[0].x + (T)e[1] * sig[1].x + (T)e[2] * sig[2].x + (T)e[3] * sig[3].x + (T)e[4] * sig[4].x +
+         (T)e[5] * sig[5].x;
+  es.y = (T)e[0] * sig[0].y + (T)e[1] * sig[1].y + (T)e[2] * sig[2].y + (T)e[3] * sig[3].y + (T)e[4] * sig[4].y +
+         (T)e[5] * sig[5].y;
+  const T tux = tx * U[0].x + ty * U[1].x + tz * U[2].x;
+  const T tuy = tx * U[0].y + ty * U[1].y + tz * U[2].y;
+  const T im = (T)g.inv_mu;
+  return mk<C>(im * (es.x - g1 * tux + g2 * p * V.x), im * (es.y - g1 * tuy + g2 * p * V.y));
+}
+
+// frequency of index i on an axis of length n (frec, fft_fftw_slab.cpp:295-330)
+template <typename T> __device__ __forceinline__ T freq_of(int i, int n) {
+  return (i >= n / 2) ? (T)(i - n) / (T)n : (T)i / (T)n;
+}
+// frequency used by the reference at index (-i mod n): -f(i) except at n/2
+template <typename T> __device__ __forceinline__ T freq_neg(int i, int n) {
+  const int j = (n - i) % n;
+  return freq_of<T>(j, n);
+}
+
+// ------------------------------------------------------------ P2
+// grid.x = ncols / ccols tiles; dynamic smem = (F*nx*ccols + nx) * sizeof(C)
+template <typename T>
+__global__ void __launch_bounds__(256) k_xpencil(cx<T> *__restrict__ spec, PencilArgs a,
+                                                 const int *__restrict__ stop) {
+  using C = cx<T>;
+  if (stop && *stop) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nx = a.nx, F = a.F, cc = a.ccols, S = a.S;
+  C *buf = reinterpret_cast<C *>(smem_raw);   // [F][nx][cc]
+  C *twx = buf + (size_t)F * nx * cc;
+  load_table(twx, a.tw_x, nx);
+  const size_t col0 = (size_t)blockIdx.x * cc;
+  const size_t ncols = a.ncols;
+  for (int i = threadIdx.x; i < F * nx * cc; i += blockDim.x) {
+    const int c = i % cc, fx = i / cc;  // fx = f*nx + x
+    buf[i] = spec[(size_t)fx * ncols + col0 + c];
+  }
+  __syncthreads();
+
+  Batch gx{F * cc, cc, 1, nx * cc, cc, true};
+  fft_forward(buf, twx, a.px, gx);
+
+  // per-k contraction
+  for (int w = threadIdx.x; w < nx * cc; w += blockDim.x) {
+    const int c = w % cc, sx = w / cc;
+    const int col = (int)(col0 + c);
+    const int sy = col / a.nzh, sz = col - sy * a.nzh;
+    const int ix = a.kx_of[sx], iy = a.ky_of[sy], iz = a.kz_of[sz];
+    const T fx = freq_of<T>(ix, a.nx), fy = freq_of<T>(iy, a.ny), fz = freq_of<T>(iz, a.nz);
+    const T gxn = freq_neg<T>(ix, a.nx), gyn = freq_neg<T>(iy, a.ny), gzn = freq_neg<T>(iz, a.nz);
+    const Green &g = a.g;
+    const T kx = fx * (T)g.four[0][0] + fy * (T)g.four[1][0] + fz * (T)g.four[2][0];
+    const T ky = fx * (T)g.four[0][1] + fy * (T)g.four[1][1] + fz * (T)g.four[2][1];
+    const T kz = fx * (T)g.four[0][2] + fy * (T)g.four[1][2] + fz * (T)g.four[2][2];
+    // B at the index -k equals B(-(-k)) by symmetry; evaluate at the vector of -k
+    const T mx = gxn * (T)g.four[0][0] + gyn * (T)g.four[1][0] + gzn * (T)g.four[2][0];
+    const T my = gxn * (T)g.four[0][1] + gyn * (T)g.four[1][1] + gzn * (T)g.four[2][1];
+    const T mz = gxn * (T)g.four[0][2] + gyn * (T)g.four[1][2] + gzn * (T)g.four[2][2];
+    C *pk = buf + sx * cc + c;
+    const size_t fs = (size_t)nx * cc;
+    if (a.imag == IMAG_FULL) {
+      // P = B(k)(Xr + i Xi), Q = B(k')(Xr - i Xi), k' = vector of index -k;
+      // Er = (P + Q)/2, Ei = (P - Q)/(2i): the real and imaginary fields of
+      // IFFT(B_index X) for the complex field X = Xr + i Xi.
+      C sr[6], si[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) { sr[q] = mk<C>((T)0, (T)0); si[q] = sr[q]; }
+      for (int b = 0; b < S; ++b) {
+        const C xr = pk[b * fs], xim = pk[(S + b) * fs];
+        const double *s = g.sig[b];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          sr[q].x += (T)s[q] * xr.x; sr[q].y += (T)s[q] * xr.y;
+          si[q].x += (T)s[q] * xim.x; si[q].y += (T)s[q] * xim.y;
+        }
+      }
+      C sp[6], sq[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        sp[q] = mk<C>(sr[q].x - si[q].y, sr[q].y + si[q].x);  // Sr + i Si
+        sq[q] = mk<C>(sr[q].x + si[q].y, sr[q].y - si[q].x);  // Sr - i Si
+      }
+      C Up[3], Uq[3], Vp, Vq;
+      T g1p, g2p, g1q, g2q;
+      bool zp, zq;
+      green_prepare<T>(g, sp, kx, ky, kz, Up, Vp, g1p, g2p, zp);
+      green_prepare<T>(g, sq, mx, my, mz, Uq, Vq, g1q, g2q, zq);
+      for (int aa = 0; aa < S; ++aa) {
+        const C P = green_apply<T>(g, aa, sp, kx, ky, kz, Up, Vp, g1p, g2p, zp);
+        const C Q = green_apply<T>(g, aa, sq, mx, my, mz, Uq, Vq, g1q, g2q, zq);
+        pk[aa * fs] = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
+        // (P - Q)/(2i) = -i (P - Q)/2
+        pk[(S + aa) * fs] = mk<C>((T)0.5 * (P.y - Q.y), (T)-0.5 * (P.x - Q.x));
+      }
+    } else {
+      // real field only: B averaged over k and index -k (the Hermitian part)
+      C sr[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) sr[q] = mk<C>((T)0, (T)0);
+      for (int b = 0; b < S; ++b) {
+        const C xr = pk[b * fs];
+        const double *s = g.sig[b];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) { sr[q].x += (T)s[q] * xr.x; sr[q].y += (T)s[q] * xr.y; }
+      }
+      C Up[3], Uq[3], Vp, Vq;
+      T g1p, g2p, g1q, g2q;
+      bool zp, zq;
+      green_prepare<T>(g, sr, kx, ky, kz, Up, Vp, g1p, g2p, zp);
+      green_prepare<T>(g, sr, mx, my, mz, Uq, Vq, g1q, g2q, zq);
+      for (int aa = 0; aa < S; ++aa) {
+        const C P = green_apply<T>(g, aa, sr, kx, ky, kz, Up, Vp, g1p, g2p, zp);
+        const C Q = green_apply<T>(g, aa, sr, mx, my, mz, Uq, Vq, g1q, g2q, zq);
+        pk[aa * fs] = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
+      }
+    }
+  }
+  __syncthreads();
+
+  fft_inverse(buf, twx, a.px, gx);
+
+  for (int i = threadIdx.x; i < F * nx * cc; i += blockDim.x) {
+    const int c = i % cc, fx = i / cc;
+    spec[(size_t)fx * ncols + col0 + c] = buf[i];
+  }
+}
+
+// ------------------------------------------------------------ core force
+// dE_core for field a at site r from Re xi (App::core_energy dispatch,
+// app.cpp:663-672).  k[] holds constants already divided by mu*dslip*b
+// (or mu) on the host, in the reference's order of operations.
+template <typename T>
+__device__ __forceinline__ T core_derivative(const Core &cm, T x, int a, size_t r, size_t N, const T *__restrict__ xin,
+                                             const T *__restrict__ site) {
+  switch (cm.flag) {
+    case 1:   // perfect / USFE(angle,tau): An' pi sin(2 pi x)
+    case 6:
+      return (T)cm.k[0] * sinpi_t<T>((T)2 * x);
+    case 3: { // sine: isf' pi sin(2 pi x) + Cn' 2 pi sin(4 pi x)
+      T s, c;
+      sincospi_t<T>((T)2 * x, &s, &c);
+      return (T)cm.k[0] * s + (T)cm.k[1] * ((T)2 * s * c);
+    }
+    case 103: { // sine with per-site multiplier m: isf' = isf m/s, Cn' = (usf m - isf'/2)/s
+      const T m = site[(size_t)a * N + r];
+      T s, c;
+      sincospi_t<T>((T)2 * x, &s, &c);
+      const T isf = (T)cm.k[2] * m;               // isf / s * m
+      const T cn = (T)cm.k[3] * m - isf * (T)cm.k[4];  // usf m / s - isf'/(2 s)
+      return (T)PFDD_PI_T * isf * s + (T)(2.0 * PFDD_PI_T) * cn * ((T)2 * s * c);
+    }
+    case 7: { // mpea: A(r)/(mu dslip b) pi sin(2 pi x)
+      const T A = site[(size_t)a * N + r];
+      return A * (T)cm.k[0] * sinpi_t<T>((T)2 * x);
+    }
+    case 4: { // pyrII: the reference writes dE_core only at the last site (fft_fftw_slab.cpp:1491)
+      if (r != N - 1) return (T)0;
+      T acc = (T)0;
+#pragma unroll
+      for (int n = 1; n <= 4; ++n) {
+        T s, c;
+        sincospi_t<T>((T)(2 * n) * x, &s, &c);
+        acc += (T)(2.0 * n * PFDD_PI_T) * ((T)cm.k[4 + n] * c - (T)cm.k[n] * s);
+      }
+      return acc;
+    }
+    case 2: { // extended, three systems per plane (fft_fftw_slab.cpp:1300-1352)
+      const int p = a / 3, w = a - 3 * p;
+      const T x1 = xin[(size_t)(3 * p) * N + r], x2 = xin[(size_t)(3 * p + 1) * N + r],
+              x3 = xin[(size_t)(3 * p + 2) * N + r];
+      const T c1 = (T)cm.k[0], c2 = (T)cm.k[1], c3 = (T)cm.k[2], c4 = (T)cm.k[3], a1 = (T)cm.k[4],
+              a3 = (T)cm.k[5], pre = (T)cm.k[6];
+      auto S2 = [](T t) { return sinpi_t<T>((T)2 * t); };
+      auto S4 = [](T t) { return sinpi_t<T>((T)4 * t); };
+      auto C2 = [](T t) { return cospi_t<T>((T)2 * t); };
+      auto C4 = [](T t) { return cospi_t<T>((T)4 * t); };
+      const T two = (T)2, three = (T)3;
+      T d;
+      if (w == 0) {  // df1core
+        d = c1 * (S2(x2 - x1) + S2(x3 - x1)) +
+            c2 * (two * S2(x2 + x3 - two * x1) + S2(two * x2 - x3 - x1) + S2(two * x3 - x1 - x2)) +
+            (two * c3) * (S4(x2 - x1) + S4(x3 - x1)) +
+            c4 * (three * S2(x2 + two * x3 - three * x1) + three * S2(two * x2 + x3 - three * x1) +
+                  two * S2(three * x2 - x3 - two * x1) + S2(three * x2 - two * x3 - x1) +
+                  S2(three * x3 - x1 - two * x2) + two * S2(three * x3 - two * x1 - x2)) +
+            a1 * (C2(x1 - x2) - C2(x3 - x1)) + (two * a3) * (C4(x1 - x2) - C4(x3 - x1));
+      } else if (w == 1) {  // df2core
+        d = c1 * (S2(x1 - x2) + S2(x3 - x2)) +
+            c2 * (S2(two * x1 - x2 - x3) + two * S2(x3 + x1 - two * x2) + S2(two * x3 - x1 - x2)) +
+            (two * c3) * (S4(x1 - x2) + S4(x3 - x2)) +
+            c4 * (S2(three * x1 - x2 - two * x3) + two * S2(three * x1 - two * x2 - x3) +
+                  three * S2(x3 + two * x1 - three * x2) + three * S2(two * x3 + x1 - three * x2) +
+                  two * S2(three * x3 - x1 - two * x2) + S2(three * x3 - two * x1 - x2)) +
+            a1 * (C2(x2 - x3) - C2(x1 - x2)) + (two * a3) * (C4(x2 - x3) - C4(x1 - x2));
+      } else {  // df3core
+        d = c1 * (S2(x2 - x3) + S2(x1 - x3)) +
+            c2 * (S2(two * x1 - x2 - x3) + S2(two * x2 - x3 - x1) + two * S2(x1 + x2 - two * x3)) +
+            (two * c3) * (S4(x2 - x3) + S4(x1 - x3)) +
+            c4 * (two * S2(three * x1 - x2 - two * x3) + S2(three * x1 - two * x2 - x3) +
+                  S2(three * x2 - x3 - two * x1) + two * S2(three * x2 - two * x3 - x1) +
+                  three * S2(x1 + two * x2 - three * x3) + three * S2(two * x1 + x2 - three * x3)) +
+            a1 * (C2(x3 - x1) - C2(x2 - x3)) + (two * a3) * (C4(x3 - x1) - C4(x2 - x3));
+      }
+      return pre * d;
+    }
+    default:
+      return (T)0;
+  }
+}
+
+// ------------------------------------------------------------ P3
+// grid.x = F * nx planes; dynamic smem as P1 + 64 doubles
+template <typename T>
+__global__ void __launch_bounds__(256) k_inv_update(const cx<T> *__restrict__ spec, const T *__restrict__ xin,
+                                                    T *__restrict__ xout, PlaneArgs a, UpdateArgs u,
+                                                    double *__restrict__ partials) {
+  using C = cx<T>;
+  if (u.stop && *u.stop) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ny = a.ny, nz = a.nz, nzh = a.nzh, M = a.M;
+  C *buf = reinterpret_cast<C *>(smem_raw);
+  C *twy = buf + ny * nzh;
+  C *twz = twy + ny;
+  C *twr = twz + M;
+  int *pos = reinterpret_cast<int *>(twr + M);
+  double *red = reinterpret_cast<double *>(pos + ((M + 1) & ~1));
+  load_table(twy, a.tw_y, ny);
+  load_table(twz, a.tw_z, M);
+  load_table(twr, a.tw_r, M);
+  for (int i = threadIdx.x; i < M; i += blockDim.x) pos[i] = a.posM[i];
+
+  const size_t plane = blockIdx.x;
+  const C *src = spec + plane * (size_t)ny * nzh;
+  for (int i = threadIdx.x; i < ny * nzh; i += blockDim.x) buf[i] = src[i];
+  __syncthreads();
+
+  Batch gy{nzh, nzh, 1, 0, nzh, true};
+  fft_inverse(buf, twy, a.py, gy);
+
+  // complex-to-real packing: Zin[k] = A + i w D, Zin[M-k] = conj(A - i w D),
+  // A = X[k] + conj X[M-k], D = X[k] - conj X[M-k], w = exp(+2 pi i k / nz)
+  const int half = M / 2 + 1;
+  for (int w = threadIdx.x; w < ny * half; w += blockDim.x) {
+    const int y = w / half, k = w - y * half;
+    C *row = buf + y * nzh;
+    const int pk = pos[k];
+    const int pm = (k == 0) ? -1 : pos[M - k];
+    const C xk = row[pk];
+    const C xm = (k == 0) ? row[M] : row[pm];
+    const C A = mk<C>(xk.x + xm.x, xk.y - xm.y);
+    const C D = mk<C>(xk.x - xm.x, xk.y + xm.y);
+    const C wd = cmulc(D, twr[k]);            // D * conj(W^k) = D * exp(+2 pi i k/nz)
+    const C iwd = mk<C>(-wd.y, wd.x);
+    row[pk] = cadd(A, iwd);
+    if (k != 0 && pm != pk) row[pm] = cconj(csub(A, iwd));
+  }
+  __syncthreads();
+
+  Batch gz{ny, ny, nzh, 0, 1, false};
+  fft_inverse(buf, twz, a.pz, gz);
+
+  // fused GSFE force + applied stress + masked explicit Euler update
+  const int f = (int)(plane / a.nx);
+  const int x = (int)(plane - (size_t)f * a.nx);
+  const bool real_field = f < u.S;
+  const int sys = real_field ? f : f - u.S;
+  const size_t N = (size_t)a.nx * ny * nz;
+  const size_t off = plane * (size_t)ny * nz;
+  const size_t rbase = (size_t)x * ny * nz;
+  const T *bufr = reinterpret_cast<const T *>(buf);
+  const T cd = (T)u.cd, invN = (T)u.invN;
+  const T tau = real_field ? (T)u.tau[sys] : (T)0;
+  const T *site = reinterpret_cast<const T *>(u.site);
+  double dsq = 0.0, sum = 0.0;
+  for (int i = threadIdx.x; i < ny * nz; i += blockDim.x) {
+    const int y = i / nz, z = i - y * nz;
+    const T el = bufr[y * 2 * nzh + z] * invN;
+    const T old = xin[off + i];
+    T nv;
+    if (real_field) {
+      const T dE = core_derivative<T>(u.core, old, sys, rbase + i, N, xin, site);
+      nv = old - cd * (el - tau + dE);
+    } else {
+      nv = old - cd * el;
+    }
+    if (u.mask && u.mask[(size_t)sys * N + rbase + i]) nv = old;
+    xout[off + i] = nv;
+    const double d = (double)nv - (double)old;
+    dsq += d * d;
+    if (real_field) sum += (double)nv;
+  }
+  block_sum2(dsq, sum, red, partials + 2 * plane);
+}
+
+// ------------------------------------------------------------ reduction
+// One block: Neumaier-compensated FP64 sums of the per-plane partials.
+// stats[step] = {xinorm, xiave}; sets *stop when 0 < tol and xinorm < tol;
+// flags a non-finite result in *bad.
+__global__ void k_finalize(const double *__restrict__ partials, int nparts, double *__restrict__ stats, int step,
+                           double tol, int *stop, int *bad, int *steps_done, const double *extra_dsq) {
+  if (stop && *stop) return;
+  __shared__ double sh[4][1024];
+  double s0 = 0, c0 = 0, s1 = 0, c1 = 0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+    double v = partials[2 * i], t = s0 + v;
+    c0 += (fabs(s0) >= fabs(v)) ? (s0 - t) + v : (v - t) + s0;
+    s0 = t;
+    v = partials[2 * i + 1];
+    t = s1 + v;
+    c1 += (fabs(s1) >= fabs(v)) ? (s1 - t) + v : (v - t) + s1;
+    s1 = t;
+  }
+  sh[0][threadIdx.x] = s0; sh[1][threadIdx.x] = c0; sh[2][threadIdx.x] = s1; sh[3][threadIdx.x] = c1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a0 = 0, e0 = 0, a1 = 0, e1 = 0;
+    for (int i = 0; i < (int)blockDim.x; ++i) {
+      double v = sh[0][i], t = a0 + v;
+      e0 += (fabs(a0) >= fabs(v)) ? (a0 - t) + v : (v - t) + a0;
+      a0 = t;
+      e0 += sh[1][i];
+      v = sh[2][i];
+      t = a1 + v;
+      e1 += (fabs(a1) >= fabs(v)) ? (a1 - t) + v : (v - t) + a1;
+      a1 = t;
+      e1 += sh[3][i];
+    }
+    double dsq = a0 + e0;
+    if (extra_dsq) dsq += *extra_dsq;
+    const double xinorm = sqrt(dsq), xiave = a1 + e1;
+    stats[2 * step] = xinorm;
+    stats[2 * step + 1] = xiave;
+    if (steps_done) *steps_done = step + 1;
+    if (!isfinite(xinorm) || !isfinite(xiave)) *bad = 1;
+    if (tol > 0.0 && xinorm < tol && stop) *stop = 1;
+  }
+}
+
+// ------------------------------------------------------------ stress state
+// sigma_rot and tau in FP64 exactly as rotate_stress + resolSS_Schmid
+// (fft_fftw_slab.cpp:242-274, 737-769); then optionally sigma += dsigma
+// (solve_GL.cpp:151-155) and clear the stop flag.
+struct StressArgs {
+  double prim[3][3], invprim[3][3];
+  int ortho;
+  int S;
+  double xn[PFDD_MAXS][3], xb[PFDD_MAXS][3];
+  double dslip;
+  double dsig[3][3];
+};
+
+__global__ void k_stress_state(double *sigma /*[9]*/, double *tau, StressArgs s, int mode, int *stop) {
+  if (threadIdx.x != 0) return;
+  if (mode == 0) {
+    double sr[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        sr[i][j] = 0.0;
+        if (s.ortho) {
+          for (int k = 0; k < 3; ++k)
+            for (int l = 0; l < 3; ++l) sr[i][j] += s.prim[i][k] * sigma[3 * k + l] * s.invprim[l][j];
+        } else {
+          sr[i][j] = sigma[3 * i + j];
+        }
+      }
+    for (int a = 0; a < s.S; ++a) {
+      double t = 0.0;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) t = t + (sr[i][j] * s.xn[a][j] * s.xb[a][i]) / s.dslip;
+      tau[a] = t;
+    }
+    if (stop) *stop = 0;
+  } else {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) sigma[3 * i + j] = sigma[3 * i + j] + s.dsig[i][j];
+  }
+}
+
+// ------------------------------------------------------------ layout helpers
+template <typename T>
+__global__ void k_from_interleaved(const double *__restrict__ src, T *__restrict__ re, T *__restrict__ im, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 v = reinterpret_cast<const double2 *>(src)[i];
+    re[i] = (T)v.x;
+    if (im) im[i] = (T)v.y;
+  }
+}
+
+template <typename T>
+__global__ void k_to_interleaved(const T *__restrict__ re, const T *__restrict__ im, double *__restrict__ dst, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double2 v;
+    v.x = (double)re[i];
+    v.y = im ? (double)im[i] : 0.0;
+    reinterpret_cast<double2 *>(dst)[i] = v;
+  }
+}
+
+template <typename T>
+__global__ void k_from_planar(const double *__restrict__ src, T *__restrict__ dst, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (T)src[i];
+}
+
+template <typename T>
+__global__ void k_to_planar(const T *__restrict__ src, double *__restrict__ dst, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+
+}  // namespace pfdd

@@ -1,0 +1,223 @@
+"""ctypes binding of libpfdd_b200.so (C ABI in include/pfdd_b200.h).
+
+This is the Python-side mirror of the boundary the reference's host code binds
+(its FFT style object replaced by the library): the same
+descriptors and calls a C++ FftStyle plugin makes.  The library is loaded from
+this package directory; when it is missing, or no sm_100 device exists, every
+call raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpfdd_b200.so")
+MAX_SLIP = 12
+
+PFDD_OK = 0
+ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "EUNSUPPORTED", -5: "EDIVERGED", -6: "ENODEVICE",
+          -7: "ESTATE"}
+FP64, FP32 = 0, 1
+IMAG_AUTO, IMAG_FULL, IMAG_NYQUIST = 0, 1, 2
+CORE_PERFECT, CORE_EXTENDED, CORE_SINE, CORE_PYRII, CORE_USFE_ANGLE, CORE_MPEA, CORE_SINE_FIELD = 1, 2, 3, 4, 6, 7, 103
+
+# every symbol include/pfdd_b200.h declares
+EXPORTS = [
+    "pfdd_gpu_create", "pfdd_gpu_set_state", "pfdd_gpu_set_state_interleaved", "pfdd_gpu_get_state",
+    "pfdd_gpu_get_state_interleaved", "pfdd_gpu_advance", "pfdd_gpu_step_history", "pfdd_gpu_energy",
+    "pfdd_gpu_tau", "pfdd_gpu_info", "pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version",
+]
+
+D33 = ctypes.c_double * 3 * 3
+DS3 = ctypes.c_double * 3 * MAX_SLIP
+DP = ctypes.POINTER(ctypes.c_double)
+
+
+class InstanceDesc(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("n_slip", ctypes.c_int),
+        ("four", D33), ("prim", D33), ("xn", DS3), ("xb", DS3),
+        ("C44", ctypes.c_double), ("C12", ctypes.c_double), ("C11", ctypes.c_double),
+        ("dslip", ctypes.c_double), ("b", ctypes.c_double), ("cd_dt", ctypes.c_double),
+        ("core_flag", ctypes.c_int),
+        ("isf", ctypes.c_double), ("usf", ctypes.c_double), ("An", ctypes.c_double),
+        ("c", ctypes.c_double * 7), ("aa", ctypes.c_double * 5), ("bb", ctypes.c_double * 4),
+        ("site_gsfe", DP), ("xo", DP),
+        ("sigma", D33), ("dsigma", D33),
+    ]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("imag_mode", ctypes.c_int), ("device", ctypes.c_int),
+                ("use_graphs", ctypes.c_int), ("check_finite", ctypes.c_int)]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [("xinorm", ctypes.c_double), ("xiave", ctypes.c_double), ("steps_done", ctypes.c_int),
+                ("converged", ctypes.c_int)]
+
+
+class PfddError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("pfdd status %d (%s): %s" % (code, ERRORS.get(code, "?"), msg))
+        self.code = code
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError("libpfdd_b200.so not built at %s (run __graft_entry__.build())" % path)
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    lib.pfdd_gpu_create.argtypes = [ctypes.POINTER(InstanceDesc), ctypes.c_int, ctypes.POINTER(Options),
+                                    ctypes.POINTER(vp)]
+    lib.pfdd_gpu_set_state.argtypes = [vp, ctypes.c_int, DP, DP]
+    lib.pfdd_gpu_set_state_interleaved.argtypes = [vp, ctypes.c_int, DP]
+    lib.pfdd_gpu_get_state.argtypes = [vp, ctypes.c_int, DP, DP]
+    lib.pfdd_gpu_get_state_interleaved.argtypes = [vp, ctypes.c_int, DP]
+    lib.pfdd_gpu_advance.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(StepStats)]
+    lib.pfdd_gpu_step_history.argtypes = [vp, ctypes.c_int, DP, DP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.pfdd_gpu_energy.argtypes = [vp, ctypes.c_int, DP, DP, DP]
+    lib.pfdd_gpu_tau.argtypes = [vp, ctypes.c_int, DP]
+    lib.pfdd_gpu_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_size_t)]
+    lib.pfdd_gpu_last_error.argtypes = [vp]
+    lib.pfdd_gpu_last_error.restype = ctypes.c_char_p
+    lib.pfdd_gpu_destroy.argtypes = [vp]
+    lib.pfdd_gpu_destroy.restype = None
+    lib.pfdd_gpu_version.restype = ctypes.c_char_p
+    for name in EXPORTS:
+        if name not in ("pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version"):
+            getattr(lib, name).restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(DP) if a is not None else None
+
+
+def desc_from_workload(w, core_flag=None, An=None):
+    """InstanceDesc for a configs.Workload (constants derived as Material does)."""
+    d = InstanceDesc()
+    d.nx, d.ny, d.nz, d.n_slip = w.nx, w.ny, w.nz, w.S
+    for i in range(3):
+        for j in range(3):
+            d.four[i][j] = float(w.four[i, j])
+            d.prim[i][j] = float(w.prim[i, j])
+            d.sigma[i][j] = float(w.sigma[i, j])
+            d.dsigma[i][j] = float(w.dsigma[i, j])
+    for a in range(w.S):
+        for j in range(3):
+            d.xn[a][j] = float(w.xn[a, j])
+            d.xb[a][j] = float(w.xb[a, j])
+    C44, C12, C11 = w.material.elastic()
+    d.C44, d.C12, d.C11 = C44, C12, C11
+    d.dslip, d.b, d.cd_dt = w.material.dslip, w.material.b, w.cd_dt
+    d.core_flag = w.core_flag if core_flag is None else core_flag
+    d.isf, d.usf = w.material.isf, w.material.usf
+    d.An = w.material.An if An is None else An
+    return d
+
+
+class Stepper:
+    """Owns one pfdd_gpu handle (one or more instances)."""
+
+    def __init__(self, descs, precision=FP64, imag_mode=IMAG_AUTO, device=0, keep=()):
+        lib = load()
+        self._lib = lib
+        self._keep = list(keep)   # host arrays referenced by descriptors during create
+        arr = (InstanceDesc * len(descs))(*descs)
+        opt = Options(precision, imag_mode, device, 1, 1)
+        h = ctypes.c_void_p()
+        st = lib.pfdd_gpu_create(arr, len(descs), ctypes.byref(opt), ctypes.byref(h))
+        if st != PFDD_OK:
+            raise PfddError(st, lib.pfdd_gpu_last_error(None).decode())
+        self.h = h
+        self.descs = descs
+        self.n = len(descs)
+
+    @classmethod
+    def from_workloads(cls, workloads, precision=FP64, imag_mode=IMAG_AUTO, device=0):
+        descs, keep = [], []
+        for w in workloads:
+            d = desc_from_workload(w)
+            if w.site is not None:
+                s = np.ascontiguousarray(w.site, dtype=np.float64).reshape(-1)
+                keep.append(s)
+                d.site_gsfe = _dp(s)
+            if w.xo is not None:
+                m = np.ascontiguousarray(w.xo, dtype=np.float64).reshape(-1)
+                keep.append(m)
+                d.xo = _dp(m)
+            descs.append(d)
+        st = cls(descs, precision, imag_mode, device, keep)
+        st._keep = []
+        return st
+
+    def _check(self, st):
+        if st != PFDD_OK:
+            raise PfddError(st, self._lib.pfdd_gpu_last_error(self.h).decode())
+
+    def set_state(self, inst, re, im=None):
+        re = np.ascontiguousarray(re, dtype=np.float64).reshape(-1)
+        im = None if im is None else np.ascontiguousarray(im, dtype=np.float64).reshape(-1)
+        self._check(self._lib.pfdd_gpu_set_state(self.h, inst, _dp(re), _dp(im)))
+
+    def get_state(self, inst):
+        d = self.descs[inst]
+        n = d.n_slip * d.nx * d.ny * d.nz
+        re = np.empty(n)
+        im = np.empty(n)
+        self._check(self._lib.pfdd_gpu_get_state(self.h, inst, _dp(re), _dp(im)))
+        shape = (d.n_slip, d.nx, d.ny, d.nz)
+        return re.reshape(shape), im.reshape(shape)
+
+    def advance(self, n_steps, stress_states=1, tol=0.0):
+        stats = (StepStats * self.n)()
+        self._check(self._lib.pfdd_gpu_advance(self.h, n_steps, stress_states, tol, stats))
+        return [(s.xinorm, s.xiave, s.steps_done, s.converged) for s in stats]
+
+    def history(self, inst, cap=1 << 20):
+        cnt = ctypes.c_int()
+        self._check(self._lib.pfdd_gpu_step_history(self.h, inst, None, None, 0, ctypes.byref(cnt)))
+        n = cnt.value
+        a = np.empty(max(n, 1))
+        b = np.empty(max(n, 1))
+        self._check(self._lib.pfdd_gpu_step_history(self.h, inst, _dp(a), _dp(b), n, ctypes.byref(cnt)))
+        return a[:n], b[:n]
+
+    def tau(self, inst):
+        t = np.empty(self.descs[inst].n_slip)
+        self._check(self._lib.pfdd_gpu_tau(self.h, inst, _dp(t)))
+        return t
+
+    def energy(self, inst):
+        e = np.empty(3)
+        self._check(self._lib.pfdd_gpu_energy(self.h, inst, _dp(e[0:1]), _dp(e[1:2]), _dp(e[2:3])))
+        return tuple(e)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.pfdd_gpu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,114 @@
+"""GPU parity: the CUDA path (through the C ABI) against the numpy oracle.
+
+Tolerances: FP64 path max |dxi| <= 1e-10 (per step and over 100 steps);
+FP32 path relative L2 of Re xi <= 2e-5 after 100 steps.
+"""
+import numpy as np
+import pytest
+
+import pfdd_oracle as O
+from common import oracle_instance, small_loop
+from pfdd_b200 import capi, configs
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_gpu(ws, steps, precision=capi.FP64, states=None, stress_states=1, imag=capi.IMAG_AUTO):
+    with capi.Stepper.from_workloads(ws, precision=precision, imag_mode=imag) as st:
+        for i, w in enumerate(ws):
+            s = w.xi0 if states is None else states[i]
+            st.set_state(i, np.real(s), np.imag(s) if np.iscomplexobj(s) else None)
+        st.advance(steps, stress_states)
+        out = [st.get_state(i) for i in range(len(ws))]
+        hist = [st.history(i) for i in range(len(ws))]
+    return out, hist
+
+
+@pytest.mark.parametrize("n,steps", [(16, 1), (16, 10), (32, 100)])
+def test_fp64_loop_matches_oracle(n, steps):
+    w = small_loop(n)
+    inst = oracle_instance(w)
+    ref, nrm, ave = O.run(inst, w.xi0, steps)
+    (re, im), (hn, ha) = [x[0] for x in _run_gpu([w], steps)]
+    assert np.abs(re - ref.real).max() <= 1e-10
+    assert np.abs(im - ref.imag).max() <= 1e-10
+    np.testing.assert_allclose(hn, nrm, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(ha, ave, rtol=1e-10, atol=1e-10)
+
+
+def test_fp64_anisotropic_grid_and_sizes():
+    # non-cubic grid with a factor-3 axis
+    w = configs.loop_workload(n=16, radius=3.0)
+    w2 = configs.Workload("aniso", 24, 16, 12, w.app, w.xn, w.xb, w.four, w.prim, w.material, 3, w.sigma,
+                          0.5, np.random.default_rng(3).uniform(-0.2, 1.0, size=(3, 24, 16, 12)))
+    inst = oracle_instance(w2)
+    ref, _, _ = O.run(inst, w2.xi0, 5)
+    (re, im), _ = [x[0] for x in _run_gpu([w2], 5)]
+    assert np.abs(re - ref.real).max() <= 1e-10
+    assert np.abs(im - ref.imag).max() <= 1e-10
+
+
+@pytest.mark.parametrize("flag", [capi.CORE_PERFECT, capi.CORE_SINE, capi.CORE_MPEA, capi.CORE_SINE_FIELD])
+def test_fp64_core_models(flag):
+    w = small_loop(16)
+    rng = np.random.default_rng(11)
+    if flag == capi.CORE_MPEA:
+        w.site = rng.uniform(0.1, 0.3, size=(w.S, w.nx, w.ny, w.nz))
+    elif flag == capi.CORE_SINE_FIELD:
+        w.site = np.exp(0.15 * rng.standard_normal((w.S, w.nx, w.ny, w.nz)))
+    if flag == capi.CORE_PERFECT:
+        w.material.An = 0.3
+    w.core_flag = flag
+    inst = oracle_instance(w)
+    ref, _, _ = O.run(inst, w.xi0, 6)
+    (re, im), _ = [x[0] for x in _run_gpu([w], 6)]
+    assert np.abs(re - ref.real).max() <= 1e-10
+    assert np.abs(im - ref.imag).max() <= 1e-10
+
+
+def test_fp64_mask_and_complex_state():
+    w = small_loop(16)
+    rng = np.random.default_rng(5)
+    w.xo = (rng.uniform(size=(w.S, 16, 16, 16)) < 0.3).astype(np.float64)
+    xi0 = w.xi0 + 1j * rng.uniform(-0.01, 0.01, size=w.xi0.shape)
+    inst = oracle_instance(w)
+    ref, _, _ = O.run(inst, xi0, 8)
+    (re, im), _ = [x[0] for x in _run_gpu([w], 8, states=[xi0])]
+    assert np.abs(re - ref.real).max() <= 1e-10
+    assert np.abs(im - ref.imag).max() <= 1e-10
+
+
+def test_fp64_multi_instance_mixed_sizes():
+    ws = [small_loop(16, seed=1), configs.loop_workload(n=32, radius=6.0, seed=2, sigma_mpa=350.0),
+          configs.loop_workload(n=24, radius=4.0, seed=3, sigma_mpa=120.0)]
+    outs, _ = _run_gpu(ws, 7)
+    for w, (re, im) in zip(ws, outs):
+        ref, _, _ = O.run(oracle_instance(w), w.xi0, 7)
+        assert np.abs(re - ref.real).max() <= 1e-10
+        assert np.abs(im - ref.imag).max() <= 1e-10
+
+
+def test_fp32_loop_error_bound():
+    w = small_loop(32)
+    inst = oracle_instance(w)
+    ref, _, _ = O.run(inst, w.xi0, 100)
+    (re, im), _ = [x[0] for x in _run_gpu([w], 100, precision=capi.FP32)]
+    rel = np.linalg.norm(re - ref.real) / np.linalg.norm(ref.real)
+    assert rel <= 2e-5, rel
+
+
+def test_fp64_stress_ramp_states():
+    w = small_loop(16)
+    w.dsigma = np.zeros((3, 3))
+    w.dsigma[0, 2] = w.dsigma[2, 0] = 1e-3
+    # 3 stress states x 2 iterations each, sigma += dsigma between states
+    xi = w.xi0.astype(complex)
+    sig = w.sigma.copy()
+    for s in range(3):
+        w2 = configs.Workload(w.name, w.nx, w.ny, w.nz, w.app, w.xn, w.xb, w.four, w.prim, w.material,
+                              w.core_flag, sig.copy(), w.cd_dt, w.xi0)
+        xi, _, _ = O.run(oracle_instance(w2), xi, 2)
+        sig = sig + w.dsigma
+    (re, im), _ = [x[0] for x in _run_gpu([w], 2, stress_states=3)]
+    assert np.abs(re - xi.real).max() <= 1e-10
+    assert np.abs(im - xi.imag).max() <= 1e-10
