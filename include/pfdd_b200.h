@@ -47,7 +47,8 @@ enum {
   PFDD_EUNSUPPORTED = -4,  /* size/model combination not built */
   PFDD_EDIVERGED = -5,     /* non-finite order parameter detected */
   PFDD_ENODEVICE = -6,     /* no usable sm_100 device */
-  PFDD_ESTATE = -7         /* call not valid in the handle's current state */
+  PFDD_ESTATE = -7,        /* call not valid in the handle's current state */
+  PFDD_ETIMEOUT = -8       /* a bounded device-side wait ran out (the step was abandoned) */
 };
 
 #define PFDD_MAX_SLIP 12
@@ -170,6 +171,22 @@ pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_
 
 /* Resolved shear stresses tau[S] of instance `inst` at the current stress state. */
 pfdd_status pfdd_gpu_tau(pfdd_gpu *h, int inst, double *tau);
+
+/* Run all later work of the handle on a caller-owned cudaStream_t (passed as
+ * void* so this header needs no CUDA include); NULL returns to the handle's
+ * own stream.  Lets a caller order the stepper against its own work and
+ * bracket it with its own events. */
+pfdd_status pfdd_gpu_set_stream(pfdd_gpu *h, void *stream);
+
+/* Kernel classes of one GL iteration, in launch order. */
+enum { PFDD_K_FWD_PLANES = 0, PFDD_K_XPENCIL = 1, PFDD_K_INV_UPDATE = 2, PFDD_K_FINALIZE = 3, PFDD_NKERNELS = 4 };
+
+/* Advance n_steps GL iterations (one stress state, no tolerance test) with a
+ * CUDA event pair around every launch and return the mean device time per
+ * launch of each kernel class in kernel_ms[PFDD_NKERNELS] (summed over
+ * instances), and the number of kernel launches one iteration makes.  The
+ * state advances exactly as with pfdd_gpu_advance. */
+pfdd_status pfdd_gpu_profile(pfdd_gpu *h, int n_steps, double *kernel_ms, int *launches_per_step);
 
 /* Number of instances, and the device bytes the handle holds. */
 pfdd_status pfdd_gpu_info(pfdd_gpu *h, int *n_instances, size_t *device_bytes);

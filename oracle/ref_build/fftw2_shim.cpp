@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <map>
 #include <utility>
 #include <vector>
@@ -222,8 +223,31 @@ void fftwnd_mpi(fftwnd_mpi_plan p, int n_fields, fftw_complex *local_data,
   double *d = reinterpret_cast<double *>(local_data);
   size_t total = (size_t)nx * ny * nz * h;
   std::vector<double> scratch(2 * total);
-  // z: nx*ny lines of nz elements, vector = fields
-  fft_lines(d, scratch.data(), nx * ny, nz, h, p->sign);
+  // z: lines of nz elements (vector = fields).  Lines are gathered in groups
+  // of B into a [nz][B*h] block so the butterfly loops run over contiguous
+  // vectors, then scattered back.
+  const int lines = nx * ny;
+  const int B = 8;
+  std::vector<double> blk(2 * (size_t)nz * B * h), bsc(2 * (size_t)nz * B * h);
+  for (int l0 = 0; l0 < lines; l0 += B) {
+    const int nb = std::min(B, lines - l0);
+    const int V = nb * h;
+    for (int b = 0; b < nb; ++b)
+      for (int i = 0; i < nz; ++i)
+        for (int f = 0; f < h; ++f) {
+          const double *src = d + 2 * (((size_t)(l0 + b) * nz + i) * h + f);
+          double *dst = blk.data() + 2 * ((size_t)i * V + b * h + f);
+          dst[0] = src[0]; dst[1] = src[1];
+        }
+    fft_lines(blk.data(), bsc.data(), 1, nz, V, p->sign);
+    for (int b = 0; b < nb; ++b)
+      for (int i = 0; i < nz; ++i)
+        for (int f = 0; f < h; ++f) {
+          double *dst = d + 2 * (((size_t)(l0 + b) * nz + i) * h + f);
+          const double *src = blk.data() + 2 * ((size_t)i * V + b * h + f);
+          dst[0] = src[0]; dst[1] = src[1];
+        }
+  }
   // y: nx transforms of ny elements, vector = nz*fields
   fft_lines(d, scratch.data(), nx, ny, nz * h, p->sign);
   // x: one transform of nx elements, vector = ny*nz*fields

@@ -42,6 +42,16 @@ def parse_setup(path):
     return out
 
 
+def _raise_stack():
+    # Bmatrix keeps an S*S*N double array on the stack (fft_fftw_slab.cpp:475)
+    import resource
+    try:
+        soft, hard = resource.getrlimit(resource.RLIMIT_STACK)
+        resource.setrlimit(resource.RLIMIT_STACK, (hard, hard))
+    except Exception:
+        pass
+
+
 def run_reference(workload, steps, state=None, xo=None, mpea=None, sets=(), want_B=False,
                   timing=False, workdir=None, timeout=3600):
     """Run `steps` GL iterations of the reference on `workload`.
@@ -52,7 +62,17 @@ def run_reference(workload, steps, state=None, xo=None, mpea=None, sets=(), want
     """
     if not available():
         raise RuntimeError("reference oracle not built: make -C oracle/ref_build")
+    own_tmp = workdir is None
     tmp = workdir or tempfile.mkdtemp(prefix="pfdd_ref_")
+    try:
+        return _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout)
+    finally:
+        if own_tmp:
+            import shutil
+            shutil.rmtree(tmp, ignore_errors=True)
+
+
+def _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout):
     S, nx, ny, nz = workload.S, workload.nx, workload.ny, workload.nz
     deck = os.path.join(tmp, "in.deck")
     with open(deck, "w") as f:
@@ -84,7 +104,8 @@ def run_reference(workload, steps, state=None, xo=None, mpea=None, sets=(), want
     if timing:
         args += ["-timing"]
     env = dict(os.environ)
-    proc = subprocess.run(args, cwd=tmp, capture_output=True, text=True, timeout=timeout, env=env)
+    proc = subprocess.run(args, cwd=tmp, capture_output=True, text=True, timeout=timeout, env=env,
+                          preexec_fn=_raise_stack)
     if proc.returncode != 0:
         raise RuntimeError("reference harness failed (%d):\n%s\n%s" % (proc.returncode, proc.stdout[-3000:],
                                                                       proc.stderr[-3000:]))

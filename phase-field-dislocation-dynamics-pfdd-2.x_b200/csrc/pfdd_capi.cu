@@ -92,14 +92,21 @@ void twiddles(int n, int count, std::vector<double> &out) {
   }
 }
 
+template <typename T> struct Threads;
+template <> struct Threads<float> { static constexpr int plane = 512, pencil = 512; };
+template <> struct Threads<double> { static constexpr int plane = 256, pencil = 256; };
+
 struct Instance {
   pfdd_instance_desc d;
   int S, F, imag;
-  int nx, ny, nz, nzh, M;
+  int nx, ny, nz, nzh, nzp, M;
   size_t N;
   FftPlan px, py, pz;
-  int ccols;
+  int ccols, fstride, ntiles;
+  int sx_n, sy_n;
   size_t smem_plane, smem_update, smem_pencil;
+  DevBuf aux;          // Nyquist spectrum of Im xi (IMAG_NYQ)
+  DevBuf ppart;        // per-tile partial sums of P2
   Green green;
   Core core;
   StressArgs stress;
@@ -118,7 +125,7 @@ struct Instance {
   double *tau() const { return small.as<double>(); }
   double *sigma() const { return small.as<double>() + PFDD_MAXS; }
   int *flags() const { return reinterpret_cast<int *>(small.as<double>() + PFDD_MAXS + 9); }
-  // flags: [0] stop, [1] bad, [2] steps_done
+  // flags: [0] stop, [1] bad, [2] steps_done, [3] a bounded wait ran out
 };
 
 }  // namespace
@@ -128,7 +135,9 @@ struct pfdd_gpu {
   int device = 0;
   pfdd_options opt{};
   std::vector<std::unique_ptr<Instance>> inst;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // stream in use
+  cudaStream_t own_stream = nullptr;  // stream created by the handle
+  DevBuf staging;                     // FP64 host<->device staging, kept across calls
   std::string err;
   size_t device_bytes = 0;
 };
@@ -282,13 +291,15 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
 
   // int16 tables: posM[M], kx_of[nx], ky_of[ny], kz_of[nzh]
   std::vector<int> pz = positions(I.pz), px = positions(I.px), py = positions(I.py);
-  std::vector<int16_t> tab(I.M + I.nx + I.ny + I.nzh);
+  std::vector<int16_t> tab(I.M + I.nx + I.ny + I.nzp, 0);
   int16_t *t_posM = tab.data(), *t_kx = t_posM + I.M, *t_ky = t_kx + I.nx, *t_kz = t_ky + I.ny;
   for (int k = 0; k < I.M; ++k) t_posM[k] = (int16_t)pz[k];
   for (int k = 0; k < I.nx; ++k) t_kx[px[k]] = (int16_t)k;
   for (int k = 0; k < I.ny; ++k) t_ky[py[k]] = (int16_t)k;
   for (int k = 0; k < I.M; ++k) t_kz[pz[k]] = (int16_t)k;
   t_kz[I.M] = (int16_t)I.M;
+  I.sx_n = px[I.nx / 2];
+  I.sy_n = py[I.ny / 2];
   CUDA_TRY(h, I.tab16.alloc(tab.size() * sizeof(int16_t)));
   CUDA_TRY(h, cudaMemcpy(I.tab16.p, tab.data(), tab.size() * sizeof(int16_t), cudaMemcpyHostToDevice));
   h->device_bytes += I.tab16.bytes;
@@ -304,7 +315,7 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
     CUDA_TRY(h, cudaMemset(I.xi[b].p, 0, fieldN * sizeof(T)));
     h->device_bytes += I.xi[b].bytes;
   }
-  CUDA_TRY(h, I.spec.alloc((size_t)I.F * I.nx * I.ny * I.nzh * sizeof(C)));
+  CUDA_TRY(h, I.spec.alloc((size_t)I.F * I.nx * I.ny * I.nzp * sizeof(C)));
   h->device_bytes += I.spec.bytes;
   CUDA_TRY(h, I.partials.alloc(2 * (size_t)I.F * I.nx * sizeof(double)));
   h->device_bytes += I.partials.bytes;
@@ -332,18 +343,42 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   }
 
   // shared-memory budgets
-  I.smem_plane = ((size_t)I.ny * I.nzh + I.ny + 2 * (size_t)I.M) * sizeof(C) + (size_t)I.M * 4 + 16;
-  I.smem_update = I.smem_plane + 4 * 2 + 64 * sizeof(double) + 16;
+  I.smem_plane = PlaneSmem<C>::bytes(I.ny, I.nzp, I.M);
+  I.smem_update = I.smem_plane;
   const size_t limit = 227 * 1024;
   if (I.smem_update > limit)
     return fail(h, PFDD_EUNSUPPORTED, "x-plane of %dx%d does not fit shared memory in this precision", I.ny, I.nz);
-  const size_t ncols = (size_t)I.ny * I.nzh;
+  const size_t ncols = (size_t)I.ny * I.nzp;
+  const int cmin = (int)(16 / sizeof(C)) > 1 ? (int)(16 / sizeof(C)) : 1;  // 16-byte row chunks
+  // field stride padded so consecutive fields start cc columns apart in the
+  // 32 shared-memory banks (the x-FFT walks columns, then fields, across a warp)
+  auto fstride_for = [&](int cc) {
+    const int wpc = (int)(sizeof(C) / 4);
+    const int target = (cc * wpc) % 32;
+    for (int pad = 0; pad < 64; ++pad)
+      if ((pad * sizeof(C)) % 16 == 0 && (((size_t)I.nx * cc + pad) * wpc) % 32 == (size_t)target)
+        return I.nx * cc + pad;
+    return I.nx * cc;
+  };
+  auto pencil_bytes = [&](int cc) {
+    return ((size_t)I.F * fstride_for(cc) + I.nx) * sizeof(C) + 64 * sizeof(double);
+  };
   int cc = 32;
-  while (cc > 1 && (ncols % cc || ((size_t)I.F * I.nx * cc + I.nx) * sizeof(C) > 200 * 1024)) cc >>= 1;
-  if (((size_t)I.F * I.nx * cc + I.nx) * sizeof(C) > limit)
+  while (cc > cmin && (ncols % cc || pencil_bytes(cc) > 200 * 1024)) cc >>= 1;
+  if (ncols % cc || pencil_bytes(cc) > limit)
     return fail(h, PFDD_EUNSUPPORTED, "x-pencil of %d x %d fields does not fit shared memory", I.nx, I.F);
   I.ccols = cc;
-  I.smem_pencil = ((size_t)I.F * I.nx * cc + I.nx) * sizeof(C);
+  I.fstride = fstride_for(cc);
+  I.ntiles = (int)(ncols / cc);
+  I.smem_pencil = pencil_bytes(cc);
+  if (I.imag == IMAG_NYQ) {
+    const size_t na = (size_t)I.S * ((size_t)I.nx * I.ny + (size_t)I.nx * I.M + (size_t)I.ny * I.M);
+    CUDA_TRY(h, I.aux.alloc(na * sizeof(C)));
+    CUDA_TRY(h, cudaMemset(I.aux.p, 0, na * sizeof(C)));
+    h->device_bytes += I.aux.bytes;
+    CUDA_TRY(h, I.ppart.alloc(2 * (size_t)I.ntiles * sizeof(double)));
+    h->device_bytes += I.ppart.bytes;
+  }
 
   build_green(d, I.green);
   if (!build_core(d, I.core)) return fail(h, PFDD_EUNSUPPORTED, "core model %d not supported", d.core_flag);
@@ -354,7 +389,7 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
 template <typename T>
 void fill_plane_args(const Instance &I, PlaneArgs &pa) {
   pa.py = I.py; pa.pz = I.pz;
-  pa.nx = I.nx; pa.ny = I.ny; pa.nz = I.nz; pa.nzh = I.nzh; pa.M = I.M;
+  pa.nx = I.nx; pa.ny = I.ny; pa.nz = I.nz; pa.nzh = I.nzh; pa.nzp = I.nzp; pa.M = I.M;
   pa.S = I.S; pa.F = I.F;
   pa.tw_y = I.tw_y.p; pa.tw_z = I.tw_z.p; pa.tw_r = I.tw_r.p;
   pa.posM = I.posM;
@@ -362,15 +397,16 @@ void fill_plane_args(const Instance &I, PlaneArgs &pa) {
 
 template <typename T>
 pfdd_status set_smem_attrs(pfdd_gpu *h, size_t plane, size_t upd, size_t pencil) {
-  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_xpencil<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pencil));
+  constexpr int NP = Threads<T>::plane, NC = Threads<T>::pencil;
+  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_xpencil<T, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pencil));
   return PFDD_OK;
 }
 
 // Enqueue one GL iteration of one instance; `step` indexes the stats record.
 template <typename T>
-void enqueue_step(Instance &I, cudaStream_t st, int step, double tol) {
+void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_t *ev = nullptr) {
   PlaneArgs pa;
   fill_plane_args<T>(I, pa);
   int *flags = I.flags();
@@ -378,19 +414,29 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol) {
   T *xout = I.xi[I.cur ^ 1].as<T>();
   cx<T> *spec = I.spec.as<cx<T>>();
   const int planes = I.F * I.nx;
-  k_fwd_planes<T><<<planes, 256, I.smem_plane, st>>>(xin, spec, pa, flags);
+  constexpr int NP = Threads<T>::plane, NC = Threads<T>::pencil;
+  if (ev) cudaEventRecord(ev[0], st);
+  k_fwd_planes<T, NP><<<planes, NP, I.smem_plane, st>>>(xin, spec, pa, flags, flags + 3);
+  if (ev) cudaEventRecord(ev[1], st);
   PencilArgs pe;
   pe.px = I.px;
-  pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.M = I.M;
+  pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.nzp = I.nzp; pe.M = I.M;
   pe.S = I.S; pe.F = I.F; pe.imag = I.imag;
-  pe.ncols = I.ny * I.nzh;
+  pe.ncols = I.ny * I.nzp;
   pe.ccols = I.ccols;
   pe.tw_x = I.tw_x.p;
   pe.kx_of = I.kx_of; pe.ky_of = I.ky_of; pe.kz_of = I.kz_of;
+  pe.mode = PASS_STEP;
+  pe.fstride = I.fstride;
+  pe.aux = I.aux.p;
+  pe.sx_n = I.sx_n; pe.sy_n = I.sy_n;
+  pe.cd = I.d.cd_dt;
+  pe.partials = I.imag == IMAG_NYQ ? I.ppart.as<double>() : nullptr;
   pe.g = I.green;
-  k_xpencil<T><<<pe.ncols / pe.ccols, 256, I.smem_pencil, st>>>(spec, pe, flags);
+  k_xpencil<T, NC><<<I.ntiles, NC, I.smem_pencil, st>>>(spec, pe, flags);
+  if (ev) cudaEventRecord(ev[2], st);
   UpdateArgs ua;
-  ua.nx = I.nx; ua.ny = I.ny; ua.nz = I.nz; ua.nzh = I.nzh; ua.S = I.S; ua.F = I.F;
+  ua.nx = I.nx; ua.ny = I.ny; ua.nz = I.nz; ua.nzh = I.nzh; ua.nzp = I.nzp; ua.S = I.S; ua.F = I.F;
   ua.cd = I.d.cd_dt;
   ua.invN = 1.0 / (double)I.N;
   ua.core = I.core;
@@ -398,9 +444,66 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol) {
   ua.mask = I.mask.as<uint8_t>();
   ua.site = I.site.p;
   ua.stop = flags;
-  k_inv_update<T><<<planes, 256, I.smem_update, st>>>(spec, xin, xout, pa, ua, I.partials.as<double>());
+  ua.err = flags + 3;
+  ua.mode = PASS_STEP;
+  k_inv_update<T, NP><<<planes, NP, I.smem_update, st>>>(spec, xin, xout, pa, ua, I.partials.as<double>());
+  if (ev) cudaEventRecord(ev[3], st);
+  const bool nyq = I.imag == IMAG_NYQ;
   k_finalize<<<1, 1024, 0, st>>>(I.partials.as<double>(), planes, I.stats.as<double>(), step, tol, flags,
-                                 flags + 1, flags + 2, nullptr);
+                                 flags + 1, flags + 2, nyq ? I.ppart.as<double>() : nullptr, nyq ? I.ntiles : 0,
+                                 1.0 / (double)I.N);
+  if (ev) cudaEventRecord(ev[4], st);
+}
+
+constexpr int kLaunchesPerStep = 4;
+
+template <typename T>
+pfdd_status profile_impl(pfdd_gpu *h, int n_steps, double *kernel_ms) {
+  cudaStream_t st = h->stream;
+  for (int k = 0; k < PFDD_NKERNELS; ++k) kernel_ms[k] = 0.0;
+  for (auto &ip : h->inst) {
+    Instance &I = *ip;
+    if (I.stats_cap < n_steps) {
+      I.stats.release();
+      CUDA_TRY(h, I.stats.alloc(2 * (size_t)n_steps * sizeof(double)));
+      I.stats_cap = n_steps;
+    }
+    k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.stress, 0, I.flags());
+  }
+  std::vector<cudaEvent_t> ev(5 * (size_t)n_steps * h->inst.size());
+  for (auto &e : ev) CUDA_TRY(h, cudaEventCreate(&e));
+  size_t q = 0;
+  for (int it = 0; it < n_steps; ++it)
+    for (auto &ip : h->inst) {
+      enqueue_step<T>(*ip, st, it, 0.0, &ev[q]);
+      ip->cur ^= 1;
+      q += 5;
+    }
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) {
+    for (size_t b = 0; b < q; b += 5)
+      for (int k = 0; k < PFDD_NKERNELS; ++k) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[b + k], ev[b + k + 1]);
+        kernel_ms[k] += ms;
+      }
+    for (int k = 0; k < PFDD_NKERNELS; ++k) kernel_ms[k] /= (double)n_steps;
+  }
+  for (auto &x : ev) cudaEventDestroy(x);
+  CUDA_TRY(h, e);
+  for (auto &ip : h->inst) {
+    Instance &I = *ip;
+    int fl[4];
+    CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+    if (fl[3]) return fail(h, PFDD_ETIMEOUT, "a bounded device wait ran out");
+    if (fl[1]) return fail(h, PFDD_EDIVERGED, "non-finite order parameter");
+    I.hist.resize(2 * (size_t)fl[2]);
+    if (fl[2]) CUDA_TRY(h, cudaMemcpy(I.hist.data(), I.stats.p, 2 * (size_t)fl[2] * sizeof(double),
+                                      cudaMemcpyDeviceToHost));
+    I.hist_count = fl[2];
+    CUDA_TRY(h, cudaMemset(I.flags() + 2, 0, sizeof(int)));
+  }
+  return PFDD_OK;
 }
 
 template <typename T>
@@ -434,8 +537,9 @@ pfdd_status advance_impl(pfdd_gpu *h, int n_steps, int stress_states, double tol
     CUDA_TRY(h, cudaStreamSynchronize(st));
     for (size_t i = 0; i < h->inst.size(); ++i) {
       Instance &I = *h->inst[i];
-      int fl[3];
+      int fl[4];
       CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+      if (fl[3]) return fail(h, PFDD_ETIMEOUT, "instance %zu: a bounded device wait ran out", i);
       if (fl[1]) return fail(h, PFDD_EDIVERGED, "instance %zu: non-finite order parameter", i);
       const int did = fl[2];
       // parity: started at cur0, flipped n_steps times on the host, but only `did` real swaps
@@ -467,10 +571,26 @@ pfdd_status advance_impl(pfdd_gpu *h, int n_steps, int stress_states, double tol
 template <typename T>
 pfdd_status set_state_impl(pfdd_gpu *h, Instance &I, const double *re, const double *im, bool interleaved) {
   const size_t n = (size_t)I.S * I.N;
-  DevBuf tmp;
-  CUDA_TRY(h, tmp.alloc(n * sizeof(double) * (interleaved ? 2 : 1)));
+  if (h->staging.bytes < 2 * n * sizeof(double)) {
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->staging.release();
+    CUDA_TRY(h, h->staging.alloc(2 * n * sizeof(double)));
+  }
+  DevBuf &tmp = h->staging;
   T *dre = I.xi[I.cur].as<T>();
   T *dim = I.F > I.S ? dre + n : nullptr;
+  if (I.imag == IMAG_NYQ) {
+    // the Nyquist carrier starts from Im xi = 0 (what every reference initial_sxtal_* sets)
+    if (im)
+      for (size_t i = 0; i < n; ++i)
+        if (im[i] != 0.0)
+          return fail(h, PFDD_EINVAL, "nonzero Im xi needs a handle created with PFDD_IMAG_FULL");
+    if (interleaved)
+      for (size_t i = 0; i < n; ++i)
+        if (re[2 * i + 1] != 0.0)
+          return fail(h, PFDD_EINVAL, "nonzero Im xi needs a handle created with PFDD_IMAG_FULL");
+    CUDA_TRY(h, cudaMemsetAsync(I.aux.p, 0, I.aux.bytes, h->stream));
+  }
   if (interleaved) {
     CUDA_TRY(h, cudaMemcpyAsync(tmp.p, re, 2 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     k_from_interleaved<T><<<1184, 256, 0, h->stream>>>(tmp.as<double>(), dre, dim, n);
@@ -479,9 +599,9 @@ pfdd_status set_state_impl(pfdd_gpu *h, Instance &I, const double *re, const dou
     k_from_planar<T><<<1184, 256, 0, h->stream>>>(tmp.as<double>(), dre, n);
     if (dim) {
       if (im) {
-        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-        CUDA_TRY(h, cudaMemcpyAsync(tmp.p, im, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        k_from_planar<T><<<1184, 256, 0, h->stream>>>(tmp.as<double>(), dim, n);
+        CUDA_TRY(h, cudaMemcpyAsync(tmp.as<double>() + n, im, n * sizeof(double), cudaMemcpyHostToDevice,
+                                    h->stream));
+        k_from_planar<T><<<1184, 256, 0, h->stream>>>(tmp.as<double>() + n, dim, n);
       } else {
         CUDA_TRY(h, cudaMemsetAsync(dim, 0, n * sizeof(T), h->stream));
       }
@@ -492,13 +612,58 @@ pfdd_status set_state_impl(pfdd_gpu *h, Instance &I, const double *re, const dou
   return PFDD_OK;
 }
 
+// Im xi of a Nyquist-carrier instance into dst [S*N] (compute precision):
+// x-inverse of the Nyquist spectrum (k_xpencil PASS_SYNTH), then the plane
+// inverse (k_inv_update PASS_SYNTH), through the spectrum buffer.
+template <typename T>
+void synth_imag(Instance &I, cudaStream_t st, T *dst) {
+  constexpr int NP = Threads<T>::plane, NC = Threads<T>::pencil;
+  PencilArgs pe;
+  memset(&pe, 0, sizeof pe);
+  pe.px = I.px;
+  pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.nzp = I.nzp; pe.M = I.M;
+  pe.S = I.S; pe.F = I.S; pe.imag = IMAG_NYQ;
+  pe.ncols = I.ny * I.nzp;
+  pe.ccols = I.ccols;
+  pe.tw_x = I.tw_x.p;
+  pe.kx_of = I.kx_of; pe.ky_of = I.ky_of; pe.kz_of = I.kz_of;
+  pe.mode = PASS_SYNTH;
+  pe.fstride = I.fstride;
+  pe.aux = I.aux.p;
+  pe.sx_n = I.sx_n; pe.sy_n = I.sy_n;
+  pe.g = I.green;
+  cx<T> *spec = I.spec.as<cx<T>>();
+  k_xpencil<T, NC><<<I.ntiles, NC, I.smem_pencil, st>>>(spec, pe, nullptr);
+  PlaneArgs pa;
+  fill_plane_args<T>(I, pa);
+  UpdateArgs ua;
+  memset(&ua, 0, sizeof ua);
+  ua.nx = I.nx; ua.ny = I.ny; ua.nz = I.nz; ua.nzh = I.nzh; ua.nzp = I.nzp; ua.S = I.S; ua.F = I.S;
+  ua.invN = 1.0 / (double)I.N;
+  ua.mode = PASS_SYNTH;
+  ua.err = I.flags() + 3;
+  // xin is not read by the synthesis pass
+  k_inv_update<T, NP><<<I.S * I.nx, NP, I.smem_update, st>>>(spec, I.xi[I.cur].as<T>(), dst, pa, ua,
+                                                              I.partials.as<double>());
+}
+
 template <typename T>
 pfdd_status get_state_impl(pfdd_gpu *h, Instance &I, double *re, double *im, double *inter) {
   const size_t n = (size_t)I.S * I.N;
-  DevBuf tmp;
-  CUDA_TRY(h, tmp.alloc(n * sizeof(double) * 2));
+  if (h->staging.bytes < 2 * n * sizeof(double)) {
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->staging.release();
+    CUDA_TRY(h, h->staging.alloc(2 * n * sizeof(double)));
+  }
+  DevBuf &tmp = h->staging;
   const T *dre = I.xi[I.cur].as<T>();
   const T *dim = I.F > I.S ? dre + n : nullptr;
+  if (I.imag == IMAG_NYQ && (inter || im)) {
+    // the other ping-pong buffer is free between steps
+    T *scratch = I.xi[I.cur ^ 1].as<T>();
+    synth_imag<T>(I, h->stream, scratch);
+    dim = scratch;
+  }
   if (inter) {
     k_to_interleaved<T><<<1184, 256, 0, h->stream>>>(dre, dim, tmp.as<double>(), n);
     CUDA_TRY(h, cudaMemcpyAsync(inter, tmp.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -557,10 +722,10 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
     const pfdd_instance_desc &d = descs[i];
     if (d.n_slip < 1 || d.n_slip > PFDD_MAX_SLIP)
       return fail(nullptr, PFDD_EINVAL, "instance %d: n_slip %d outside 1..%d", i, d.n_slip, PFDD_MAX_SLIP);
-    if (!valid_size(d.nx) || !valid_size(d.ny) || !valid_size(d.nz) || d.nz < 4)
+    if (!valid_size(d.nx) || !valid_size(d.ny) || !valid_size(d.nz) || d.nz % 4)
       return fail(nullptr, PFDD_EUNSUPPORTED,
-                  "instance %d: grid %dx%dx%d: each extent must be even, 2^a 3^b, <= 1024 (nz >= 4)", i, d.nx,
-                  d.ny, d.nz);
+                  "instance %d: grid %dx%dx%d: each extent must be even and 2^a 3^b, <= 1024, nz a multiple of 4",
+                  i, d.nx, d.ny, d.nz);
     if (!(d.dslip > 0) || !(d.b > 0) || !(d.C44 > 0))
       return fail(nullptr, PFDD_EINVAL, "instance %d: dslip, b and C44 must be positive", i);
   }
@@ -569,8 +734,9 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
   h->precision = o.precision;
   h->device = o.device;
   if (cudaSetDevice(o.device) != cudaSuccess) return fail(nullptr, PFDD_ECUDA, "cudaSetDevice failed");
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(nullptr, PFDD_ECUDA, "stream creation failed");
+  h->stream = h->own_stream;
   size_t max_plane = 0, max_upd = 0, max_pen = 0;
   for (int i = 0; i < n_instances; ++i) {
     std::unique_ptr<Instance> I(new Instance);
@@ -579,13 +745,18 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
     I->d.xo = nullptr;
     I->S = descs[i].n_slip;
     int imag = o.imag_mode;
-    if (imag == PFDD_IMAG_AUTO) imag = PFDD_IMAG_FULL;  // the Nyquist-only carrier is not built yet
-    if (imag == PFDD_IMAG_NYQUIST) return fail(nullptr, PFDD_EUNSUPPORTED, "PFDD_IMAG_NYQUIST is not built yet");
-    I->imag = (imag == PFDD_IMAG_FULL) ? IMAG_FULL : IMAG_NONE;
+    if (imag == PFDD_IMAG_AUTO) imag = descs[i].xo ? PFDD_IMAG_FULL : PFDD_IMAG_NYQUIST;
+    if (imag == PFDD_IMAG_NYQUIST && descs[i].xo)
+      return fail(nullptr, PFDD_EINVAL, "instance %d: PFDD_IMAG_NYQUIST is exact only without an obstacle mask", i);
+    if (imag != PFDD_IMAG_FULL && imag != PFDD_IMAG_NYQUIST)
+      return fail(nullptr, PFDD_EINVAL, "instance %d: unknown imag_mode %d", i, imag);
+    I->imag = (imag == PFDD_IMAG_FULL) ? IMAG_FULL : IMAG_NYQ;
     I->F = I->imag == IMAG_FULL ? 2 * I->S : I->S;
     I->nx = descs[i].nx; I->ny = descs[i].ny; I->nz = descs[i].nz;
     I->M = I->nz / 2;
     I->nzh = I->M + 1;
+    // spectrum rows padded to whole 16-byte units so a plane moves in one bulk copy
+    I->nzp = (o.precision == PFDD_FP32) ? ((I->nzh + 1) & ~1) : I->nzh;
     I->N = (size_t)I->nx * I->ny * I->nz;
     make_plan(I->nx, I->px);
     make_plan(I->ny, I->py);
@@ -686,6 +857,23 @@ pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_
   return fail(h, PFDD_EUNSUPPORTED, "energy reduction not built yet");
 }
 
+pfdd_status pfdd_gpu_set_stream(pfdd_gpu *h, void *stream) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  cudaSetDevice(h->device);
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  h->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : h->own_stream;
+  return PFDD_OK;
+}
+
+pfdd_status pfdd_gpu_profile(pfdd_gpu *h, int n_steps, double *kernel_ms, int *launches_per_step) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (n_steps < 1 || !kernel_ms) return fail(h, PFDD_EINVAL, "need n_steps >= 1 and kernel_ms");
+  cudaSetDevice(h->device);
+  if (launches_per_step) *launches_per_step = kLaunchesPerStep * (int)h->inst.size();
+  return h->precision == PFDD_FP64 ? profile_impl<double>(h, n_steps, kernel_ms)
+                                   : profile_impl<float>(h, n_steps, kernel_ms);
+}
+
 pfdd_status pfdd_gpu_info(pfdd_gpu *h, int *n_instances, size_t *device_bytes) {
   if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
   if (n_instances) *n_instances = (int)h->inst.size();
@@ -700,7 +888,8 @@ void pfdd_gpu_destroy(pfdd_gpu *h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   h->inst.clear();
-  if (h->stream) cudaStreamDestroy(h->stream);
+  h->staging.release();
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
 

@@ -134,6 +134,20 @@ struct FftPlan {
   int L[8];
 };
 
+// Division by a block-uniform divisor: shift when it is a power of two.
+struct FastDiv {
+  int d, sh;
+  __host__ __device__ FastDiv() : d(1), sh(0) {}
+  __host__ __device__ explicit FastDiv(int v) : d(v), sh(-1) {
+    if (v > 0 && (v & (v - 1)) == 0) {
+      sh = 0;
+      while ((1 << sh) < v) ++sh;
+    }
+  }
+  __device__ __forceinline__ int div(int x) const { return sh >= 0 ? (x >> sh) : x / d; }
+  __device__ __forceinline__ int mod(int x) const { return sh >= 0 ? (x & (d - 1)) : x % d; }
+};
+
 // Batched transform geometry in shared memory: transform b (0 <= b < batch)
 // starts at (b % bin) * bs_in + (b / bin) * bs_out and its element i sits at
 // start + i * es.  If batch_fast, consecutive threads take consecutive b (use
@@ -143,6 +157,27 @@ struct Batch {
   bool batch_fast;
 };
 
+// Twiddles W^(j*k) for k = 1..R-1 from at most four table reads:
+// W^(j), W^(2j), W^(4j), W^(8j) and their products.
+template <int R, typename C>
+__device__ __forceinline__ void stage_twiddles(const C *__restrict__ tw, int jt, C (&w)[R]) {
+  if constexpr (R == 2) {
+    w[1] = tw[jt];
+  } else if constexpr (R == 3) {
+    w[1] = tw[jt]; w[2] = tw[2 * jt];
+  } else if constexpr (R == 4) {
+    w[1] = tw[jt]; w[2] = tw[2 * jt]; w[3] = tw[3 * jt];
+  } else if constexpr (R == 8) {
+    w[1] = tw[jt]; w[2] = tw[2 * jt]; w[4] = tw[4 * jt];
+    w[3] = cmul(w[1], w[2]); w[5] = cmul(w[1], w[4]); w[6] = cmul(w[2], w[4]); w[7] = cmul(w[3], w[4]);
+  } else if constexpr (R == 16) {
+    w[1] = tw[jt]; w[2] = tw[2 * jt]; w[4] = tw[4 * jt]; w[8] = tw[8 * jt];
+    w[3] = cmul(w[1], w[2]); w[5] = cmul(w[1], w[4]); w[6] = cmul(w[2], w[4]); w[7] = cmul(w[3], w[4]);
+    w[9] = cmul(w[1], w[8]); w[10] = cmul(w[2], w[8]); w[11] = cmul(w[3], w[8]); w[12] = cmul(w[4], w[8]);
+    w[13] = cmul(w[5], w[8]); w[14] = cmul(w[6], w[8]); w[15] = cmul(w[7], w[8]);
+  }
+}
+
 template <int R, bool INV, typename C>
 __device__ __forceinline__ void fft_stage(C *__restrict__ x, const C *__restrict__ tw, int n, int L,
                                           const Batch &g, int tid, int nthr) {
@@ -150,23 +185,30 @@ __device__ __forceinline__ void fft_stage(C *__restrict__ x, const C *__restrict
   const int per = n / R;
   const int total = g.batch * per;
   const int twstep = n / L;
+  const FastDiv dB(g.batch), dP(per), dL(Lr), dI(g.bin);
   for (int w = tid; w < total; w += nthr) {
     int b, bf;
-    if (g.batch_fast) { b = w % g.batch; bf = w / g.batch; }
-    else { bf = w % per; b = w / per; }
-    const int blk = bf / Lr, j = bf - blk * Lr;
-    C *base = x + (b % g.bin) * g.bs_in + (b / g.bin) * g.bs_out + (blk * L + j) * g.es;
+    if (g.batch_fast) { b = dB.mod(w); bf = dB.div(w); }
+    else { bf = dP.mod(w); b = dP.div(w); }
+    const int blk = dL.div(bf), j = bf - blk * Lr;
+    C *base = x + dI.mod(b) * g.bs_in + dI.div(b) * g.bs_out + (blk * L + j) * g.es;
     const int st = Lr * g.es;
     C v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = base[r * st];
+    C tv[R];
+    if (j) stage_twiddles<R>(tw, j * twstep, tv);
     if constexpr (!INV) {
       dft<R, -1>(v);
+      if (j) {
 #pragma unroll
-      for (int k = 1; k < R; ++k) v[k] = cmul(v[k], tw[j * k * twstep]);
+        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], tv[k]);
+      }
     } else {
+      if (j) {
 #pragma unroll
-      for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], tw[j * k * twstep]);
+        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], tv[k]);
+      }
       dft<R, 1>(v);
     }
 #pragma unroll
@@ -203,6 +245,61 @@ __device__ void fft_inverse(C *x, const C *tw, const FftPlan &p, const Batch &g)
     fft_stage_dispatch<true>(x, tw, p.n, p.radix[s], p.L[s], g, threadIdx.x, blockDim.x);
     __syncthreads();
   }
+}
+
+// ------------------------------------------------------------ async copies
+// Bulk (TMA) copies between global and shared memory with an mbarrier; every
+// wait is bounded and reports a timeout instead of spinning forever.
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// Returns false if the phase did not complete within the iteration limit.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (int it = 0; it < (1 << 22); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity), "r"(1000000)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst_smem)),
+      "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void bulk_s2g(void *dst_gmem, const void *src_smem, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst_gmem),
+               "r"(smem_u32(src_smem)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// 16-byte asynchronous global->shared copy (cp.async), waited by cp_async_wait_all.
+__device__ __forceinline__ void cp_async16(void *dst_smem, const void *src_gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst_smem)), "l"(src_gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
 }  // namespace pfdd

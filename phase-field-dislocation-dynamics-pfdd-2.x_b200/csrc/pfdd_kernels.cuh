@@ -43,11 +43,16 @@ struct Core {
   double k[12];               // scaled constants, see core_derivative
 };
 
-enum { IMAG_NONE = 0, IMAG_FULL = 1 };
+// IMAG_NONE: Re xi only, B averaged over k and index -k (not reference-exact)
+// IMAG_FULL: Im xi carried as a second real field through every pass
+// IMAG_NYQ:  Im xi carried as its spectrum on the Nyquist planes only, where
+//            it lives when no obstacle mask is set (updated inside P2)
+enum { IMAG_NONE = 0, IMAG_FULL = 1, IMAG_NYQ = 2 };
+enum { PASS_STEP = 0, PASS_SYNTH = 1 };
 
 struct PlaneArgs {
   FftPlan py, pz;
-  int nx, ny, nz, nzh, M;
+  int nx, ny, nz, nzh, nzp, M;   // nzp: complex entries per stored spectrum row (>= nzh, 16-byte rows)
   int S, F;                   // slip systems; fields in flight (S, or 2S with Im xi)
   const void *tw_y, *tw_z, *tw_r;   // W_ny^m, W_M^m, W_nz^k tables in compute precision
   const int16_t *posM;        // position of z-frequency k (< M) after the M-point transform
@@ -55,17 +60,26 @@ struct PlaneArgs {
 
 struct PencilArgs {
   FftPlan px;
-  int nx, ny, nz, nzh, M;
+  int nx, ny, nz, nzh, nzp, M;
   int S, F, imag;
-  int ncols;                  // ny * nzh
+  int ncols;                  // ny * nzp
   int ccols;                  // columns per CTA
   const void *tw_x;
-  const int16_t *kx_of, *ky_of, *kz_of;   // frequency index of each slot (kz_of has nzh entries)
+  const int16_t *kx_of, *ky_of, *kz_of;   // frequency index of each slot (kz_of has nzp entries)
+  int mode;                   // PASS_STEP or PASS_SYNTH (rebuild Im xi from the Nyquist spectrum)
+  int fstride;                // shared-memory stride between fields (complex), bank-conflict padded
+  // Nyquist spectrum of Im xi (IMAG_NYQ): kz = nz/2 plane [S][nx][ny], ky = ny/2
+  // plane [S][nx][M], kx = nx/2 plane [S][ny][M] (slot coordinates)
+  void *aux;
+  int sx_n, sy_n;             // slots of kx = nx/2 and ky = ny/2
+  double cd;                  // CD * timestep
+  double *partials;           // per-CTA sum of |d Im xi|^2 * N (Parseval weight), or null
   Green g;
 };
 
 struct UpdateArgs {
-  int nx, ny, nz, nzh, S, F;
+  int nx, ny, nz, nzh, nzp, S, F;
+  int mode;                   // PASS_STEP: GL update; PASS_SYNTH: xout = IFFT(spec)/N
   double cd;                  // CD * timestep
   double invN;
   Core core;
@@ -73,6 +87,7 @@ struct UpdateArgs {
   const uint8_t *mask;        // [S*N] or null
   const void *site;           // [S*N] per-site GSFE field (compute precision) or null
   const int *stop;            // device flag: skip the step when nonzero
+  int *err;                   // device flag: a bounded wait ran out
 };
 
 // ------------------------------------------------------------ small helpers
@@ -116,46 +131,80 @@ __device__ __forceinline__ void load_table(C *dst, const void *src, int n) {
 }
 
 // ------------------------------------------------------------ P1
-// grid.x = F * nx planes; dynamic smem = (ny*nzh + ny + 2M) * sizeof(C) + M * 4
-template <typename T>
-__global__ void __launch_bounds__(256) k_fwd_planes(const T *__restrict__ xi, cx<T> *__restrict__ spec,
-                                                    PlaneArgs a, const int *__restrict__ stop) {
+// Shared memory of a plane kernel: the ny x nzp complex plane, then the y, z
+// and real-to-complex twiddle tables, the z position table and one mbarrier.
+template <typename C> struct PlaneSmem {
+  C *buf, *twy, *twz, *twr;
+  int *pos;
+  uint64_t *bar;
+  double *red;
+  __device__ PlaneSmem(unsigned char *raw, const PlaneArgs &a) {
+    buf = reinterpret_cast<C *>(raw);
+    twy = buf + (size_t)a.ny * a.nzp;
+    twz = twy + a.ny;
+    twr = twz + a.M;
+    pos = reinterpret_cast<int *>(twr + a.M);
+    bar = reinterpret_cast<uint64_t *>(pos + ((a.M + 1) & ~1));
+    red = reinterpret_cast<double *>(bar + 1);
+  }
+  static size_t bytes(int ny, int nzp, int M) {
+    return ((size_t)ny * nzp + ny + 2 * (size_t)M) * sizeof(C) + (size_t)((M + 1) & ~1) * 4 + 8 + 64 * 8;
+  }
+};
+
+template <typename C>
+__device__ __forceinline__ void load_plane_tables(const PlaneSmem<C> &sm, const PlaneArgs &a) {
+  load_table(sm.twy, a.tw_y, a.ny);
+  load_table(sm.twz, a.tw_z, a.M);
+  load_table(sm.twr, a.tw_r, a.M);
+  for (int i = threadIdx.x; i < a.M; i += blockDim.x) sm.pos[i] = a.posM[i];
+}
+
+// grid.x = F * nx planes
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_fwd_planes(const T *__restrict__ xi, cx<T> *__restrict__ spec,
+                                                   PlaneArgs a, const int *__restrict__ stop, int *err) {
   using C = cx<T>;
   if (stop && *stop) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int ny = a.ny, nz = a.nz, nzh = a.nzh, M = a.M;
-  C *buf = reinterpret_cast<C *>(smem_raw);
-  C *twy = buf + ny * nzh;
-  C *twz = twy + ny;
-  C *twr = twz + M;
-  int *pos = reinterpret_cast<int *>(twr + M);
-  load_table(twy, a.tw_y, ny);
-  load_table(twz, a.tw_z, M);
-  load_table(twr, a.tw_r, M);
-  for (int i = threadIdx.x; i < M; i += blockDim.x) pos[i] = a.posM[i];
-
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const PlaneSmem<C> sm(smem_raw, a);
+  const int ny = a.ny, nz = a.nz, nzh = a.nzh, nzp = a.nzp, M = a.M;
   const size_t plane = blockIdx.x;
-  const T *src = xi + plane * (size_t)ny * nz;
-  T *bufr = reinterpret_cast<T *>(buf);
-  for (int i = threadIdx.x; i < ny * nz; i += blockDim.x) {
-    const int y = i / nz, z = i - y * nz;
-    bufr[y * 2 * nzh + z] = src[i];
-  }
+  if (threadIdx.x == 0) mbar_init(sm.bar, 1);
   __syncthreads();
+  // rows of the real plane -> shared rows of stride 2*nzp reals (bulk copies)
+  if (threadIdx.x < 32) {
+    if (threadIdx.x == 0) mbar_expect_tx(sm.bar, (uint32_t)(ny * nz * sizeof(T)));
+    __syncwarp();
+    const T *src = xi + plane * (size_t)ny * nz;
+    T *bufr = reinterpret_cast<T *>(sm.buf);
+    for (int y = threadIdx.x; y < ny; y += 32)
+      bulk_g2s(bufr + (size_t)y * 2 * nzp, src + (size_t)y * nz, (uint32_t)(nz * sizeof(T)), sm.bar);
+  }
+  load_plane_tables(sm, a);
+  const bool ok = __syncthreads_and(mbar_wait(sm.bar, 0));
+  if (!ok) {
+    if (threadIdx.x == 0) atomicExch(err, 1);
+    return;
+  }
+  C *buf = sm.buf;
+  const C *twr = sm.twr;
+  const int *pos = sm.pos;
 
   // z: M-point complex transform of the packed rows
-  Batch gz{ny, ny, nzh, 0, 1, false};
-  fft_forward(buf, twz, a.pz, gz);
+  Batch gz{ny, ny, nzp, 0, 1, false};
+  fft_forward(buf, sm.twz, a.pz, gz);
 
   // real-to-complex unpacking, pairs (k, M-k); X[M] goes to slot M
   const int half = M / 2 + 1;
   for (int w = threadIdx.x; w < ny * half; w += blockDim.x) {
     const int y = w / half, k = w - y * half;
-    C *row = buf + y * nzh;
+    C *row = buf + (size_t)y * nzp;
     if (k == 0) {
       C z0 = row[pos[0]];
       row[pos[0]] = mk<C>(z0.x + z0.y, (T)0);
       row[M] = mk<C>(z0.x - z0.y, (T)0);
+      for (int q = nzh; q < nzp; ++q) row[q] = mk<C>((T)0, (T)0);
     } else {
       const int pk = pos[k], pm = pos[M - k];
       C zk = row[pk], zm = row[pm];
@@ -170,11 +219,17 @@ __global__ void __launch_bounds__(256) k_fwd_planes(const T *__restrict__ xi, cx
   __syncthreads();
 
   // y: ny-point transforms over the nzh slot columns
-  Batch gy{nzh, nzh, 1, 0, nzh, true};
-  fft_forward(buf, twy, a.py, gy);
+  Batch gy{nzh, nzh, 1, 0, nzp, true};
+  fft_forward(buf, sm.twy, a.py, gy);
 
-  C *dst = spec + plane * (size_t)ny * nzh;
-  for (int i = threadIdx.x; i < ny * nzh; i += blockDim.x) dst[i] = buf[i];
+  // whole plane -> spectrum with one bulk store
+  fence_proxy_async();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bulk_s2g(spec + plane * (size_t)ny * nzp, buf, (uint32_t)((size_t)ny * nzp * sizeof(C)));
+    bulk_commit();
+    bulk_wait_all();
+  }
 }
 
 // ------------------------------------------------------------ B(k) operator
@@ -232,60 +287,99 @@ template <typename T> __device__ __forceinline__ T freq_neg(int i, int n) {
 
 // ------------------------------------------------------------ P2
 // grid.x = ncols / ccols tiles; dynamic smem = (F*nx*ccols + nx) * sizeof(C)
-template <typename T>
-__global__ void __launch_bounds__(256) k_xpencil(cx<T> *__restrict__ spec, PencilArgs a,
-                                                 const int *__restrict__ stop) {
+template <typename T, typename C>
+__device__ __forceinline__ size_t nyq_index(const PencilArgs &a, int f, int sx, int sy, int sz, bool &is_nyq) {
+  // returns the aux slot of a Nyquist point; is_nyq false for ordinary points
+  const size_t nzZ = (size_t)a.S * a.nx * a.ny, nzY = (size_t)a.S * a.nx * a.M;
+  is_nyq = true;
+  if (sz == a.M) return ((size_t)f * a.nx + sx) * a.ny + sy;
+  if (sz > a.M) { is_nyq = false; return 0; }   // row padding
+  if (sy == a.sy_n) return nzZ + ((size_t)f * a.nx + sx) * a.M + sz;
+  if (sx == a.sx_n) return nzZ + nzY + ((size_t)f * a.ny + sy) * a.M + sz;
+  is_nyq = false;
+  return 0;
+}
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_xpencil(cx<T> *__restrict__ spec, PencilArgs a,
+                                                const int *__restrict__ stop) {
   using C = cx<T>;
   if (stop && *stop) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int nx = a.nx, F = a.F, cc = a.ccols, S = a.S;
-  C *buf = reinterpret_cast<C *>(smem_raw);   // [F][nx][cc]
-  C *twx = buf + (size_t)F * nx * cc;
-  load_table(twx, a.tw_x, nx);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int nx = a.nx, F = a.F, cc = a.ccols, S = a.S, fst = a.fstride;
+  C *buf = reinterpret_cast<C *>(smem_raw);   // [F][fstride >= nx*cc]
+  C *twx = buf + (size_t)F * fst;
+  double *red = reinterpret_cast<double *>(twx + nx);
   const size_t col0 = (size_t)blockIdx.x * cc;
   const size_t ncols = a.ncols;
-  for (int i = threadIdx.x; i < F * nx * cc; i += blockDim.x) {
-    const int c = i % cc, fx = i / cc;  // fx = f*nx + x
-    buf[i] = spec[(size_t)fx * ncols + col0 + c];
+  const int cpr = (int)(cc * sizeof(C) / 16);    // 16-byte chunks per (field, x) row
+  const int nchunks = F * nx * cpr;
+  const FastDiv dc(cpr), dnx(nx);
+  C *caux = reinterpret_cast<C *>(a.aux);
+  if (a.mode == PASS_STEP) {
+    for (int q = threadIdx.x; q < nchunks; q += blockDim.x) {
+      const int fx = dc.div(q), ch = q - fx * cpr;
+      const int f = dnx.div(fx), x = fx - f * nx;
+      const char *src = reinterpret_cast<const char *>(spec + (size_t)fx * ncols + col0) + 16 * ch;
+      cp_async16(reinterpret_cast<char *>(buf + (size_t)f * fst + (size_t)x * cc) + 16 * ch, src);
+    }
+  } else {
+    for (int i = threadIdx.x; i < F * fst; i += blockDim.x) buf[i] = mk<C>((T)0, (T)0);
   }
+  load_table(twx, a.tw_x, nx);
+  if (a.mode == PASS_STEP) cp_async_wait_all();
   __syncthreads();
 
-  Batch gx{F * cc, cc, 1, nx * cc, cc, true};
-  fft_forward(buf, twx, a.px, gx);
+  Batch gx{F * cc, cc, 1, fst, cc, true};
+  if (a.mode == PASS_STEP) fft_forward(buf, twx, a.px, gx);
 
-  // per-k contraction
+  double dsq = 0.0;
   for (int w = threadIdx.x; w < nx * cc; w += blockDim.x) {
     const int c = w % cc, sx = w / cc;
     const int col = (int)(col0 + c);
-    const int sy = col / a.nzh, sz = col - sy * a.nzh;
+    const int sy = col / a.nzp, sz = col - sy * a.nzp;
+    C *pk = buf + sx * cc + c;
+    if (a.mode == PASS_SYNTH) {
+      bool nq;
+      for (int f = 0; f < S; ++f) {
+        const size_t ai = nyq_index<T, C>(a, f, sx, sy, sz, nq);
+        if (nq) pk[(size_t)f * fst] = caux[ai];
+      }
+      continue;
+    }
     const int ix = a.kx_of[sx], iy = a.ky_of[sy], iz = a.kz_of[sz];
     const T fx = freq_of<T>(ix, a.nx), fy = freq_of<T>(iy, a.ny), fz = freq_of<T>(iz, a.nz);
-    const T gxn = freq_neg<T>(ix, a.nx), gyn = freq_neg<T>(iy, a.ny), gzn = freq_neg<T>(iz, a.nz);
     const Green &g = a.g;
     const T kx = fx * (T)g.four[0][0] + fy * (T)g.four[1][0] + fz * (T)g.four[2][0];
     const T ky = fx * (T)g.four[0][1] + fy * (T)g.four[1][1] + fz * (T)g.four[2][1];
     const T kz = fx * (T)g.four[0][2] + fy * (T)g.four[1][2] + fz * (T)g.four[2][2];
-    // B at the index -k equals B(-(-k)) by symmetry; evaluate at the vector of -k
+    // B at the index -k is B evaluated at the wave vector the reference assigns to -k
+    const T gxn = freq_neg<T>(ix, a.nx), gyn = freq_neg<T>(iy, a.ny), gzn = freq_neg<T>(iz, a.nz);
     const T mx = gxn * (T)g.four[0][0] + gyn * (T)g.four[1][0] + gzn * (T)g.four[2][0];
     const T my = gxn * (T)g.four[0][1] + gyn * (T)g.four[1][1] + gzn * (T)g.four[2][1];
     const T mz = gxn * (T)g.four[0][2] + gyn * (T)g.four[1][2] + gzn * (T)g.four[2][2];
-    C *pk = buf + sx * cc + c;
-    const size_t fs = (size_t)nx * cc;
+    const size_t fs = (size_t)fst;
+    C sr[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) sr[q] = mk<C>((T)0, (T)0);
+    for (int b = 0; b < S; ++b) {
+      const C xr = pk[b * fs];
+      const double *s = g.sig[b];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) { sr[q].x += (T)s[q] * xr.x; sr[q].y += (T)s[q] * xr.y; }
+    }
     if (a.imag == IMAG_FULL) {
       // P = B(k)(Xr + i Xi), Q = B(k')(Xr - i Xi), k' = vector of index -k;
       // Er = (P + Q)/2, Ei = (P - Q)/(2i): the real and imaginary fields of
       // IFFT(B_index X) for the complex field X = Xr + i Xi.
-      C sr[6], si[6];
+      C si[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) { sr[q] = mk<C>((T)0, (T)0); si[q] = sr[q]; }
+      for (int q = 0; q < 6; ++q) si[q] = mk<C>((T)0, (T)0);
       for (int b = 0; b < S; ++b) {
-        const C xr = pk[b * fs], xim = pk[(S + b) * fs];
+        const C xim = pk[(S + b) * fs];
         const double *s = g.sig[b];
 #pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          sr[q].x += (T)s[q] * xr.x; sr[q].y += (T)s[q] * xr.y;
-          si[q].x += (T)s[q] * xim.x; si[q].y += (T)s[q] * xim.y;
-        }
+        for (int q = 0; q < 6; ++q) { si[q].x += (T)s[q] * xim.x; si[q].y += (T)s[q] * xim.y; }
       }
       C sp[6], sq[6];
 #pragma unroll
@@ -305,36 +399,76 @@ __global__ void __launch_bounds__(256) k_xpencil(cx<T> *__restrict__ spec, Penci
         // (P - Q)/(2i) = -i (P - Q)/2
         pk[(S + aa) * fs] = mk<C>((T)0.5 * (P.y - Q.y), (T)-0.5 * (P.x - Q.x));
       }
-    } else {
-      // real field only: B averaged over k and index -k (the Hermitian part)
-      C sr[6];
-#pragma unroll
-      for (int q = 0; q < 6; ++q) sr[q] = mk<C>((T)0, (T)0);
-      for (int b = 0; b < S; ++b) {
-        const C xr = pk[b * fs];
-        const double *s = g.sig[b];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) { sr[q].x += (T)s[q] * xr.x; sr[q].y += (T)s[q] * xr.y; }
-      }
+      continue;
+    }
+    bool nyq = false;
+    size_t a0 = 0;
+    if (a.imag == IMAG_NYQ) a0 = nyq_index<T, C>(a, 0, sx, sy, sz, nyq);
+    if (!nyq) {
+      // B(k) = B(index -k) here; real field: Er = B Xr (the Hermitian part for IMAG_NONE)
       C Up[3], Uq[3], Vp, Vq;
       T g1p, g2p, g1q, g2q;
       bool zp, zq;
       green_prepare<T>(g, sr, kx, ky, kz, Up, Vp, g1p, g2p, zp);
-      green_prepare<T>(g, sr, mx, my, mz, Uq, Vq, g1q, g2q, zq);
+      if (a.imag == IMAG_NONE) green_prepare<T>(g, sr, mx, my, mz, Uq, Vq, g1q, g2q, zq);
       for (int aa = 0; aa < S; ++aa) {
-        const C P = green_apply<T>(g, aa, sr, kx, ky, kz, Up, Vp, g1p, g2p, zp);
-        const C Q = green_apply<T>(g, aa, sr, mx, my, mz, Uq, Vq, g1q, g2q, zq);
-        pk[aa * fs] = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
+        C P = green_apply<T>(g, aa, sr, kx, ky, kz, Up, Vp, g1p, g2p, zp);
+        if (a.imag == IMAG_NONE) {
+          const C Q = green_apply<T>(g, aa, sr, mx, my, mz, Uq, Vq, g1q, g2q, zq);
+          P = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
+        }
+        pk[aa * fs] = P;
       }
+      continue;
+    }
+    // Nyquist point: Im xi spectrum Xi from aux; Er as in IMAG_FULL, and
+    // Xi <- Xi - cd Ei entirely in k-space (no mask, no core force on Im xi)
+    const size_t astride = (sz == a.M) ? (size_t)a.nx * a.ny : (sy == a.sy_n ? (size_t)a.nx * a.M : (size_t)a.ny * a.M);
+    C si[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) si[q] = mk<C>((T)0, (T)0);
+    for (int b = 0; b < S; ++b) {
+      const C xim = caux[a0 + b * astride];
+      const double *s = g.sig[b];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) { si[q].x += (T)s[q] * xim.x; si[q].y += (T)s[q] * xim.y; }
+    }
+    C sp[6], sq[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      sp[q] = mk<C>(sr[q].x - si[q].y, sr[q].y + si[q].x);
+      sq[q] = mk<C>(sr[q].x + si[q].y, sr[q].y - si[q].x);
+    }
+    C Up[3], Uq[3], Vp, Vq;
+    T g1p, g2p, g1q, g2q;
+    bool zp, zq;
+    green_prepare<T>(g, sp, kx, ky, kz, Up, Vp, g1p, g2p, zp);
+    green_prepare<T>(g, sq, mx, my, mz, Uq, Vq, g1q, g2q, zq);
+    const T cd = (T)a.cd;
+    const double wgt = (iz == 0 || iz == a.M) ? 1.0 : 2.0;   // k and its unstored partner -k
+    for (int aa = 0; aa < S; ++aa) {
+      const C P = green_apply<T>(g, aa, sp, kx, ky, kz, Up, Vp, g1p, g2p, zp);
+      const C Q = green_apply<T>(g, aa, sq, mx, my, mz, Uq, Vq, g1q, g2q, zq);
+      pk[aa * fs] = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
+      const C ei = mk<C>((T)0.5 * (P.y - Q.y), (T)-0.5 * (P.x - Q.x));
+      const C d = mk<C>(-cd * ei.x, -cd * ei.y);
+      C *ap = caux + a0 + aa * astride;
+      const C old = *ap;
+      *ap = mk<C>(old.x + d.x, old.y + d.y);
+      dsq += wgt * ((double)d.x * (double)d.x + (double)d.y * (double)d.y);
     }
   }
+  if (a.partials) block_sum2(dsq, 0.0, red, a.partials + 2 * blockIdx.x);
   __syncthreads();
 
   fft_inverse(buf, twx, a.px, gx);
 
-  for (int i = threadIdx.x; i < F * nx * cc; i += blockDim.x) {
-    const int c = i % cc, fx = i / cc;
-    spec[(size_t)fx * ncols + col0 + c] = buf[i];
+  for (int q = threadIdx.x; q < nchunks; q += blockDim.x) {
+    const int fx = dc.div(q), ch = q - fx * cpr;
+    const int f = dnx.div(fx), x = fx - f * nx;
+    float4 *dst = reinterpret_cast<float4 *>(reinterpret_cast<char *>(spec + (size_t)fx * ncols + col0) + 16 * ch);
+    *dst = *reinterpret_cast<const float4 *>(reinterpret_cast<const char *>(buf + (size_t)f * fst + (size_t)x * cc) +
+                                             16 * ch);
   }
 }
 
@@ -422,40 +556,60 @@ __device__ __forceinline__ T core_derivative(const Core &cm, T x, int a, size_t 
 }
 
 // ------------------------------------------------------------ P3
-// grid.x = F * nx planes; dynamic smem as P1 + 64 doubles
+template <typename T> struct Vec;
+template <> struct Vec<float> { using type = float4; static constexpr int n = 4; };
+template <> struct Vec<double> { using type = double2; static constexpr int n = 2; };
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_inv_update(const cx<T> *__restrict__ spec, const T *__restrict__ xin,
-                                                    T *__restrict__ xout, PlaneArgs a, UpdateArgs u,
-                                                    double *__restrict__ partials) {
+__device__ __forceinline__ T update_one(const UpdateArgs &u, bool real_field, int sys, T el, T old, T tau, size_t r,
+                                        size_t N, const T *__restrict__ xin, const T *__restrict__ site) {
+  const T cd = (T)u.cd;
+  if (real_field) {
+    const T dE = core_derivative<T>(u.core, old, sys, r, N, xin, site);
+    return old - cd * (el - tau + dE);
+  }
+  return old - cd * el;
+}
+
+// grid.x = F * nx planes
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spec, const T *__restrict__ xin,
+                                                   T *__restrict__ xout, PlaneArgs a, UpdateArgs u,
+                                                   double *__restrict__ partials) {
   using C = cx<T>;
+  using V = typename Vec<T>::type;
+  constexpr int VN = Vec<T>::n;
   if (u.stop && *u.stop) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int ny = a.ny, nz = a.nz, nzh = a.nzh, M = a.M;
-  C *buf = reinterpret_cast<C *>(smem_raw);
-  C *twy = buf + ny * nzh;
-  C *twz = twy + ny;
-  C *twr = twz + M;
-  int *pos = reinterpret_cast<int *>(twr + M);
-  double *red = reinterpret_cast<double *>(pos + ((M + 1) & ~1));
-  load_table(twy, a.tw_y, ny);
-  load_table(twz, a.tw_z, M);
-  load_table(twr, a.tw_r, M);
-  for (int i = threadIdx.x; i < M; i += blockDim.x) pos[i] = a.posM[i];
-
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const PlaneSmem<C> sm(smem_raw, a);
+  const int ny = a.ny, nz = a.nz, nzh = a.nzh, nzp = a.nzp, M = a.M;
   const size_t plane = blockIdx.x;
-  const C *src = spec + plane * (size_t)ny * nzh;
-  for (int i = threadIdx.x; i < ny * nzh; i += blockDim.x) buf[i] = src[i];
+  if (threadIdx.x == 0) {
+    mbar_init(sm.bar, 1);
+    const uint32_t bytes = (uint32_t)((size_t)ny * nzp * sizeof(C));
+    mbar_expect_tx(sm.bar, bytes);
+    bulk_g2s(sm.buf, spec + plane * (size_t)ny * nzp, bytes, sm.bar);
+  }
+  load_plane_tables(sm, a);
   __syncthreads();
+  const bool ok = __syncthreads_and(mbar_wait(sm.bar, 0));
+  if (!ok) {
+    if (threadIdx.x == 0) atomicExch(u.err, 1);
+    return;
+  }
+  C *buf = sm.buf;
+  const C *twr = sm.twr;
+  const int *pos = sm.pos;
 
-  Batch gy{nzh, nzh, 1, 0, nzh, true};
-  fft_inverse(buf, twy, a.py, gy);
+  Batch gy{nzh, nzh, 1, 0, nzp, true};
+  fft_inverse(buf, sm.twy, a.py, gy);
 
   // complex-to-real packing: Zin[k] = A + i w D, Zin[M-k] = conj(A - i w D),
   // A = X[k] + conj X[M-k], D = X[k] - conj X[M-k], w = exp(+2 pi i k / nz)
   const int half = M / 2 + 1;
   for (int w = threadIdx.x; w < ny * half; w += blockDim.x) {
     const int y = w / half, k = w - y * half;
-    C *row = buf + y * nzh;
+    C *row = buf + (size_t)y * nzp;
     const int pk = pos[k];
     const int pm = (k == 0) ? -1 : pos[M - k];
     const C xk = row[pk];
@@ -469,10 +623,11 @@ __global__ void __launch_bounds__(256) k_inv_update(const cx<T> *__restrict__ sp
   }
   __syncthreads();
 
-  Batch gz{ny, ny, nzh, 0, 1, false};
-  fft_inverse(buf, twz, a.pz, gz);
+  Batch gz{ny, ny, nzp, 0, 1, false};
+  fft_inverse(buf, sm.twz, a.pz, gz);
 
-  // fused GSFE force + applied stress + masked explicit Euler update
+  // fused GSFE force + applied stress + masked explicit Euler update,
+  // VN consecutive z per thread, two vectors in flight per iteration
   const int f = (int)(plane / a.nx);
   const int x = (int)(plane - (size_t)f * a.nx);
   const bool real_field = f < u.S;
@@ -481,28 +636,57 @@ __global__ void __launch_bounds__(256) k_inv_update(const cx<T> *__restrict__ sp
   const size_t off = plane * (size_t)ny * nz;
   const size_t rbase = (size_t)x * ny * nz;
   const T *bufr = reinterpret_cast<const T *>(buf);
-  const T cd = (T)u.cd, invN = (T)u.invN;
+  const T invN = (T)u.invN;
+  const int nvec = nz / VN;
+  const int total = ny * nvec;
+  const FastDiv dv(nvec);
+  if (u.mode == PASS_SYNTH) {
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int y = dv.div(i), zq = i - y * nvec;
+      T e[VN];
+      *reinterpret_cast<V *>(e) = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzp + zq * VN);
+#pragma unroll
+      for (int q = 0; q < VN; ++q) e[q] *= invN;
+      *reinterpret_cast<V *>(xout + off + y * nz + zq * VN) = *reinterpret_cast<V *>(e);
+    }
+    return;
+  }
+  // update pass only: tau, mask and per-site GSFE are read from here on
   const T tau = real_field ? (T)u.tau[sys] : (T)0;
   const T *site = reinterpret_cast<const T *>(u.site);
   double dsq = 0.0, sum = 0.0;
-  for (int i = threadIdx.x; i < ny * nz; i += blockDim.x) {
-    const int y = i / nz, z = i - y * nz;
-    const T el = bufr[y * 2 * nzh + z] * invN;
-    const T old = xin[off + i];
-    T nv;
-    if (real_field) {
-      const T dE = core_derivative<T>(u.core, old, sys, rbase + i, N, xin, site);
-      nv = old - cd * (el - tau + dE);
-    } else {
-      nv = old - cd * el;
+  for (int i0 = threadIdx.x; i0 < total; i0 += 2 * blockDim.x) {
+    V oldv[2], elv[2];
+    int idx[2];
+    bool on[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int i = i0 + h * blockDim.x;
+      on[h] = i < total;
+      const int y = dv.div(on[h] ? i : 0), zq = (on[h] ? i : 0) - y * nvec;
+      idx[h] = y * nz + zq * VN;
+      oldv[h] = *reinterpret_cast<const V *>(xin + off + idx[h]);
+      elv[h] = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzp + zq * VN);
     }
-    if (u.mask && u.mask[(size_t)sys * N + rbase + i]) nv = old;
-    xout[off + i] = nv;
-    const double d = (double)nv - (double)old;
-    dsq += d * d;
-    if (real_field) sum += (double)nv;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (!on[h]) continue;
+      T o[VN], e[VN], nv[VN];
+      *reinterpret_cast<V *>(o) = oldv[h];
+      *reinterpret_cast<V *>(e) = elv[h];
+#pragma unroll
+      for (int q = 0; q < VN; ++q) {
+        const size_t r = rbase + idx[h] + q;
+        nv[q] = update_one<T>(u, real_field, sys, e[q] * invN, o[q], tau, r, N, xin, site);
+        if (u.mask && u.mask[(size_t)sys * N + r]) nv[q] = o[q];
+        const double d = (double)nv[q] - (double)o[q];
+        dsq += d * d;
+        if (real_field) sum += (double)nv[q];
+      }
+      *reinterpret_cast<V *>(xout + off + idx[h]) = *reinterpret_cast<V *>(nv);
+    }
   }
-  block_sum2(dsq, sum, red, partials + 2 * plane);
+  block_sum2(dsq, sum, sm.red, partials + 2 * plane);
 }
 
 // ------------------------------------------------------------ reduction
@@ -510,7 +694,8 @@ __global__ void __launch_bounds__(256) k_inv_update(const cx<T> *__restrict__ sp
 // stats[step] = {xinorm, xiave}; sets *stop when 0 < tol and xinorm < tol;
 // flags a non-finite result in *bad.
 __global__ void k_finalize(const double *__restrict__ partials, int nparts, double *__restrict__ stats, int step,
-                           double tol, int *stop, int *bad, int *steps_done, const double *extra_dsq) {
+                           double tol, int *stop, int *bad, int *steps_done, const double *__restrict__ partials2,
+                           int nparts2, double scale2) {
   if (stop && *stop) return;
   __shared__ double sh[4][1024];
   double s0 = 0, c0 = 0, s1 = 0, c1 = 0;
@@ -522,6 +707,11 @@ __global__ void k_finalize(const double *__restrict__ partials, int nparts, doub
     t = s1 + v;
     c1 += (fabs(s1) >= fabs(v)) ? (s1 - t) + v : (v - t) + s1;
     s1 = t;
+  }
+  for (int i = threadIdx.x; i < nparts2; i += blockDim.x) {
+    double v = partials2[2 * i] * scale2, t = s0 + v;
+    c0 += (fabs(s0) >= fabs(v)) ? (s0 - t) + v : (v - t) + s0;
+    s0 = t;
   }
   sh[0][threadIdx.x] = s0; sh[1][threadIdx.x] = c0; sh[2][threadIdx.x] = s1; sh[3][threadIdx.x] = c1;
   __syncthreads();
@@ -539,7 +729,6 @@ __global__ void k_finalize(const double *__restrict__ partials, int nparts, doub
       e1 += sh[3][i];
     }
     double dsq = a0 + e0;
-    if (extra_dsq) dsq += *extra_dsq;
     const double xinorm = sqrt(dsq), xiave = a1 + e1;
     stats[2 * step] = xinorm;
     stats[2 * step + 1] = xiave;

@@ -19,7 +19,7 @@ MAX_SLIP = 12
 
 PFDD_OK = 0
 ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "EUNSUPPORTED", -5: "EDIVERGED", -6: "ENODEVICE",
-          -7: "ESTATE"}
+          -7: "ESTATE", -8: "ETIMEOUT"}
 FP64, FP32 = 0, 1
 IMAG_AUTO, IMAG_FULL, IMAG_NYQUIST = 0, 1, 2
 CORE_PERFECT, CORE_EXTENDED, CORE_SINE, CORE_PYRII, CORE_USFE_ANGLE, CORE_MPEA, CORE_SINE_FIELD = 1, 2, 3, 4, 6, 7, 103
@@ -29,7 +29,9 @@ EXPORTS = [
     "pfdd_gpu_create", "pfdd_gpu_set_state", "pfdd_gpu_set_state_interleaved", "pfdd_gpu_get_state",
     "pfdd_gpu_get_state_interleaved", "pfdd_gpu_advance", "pfdd_gpu_step_history", "pfdd_gpu_energy",
     "pfdd_gpu_tau", "pfdd_gpu_info", "pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version",
+    "pfdd_gpu_set_stream", "pfdd_gpu_profile",
 ]
+KERNELS = ["fwd_planes", "xpencil", "inv_update", "finalize"]
 
 D33 = ctypes.c_double * 3 * 3
 DS3 = ctypes.c_double * 3 * MAX_SLIP
@@ -88,6 +90,8 @@ def load(path: str = LIB_PATH):
     lib.pfdd_gpu_step_history.argtypes = [vp, ctypes.c_int, DP, DP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.pfdd_gpu_energy.argtypes = [vp, ctypes.c_int, DP, DP, DP]
     lib.pfdd_gpu_tau.argtypes = [vp, ctypes.c_int, DP]
+    lib.pfdd_gpu_set_stream.argtypes = [vp, vp]
+    lib.pfdd_gpu_profile.argtypes = [vp, ctypes.c_int, DP, ctypes.POINTER(ctypes.c_int)]
     lib.pfdd_gpu_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_size_t)]
     lib.pfdd_gpu_last_error.argtypes = [vp]
     lib.pfdd_gpu_last_error.restype = ctypes.c_char_p
@@ -204,6 +208,23 @@ class Stepper:
         e = np.empty(3)
         self._check(self._lib.pfdd_gpu_energy(self.h, inst, _dp(e[0:1]), _dp(e[1:2]), _dp(e[2:3])))
         return tuple(e)
+
+    def set_stream(self, stream_handle):
+        """Run on a caller stream (an int cudaStream_t, e.g. torch.cuda.current_stream().cuda_stream)."""
+        self._check(self._lib.pfdd_gpu_set_stream(self.h, ctypes.c_void_p(stream_handle or None)))
+
+    def profile(self, n_steps):
+        """Mean device ms per launch of each kernel class over n_steps GL iterations."""
+        ms = np.zeros(len(KERNELS))
+        lps = ctypes.c_int()
+        self._check(self._lib.pfdd_gpu_profile(self.h, n_steps, _dp(ms), ctypes.byref(lps)))
+        return dict(zip(KERNELS, ms)), lps.value
+
+    def info(self):
+        n = ctypes.c_int()
+        b = ctypes.c_size_t()
+        self._check(self._lib.pfdd_gpu_info(self.h, ctypes.byref(n), ctypes.byref(b)))
+        return n.value, b.value
 
     def close(self):
         if getattr(self, "h", None):

@@ -112,3 +112,35 @@ def test_fp64_stress_ramp_states():
     (re, im), _ = [x[0] for x in _run_gpu([w], 2, stress_states=3)]
     assert np.abs(re - xi.real).max() <= 1e-10
     assert np.abs(im - xi.imag).max() <= 1e-10
+
+
+@pytest.mark.parametrize("prec,tol", [(capi.FP64, 1e-10), (capi.FP32, 5e-5)])
+def test_nyquist_carrier_equals_full(prec, tol):
+    """Im xi carried only on the Nyquist planes (no mask) gives the same Re and
+    Im xi as carrying the full second field, and both match the oracle."""
+    w = small_loop(32)
+    ref, nrm, _ = O.run(oracle_instance(w), w.xi0, 30)
+    outs = {}
+    for mode in (capi.IMAG_NYQUIST, capi.IMAG_FULL):
+        (re, im), (hn, _) = [x[0] for x in _run_gpu([w], 30, precision=prec, imag=mode)]
+        outs[mode] = (re, im)
+        scale = np.abs(ref.real).max()
+        assert np.abs(re - ref.real).max() <= tol * scale
+        assert np.abs(im - ref.imag).max() <= tol * scale
+        np.testing.assert_allclose(hn, nrm, rtol=1e-9 if prec == capi.FP64 else 1e-3)
+    assert np.abs(outs[capi.IMAG_NYQUIST][0] - outs[capi.IMAG_FULL][0]).max() <= tol
+
+
+def test_nyquist_rejects_imaginary_state():
+    w = small_loop(16)
+    with capi.Stepper.from_workloads([w], imag_mode=capi.IMAG_NYQUIST) as st:
+        with pytest.raises(capi.PfddError) as e:
+            st.set_state(0, w.xi0, np.full(w.xi0.shape, 1e-3))
+        assert e.value.code == -1
+
+
+def test_nyquist_rejects_mask():
+    w = small_loop(16)
+    w.xo = np.zeros((w.S, 16, 16, 16))
+    with pytest.raises(capi.PfddError):
+        capi.Stepper.from_workloads([w], imag_mode=capi.IMAG_NYQUIST)
