@@ -19,8 +19,10 @@
 
 #include "pfdd_b200.h"
 #include "pfdd_kernels.cuh"
+#include "pfdd_setup.cuh"
 
 using namespace pfdd;
+using namespace pfdd::host;
 
 namespace {
 
@@ -41,56 +43,6 @@ struct DevBuf {
   }
   template <typename T> T *as() const { return reinterpret_cast<T *>(p); }
 };
-
-// Radix plan: greedy 16, 8, 4, 2, 3 factors; sub-lengths L_s.
-bool make_plan(int n, FftPlan &p) {
-  p.n = n;
-  p.nst = 0;
-  int rem = n, L = n;
-  while (rem > 1) {
-    int r;
-    if (rem % 16 == 0) r = 16;
-    else if (rem % 8 == 0) r = 8;
-    else if (rem % 4 == 0) r = 4;
-    else if (rem % 2 == 0) r = 2;
-    else if (rem % 3 == 0) r = 3;
-    else return false;
-    if (p.nst >= 8) return false;
-    p.radix[p.nst] = r;
-    p.L[p.nst] = L;
-    ++p.nst;
-    L /= r;
-    rem /= r;
-  }
-  return true;
-}
-
-// position of frequency k after the forward (digit-reversing) transform
-std::vector<int> positions(const FftPlan &p) {
-  std::vector<int> pos(p.n);
-  for (int k = 0; k < p.n; ++k) {
-    int rem = k, q = 0;
-    for (int s = 0; s < p.nst; ++s) {
-      int d = rem % p.radix[s];
-      rem /= p.radix[s];
-      q += d * (p.L[s] / p.radix[s]);
-    }
-    pos[k] = q;
-  }
-  return pos;
-}
-
-// W_n^m = exp(-2 pi i m / n), m = 0..count-1, evaluated in FP64 with the
-// angle reduced to the first octant's neighbourhood before cos/sin.
-void twiddles(int n, int count, std::vector<double> &out) {
-  out.resize(2 * (size_t)count);
-  for (int m = 0; m < count; ++m) {
-    long long e = m % n;
-    double ang = 2.0 * M_PI * (double)e / (double)n;
-    out[2 * m] = std::cos(ang);
-    out[2 * m + 1] = -std::sin(ang);
-  }
-}
 
 template <typename T> struct Threads;
 template <> struct Threads<float> { static constexpr int plane = 512, pencil = 512; };
@@ -164,108 +116,6 @@ pfdd_status fail(pfdd_gpu *h, pfdd_status code, const char *fmt, ...) {
   } while (0)
 
 template <typename T> size_t csize() { return sizeof(cx<T>); }
-
-// Green constants in FP64: sigma^a = C44 (eps^a + eps^a^T) + C12 tr(eps^a) I,
-// eps^a = xb_a (x) xn_a / dslip (fft_fftw_slab.cpp:559-566); mu and nu by the
-// Voigt average (fft_fftw_slab.cpp:483-491).
-void build_green(const pfdd_instance_desc &d, Green &g) {
-  memset(&g, 0, sizeof g);
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) g.four[i][j] = d.four[i][j];
-  const double C44 = d.C44, C12 = d.C12, C11 = d.C11;
-  const double mu = C44 - (2.0 * C44 + C12 - C11) / 5.0;
-  const double ll = C12 - (2.0 * C44 + C12 - C11) / 5.0;
-  const double young = mu * (3 * ll + 2 * mu) / (ll + mu);
-  const double xnu = young / 2.0 / mu - 1.0;
-  g.inv_mu = 1.0 / mu;
-  g.c2 = 1.0 / (2.0 * C44);
-  g.c1nu = 1.0 / (1.0 - xnu);
-  for (int a = 0; a < d.n_slip; ++a) {
-    double e[3][3];
-    for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 3; ++j) e[i][j] = d.xb[a][i] * d.xn[a][j] / d.dslip;
-    const double tr = e[0][0] + e[1][1] + e[2][2];
-    double s[3][3];
-    for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 3; ++j) s[i][j] = C44 * (e[i][j] + e[j][i]) + (i == j ? C12 * tr : 0.0);
-    g.sig[a][0] = s[0][0]; g.sig[a][1] = s[1][1]; g.sig[a][2] = s[2][2];
-    g.sig[a][3] = s[0][1]; g.sig[a][4] = s[0][2]; g.sig[a][5] = s[1][2];
-    g.eps[a][0] = e[0][0]; g.eps[a][1] = e[1][1]; g.eps[a][2] = e[2][2];
-    g.eps[a][3] = e[0][1] + e[1][0]; g.eps[a][4] = e[0][2] + e[2][0]; g.eps[a][5] = e[1][2] + e[2][1];
-  }
-}
-
-// Core constants with the reference's order of operations.
-bool build_core(const pfdd_instance_desc &d, Core &c) {
-  memset(&c, 0, sizeof c);
-  c.flag = d.core_flag;
-  const double C44 = d.C44, C12 = d.C12, C11 = d.C11;
-  const double mu = C44 - (2.0 * C44 + C12 - C11) / 5.0;
-  const double s = mu * d.dslip * d.b;
-  switch (d.core_flag) {
-    case PFDD_CORE_PERFECT:
-    case PFDD_CORE_USFE_ANGLE:
-      c.k[0] = d.An / s * M_PI;  // An' pi, core_energy_perfect fft_fftw_slab.cpp:1181,1187
-      return true;
-    case PFDD_CORE_SINE: {
-      const double isf = d.isf / s;               // fft_fftw_slab.cpp:1403
-      const double Cn = (d.usf - (isf / 2.0)) / s; // fft_fftw_slab.cpp:1405 (uses the scaled isf)
-      c.k[0] = isf * M_PI;
-      c.k[1] = Cn * 2 * M_PI;
-      return true;
-    }
-    case PFDD_CORE_SINE_FIELD:
-      c.k[2] = d.isf / s;
-      c.k[3] = d.usf / s;
-      c.k[4] = 1.0 / (2.0 * s);
-      return true;
-    case PFDD_CORE_MPEA:
-      c.k[0] = M_PI / s;   // A(r)/(mu dslip b) pi, fft_fftw_slab.cpp:1231
-      return true;
-    case PFDD_CORE_PYRII:
-      for (int n = 1; n <= 4; ++n) {
-        c.k[n] = d.aa[n] / s;
-        c.k[4 + n] = d.bb[n - 1] / s;
-      }
-      return true;
-    case PFDD_CORE_EXTENDED:
-      if (d.n_slip % 3) return false;
-      c.k[0] = d.c[1] / mu; c.k[1] = d.c[2] / mu; c.k[2] = d.c[3] / mu; c.k[3] = d.c[4] / mu;
-      c.k[4] = d.c[5] / mu; c.k[5] = d.c[6] / mu;
-      c.k[6] = (2.0 * M_PI) / (d.dslip * d.b);
-      return true;
-  }
-  return false;
-}
-
-void build_stress(const pfdd_instance_desc &d, StressArgs &s) {
-  memset(&s, 0, sizeof s);
-  const double (*p)[3] = d.prim;
-  // determinant and inverse as fft.cpp computes them (cofactors / norvol)
-  double norvol = p[1][0] * p[2][1] * p[0][2] - p[2][0] * p[1][1] * p[0][2] + p[2][0] * p[0][1] * p[1][2] -
-                  p[0][0] * p[2][1] * p[1][2] + p[0][0] * p[1][1] * p[2][2] - p[1][0] * p[0][1] * p[2][2];
-  double inv[3][3];
-  inv[0][0] = (p[1][1] * p[2][2] - p[2][1] * p[1][2]) / norvol;
-  inv[0][1] = (p[2][1] * p[0][2] - p[0][1] * p[2][2]) / norvol;
-  inv[0][2] = (p[0][1] * p[1][2] - p[1][1] * p[0][2]) / norvol;
-  inv[1][0] = (p[1][2] * p[2][0] - p[2][2] * p[1][0]) / norvol;
-  inv[1][1] = (p[2][2] * p[0][0] - p[0][2] * p[2][0]) / norvol;
-  inv[1][2] = (p[0][2] * p[1][0] - p[1][2] * p[0][0]) / norvol;
-  inv[2][0] = (p[1][0] * p[2][1] - p[2][0] * p[1][1]) / norvol;
-  inv[2][1] = (p[2][0] * p[0][1] - p[0][0] * p[2][1]) / norvol;
-  inv[2][2] = (p[0][0] * p[1][1] - p[1][0] * p[0][1]) / norvol;
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      s.prim[i][j] = p[i][j];
-      s.invprim[i][j] = inv[i][j];
-      s.dsig[i][j] = d.dsigma[i][j];
-    }
-  s.ortho = (std::fabs(norvol) < 1.01 && std::fabs(norvol) > 0.99) ? 1 : 0;
-  s.S = d.n_slip;
-  s.dslip = d.dslip;
-  for (int a = 0; a < d.n_slip; ++a)
-    for (int i = 0; i < 3; ++i) { s.xn[a][i] = d.xn[a][i]; s.xb[a][i] = d.xb[a][i]; }
-}
 
 template <typename T>
 pfdd_status upload_twiddles(pfdd_gpu *h, DevBuf &dst, int n, int count) {
