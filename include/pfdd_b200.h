@@ -197,6 +197,35 @@ const char *pfdd_gpu_last_error(pfdd_gpu *h);
 /* Release the handle and all its device memory. */
 void pfdd_gpu_destroy(pfdd_gpu *h);
 
+/* Size of the device array behind pfdd_gl_step_noalloc (16 MiB per GPU). */
+#define PFDD_STATIC_SCRATCH_BYTES (16u << 20)
+
+/* No counterpart in the reference.  One FP64 GL iteration of one instance
+ * (Re and Im carried as full fields, so the result is the reference's) that
+ * allocates nothing, for callers that cannot call cudaMalloc: code running
+ * while a CUDA graph is captured, runtimes that own all device memory through
+ * their own pool, and hosts that must not allocate after start-up.
+ *   d_xi_in, d_xi_out  caller-owned DEVICE arrays of 2*S*N doubles: the S Re
+ *                      planes, then the S Im planes (reference site order);
+ *                      they must not alias
+ *   h_stats            NULL, or host double[2] receiving {xinorm, xiave}; when
+ *                      given, the call waits for the step and reports
+ *                      PFDD_EDIVERGED / PFDD_ETIMEOUT, otherwise it returns
+ *                      after enqueueing on `stream` (a cudaStream_t, NULL =
+ *                      legacy default stream)
+ * All scratch (half spectrum, partial sums, tables) lives in one file-scope
+ * device array of PFDD_STATIC_SCRATCH_BYTES that every GPU loading the library
+ * holds until exit; a grid needing more (e.g. above 64^3 with 3 systems)
+ * returns PFDD_EINVAL and computes nothing -- use pfdd_gpu_create for those.
+ * The first call on a device (with that device current) looks up the array's
+ * device address and sets kernel attributes, so make it before any stream
+ * capture.  Calls share the array and it keeps the last call's contents;
+ * calls whose GPU work overlaps race on it.  The descriptor's mask, per-site
+ * GSFE field and dsigma are not used (xo and site_gsfe must be NULL); tau is
+ * taken at `sigma`. */
+pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, const double *d_xi_in, double *d_xi_out,
+                                 double *h_stats, void *stream);
+
 /* Library version string. */
 const char *pfdd_gpu_version(void);
 

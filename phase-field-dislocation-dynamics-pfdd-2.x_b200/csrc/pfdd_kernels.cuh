@@ -693,7 +693,7 @@ __global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spe
 // One block: Neumaier-compensated FP64 sums of the per-plane partials.
 // stats[step] = {xinorm, xiave}; sets *stop when 0 < tol and xinorm < tol;
 // flags a non-finite result in *bad.
-__global__ void k_finalize(const double *__restrict__ partials, int nparts, double *__restrict__ stats, int step,
+static __global__ void k_finalize(const double *__restrict__ partials, int nparts, double *__restrict__ stats, int step,
                            double tol, int *stop, int *bad, int *steps_done, const double *__restrict__ partials2,
                            int nparts2, double scale2) {
   if (stop && *stop) return;
@@ -751,7 +751,7 @@ struct StressArgs {
   double dsig[3][3];
 };
 
-__global__ void k_stress_state(double *sigma /*[9]*/, double *tau, StressArgs s, int mode, int *stop) {
+static __global__ void k_stress_state(double *sigma /*[9]*/, double *tau, StressArgs s, int mode, int *stop) {
   if (threadIdx.x != 0) return;
   if (mode == 0) {
     double sr[3][3];
