@@ -174,8 +174,8 @@ class CoreModel:
         if f == 7:
             return self.site / s * PI * np.sin(2.0 * PI * xr)
         if f == 4:
-            aa = np.asarray(self.aa) / s
-            bb = np.asarray(self.bb) / s
+            aa = np.asarray(self.aa, dtype=float) / s
+            bb = np.asarray(self.bb, dtype=float) / s
             out = np.zeros_like(xr)
             S = xr.shape[0]
             last = xr.reshape(S, -1)[:, -1]

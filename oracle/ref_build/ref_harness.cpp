@@ -228,6 +228,13 @@ int main(int argc, char **argv) {
     fprintf(f, "mu %.17g\nxnu %.17g\nb %.17g\ndslip %.17g\n", mat->mu, mat->xnu, mat->b, mat->dslip);
     fprintf(f, "isf %.17g\nusf %.17g\nAn %.17g\n", mat->isf, mat->usf, mat->An);
     fprintf(f, "core_flag %d\n", app->core_flag);
+    fprintf(f, "young %.17g\nC44in %.17g\n", mat->young, mat->C44);
+    const double *cs[7] = {&mat->c0, &mat->c1, &mat->c2, &mat->c3, &mat->c4, &mat->a1, &mat->a3};
+    for (int i = 0; i < 7; ++i) fprintf(f, "c%d %.17g\n", i, *cs[i]);
+    const double *as[5] = {&mat->aa0, &mat->aa1, &mat->aa2, &mat->aa3, &mat->aa4};
+    for (int i = 0; i < 5; ++i) fprintf(f, "aa%d %.17g\n", i, *as[i]);
+    const double *bs[4] = {&mat->bb1, &mat->bb2, &mat->bb3, &mat->bb4};
+    for (int i = 0; i < 4; ++i) fprintf(f, "bb%d %.17g\n", i + 1, *bs[i]);
     for (int a = 0; a < S; ++a)
       fprintf(f, "slip %d %.17g %.17g %.17g %.17g %.17g %.17g\n", a, fft->xn[a][0], fft->xn[a][1],
               fft->xn[a][2], fft->xb[a][0], fft->xb[a][1], fft->xb[a][2]);

@@ -53,7 +53,7 @@ def _raise_stack():
 
 
 def run_reference(workload, steps, state=None, xo=None, mpea=None, sets=(), want_B=False,
-                  timing=False, workdir=None, timeout=3600):
+                  timing=False, workdir=None, timeout=3600, set_b=True, stress_states=None):
     """Run `steps` GL iterations of the reference on `workload`.
 
     state: complex or real array [S, nx, ny, nz] (default workload.xi0).
@@ -65,25 +65,25 @@ def run_reference(workload, steps, state=None, xo=None, mpea=None, sets=(), want
     own_tmp = workdir is None
     tmp = workdir or tempfile.mkdtemp(prefix="pfdd_ref_")
     try:
-        return _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout)
+        return _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, set_b, stress_states)
     finally:
         if own_tmp:
             import shutil
             shutil.rmtree(tmp, ignore_errors=True)
 
 
-def _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout):
+def _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, set_b, stress_states):
     S, nx, ny, nz = workload.S, workload.nx, workload.ny, workload.nz
     deck = os.path.join(tmp, "in.deck")
     with open(deck, "w") as f:
-        f.write(workload.deck(steps))
+        f.write(workload.deck(steps, run_T=stress_states or 1))
     st = workload.xi0 if state is None else state
     st = np.asarray(st)
     inter = np.empty((S * nx * ny * nz, 2))
     inter[:, 0] = np.real(st).reshape(-1)
     inter[:, 1] = np.imag(st).reshape(-1) if np.iscomplexobj(st) else 0.0
     inter.tofile(os.path.join(tmp, "xi0.bin"))
-    args = [HARNESS, "-deck", deck, "-steps", str(steps),
+    args = [HARNESS, "-deck", deck] + ([] if stress_states else ["-steps", str(steps)]) + [
             "-state_in", os.path.join(tmp, "xi0.bin"),
             "-state_out", os.path.join(tmp, "xi.bin"),
             "-stats_out", os.path.join(tmp, "stats.txt"),
@@ -96,7 +96,8 @@ def _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout):
         np.asarray(mpea, dtype=np.float64).tofile(os.path.join(tmp, "mpea.bin"))
         args += ["-mpea_in", os.path.join(tmp, "mpea.bin")]
     m = workload.material
-    for k, v in (("b", m.b), ("dslip", m.dslip)) + tuple(sets):
+    base = (("b", m.b), ("dslip", m.dslip)) if set_b else ()
+    for k, v in base + tuple(sets):
         args += ["-set", k, repr(float(v))]
     args += ["-set", "CD", repr(float(workload.cd_dt))]
     if want_B:

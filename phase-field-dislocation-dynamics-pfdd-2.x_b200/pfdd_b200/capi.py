@@ -129,6 +129,12 @@ def desc_from_workload(w, core_flag=None, An=None):
     d.core_flag = w.core_flag if core_flag is None else core_flag
     d.isf, d.usf = w.material.isf, w.material.usf
     d.An = w.material.An if An is None else An
+    extra = getattr(w, "core_extra", None) or {}
+    for key, n in (("c", 7), ("aa", 5), ("bb", 4)):
+        if key in extra:
+            arr = getattr(d, key)
+            for i in range(n):
+                arr[i] = float(extra[key][i])
     return d
 
 

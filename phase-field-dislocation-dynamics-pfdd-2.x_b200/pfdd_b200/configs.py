@@ -100,8 +100,12 @@ class Material:
     usf: float = 0.175
     An: float = 0.0
     dslip: float = 0.8165
+    deck_line: str | None = None   # verbatim `material ...` deck line (preset constants as they are)
+    elastic_override: tuple | None = None  # (C44, C12, C11) exactly as a deck produced them
 
     def elastic(self):
+        if self.elastic_override is not None:
+            return tuple(self.elastic_override)
         C44 = self.mu
         nu = self.young / 2.0 / self.mu - 1.0
         C12 = 2.0 * nu * C44 / (1.0 - 2.0 * nu)
@@ -128,6 +132,7 @@ class Workload:
     xo: np.ndarray | None = None
     site: np.ndarray | None = None  # per-site GSFE amplitude/multiplier [S, nx, ny, nz]
     dsigma: np.ndarray = field(default_factory=lambda: np.zeros((3, 3)))
+    core_extra: dict | None = None  # c (7), aa (5), bb (4) GSFE constants for the extended / pyrII cores
 
     @property
     def S(self):
@@ -137,7 +142,7 @@ class Workload:
     def N(self):
         return self.nx * self.ny * self.nz
 
-    def deck(self, steps: int, fft_style: str = "fftw_slab") -> str:
+    def deck(self, steps: int, fft_style: str = "fftw_slab", run_T: int = 1) -> str:
         """Reference input deck for this workload (syntax of src/in.fcc-pfdd)."""
         p = self.prim
         m = self.material
@@ -157,7 +162,7 @@ class Workload:
             "region box block 0 %d 0 %d 0 %d" % (self.nx, self.ny, self.nz),
             "create_box box",
             "create_sites box",
-            "material preset %s mu %r young %r isf %r usf %r An %r" % (
+            m.deck_line or "material preset %s mu %r young %r isf %r usf %r An %r" % (
                 m.preset, m.mu, m.young, m.isf, m.usf, m.An),
             "solve_style GL max_iter %d tol 0" % steps,
             "temperature 0",
@@ -166,7 +171,7 @@ class Workload:
                 float(v) for v in (s[0, 0], s[1, 1], s[2, 2], s[0, 1], s[0, 2], s[1, 2],
                                    d[0, 0], d[1, 1], d[2, 2], d[0, 1], d[0, 2], d[1, 2])),
             "stats 1e12",
-            "run 1",
+            "run %d" % run_T,
         ]
         return "\n".join(lines) + "\n"
 
@@ -186,10 +191,12 @@ def _disc(nx, ny, cx, cy, r):
 
 
 def loop_workload(n=64, radius=12.0, noise=1e-3, seed=576, sigma_mpa=200.0, name="loop64",
-                  material: Material | None = None):
-    """Circular loop on system 0 in the z = n/2 plane of an n^3 grid, 3 systems."""
+                  material: Material | None = None, nz: int | None = None):
+    """Circular loop on system 0 in the z = nz/2 plane of an n x n x nz grid
+    (nz defaults to n), 3 systems on that plane."""
     m = material or Material()
-    nx = ny = nz = n
+    nx = ny = n
+    nz = n if nz is None else nz
     prim = np.eye(3)
     four, _ = reciprocal_basis(prim)
     xn, xb = slip_hcp_basal()

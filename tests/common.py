@@ -11,6 +11,10 @@ def oracle_instance(w, core_flag=None, An=None, extra=None):
     mu, ll, young, xnu = O.voigt_constants(C44, C12, C11)
     flag = w.core_flag if core_flag is None else core_flag
     kw = dict(isf=w.material.isf, usf=w.material.usf, An=w.material.An if An is None else An)
+    ce = getattr(w, "core_extra", None) or {}
+    for key in ("c", "aa", "bb"):
+        if key in ce:
+            kw[key] = tuple(float(v) for v in ce[key])
     if extra:
         kw.update(extra)
     core = O.CoreModel(flag, mu, w.material.dslip, w.material.b, site=w.site, **kw)
@@ -22,3 +26,40 @@ def oracle_instance(w, core_flag=None, An=None, extra=None):
 
 def small_loop(n=16, seed=576, sigma_mpa=200.0):
     return configs.loop_workload(n=n, radius=n * 12.0 / 64.0, seed=seed, sigma_mpa=sigma_mpa)
+
+
+def golden_names():
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    return sorted(f[:-4] for f in os.listdir(here) if f.endswith(".npz"))
+
+
+def load_golden(name):
+    """(workload, fixture dict) for tests/golden/<name>.npz, with every constant
+    exactly as the reference used it."""
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    fx = dict(np.load(os.path.join(here, name + ".npz")))
+    m = configs.Material(b=float(fx["b"]), dslip=float(fx["dslip"]), isf=float(fx["isf"]),
+                         usf=float(fx["usf"]), An=float(fx["An"]), mu=float(fx["C44"]),
+                         elastic_override=(float(fx["C44"]), float(fx["C12"]), float(fx["C11"])))
+    w = configs.Workload(name, int(fx["nx"]), int(fx["ny"]), int(fx["nz"]), str(fx["app"]), fx["xn"], fx["xb"],
+                         fx["four"], fx["prim"], m, int(fx["core_flag"]), fx["sigma"], float(fx["cd_dt"]),
+                         fx["xi0"], xo=fx.get("xo"), site=fx.get("site"), dsigma=fx["dsigma"],
+                         core_extra={"c": fx["c"], "aa": fx["aa"], "bb": fx["bb"]})
+    return w, fx
+
+
+def oracle_run_golden(w, fx):
+    """Run the numpy oracle over the fixture's stress states and steps."""
+    xi = np.asarray(fx["xi0"], dtype=np.complex128)
+    sig = np.array(fx["sigma"], dtype=float)
+    norms, aves = [], []
+    for _ in range(int(fx["stress_states"])):
+        w2 = configs.Workload(w.name, w.nx, w.ny, w.nz, w.app, w.xn, w.xb, w.four, w.prim, w.material, w.core_flag,
+                              sig.copy(), w.cd_dt, w.xi0, xo=w.xo, site=w.site, core_extra=w.core_extra)
+        xi, n, a = O.run(oracle_instance(w2), xi, int(fx["steps"]))
+        norms += list(n)
+        aves += list(a)
+        sig = sig + np.asarray(fx["dsigma"])
+    return xi, np.array(norms), np.array(aves)
