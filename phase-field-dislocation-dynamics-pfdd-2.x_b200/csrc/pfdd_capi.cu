@@ -608,9 +608,11 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
     // spectrum rows padded to whole 16-byte units so a plane moves in one bulk copy
     I->nzp = (o.precision == PFDD_FP32) ? ((I->nzh + 1) & ~1) : I->nzh;
     I->N = (size_t)I->nx * I->ny * I->nz;
-    make_plan(I->nx, I->px);
-    make_plan(I->ny, I->py);
-    make_plan(I->M, I->pz);
+    const int maxr = (o.precision == PFDD_FP32) ? MaxRadix<Threads<float>::plane>::value
+                                                : MaxRadix<Threads<double>::plane>::value;
+    make_plan(I->nx, I->px, maxr);
+    make_plan(I->ny, I->py, maxr);
+    make_plan(I->M, I->pz, maxr);
     pfdd_instance_desc d = descs[i];
     I->d.xo = d.xo;               // used during set-up only
     I->d.site_gsfe = d.site_gsfe;

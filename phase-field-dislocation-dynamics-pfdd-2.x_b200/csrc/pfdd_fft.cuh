@@ -157,24 +157,32 @@ struct Batch {
   bool batch_fast;
 };
 
-// Twiddles W^(j*k) for k = 1..R-1 from at most four table reads:
-// W^(j), W^(2j), W^(4j), W^(8j) and their products.
-template <int R, typename C>
-__device__ __forceinline__ void stage_twiddles(const C *__restrict__ tw, int jt, C (&w)[R]) {
-  if constexpr (R == 2) {
-    w[1] = tw[jt];
-  } else if constexpr (R == 3) {
-    w[1] = tw[jt]; w[2] = tw[2 * jt];
-  } else if constexpr (R == 4) {
-    w[1] = tw[jt]; w[2] = tw[2 * jt]; w[3] = tw[3 * jt];
-  } else if constexpr (R == 8) {
-    w[1] = tw[jt]; w[2] = tw[2 * jt]; w[4] = tw[4 * jt];
-    w[3] = cmul(w[1], w[2]); w[5] = cmul(w[1], w[4]); w[6] = cmul(w[2], w[4]); w[7] = cmul(w[3], w[4]);
-  } else if constexpr (R == 16) {
-    w[1] = tw[jt]; w[2] = tw[2 * jt]; w[4] = tw[4 * jt]; w[8] = tw[8 * jt];
-    w[3] = cmul(w[1], w[2]); w[5] = cmul(w[1], w[4]); w[6] = cmul(w[2], w[4]); w[7] = cmul(w[3], w[4]);
-    w[9] = cmul(w[1], w[8]); w[10] = cmul(w[2], w[8]); w[11] = cmul(w[3], w[8]); w[12] = cmul(w[4], w[8]);
-    w[13] = cmul(w[5], w[8]); w[14] = cmul(w[6], w[8]); w[15] = cmul(w[7], w[8]);
+// multiply v[k] (k = 1..R-1) by W^(j k) (or its conjugate), W^(j k) built from
+// at most four table reads W^j, W^2j, W^4j, W^8j as the loop goes
+template <int R, bool CONJ, typename C>
+__device__ __forceinline__ void apply_twiddles(C *v, const C *__restrict__ tw, int jt) {
+  if constexpr (R == 3) {
+    const C w1 = tw[jt], w2 = tw[2 * jt];
+    v[1] = CONJ ? cmulc(v[1], w1) : cmul(v[1], w1);
+    v[2] = CONJ ? cmulc(v[2], w2) : cmul(v[2], w2);
+  } else {
+    C p[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+      if ((1 << b) < R) p[b] = tw[(1 << b) * jt];
+#pragma unroll
+    for (int k = 1; k < R; ++k) {
+      // W^(jk) = product of W^(2^b j) over the set bits b of k
+      C w;
+      bool first = true;
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        if (k & (1 << b)) {
+          w = first ? p[b] : cmul(w, p[b]);
+          first = false;
+        }
+      v[k] = CONJ ? cmulc(v[k], w) : cmul(v[k], w);
+    }
   }
 }
 
@@ -196,19 +204,11 @@ __device__ __forceinline__ void fft_stage(C *__restrict__ x, const C *__restrict
     C v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = base[r * st];
-    C tv[R];
-    if (j) stage_twiddles<R>(tw, j * twstep, tv);
     if constexpr (!INV) {
       dft<R, -1>(v);
-      if (j) {
-#pragma unroll
-        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], tv[k]);
-      }
+      if (j) apply_twiddles<R, false>(v, tw, j * twstep);
     } else {
-      if (j) {
-#pragma unroll
-        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], tv[k]);
-      }
+      if (j) apply_twiddles<R, true>(v, tw, j * twstep);
       dft<R, 1>(v);
     }
 #pragma unroll
@@ -216,33 +216,35 @@ __device__ __forceinline__ void fft_stage(C *__restrict__ x, const C *__restrict
   }
 }
 
-template <bool INV, typename C>
+// Radices above MAXR are compiled out (the host plans never use them for
+// such a kernel), which bounds the registers a butterfly needs.
+template <bool INV, int MAXR, typename C>
 __device__ __forceinline__ void fft_stage_dispatch(C *x, const C *tw, int n, int R, int L, const Batch &g,
                                                    int tid, int nthr) {
   switch (R) {
     case 2: fft_stage<2, INV>(x, tw, n, L, g, tid, nthr); break;
     case 3: fft_stage<3, INV>(x, tw, n, L, g, tid, nthr); break;
     case 4: fft_stage<4, INV>(x, tw, n, L, g, tid, nthr); break;
-    case 8: fft_stage<8, INV>(x, tw, n, L, g, tid, nthr); break;
-    case 16: fft_stage<16, INV>(x, tw, n, L, g, tid, nthr); break;
+    case 8: if constexpr (MAXR >= 8) fft_stage<8, INV>(x, tw, n, L, g, tid, nthr); break;
+    case 16: if constexpr (MAXR >= 16) fft_stage<16, INV>(x, tw, n, L, g, tid, nthr); break;
     default: break;
   }
 }
 
 // Forward (natural -> digit-reversed).  Ends with __syncthreads().
-template <typename C>
+template <int MAXR = 16, typename C>
 __device__ void fft_forward(C *x, const C *tw, const FftPlan &p, const Batch &g) {
   for (int s = 0; s < p.nst; ++s) {
-    fft_stage_dispatch<false>(x, tw, p.n, p.radix[s], p.L[s], g, threadIdx.x, blockDim.x);
+    fft_stage_dispatch<false, MAXR>(x, tw, p.n, p.radix[s], p.L[s], g, threadIdx.x, blockDim.x);
     __syncthreads();
   }
 }
 
 // Inverse, unnormalised (digit-reversed -> natural).  Ends with __syncthreads().
-template <typename C>
+template <int MAXR = 16, typename C>
 __device__ void fft_inverse(C *x, const C *tw, const FftPlan &p, const Batch &g) {
   for (int s = p.nst - 1; s >= 0; --s) {
-    fft_stage_dispatch<true>(x, tw, p.n, p.radix[s], p.L[s], g, threadIdx.x, blockDim.x);
+    fft_stage_dispatch<true, MAXR>(x, tw, p.n, p.radix[s], p.L[s], g, threadIdx.x, blockDim.x);
     __syncthreads();
   }
 }

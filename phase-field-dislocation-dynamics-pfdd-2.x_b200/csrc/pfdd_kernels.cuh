@@ -28,7 +28,21 @@
 
 namespace pfdd {
 
+// Largest FFT radix a kernel with NT threads compiles (bounds registers:
+// 1024-thread blocks must fit 64 registers per thread).
+template <int NT> struct MaxRadix { static constexpr int value = NT >= 1024 ? 8 : 16; };
+
 // Per-instance constants of the contraction and the update (FP64 on the host).
+// Each table is kept in FP64 (set-up, FP64 path) and rounded once to FP32
+// (FP32 path), so the kernels never convert constants in their inner loops.
+template <typename T> struct GreenT {
+  T four[3][3];
+  T sig[PFDD_MAXS][6];    // sigma^a = C : eps^a  (xx yy zz xy xz yz), to build Sig = sum_b Y_b sigma^b
+  T sigo[PFDD_MAXS][6];   // sigma^a / mu with off-diagonals counted twice (contracts the symmetric T)
+  T epso[PFDD_MAXS][6];   // eps^a / mu: xx yy zz, xy+yx, xz+zx, yz+zy (contracts Sig)
+  T c2;                   // 1 / (2 C44), Green's function prefactor, fft_fftw_slab.cpp:597
+  T c1nu;                 // 1 / (1 - nu) (Voigt nu)
+};
 struct Green {
   double four[3][3];
   double sig[PFDD_MAXS][6];   // sigma^a = C : eps^a  (xx yy zz xy xz yz)
@@ -36,12 +50,21 @@ struct Green {
   double inv_mu;              // 1 / mu (Voigt), fft_fftw_slab.cpp:628
   double c2;                  // 1 / (2 C44), Green's function prefactor, fft_fftw_slab.cpp:597
   double c1nu;                // 1 / (1 - nu) (Voigt nu)
+  GreenT<double> d;
+  GreenT<float> f;
 };
+template <typename T> __device__ __forceinline__ const GreenT<T> &green_t(const Green &g);
+template <> __device__ __forceinline__ const GreenT<double> &green_t<double>(const Green &g) { return g.d; }
+template <> __device__ __forceinline__ const GreenT<float> &green_t<float>(const Green &g) { return g.f; }
 
 struct Core {
   int flag;
   double k[12];               // scaled constants, see core_derivative
+  float kf[12];               // the same, rounded once for the FP32 path
 };
+template <typename T> __device__ __forceinline__ T core_k(const Core &c, int i);
+template <> __device__ __forceinline__ double core_k<double>(const Core &c, int i) { return c.k[i]; }
+template <> __device__ __forceinline__ float core_k<float>(const Core &c, int i) { return c.kf[i]; }
 
 // IMAG_NONE: Re xi only, B averaged over k and index -k (not reference-exact)
 // IMAG_FULL: Im xi carried as a second real field through every pass
@@ -193,7 +216,7 @@ __global__ void __launch_bounds__(NT) k_fwd_planes(const T *__restrict__ xi, cx<
 
   // z: M-point complex transform of the packed rows
   Batch gz{ny, ny, nzp, 0, 1, false};
-  fft_forward(buf, sm.twz, a.pz, gz);
+  fft_forward<MaxRadix<NT>::value>(buf, sm.twz, a.pz, gz);
 
   // real-to-complex unpacking, pairs (k, M-k); X[M] goes to slot M
   const int half = M / 2 + 1;
@@ -220,7 +243,7 @@ __global__ void __launch_bounds__(NT) k_fwd_planes(const T *__restrict__ xi, cx<
 
   // y: ny-point transforms over the nzh slot columns
   Batch gy{nzh, nzh, 1, 0, nzp, true};
-  fft_forward(buf, sm.twy, a.py, gy);
+  fft_forward<MaxRadix<NT>::value>(buf, sm.twy, a.py, gy);
 
   // whole plane -> spectrum with one bulk store
   fence_proxy_async();
@@ -236,43 +259,56 @@ __global__ void __launch_bounds__(NT) k_fwd_planes(const T *__restrict__ xi, cx<
 // out_a = sum_b B_ab(k) Y_b for complex Y, with the closed form of Bmatrix
 // (fft_fftw_slab.cpp:587-629):  B_ab = (eps^a:C:eps^b - t^b.G.t^a)/mu,
 // t^a = sigma^a k, G = (2 I/k^2 - k k^T/((1-nu) k^4)) / (2 C44).
-// Because t^a is linear in sigma^a, sum_b B_ab Y_b =
-//   (eps^a : Sig - [2 (t^a . U)/k^2 - (k.t^a)(k.U)/((1-nu)k^4)]/(2 C44)) / mu
-// with Sig = sum_b Y_b sigma^b and U = Sig k: O(S) work per k instead of O(S^2).
+// Because t^a is linear in sigma^a, with Sig = sum_b Y_b sigma^b, U = Sig k,
+// V = k.U:
+//   sum_b B_ab Y_b = (eps^a : Sig + sigma^a : Tq) / mu,
+//   Tq = -2 sym(U k^T)/(2 C44 k^2) + V k k^T/((1-nu) 2 C44 k^4)
+// so each k costs one 6-component Tq and 12 complex-real products per system.
+// B(0) = 0 (A = 0 at k = 0 in the reference): green_tensor reports zero.
 template <typename T, typename C>
-__device__ __forceinline__ void green_prepare(const Green &g, const C (&sig)[6], T kx, T ky, T kz, C (&U)[3],
-                                              C &V, T &g1, T &g2, bool &zero) {
+__device__ __forceinline__ bool green_tensor(const GreenT<T> &g, const C (&sig)[6], T kx, T ky, T kz, C (&Tq)[6]) {
   const T k2 = kx * kx + ky * ky + kz * kz;
-  zero = !(k2 > (T)0);
-  const T ik2 = zero ? (T)0 : (T)1 / k2;
-  g1 = (T)2 * ik2 * (T)g.c2;
-  g2 = ik2 * ik2 * (T)g.c1nu * (T)g.c2;
+  if (!(k2 > (T)0)) return false;
+  const T ik2 = (T)1 / k2;
+  const T g1 = (T)2 * ik2 * g.c2;
+  const T g2 = ik2 * ik2 * g.c1nu * g.c2;
   // sig order: xx yy zz xy xz yz
-  U[0] = mk<C>(sig[0].x * kx + sig[3].x * ky + sig[4].x * kz, sig[0].y * kx + sig[3].y * ky + sig[4].y * kz);
-  U[1] = mk<C>(sig[3].x * kx + sig[1].x * ky + sig[5].x * kz, sig[3].y * kx + sig[1].y * ky + sig[5].y * kz);
-  U[2] = mk<C>(sig[4].x * kx + sig[5].x * ky + sig[2].x * kz, sig[4].y * kx + sig[5].y * ky + sig[2].y * kz);
-  V = mk<C>(kx * U[0].x + ky * U[1].x + kz * U[2].x, kx * U[0].y + ky * U[1].y + kz * U[2].y);
+  const C U0 = mk<C>(sig[0].x * kx + sig[3].x * ky + sig[4].x * kz, sig[0].y * kx + sig[3].y * ky + sig[4].y * kz);
+  const C U1 = mk<C>(sig[3].x * kx + sig[1].x * ky + sig[5].x * kz, sig[3].y * kx + sig[1].y * ky + sig[5].y * kz);
+  const C U2 = mk<C>(sig[4].x * kx + sig[5].x * ky + sig[2].x * kz, sig[4].y * kx + sig[5].y * ky + sig[2].y * kz);
+  const C V = mk<C>(kx * U0.x + ky * U1.x + kz * U2.x, kx * U0.y + ky * U1.y + kz * U2.y);
+  const C gv = mk<C>(g2 * V.x, g2 * V.y);
+  // diagonal: -g1 U_i k_i + g2 V k_i^2 ; off-diagonal pair sums: -g1 (U_i k_j + U_j k_i) + 2 g2 V k_i k_j
+  Tq[0] = mk<C>(-g1 * U0.x * kx + gv.x * kx * kx, -g1 * U0.y * kx + gv.y * kx * kx);
+  Tq[1] = mk<C>(-g1 * U1.x * ky + gv.x * ky * ky, -g1 * U1.y * ky + gv.y * ky * ky);
+  Tq[2] = mk<C>(-g1 * U2.x * kz + gv.x * kz * kz, -g1 * U2.y * kz + gv.y * kz * kz);
+  const T kxy = (T)2 * kx * ky, kxz = (T)2 * kx * kz, kyz = (T)2 * ky * kz;
+  Tq[3] = mk<C>(-g1 * (U0.x * ky + U1.x * kx) + gv.x * kxy, -g1 * (U0.y * ky + U1.y * kx) + gv.y * kxy);
+  Tq[4] = mk<C>(-g1 * (U0.x * kz + U2.x * kx) + gv.x * kxz, -g1 * (U0.y * kz + U2.y * kx) + gv.y * kxz);
+  Tq[5] = mk<C>(-g1 * (U1.x * kz + U2.x * ky) + gv.x * kyz, -g1 * (U1.y * kz + U2.y * ky) + gv.y * kyz);
+  return true;
+}
+
+// (eps^a : Sig + sigma^a : Tq) / mu for system a; zero when k = 0
+template <typename T, typename C>
+__device__ __forceinline__ C green_out(const GreenT<T> &g, int a, const C (&sig)[6], const C (&Tq)[6], bool nz) {
+  if (!nz) return mk<C>((T)0, (T)0);
+  const T *e = g.epso[a];
+  const T *o = g.sigo[a];
+  C r = mk<C>((T)0, (T)0);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    r.x += e[q] * sig[q].x + o[q] * Tq[q].x;
+    r.y += e[q] * sig[q].y + o[q] * Tq[q].y;
+  }
+  return r;
 }
 
 template <typename T, typename C>
-__device__ __forceinline__ C green_apply(const Green &g, int a, const C (&sig)[6], T kx, T ky, T kz,
-                                         const C (&U)[3], C V, T g1, T g2, bool zero) {
-  if (zero) return mk<C>((T)0, (T)0);
-  const double *s = g.sig[a];
-  const double *e = g.eps[a];
-  const T tx = (T)s[0] * kx + (T)s[3] * ky + (T)s[4] * kz;
-  const T ty = (T)s[3] * kx + (T)s[1] * ky + (T)s[5] * kz;
-  const T tz = (T)s[4] * kx + (T)s[5] * ky + (T)s[2] * kz;
-  const T p = kx * tx + ky * ty + kz * tz;
-  C es;
-  es.x = (T)e[0] * sig[0].x + (T)e[1] * sig[1].x + (T)e[2] * sig[2].x + (T)e[3] * sig[3].x + (T)e[4] * sig[4].x +
-         (T)e[5] * sig[5].x;
-  es.y = (T)e[0] * sig[0].y + (T)e[1] * sig[1].y + (T)e[2] * sig[2].y + (T)e[3] * sig[3].y + (T)e[4] * sig[4].y +
-         (T)e[5] * sig[5].y;
-  const T tux = tx * U[0].x + ty * U[1].x + tz * U[2].x;
-  const T tuy = tx * U[0].y + ty * U[1].y + tz * U[2].y;
-  const T im = (T)g.inv_mu;
-  return mk<C>(im * (es.x - g1 * tux + g2 * p * V.x), im * (es.y - g1 * tuy + g2 * p * V.y));
+__device__ __forceinline__ void green_accumulate(const GreenT<T> &g, int b, C x, C (&sig)[6]) {
+  const T *s = g.sig[b];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) { sig[q].x += s[q] * x.x; sig[q].y += s[q] * x.y; }
 }
 
 // frequency of index i on an axis of length n (frec, fft_fftw_slab.cpp:295-330)
@@ -331,7 +367,7 @@ __global__ void __launch_bounds__(NT) k_xpencil(cx<T> *__restrict__ spec, Pencil
   __syncthreads();
 
   Batch gx{F * cc, cc, 1, fst, cc, true};
-  if (a.mode == PASS_STEP) fft_forward(buf, twx, a.px, gx);
+  if (a.mode == PASS_STEP) fft_forward<MaxRadix<NT>::value>(buf, twx, a.px, gx);
 
   double dsq = 0.0;
   for (int w = threadIdx.x; w < nx * cc; w += blockDim.x) {
@@ -349,119 +385,84 @@ __global__ void __launch_bounds__(NT) k_xpencil(cx<T> *__restrict__ spec, Pencil
     }
     const int ix = a.kx_of[sx], iy = a.ky_of[sy], iz = a.kz_of[sz];
     const T fx = freq_of<T>(ix, a.nx), fy = freq_of<T>(iy, a.ny), fz = freq_of<T>(iz, a.nz);
-    const Green &g = a.g;
-    const T kx = fx * (T)g.four[0][0] + fy * (T)g.four[1][0] + fz * (T)g.four[2][0];
-    const T ky = fx * (T)g.four[0][1] + fy * (T)g.four[1][1] + fz * (T)g.four[2][1];
-    const T kz = fx * (T)g.four[0][2] + fy * (T)g.four[1][2] + fz * (T)g.four[2][2];
+    const GreenT<T> &g = green_t<T>(a.g);
+    const T kx = fx * g.four[0][0] + fy * g.four[1][0] + fz * g.four[2][0];
+    const T ky = fx * g.four[0][1] + fy * g.four[1][1] + fz * g.four[2][1];
+    const T kz = fx * g.four[0][2] + fy * g.four[1][2] + fz * g.four[2][2];
     // B at the index -k is B evaluated at the wave vector the reference assigns to -k
     const T gxn = freq_neg<T>(ix, a.nx), gyn = freq_neg<T>(iy, a.ny), gzn = freq_neg<T>(iz, a.nz);
-    const T mx = gxn * (T)g.four[0][0] + gyn * (T)g.four[1][0] + gzn * (T)g.four[2][0];
-    const T my = gxn * (T)g.four[0][1] + gyn * (T)g.four[1][1] + gzn * (T)g.four[2][1];
-    const T mz = gxn * (T)g.four[0][2] + gyn * (T)g.four[1][2] + gzn * (T)g.four[2][2];
+    const T mx = gxn * g.four[0][0] + gyn * g.four[1][0] + gzn * g.four[2][0];
+    const T my = gxn * g.four[0][1] + gyn * g.four[1][1] + gzn * g.four[2][1];
+    const T mz = gxn * g.four[0][2] + gyn * g.four[1][2] + gzn * g.four[2][2];
     const size_t fs = (size_t)fst;
     C sr[6];
 #pragma unroll
     for (int q = 0; q < 6; ++q) sr[q] = mk<C>((T)0, (T)0);
-    for (int b = 0; b < S; ++b) {
-      const C xr = pk[b * fs];
-      const double *s = g.sig[b];
-#pragma unroll
-      for (int q = 0; q < 6; ++q) { sr[q].x += (T)s[q] * xr.x; sr[q].y += (T)s[q] * xr.y; }
+    for (int b = 0; b < S; ++b) green_accumulate<T>(g, b, pk[b * fs], sr);
+    bool nyq = false;
+    size_t a0 = 0, astride = 0;
+    if (a.imag == IMAG_NYQ) {
+      a0 = nyq_index<T, C>(a, 0, sx, sy, sz, nyq);
+      astride = (sz == a.M) ? (size_t)a.nx * a.ny : (sy == a.sy_n ? (size_t)a.nx * a.M : (size_t)a.ny * a.M);
     }
-    if (a.imag == IMAG_FULL) {
+    if (a.imag == IMAG_FULL || nyq) {
       // P = B(k)(Xr + i Xi), Q = B(k')(Xr - i Xi), k' = vector of index -k;
       // Er = (P + Q)/2, Ei = (P - Q)/(2i): the real and imaginary fields of
       // IFFT(B_index X) for the complex field X = Xr + i Xi.
       C si[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) si[q] = mk<C>((T)0, (T)0);
-      for (int b = 0; b < S; ++b) {
-        const C xim = pk[(S + b) * fs];
-        const double *s = g.sig[b];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) { si[q].x += (T)s[q] * xim.x; si[q].y += (T)s[q] * xim.y; }
-      }
+      for (int b = 0; b < S; ++b)
+        green_accumulate<T>(g, b, a.imag == IMAG_FULL ? pk[(S + b) * fs] : caux[a0 + b * astride], si);
       C sp[6], sq[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
         sp[q] = mk<C>(sr[q].x - si[q].y, sr[q].y + si[q].x);  // Sr + i Si
         sq[q] = mk<C>(sr[q].x + si[q].y, sr[q].y - si[q].x);  // Sr - i Si
       }
-      C Up[3], Uq[3], Vp, Vq;
-      T g1p, g2p, g1q, g2q;
-      bool zp, zq;
-      green_prepare<T>(g, sp, kx, ky, kz, Up, Vp, g1p, g2p, zp);
-      green_prepare<T>(g, sq, mx, my, mz, Uq, Vq, g1q, g2q, zq);
+      C Tp[6], Tm[6];
+      const bool zp = green_tensor<T>(g, sp, kx, ky, kz, Tp);
+      const bool zq = green_tensor<T>(g, sq, mx, my, mz, Tm);
+      const T cd = (T)a.cd;
+      const double wgt = (iz == 0 || iz == a.M) ? 1.0 : 2.0;   // k and its unstored partner -k
       for (int aa = 0; aa < S; ++aa) {
-        const C P = green_apply<T>(g, aa, sp, kx, ky, kz, Up, Vp, g1p, g2p, zp);
-        const C Q = green_apply<T>(g, aa, sq, mx, my, mz, Uq, Vq, g1q, g2q, zq);
+        const C P = green_out<T>(g, aa, sp, Tp, zp);
+        const C Q = green_out<T>(g, aa, sq, Tm, zq);
         pk[aa * fs] = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
         // (P - Q)/(2i) = -i (P - Q)/2
-        pk[(S + aa) * fs] = mk<C>((T)0.5 * (P.y - Q.y), (T)-0.5 * (P.x - Q.x));
-      }
-      continue;
-    }
-    bool nyq = false;
-    size_t a0 = 0;
-    if (a.imag == IMAG_NYQ) a0 = nyq_index<T, C>(a, 0, sx, sy, sz, nyq);
-    if (!nyq) {
-      // B(k) = B(index -k) here; real field: Er = B Xr (the Hermitian part for IMAG_NONE)
-      C Up[3], Uq[3], Vp, Vq;
-      T g1p, g2p, g1q, g2q;
-      bool zp, zq;
-      green_prepare<T>(g, sr, kx, ky, kz, Up, Vp, g1p, g2p, zp);
-      if (a.imag == IMAG_NONE) green_prepare<T>(g, sr, mx, my, mz, Uq, Vq, g1q, g2q, zq);
-      for (int aa = 0; aa < S; ++aa) {
-        C P = green_apply<T>(g, aa, sr, kx, ky, kz, Up, Vp, g1p, g2p, zp);
-        if (a.imag == IMAG_NONE) {
-          const C Q = green_apply<T>(g, aa, sr, mx, my, mz, Uq, Vq, g1q, g2q, zq);
-          P = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
+        const C ei = mk<C>((T)0.5 * (P.y - Q.y), (T)-0.5 * (P.x - Q.x));
+        if (a.imag == IMAG_FULL) {
+          pk[(S + aa) * fs] = ei;
+        } else {
+          // Nyquist point: Im xi spectrum updated in k-space (no mask, no core force on Im xi)
+          const C dlt = mk<C>(-cd * ei.x, -cd * ei.y);
+          C *ap = caux + a0 + aa * astride;
+          const C old = *ap;
+          *ap = mk<C>(old.x + dlt.x, old.y + dlt.y);
+          dsq += wgt * ((double)dlt.x * (double)dlt.x + (double)dlt.y * (double)dlt.y);
         }
-        pk[aa * fs] = P;
       }
       continue;
     }
-    // Nyquist point: Im xi spectrum Xi from aux; Er as in IMAG_FULL, and
-    // Xi <- Xi - cd Ei entirely in k-space (no mask, no core force on Im xi)
-    const size_t astride = (sz == a.M) ? (size_t)a.nx * a.ny : (sy == a.sy_n ? (size_t)a.nx * a.M : (size_t)a.ny * a.M);
-    C si[6];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) si[q] = mk<C>((T)0, (T)0);
-    for (int b = 0; b < S; ++b) {
-      const C xim = caux[a0 + b * astride];
-      const double *s = g.sig[b];
-#pragma unroll
-      for (int q = 0; q < 6; ++q) { si[q].x += (T)s[q] * xim.x; si[q].y += (T)s[q] * xim.y; }
+    // B(k) = B(index -k) off the Nyquist planes: Er = B Xr
+    C Tp[6];
+    const bool zp = green_tensor<T>(g, sr, kx, ky, kz, Tp);
+    if (a.imag == IMAG_NONE) {
+      // real field only: average B over k and index -k (the Hermitian part)
+      C Tm[6];
+      const bool zq = green_tensor<T>(g, sr, mx, my, mz, Tm);
+      for (int aa = 0; aa < S; ++aa) {
+        const C P = green_out<T>(g, aa, sr, Tp, zp), Q = green_out<T>(g, aa, sr, Tm, zq);
+        pk[aa * fs] = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
+      }
+      continue;
     }
-    C sp[6], sq[6];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      sp[q] = mk<C>(sr[q].x - si[q].y, sr[q].y + si[q].x);
-      sq[q] = mk<C>(sr[q].x + si[q].y, sr[q].y - si[q].x);
-    }
-    C Up[3], Uq[3], Vp, Vq;
-    T g1p, g2p, g1q, g2q;
-    bool zp, zq;
-    green_prepare<T>(g, sp, kx, ky, kz, Up, Vp, g1p, g2p, zp);
-    green_prepare<T>(g, sq, mx, my, mz, Uq, Vq, g1q, g2q, zq);
-    const T cd = (T)a.cd;
-    const double wgt = (iz == 0 || iz == a.M) ? 1.0 : 2.0;   // k and its unstored partner -k
-    for (int aa = 0; aa < S; ++aa) {
-      const C P = green_apply<T>(g, aa, sp, kx, ky, kz, Up, Vp, g1p, g2p, zp);
-      const C Q = green_apply<T>(g, aa, sq, mx, my, mz, Uq, Vq, g1q, g2q, zq);
-      pk[aa * fs] = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
-      const C ei = mk<C>((T)0.5 * (P.y - Q.y), (T)-0.5 * (P.x - Q.x));
-      const C d = mk<C>(-cd * ei.x, -cd * ei.y);
-      C *ap = caux + a0 + aa * astride;
-      const C old = *ap;
-      *ap = mk<C>(old.x + d.x, old.y + d.y);
-      dsq += wgt * ((double)d.x * (double)d.x + (double)d.y * (double)d.y);
-    }
+    for (int aa = 0; aa < S; ++aa) pk[aa * fs] = green_out<T>(g, aa, sr, Tp, zp);
   }
   if (a.partials) block_sum2(dsq, 0.0, red, a.partials + 2 * blockIdx.x);
   __syncthreads();
 
-  fft_inverse(buf, twx, a.px, gx);
+  fft_inverse<MaxRadix<NT>::value>(buf, twx, a.px, gx);
 
   for (int q = threadIdx.x; q < nchunks; q += blockDim.x) {
     const int fx = dc.div(q), ch = q - fx * cpr;
@@ -482,23 +483,23 @@ __device__ __forceinline__ T core_derivative(const Core &cm, T x, int a, size_t 
   switch (cm.flag) {
     case 1:   // perfect / USFE(angle,tau): An' pi sin(2 pi x)
     case 6:
-      return (T)cm.k[0] * sinpi_t<T>((T)2 * x);
+      return core_k<T>(cm, 0) * sinpi_t<T>((T)2 * x);
     case 3: { // sine: isf' pi sin(2 pi x) + Cn' 2 pi sin(4 pi x)
       T s, c;
       sincospi_t<T>((T)2 * x, &s, &c);
-      return (T)cm.k[0] * s + (T)cm.k[1] * ((T)2 * s * c);
+      return core_k<T>(cm, 0) * s + core_k<T>(cm, 1) * ((T)2 * s * c);
     }
     case 103: { // sine with per-site multiplier m: isf' = isf m/s, Cn' = (usf m - isf'/2)/s
       const T m = site[(size_t)a * N + r];
       T s, c;
       sincospi_t<T>((T)2 * x, &s, &c);
-      const T isf = (T)cm.k[2] * m;               // isf / s * m
-      const T cn = (T)cm.k[3] * m - isf * (T)cm.k[4];  // usf m / s - isf'/(2 s)
+      const T isf = core_k<T>(cm, 2) * m;               // isf / s * m
+      const T cn = core_k<T>(cm, 3) * m - isf * core_k<T>(cm, 4);  // usf m / s - isf'/(2 s)
       return (T)PFDD_PI_T * isf * s + (T)(2.0 * PFDD_PI_T) * cn * ((T)2 * s * c);
     }
     case 7: { // mpea: A(r)/(mu dslip b) pi sin(2 pi x)
       const T A = site[(size_t)a * N + r];
-      return A * (T)cm.k[0] * sinpi_t<T>((T)2 * x);
+      return A * core_k<T>(cm, 0) * sinpi_t<T>((T)2 * x);
     }
     case 4: { // pyrII: the reference writes dE_core only at the last site (fft_fftw_slab.cpp:1491)
       if (r != N - 1) return (T)0;
@@ -507,7 +508,7 @@ __device__ __forceinline__ T core_derivative(const Core &cm, T x, int a, size_t 
       for (int n = 1; n <= 4; ++n) {
         T s, c;
         sincospi_t<T>((T)(2 * n) * x, &s, &c);
-        acc += (T)(2.0 * n * PFDD_PI_T) * ((T)cm.k[4 + n] * c - (T)cm.k[n] * s);
+        acc += (T)(2.0 * n * PFDD_PI_T) * (core_k<T>(cm, 4 + n) * c - core_k<T>(cm, n) * s);
       }
       return acc;
     }
@@ -515,8 +516,8 @@ __device__ __forceinline__ T core_derivative(const Core &cm, T x, int a, size_t 
       const int p = a / 3, w = a - 3 * p;
       const T x1 = xin[(size_t)(3 * p) * N + r], x2 = xin[(size_t)(3 * p + 1) * N + r],
               x3 = xin[(size_t)(3 * p + 2) * N + r];
-      const T c1 = (T)cm.k[0], c2 = (T)cm.k[1], c3 = (T)cm.k[2], c4 = (T)cm.k[3], a1 = (T)cm.k[4],
-              a3 = (T)cm.k[5], pre = (T)cm.k[6];
+      const T c1 = core_k<T>(cm, 0), c2 = core_k<T>(cm, 1), c3 = core_k<T>(cm, 2), c4 = core_k<T>(cm, 3), a1 = core_k<T>(cm, 4),
+              a3 = core_k<T>(cm, 5), pre = core_k<T>(cm, 6);
       auto S2 = [](T t) { return sinpi_t<T>((T)2 * t); };
       auto S4 = [](T t) { return sinpi_t<T>((T)4 * t); };
       auto C2 = [](T t) { return cospi_t<T>((T)2 * t); };
@@ -602,7 +603,7 @@ __global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spe
   const int *pos = sm.pos;
 
   Batch gy{nzh, nzh, 1, 0, nzp, true};
-  fft_inverse(buf, sm.twy, a.py, gy);
+  fft_inverse<MaxRadix<NT>::value>(buf, sm.twy, a.py, gy);
 
   // complex-to-real packing: Zin[k] = A + i w D, Zin[M-k] = conj(A - i w D),
   // A = X[k] + conj X[M-k], D = X[k] - conj X[M-k], w = exp(+2 pi i k / nz)
@@ -624,7 +625,7 @@ __global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spe
   __syncthreads();
 
   Batch gz{ny, ny, nzp, 0, 1, false};
-  fft_inverse(buf, sm.twz, a.pz, gz);
+  fft_inverse<MaxRadix<NT>::value>(buf, sm.twz, a.pz, gz);
 
   // fused GSFE force + applied stress + masked explicit Euler update,
   // VN consecutive z per thread, two vectors in flight per iteration

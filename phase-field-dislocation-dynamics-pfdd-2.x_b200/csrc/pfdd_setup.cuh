@@ -6,6 +6,7 @@
 #pragma once
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "pfdd_b200.h"
@@ -15,14 +16,14 @@ namespace pfdd {
 namespace host {
 
 // Radix plan: greedy 16, 8, 4, 2, 3 factors; sub-lengths L_s.
-inline bool make_plan(int n, FftPlan &p) {
+inline bool make_plan(int n, FftPlan &p, int maxr = 16) {
   p.n = n;
   p.nst = 0;
   int rem = n, L = n;
   while (rem > 1) {
     int r;
-    if (rem % 16 == 0) r = 16;
-    else if (rem % 8 == 0) r = 8;
+    if (rem % 16 == 0 && maxr >= 16) r = 16;
+    else if (rem % 8 == 0 && maxr >= 8) r = 8;
     else if (rem % 4 == 0) r = 4;
     else if (rem % 2 == 0) r = 2;
     else if (rem % 3 == 0) r = 3;
@@ -92,6 +93,22 @@ inline void build_green(const pfdd_instance_desc &d, Green &g) {
     g.eps[a][0] = e[0][0]; g.eps[a][1] = e[1][1]; g.eps[a][2] = e[2][2];
     g.eps[a][3] = e[0][1] + e[1][0]; g.eps[a][4] = e[0][2] + e[2][0]; g.eps[a][5] = e[1][2] + e[2][1];
   }
+  // per-precision tables: sigma for Sig, sigma/mu and eps/mu for the output
+  auto fill = [&](auto &t) {
+    using T = typename std::remove_reference<decltype(t.c2)>::type;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) t.four[i][j] = (T)g.four[i][j];
+    for (int a = 0; a < d.n_slip; ++a)
+      for (int q = 0; q < 6; ++q) {
+        t.sig[a][q] = (T)g.sig[a][q];
+        t.sigo[a][q] = (T)(g.sig[a][q] * g.inv_mu);
+        t.epso[a][q] = (T)(g.eps[a][q] * g.inv_mu);
+      }
+    t.c2 = (T)g.c2;
+    t.c1nu = (T)g.c1nu;
+  };
+  fill(g.d);
+  fill(g.f);
 }
 
 // Core constants with the reference's order of operations.
@@ -105,36 +122,39 @@ inline bool build_core(const pfdd_instance_desc &d, Core &c) {
     case PFDD_CORE_PERFECT:
     case PFDD_CORE_USFE_ANGLE:
       c.k[0] = d.An / s * M_PI;  // An' pi, core_energy_perfect fft_fftw_slab.cpp:1181,1187
-      return true;
+      break;
     case PFDD_CORE_SINE: {
       const double isf = d.isf / s;               // fft_fftw_slab.cpp:1403
       const double Cn = (d.usf - (isf / 2.0)) / s; // fft_fftw_slab.cpp:1405 (uses the scaled isf)
       c.k[0] = isf * M_PI;
       c.k[1] = Cn * 2 * M_PI;
-      return true;
+      break;
     }
     case PFDD_CORE_SINE_FIELD:
       c.k[2] = d.isf / s;
       c.k[3] = d.usf / s;
       c.k[4] = 1.0 / (2.0 * s);
-      return true;
+      break;
     case PFDD_CORE_MPEA:
       c.k[0] = M_PI / s;   // A(r)/(mu dslip b) pi, fft_fftw_slab.cpp:1231
-      return true;
+      break;
     case PFDD_CORE_PYRII:
       for (int n = 1; n <= 4; ++n) {
         c.k[n] = d.aa[n] / s;
         c.k[4 + n] = d.bb[n - 1] / s;
       }
-      return true;
+      break;
     case PFDD_CORE_EXTENDED:
       if (d.n_slip % 3) return false;
       c.k[0] = d.c[1] / mu; c.k[1] = d.c[2] / mu; c.k[2] = d.c[3] / mu; c.k[3] = d.c[4] / mu;
       c.k[4] = d.c[5] / mu; c.k[5] = d.c[6] / mu;
       c.k[6] = (2.0 * M_PI) / (d.dslip * d.b);
-      return true;
+      break;
+    default:
+      return false;
   }
-  return false;
+  for (int i = 0; i < 12; ++i) c.kf[i] = (float)c.k[i];
+  return true;
 }
 
 inline void build_stress(const pfdd_instance_desc &d, StressArgs &s) {
