@@ -169,6 +169,23 @@ pfdd_status pfdd_gpu_step_history(pfdd_gpu *h, int inst, double *xinorm, double 
 pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_core,
                             double *e_applied);
 
+/* No counterpart in the reference (a hand-written adjoint of the GL step).
+ * Gradient of J = sum over sites and systems of (Re xi_N - target)^2, where
+ * xi_N is instance `inst` after n_steps GL iterations from its current state
+ * at the current stress state, with respect to the GSFE parameters and the
+ * applied stress.  Forward pass with a state checkpoint every ckpt_every
+ * steps; backward pass per segment (forward recompute, then adjoint steps
+ *   lam_n = lam_{n+1} - CD dt (L lam_{n+1} + f''(xi_n) lam_{n+1}),
+ * L the self-adjoint elastic operator, masked sites frozen).
+ *   xi_target  host [S*N] target for Re xi_N (reference site order)
+ *   loss       receives J (may be NULL)
+ *   dL_dparams [2]: sine / sine-field cores dJ/d(isf, usf); perfect / USFE
+ *              dJ/d(An, -); MPEA (0, 0)  (J/m^2)
+ *   dL_dsigma  [6]: dJ/d(sigma xx yy zz xy xz yz), deck units (stress / mu)
+ * The instance ends at xi_N, as after pfdd_gpu_advance(h, n_steps, 1, 0, .). */
+pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every, const double *xi_target,
+                             double *loss, double *dL_dparams, double *dL_dsigma);
+
 /* Resolved shear stresses tau[S] of instance `inst` at the current stress state. */
 pfdd_status pfdd_gpu_tau(pfdd_gpu *h, int inst, double *tau);
 

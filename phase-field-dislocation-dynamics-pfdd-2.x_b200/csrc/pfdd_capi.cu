@@ -255,13 +255,25 @@ pfdd_status set_smem_attrs(pfdd_gpu *h, size_t plane, size_t upd, size_t pencil)
 }
 
 // Enqueue one GL iteration of one instance; `step` indexes the stats record.
+// One GL iteration (PASS_STEP) of instance I from xi[cur] into xi[cur^1];
+// with `adj`, one adjoint iteration of the fields in adj->lam[cur] into
+// adj->lam[cur^1] at forward state adj->xfwd (P1 and P2 unchanged: the
+// elastic operator is self-adjoint).
+struct AdjointPass {
+  void *lam_in, *lam_out;
+  const void *xfwd;
+  void *aux;
+  double *gpart;
+};
+
 template <typename T>
-void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_t *ev = nullptr) {
+void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_t *ev = nullptr,
+                  const AdjointPass *adj = nullptr) {
   PlaneArgs pa;
   fill_plane_args<T>(I, pa);
   int *flags = I.flags();
-  const T *xin = I.xi[I.cur].as<T>();
-  T *xout = I.xi[I.cur ^ 1].as<T>();
+  const T *xin = adj ? static_cast<const T *>(adj->lam_in) : I.xi[I.cur].as<T>();
+  T *xout = adj ? static_cast<T *>(adj->lam_out) : I.xi[I.cur ^ 1].as<T>();
   cx<T> *spec = I.spec.as<cx<T>>();
   const int planes = I.F * I.nx;
   constexpr int NP = Threads<T>::plane, NC = Threads<T>::pencil;
@@ -278,10 +290,10 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   pe.kx_of = I.kx_of; pe.ky_of = I.ky_of; pe.kz_of = I.kz_of;
   pe.mode = PASS_STEP;
   pe.fstride = I.fstride;
-  pe.aux = I.aux.p;
+  pe.aux = adj ? adj->aux : I.aux.p;
   pe.sx_n = I.sx_n; pe.sy_n = I.sy_n;
   pe.cd = I.d.cd_dt;
-  pe.partials = I.imag == IMAG_NYQ ? I.ppart.as<double>() : nullptr;
+  pe.partials = (I.imag == IMAG_NYQ && !adj) ? I.ppart.as<double>() : nullptr;
   pe.g = I.green;
   k_xpencil<T, NC><<<I.ntiles, NC, I.smem_pencil, st>>>(spec, pe, flags);
   if (ev) cudaEventRecord(ev[2], st);
@@ -295,9 +307,12 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   ua.site = I.site.p;
   ua.stop = flags;
   ua.err = flags + 3;
-  ua.mode = PASS_STEP;
+  ua.mode = adj ? PASS_ADJOINT : PASS_STEP;
+  ua.xfwd = adj ? adj->xfwd : nullptr;
+  ua.gpart = adj ? adj->gpart : nullptr;
   k_inv_update<T, NP><<<planes, NP, I.smem_update, st>>>(spec, xin, xout, pa, ua, I.partials.as<double>());
   if (ev) cudaEventRecord(ev[3], st);
+  if (adj) return;
   const bool nyq = I.imag == IMAG_NYQ;
   k_finalize<<<1, 1024, 0, st>>>(I.partials.as<double>(), planes, I.stats.as<double>(), step, tol, flags,
                                  flags + 1, flags + 2, nyq ? I.ppart.as<double>() : nullptr, nyq ? I.ntiles : 0,
@@ -352,6 +367,139 @@ pfdd_status profile_impl(pfdd_gpu *h, int n_steps, double *kernel_ms) {
                                       cudaMemcpyDeviceToHost));
     I.hist_count = fl[2];
     CUDA_TRY(h, cudaMemset(I.flags() + 2, 0, sizeof(int)));
+  }
+  return PFDD_OK;
+}
+
+
+// ------------------------------------------------------------ adjoint
+// Gradient of J = sum (Re xi_N - target)^2 over the S real fields, N = n_steps
+// GL iterations from the current state (one stress state), with respect to
+// the GSFE parameters and the applied stress.  Checkpoints every K steps;
+// each segment is recomputed forward (storing Re xi_n) and then stepped
+// backward.  The instance ends at xi_N, as after pfdd_gpu_advance.
+template <typename T>
+pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const double *target, double *loss,
+                         double *dparams, double *dsigma) {
+  cudaStream_t st = h->stream;
+  const size_t n_re = (size_t)I.S * I.N;
+  const size_t n_all = (size_t)I.F * I.N;
+  const size_t aux_bytes = I.aux.bytes;
+  const int nck = (n_steps + K - 1) / K;
+  DevBuf ck, seg, lam[2], tgt, auxa, gpart, acc, lpart;
+  CUDA_TRY(h, ck.alloc((size_t)nck * (n_all * sizeof(T) + aux_bytes)));
+  CUDA_TRY(h, seg.alloc((size_t)K * n_re * sizeof(T)));
+  for (int b = 0; b < 2; ++b) CUDA_TRY(h, lam[b].alloc(n_all * sizeof(T)));
+  CUDA_TRY(h, tgt.alloc(n_re * sizeof(T)));
+  if (aux_bytes) CUDA_TRY(h, auxa.alloc(aux_bytes));
+  CUDA_TRY(h, gpart.alloc(4 * (size_t)I.F * I.nx * sizeof(double)));
+  CUDA_TRY(h, acc.alloc(2 * (2 + PFDD_MAXS) * sizeof(double)));
+  CUDA_TRY(h, lpart.alloc(2 * 1184 * sizeof(double)));
+  CUDA_TRY(h, cudaMemsetAsync(acc.p, 0, acc.bytes, st));
+  if (I.stats_cap < 1) {  // the forward steps record their stats at index 0
+    CUDA_TRY(h, I.stats.alloc(2 * sizeof(double)));
+    I.stats_cap = 1;
+  }
+  {  // target in compute precision, through the staging buffer
+    if (h->staging.bytes < 2 * n_re * sizeof(double)) {
+      CUDA_TRY(h, cudaStreamSynchronize(st));
+      h->staging.release();
+      CUDA_TRY(h, h->staging.alloc(2 * n_re * sizeof(double)));
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(h->staging.p, target, n_re * sizeof(double), cudaMemcpyHostToDevice, st));
+    k_from_planar<T><<<1184, 256, 0, st>>>(h->staging.as<double>(), tgt.as<T>(), n_re);
+  }
+  auto ck_state = [&](int j) { return ck.as<char>() + (size_t)j * (n_all * sizeof(T) + aux_bytes); };
+  auto save = [&](int j) -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(ck_state(j), I.xi[I.cur].p, n_all * sizeof(T), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && aux_bytes)
+      e = cudaMemcpyAsync(ck_state(j) + n_all * sizeof(T), I.aux.p, aux_bytes, cudaMemcpyDeviceToDevice, st);
+    return e;
+  };
+  auto restore = [&](int j) -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(I.xi[I.cur].p, ck_state(j), n_all * sizeof(T), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && aux_bytes)
+      e = cudaMemcpyAsync(I.aux.p, ck_state(j) + n_all * sizeof(T), aux_bytes, cudaMemcpyDeviceToDevice, st);
+    return e;
+  };
+  k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.stress, 0, I.flags());
+  // forward with checkpoints
+  for (int n = 0; n < n_steps; ++n) {
+    if (n % K == 0) CUDA_TRY(h, save(n / K));
+    enqueue_step<T>(I, st, 0, 0.0);
+    I.cur ^= 1;
+  }
+  // keep the final state to hand back; seed lambda = 2 (Re xi_N - target), mu = 0
+  DevBuf fin, finaux;
+  CUDA_TRY(h, fin.alloc(n_all * sizeof(T)));
+  CUDA_TRY(h, cudaMemcpyAsync(fin.p, I.xi[I.cur].p, n_all * sizeof(T), cudaMemcpyDeviceToDevice, st));
+  if (aux_bytes) {
+    CUDA_TRY(h, finaux.alloc(aux_bytes));
+    CUDA_TRY(h, cudaMemcpyAsync(finaux.p, I.aux.p, aux_bytes, cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemsetAsync(auxa.p, 0, aux_bytes, st));
+  }
+  CUDA_TRY(h, cudaMemsetAsync(lam[0].p, 0, n_all * sizeof(T), st));
+  k_loss_seed<T><<<1184, 256, 0, st>>>(I.xi[I.cur].as<T>(), tgt.as<T>(), lam[0].as<T>(), n_re, lpart.as<double>());
+  int lc = 0;
+  // backward over segments
+  for (int j = nck - 1; j >= 0; --j) {
+    const int n0 = j * K, n1 = std::min(n_steps, n0 + K);
+    CUDA_TRY(h, restore(j));
+    for (int n = n0; n < n1; ++n) {
+      CUDA_TRY(h, cudaMemcpyAsync(seg.as<T>() + (size_t)(n - n0) * n_re, I.xi[I.cur].p, n_re * sizeof(T),
+                                  cudaMemcpyDeviceToDevice, st));
+      if (n + 1 < n1) {
+        enqueue_step<T>(I, st, 0, 0.0);
+        I.cur ^= 1;
+      }
+    }
+    for (int n = n1 - 1; n >= n0; --n) {
+      AdjointPass ap{lam[lc].p, lam[lc ^ 1].p, seg.as<T>() + (size_t)(n - n0) * n_re, auxa.p, gpart.as<double>()};
+      enqueue_step<T>(I, st, 0, 0.0, nullptr, &ap);
+      lc ^= 1;
+      k_grad_accum<<<1, 32, 0, st>>>(gpart.as<double>(), I.S, I.nx, acc.as<double>(), acc.as<double>() + 2 + PFDD_MAXS);
+    }
+  }
+  // hand back xi_N
+  CUDA_TRY(h, cudaMemcpyAsync(I.xi[I.cur].p, fin.p, n_all * sizeof(T), cudaMemcpyDeviceToDevice, st));
+  if (aux_bytes) CUDA_TRY(h, cudaMemcpyAsync(I.aux.p, finaux.p, aux_bytes, cudaMemcpyDeviceToDevice, st));
+  double hacc[2 * (2 + PFDD_MAXS)], hl[2 * 1184];
+  CUDA_TRY(h, cudaMemcpyAsync(hacc, acc.p, sizeof hacc, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(h, cudaMemcpyAsync(hl, lpart.p, sizeof hl, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  int fl[4];
+  CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+  if (fl[3]) return fail(h, PFDD_ETIMEOUT, "a bounded device wait ran out");
+  double L = 0.0;
+  for (int b = 0; b < 1184; ++b) L += hl[2 * b];
+  const double cd = I.d.cd_dt;
+  double A[2 + PFDD_MAXS];
+  for (int t = 0; t < 2 + I.S; ++t) A[t] = hacc[t] + hacc[2 + PFDD_MAXS + t];
+  if (loss) *loss = L;
+  if (dparams) {
+    dparams[0] = -cd * A[0];
+    dparams[1] = -cd * A[1];
+  }
+  if (dsigma) {
+    // dJ/dtau_a = cd * sum lambda_a; tau_a = sum_ij sigma_rot_ij xn_aj xb_ai / dslip
+    const StressArgs &sa = I.stress;
+    const int comp[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+    for (int c = 0; c < 6; ++c) {
+      double g = 0.0;
+      for (int a = 0; a < I.S; ++a) {
+        double dt = 0.0;
+        for (int pass = 0; pass < (comp[c][0] == comp[c][1] ? 1 : 2); ++pass) {
+          const int k = pass ? comp[c][1] : comp[c][0], l = pass ? comp[c][0] : comp[c][1];
+          for (int i = 0; i < 3; ++i)
+            for (int jj = 0; jj < 3; ++jj) {
+              const double dr = sa.ortho ? sa.prim[i][k] * sa.invprim[l][jj] : ((i == k && jj == l) ? 1.0 : 0.0);
+              dt += dr * sa.xn[a][jj] * sa.xb[a][i] / sa.dslip;
+            }
+        }
+        g += cd * A[2 + a] * dt;
+      }
+      dsigma[c] = g;
+    }
   }
   return PFDD_OK;
 }
@@ -707,6 +855,21 @@ pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_
   if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
   (void)inst; (void)e_elastic; (void)e_core; (void)e_applied;
   return fail(h, PFDD_EUNSUPPORTED, "energy reduction not built yet");
+}
+
+pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every, const double *xi_target,
+                             double *loss, double *dL_dparams, double *dL_dsigma) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  if (n_steps < 1 || ckpt_every < 1 || !xi_target) return fail(h, PFDD_EINVAL, "need n_steps, ckpt_every >= 1, target");
+  Instance &I = *h->inst[inst];
+  const int f = I.d.core_flag;
+  if (f == PFDD_CORE_EXTENDED || f == PFDD_CORE_PYRII)
+    return fail(h, PFDD_EUNSUPPORTED, "no adjoint for core model %d", f);
+  cudaSetDevice(h->device);
+  return h->precision == PFDD_FP64
+             ? adjoint_impl<double>(h, I, n_steps, ckpt_every, xi_target, loss, dL_dparams, dL_dsigma)
+             : adjoint_impl<float>(h, I, n_steps, ckpt_every, xi_target, loss, dL_dparams, dL_dsigma);
 }
 
 pfdd_status pfdd_gpu_set_stream(pfdd_gpu *h, void *stream) {

@@ -71,7 +71,7 @@ template <> __device__ __forceinline__ float core_k<float>(const Core &c, int i)
 // IMAG_NYQ:  Im xi carried as its spectrum on the Nyquist planes only, where
 //            it lives when no obstacle mask is set (updated inside P2)
 enum { IMAG_NONE = 0, IMAG_FULL = 1, IMAG_NYQ = 2 };
-enum { PASS_STEP = 0, PASS_SYNTH = 1 };
+enum { PASS_STEP = 0, PASS_SYNTH = 1, PASS_ADJOINT = 2 };
 
 struct PlaneArgs {
   FftPlan py, pz;
@@ -102,7 +102,10 @@ struct PencilArgs {
 
 struct UpdateArgs {
   int nx, ny, nz, nzh, nzp, S, F;
-  int mode;                   // PASS_STEP: GL update; PASS_SYNTH: xout = IFFT(spec)/N
+  int mode;                   // PASS_STEP: GL update; PASS_SYNTH: xout = IFFT(spec)/N;
+                              // PASS_ADJOINT: adjoint update of lambda (xin) at forward state xfwd
+  const void *xfwd;           // PASS_ADJOINT: Re xi_n [S][N] (compute precision)
+  double *gpart;              // PASS_ADJOINT: per-plane {sum lam df'/d p0, sum lam df'/d p1, sum lam}
   double cd;                  // CD * timestep
   double invN;
   Core core;
@@ -556,6 +559,51 @@ __device__ __forceinline__ T core_derivative(const Core &cm, T x, int a, size_t 
   }
 }
 
+// ------------------------------------------------------------ adjoint helpers
+// f''(x) and the derivatives of f'(x) with respect to the model's parameters
+// p0, p1 (sine: isf, usf; perfect / USFE: An, -; sine field: isf, usf;
+// MPEA: none), in J/m^2, with the reference's constants (core_derivative).
+template <typename T>
+__device__ __forceinline__ void core_adjoint_terms(const Core &cm, T x, int a, size_t r, size_t N,
+                                                   const T *__restrict__ site, T &d2, T &dp0, T &dp1) {
+  const T pi = (T)PFDD_PI_T;
+  T s2, c2, s4, c4;
+  sincospi_t<T>((T)2 * x, &s2, &c2);
+  s4 = (T)2 * s2 * c2;
+  c4 = (T)1 - (T)2 * s2 * s2;
+  dp0 = (T)0;
+  dp1 = (T)0;
+  switch (cm.flag) {
+    case 1:
+    case 6:  // k0 = An' pi ; f' = k0 sin(2 pi x); d/dAn = (pi/s) sin(2 pi x)
+      d2 = core_k<T>(cm, 0) * (T)2 * pi * c2;
+      dp0 = core_k<T>(cm, 7) * s2;
+      return;
+    case 3:  // k0 = isf' pi, k1 = Cn' 2 pi
+      d2 = core_k<T>(cm, 0) * (T)2 * pi * c2 + core_k<T>(cm, 1) * (T)4 * pi * c4;
+      dp0 = core_k<T>(cm, 7) * s2 - core_k<T>(cm, 8) * s4;   // (pi/s) sin2 - (pi/s^2) sin4
+      dp1 = core_k<T>(cm, 9) * s4;                             // (2 pi/s) sin4
+      return;
+    case 103: {
+      const T m = site[(size_t)a * N + r];
+      const T isf = core_k<T>(cm, 2) * m;
+      const T cn = core_k<T>(cm, 3) * m - isf * core_k<T>(cm, 4);
+      d2 = (T)2 * pi * pi * isf * c2 + (T)8 * pi * pi * cn * c4;
+      dp0 = m * (core_k<T>(cm, 7) * s2 - core_k<T>(cm, 8) * s4);
+      dp1 = m * core_k<T>(cm, 9) * s4;
+      return;
+    }
+    case 7: {
+      const T A = site[(size_t)a * N + r];
+      d2 = A * core_k<T>(cm, 0) * (T)2 * pi * c2;
+      return;
+    }
+    default:
+      d2 = (T)0;
+      return;
+  }
+}
+
 // ------------------------------------------------------------ P3
 template <typename T> struct Vec;
 template <> struct Vec<float> { using type = float4; static constexpr int n = 4; };
@@ -650,6 +698,43 @@ __global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spe
       for (int q = 0; q < VN; ++q) e[q] *= invN;
       *reinterpret_cast<V *>(xout + off + y * nz + zq * VN) = *reinterpret_cast<V *>(e);
     }
+    return;
+  }
+  if (u.mode == PASS_ADJOINT) {
+    // lam_n = lam_{n+1} - cd (L lam + f''(xi_n) lam_{n+1}) on unmasked sites
+    // (the elastic operator is self-adjoint; tau is constant and drops out);
+    // parameter gradients use lam_{n+1} and xi_n on the same sites.
+    const T *site = reinterpret_cast<const T *>(u.site);
+    const T *xf = reinterpret_cast<const T *>(u.xfwd);
+    const T cd = (T)u.cd;
+    double g0 = 0.0, g1 = 0.0, gl = 0.0;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int y = dv.div(i), zq = i - y * nvec;
+      const int idx = y * nz + zq * VN;
+      T lam[VN], e[VN], nv[VN];
+      *reinterpret_cast<V *>(lam) = *reinterpret_cast<const V *>(xin + off + idx);
+      *reinterpret_cast<V *>(e) = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzp + zq * VN);
+#pragma unroll
+      for (int q = 0; q < VN; ++q) {
+        const size_t r = rbase + idx + q;
+        const bool frozen = u.mask && u.mask[(size_t)sys * N + r];
+        if (real_field) {
+          T d2, dp0, dp1;
+          core_adjoint_terms<T>(u.core, xf[(size_t)sys * N + r], sys, r, N, site, d2, dp0, dp1);
+          nv[q] = frozen ? lam[q] : lam[q] - cd * (e[q] * invN + d2 * lam[q]);
+          if (!frozen) {
+            g0 += (double)lam[q] * (double)dp0;
+            g1 += (double)lam[q] * (double)dp1;
+            gl += (double)lam[q];
+          }
+        } else {
+          nv[q] = frozen ? lam[q] : lam[q] - cd * e[q] * invN;
+        }
+      }
+      *reinterpret_cast<V *>(xout + off + idx) = *reinterpret_cast<V *>(nv);
+    }
+    block_sum2(g0, g1, sm.red, u.gpart + 4 * plane);
+    block_sum2(gl, 0.0, sm.red, u.gpart + 4 * plane + 2);
     return;
   }
   // update pass only: tau, mask and per-site GSFE are read from here on
@@ -777,6 +862,41 @@ static __global__ void k_stress_state(double *sigma /*[9]*/, double *tau, Stress
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) sigma[3 * i + j] = sigma[3 * i + j] + s.dsig[i][j];
   }
+}
+
+// ------------------------------------------------------------ adjoint reductions
+// acc[0..1] += sums of the per-plane parameter partials over the real-field
+// planes, acc[2 + a] += sum of lambda over system a's planes; comp[] holds
+// the Neumaier compensation terms across calls.
+static __global__ void k_grad_accum(const double *__restrict__ gpart, int S, int nx, double *acc, double *comp) {
+  const int t = threadIdx.x;
+  if (t >= 2 + S) return;
+  double s = 0.0, c = 0.0;
+  const int col = t < 2 ? t : 2;
+  const int p0 = t < 2 ? 0 : (t - 2) * nx, p1 = t < 2 ? S * nx : (t - 1) * nx;
+  for (int p = p0; p < p1; ++p) {
+    const double v = gpart[4 * p + col], u = s + v;
+    c += (fabs(s) >= fabs(v)) ? (s - u) + v : (v - u) + s;
+    s = u;
+  }
+  const double v = s + c, u = acc[t] + v;
+  comp[t] += (fabs(acc[t]) >= fabs(v)) ? (acc[t] - u) + v : (v - u) + acc[t];
+  acc[t] = u;
+}
+
+// lam = 2 (Re xi - target) on the S real fields; FP64 partial sums of the
+// squared residual per block.
+template <typename T>
+__global__ void k_loss_seed(const T *__restrict__ xr, const T *__restrict__ target, T *__restrict__ lam, size_t n,
+                            double *__restrict__ partial) {
+  __shared__ double red[64];
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const T d = xr[i] - target[i];
+    lam[i] = (T)2 * d;
+    acc += (double)d * (double)d;
+  }
+  block_sum2(acc, 0.0, red, partial + 2 * blockIdx.x);
 }
 
 // ------------------------------------------------------------ layout helpers

@@ -153,6 +153,12 @@ inline bool build_core(const pfdd_instance_desc &d, Core &c) {
     default:
       return false;
   }
+  // derivatives of f' with respect to the GSFE parameters (adjoint step)
+  if (d.core_flag != PFDD_CORE_EXTENDED && d.core_flag != PFDD_CORE_PYRII) {
+    c.k[7] = M_PI / s;
+    c.k[8] = M_PI / (s * s);
+    c.k[9] = 2.0 * M_PI / s;
+  }
   for (int i = 0; i < 12; ++i) c.kf[i] = (float)c.k[i];
   return true;
 }

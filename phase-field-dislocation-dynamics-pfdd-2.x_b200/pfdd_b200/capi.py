@@ -29,7 +29,7 @@ EXPORTS = [
     "pfdd_gpu_create", "pfdd_gpu_set_state", "pfdd_gpu_set_state_interleaved", "pfdd_gpu_get_state",
     "pfdd_gpu_get_state_interleaved", "pfdd_gpu_advance", "pfdd_gpu_step_history", "pfdd_gpu_energy",
     "pfdd_gpu_tau", "pfdd_gpu_info", "pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version",
-    "pfdd_gpu_set_stream", "pfdd_gpu_profile",
+    "pfdd_gpu_set_stream", "pfdd_gpu_profile", "pfdd_gpu_adjoint",
 ]
 KERNELS = ["fwd_planes", "xpencil", "inv_update", "finalize"]
 
@@ -90,6 +90,7 @@ def load(path: str = LIB_PATH):
     lib.pfdd_gpu_step_history.argtypes = [vp, ctypes.c_int, DP, DP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.pfdd_gpu_energy.argtypes = [vp, ctypes.c_int, DP, DP, DP]
     lib.pfdd_gpu_tau.argtypes = [vp, ctypes.c_int, DP]
+    lib.pfdd_gpu_adjoint.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, DP, DP, DP, DP]
     lib.pfdd_gpu_set_stream.argtypes = [vp, vp]
     lib.pfdd_gpu_profile.argtypes = [vp, ctypes.c_int, DP, ctypes.POINTER(ctypes.c_int)]
     lib.pfdd_gpu_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_size_t)]
@@ -214,6 +215,16 @@ class Stepper:
         e = np.empty(3)
         self._check(self._lib.pfdd_gpu_energy(self.h, inst, _dp(e[0:1]), _dp(e[1:2]), _dp(e[2:3])))
         return tuple(e)
+
+    def adjoint(self, inst, n_steps, ckpt_every, target):
+        """(loss, dJ/d(p0, p1), dJ/dsigma[6]) of J = sum (Re xi_N - target)^2."""
+        t = np.ascontiguousarray(target, dtype=np.float64).reshape(-1)
+        loss = np.zeros(1)
+        dp = np.zeros(2)
+        ds = np.zeros(6)
+        self._check(self._lib.pfdd_gpu_adjoint(self.h, inst, n_steps, ckpt_every, _dp(t), _dp(loss), _dp(dp),
+                                               _dp(ds)))
+        return float(loss[0]), dp, ds
 
     def set_stream(self, stream_handle):
         """Run on a caller stream (an int cudaStream_t, e.g. torch.cuda.current_stream().cuda_stream)."""
