@@ -155,7 +155,8 @@ pfdd_status pfdd_gpu_get_state_interleaved(pfdd_gpu *h, int inst, double *xi);
 pfdd_status pfdd_gpu_advance(pfdd_gpu *h, int n_steps, int stress_states, double tol,
                              pfdd_step_stats *stats);
 
-/* Per-step xinorm/xiave history of instance `inst` for the last advance call:
+/* Per-step xinorm/xiave history of instance `inst` for the last advance call
+ * (every GL iteration of every stress state, in order):
  * up to `cap` records are written to xinorm[] / xiave[]; *count gets the
  * number of steps recorded. */
 pfdd_status pfdd_gpu_step_history(pfdd_gpu *h, int inst, double *xinorm, double *xiave, int cap,

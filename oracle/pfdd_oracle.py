@@ -330,18 +330,22 @@ def run(inst: Instance, xi0: np.ndarray, steps: int):
 
 
 # ---------------------------------------------------------------- energy
-def total_energy(inst: Instance, xr: np.ndarray):
-    """E = 1/2 <xi, L xi> + sum f(xi) - sum tau_a xi_a per unit site.
+def total_energy(inst: Instance, xi: np.ndarray):
+    """E = 1/2 <xi, L xi> + sum f(Re xi) - sum tau_a Re xi_a over all sites.
 
     The reference never reduces an energy (E_core is accumulated and unused,
     fft_fftw_slab.cpp:1399); this is the functional whose gradient is the
-    drift term of update_order_parameter, data_real/N - tau + dE_core
-    (fft_fftw_slab.cpp:1773), so d E / d xi_a(r) equals that drift.
-    Returns (elastic, core, applied) summed over sites.
+    drift of update_order_parameter, data_real/N - tau + dE_core
+    (fft_fftw_slab.cpp:1773): L = IFFT B FFT / N is self-adjoint, so
+    dE/d Re xi = (L xi)_re - tau + f' and dE/d Im xi = (L xi)_im.
+    xi may be complex.  Returns (elastic, core, applied).
     """
-    X = np.fft.fftn(xr, axes=(1, 2, 3))
+    xi = np.asarray(xi)
+    X = np.fft.fftn(xi, axes=(1, 2, 3))
     R = np.einsum("abxyz,bxyz->axyz", inst.BB, X)
-    el = 0.5 * float(np.real(np.sum(np.conj(X) * R))) / inst.N
+    Lx = np.fft.ifftn(R, axes=(1, 2, 3))
+    el = 0.5 * float(np.real(np.sum(np.conj(xi) * Lx)))
+    xr = np.real(xi)
     core = float(np.sum(inst.core.energy_density(xr)))
     app = -float(np.sum(inst.tau[:, None, None, None] * xr))
     return el, core, app

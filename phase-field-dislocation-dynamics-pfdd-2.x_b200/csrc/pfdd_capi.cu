@@ -68,25 +68,41 @@ struct Instance {
   DevBuf partials;     // 2 * F * nx doubles
   DevBuf stats;        // 2 * cap doubles
   int stats_cap = 0;
-  DevBuf small;        // tau[S], sigma[9], flags
+  DevBuf small;        // tau[12], sigma[9], dsigma[9], flags[8]
   DevBuf mask, site;
   DevBuf tw_x, tw_y, tw_z, tw_r, tab16;  // twiddles in compute precision, int16 tables
   const int16_t *posM = nullptr, *kx_of = nullptr, *ky_of = nullptr, *kz_of = nullptr;
   std::vector<double> hist;  // host copy of the last advance's per-step stats
   int hist_count = 0;
+  int group = -1;       // index of the batched group this instance belongs to
   double *tau() const { return small.as<double>(); }
-  double *sigma() const { return small.as<double>() + PFDD_MAXS; }
-  int *flags() const { return reinterpret_cast<int *>(small.as<double>() + PFDD_MAXS + 9); }
-  // flags: [0] stop, [1] bad, [2] steps_done, [3] a bounded wait ran out
+  double *sigma() const { return small.as<double>() + PFDD_MAXS; }   // sigma[9] then dsigma[9]
+  int *flags() const { return reinterpret_cast<int *>(small.as<double>() + PFDD_MAXS + 18); }
+  // flags: [0] stop, [1] bad, [2] steps_done, [3] a bounded wait ran out, [4] current xi buffer
 };
 
 }  // namespace
+
+// Instances whose grid, slip systems, material, core model and carrier mode
+// agree run as one group: one launch per kernel per step for all of them.
+struct Group {
+  std::vector<int> members;
+  DevBuf table;   // InstPtrs[members.size()]
+};
+
+struct GraphKey {
+  int steps;
+  double tol;
+  bool operator<(const GraphKey &o) const { return steps < o.steps || (steps == o.steps && tol < o.tol); }
+};
 
 struct pfdd_gpu {
   int precision = PFDD_FP64;
   int device = 0;
   pfdd_options opt{};
   std::vector<std::unique_ptr<Instance>> inst;
+  std::vector<Group> groups;
+  std::map<GraphKey, cudaGraphExec_t> graphs;   // K-step launch sequences, replayed by advance
   cudaStream_t stream = nullptr;      // stream in use
   cudaStream_t own_stream = nullptr;  // stream created by the handle
   DevBuf staging;                     // FP64 host<->device staging, kept across calls
@@ -169,12 +185,15 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   h->device_bytes += I.spec.bytes;
   CUDA_TRY(h, I.partials.alloc(2 * (size_t)I.F * I.nx * sizeof(double)));
   h->device_bytes += I.partials.bytes;
-  CUDA_TRY(h, I.small.alloc((PFDD_MAXS + 9 + 8) * sizeof(double)));
-  CUDA_TRY(h, cudaMemset(I.small.p, 0, (PFDD_MAXS + 9 + 8) * sizeof(double)));
-  double sig9[9];
+  CUDA_TRY(h, I.small.alloc((PFDD_MAXS + 18 + 4) * sizeof(double)));
+  CUDA_TRY(h, cudaMemset(I.small.p, 0, (PFDD_MAXS + 18 + 4) * sizeof(double)));
+  double sig18[18];
   for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) sig9[3 * i + j] = d.sigma[i][j];
-  CUDA_TRY(h, cudaMemcpy(I.sigma(), sig9, sizeof sig9, cudaMemcpyHostToDevice));
+    for (int j = 0; j < 3; ++j) {
+      sig18[3 * i + j] = d.sigma[i][j];
+      sig18[9 + 3 * i + j] = d.dsigma[i][j];
+    }
+  CUDA_TRY(h, cudaMemcpy(I.sigma(), sig18, sizeof sig18, cudaMemcpyHostToDevice));
 
   if (d.xo) {
     std::vector<uint8_t> m((size_t)I.S * I.N);
@@ -251,6 +270,9 @@ pfdd_status set_smem_attrs(pfdd_gpu *h, size_t plane, size_t upd, size_t pencil)
   CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
   CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd));
   CUDA_TRY(h, cudaFuncSetAttribute(k_xpencil<T, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pencil));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes_tab<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update_tab<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_xpencil_tab<T, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pencil));
   return PFDD_OK;
 }
 
@@ -320,28 +342,134 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   if (ev) cudaEventRecord(ev[4], st);
 }
 
+
+// ------------------------------------------------------------ batched groups
+bool same_group(const Instance &a, const Instance &b) {
+  const pfdd_instance_desc &x = a.d, &y = b.d;
+  if (a.nx != b.nx || a.ny != b.ny || a.nz != b.nz || a.S != b.S || a.F != b.F || a.imag != b.imag) return false;
+  if (x.core_flag != y.core_flag || x.C44 != y.C44 || x.C12 != y.C12 || x.C11 != y.C11 || x.dslip != y.dslip ||
+      x.b != y.b || x.cd_dt != y.cd_dt || x.isf != y.isf || x.usf != y.usf || x.An != y.An)
+    return false;
+  if (memcmp(x.four, y.four, sizeof x.four) || memcmp(x.prim, y.prim, sizeof x.prim) ||
+      memcmp(x.xn, y.xn, sizeof(double) * 3 * a.S) || memcmp(x.xb, y.xb, sizeof(double) * 3 * a.S) ||
+      memcmp(x.c, y.c, sizeof x.c) || memcmp(x.aa, y.aa, sizeof x.aa) || memcmp(x.bb, y.bb, sizeof x.bb))
+    return false;
+  if ((a.mask.p == nullptr) != (b.mask.p == nullptr) || (a.site.p == nullptr) != (b.site.p == nullptr)) return false;
+  return true;
+}
+
+// Write every group's InstPtrs table (after any per-instance buffer changes).
+pfdd_status refresh_tables(pfdd_gpu *h) {
+  for (auto &G : h->groups) {
+    std::vector<InstPtrs> t(G.members.size());
+    for (size_t k = 0; k < G.members.size(); ++k) {
+      Instance &I = *h->inst[G.members[k]];
+      InstPtrs &p = t[k];
+      p.xi[0] = I.xi[0].p;
+      p.xi[1] = I.xi[1].p;
+      p.spec = I.spec.p;
+      p.aux = I.aux.p;
+      p.ppart = I.imag == IMAG_NYQ ? I.ppart.as<double>() : nullptr;
+      p.partials = I.partials.as<double>();
+      p.tau = I.tau();
+      p.sigma = I.sigma();
+      p.flags = I.flags();
+      p.stats = I.stats.as<double>();
+      p.stats_cap = I.stats_cap;
+      p.mask = I.mask.as<uint8_t>();
+      p.site = I.site.p;
+    }
+    if (!G.table.p) CUDA_TRY(h, G.table.alloc(t.size() * sizeof(InstPtrs)));
+    CUDA_TRY(h, cudaMemcpy(G.table.p, t.data(), t.size() * sizeof(InstPtrs), cudaMemcpyHostToDevice));
+  }
+  return PFDD_OK;
+}
+
+void build_groups(pfdd_gpu *h) {
+  h->groups.clear();
+  for (size_t i = 0; i < h->inst.size(); ++i) {
+    Instance &I = *h->inst[i];
+    int g = -1;
+    for (size_t k = 0; k < h->groups.size() && g < 0; ++k)
+      if (same_group(*h->inst[h->groups[k].members[0]], I)) g = (int)k;
+    if (g < 0) {
+      h->groups.emplace_back();
+      g = (int)h->groups.size() - 1;
+    }
+    h->groups[g].members.push_back((int)i);
+    I.group = g;
+  }
+}
+
+// One GL iteration of every instance of group G (4 launches for the group).
+template <typename T>
+void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol, cudaEvent_t *ev = nullptr) {
+  constexpr int NP = Threads<T>::plane, NC = Threads<T>::pencil;
+  const unsigned B = (unsigned)G.members.size();
+  const InstPtrs *tab = static_cast<const InstPtrs *>(G.table.p);
+  PlaneArgs pa;
+  fill_plane_args<T>(L, pa);
+  const int planes = L.F * L.nx;
+  if (ev) cudaEventRecord(ev[0], st);
+  k_fwd_planes_tab<T, NP><<<dim3(planes, B), NP, L.smem_plane, st>>>(tab, pa);
+  if (ev) cudaEventRecord(ev[1], st);
+  PencilArgs pe;
+  memset(&pe, 0, sizeof pe);
+  pe.px = L.px;
+  pe.nx = L.nx; pe.ny = L.ny; pe.nz = L.nz; pe.nzh = L.nzh; pe.nzp = L.nzp; pe.M = L.M;
+  pe.S = L.S; pe.F = L.F; pe.imag = L.imag;
+  pe.ncols = L.ny * L.nzp;
+  pe.ccols = L.ccols;
+  pe.tw_x = L.tw_x.p;
+  pe.kx_of = L.kx_of; pe.ky_of = L.ky_of; pe.kz_of = L.kz_of;
+  pe.mode = PASS_STEP;
+  pe.fstride = L.fstride;
+  pe.sx_n = L.sx_n; pe.sy_n = L.sy_n;
+  pe.cd = L.d.cd_dt;
+  pe.g = L.green;
+  k_xpencil_tab<T, NC><<<dim3(L.ntiles, B), NC, L.smem_pencil, st>>>(tab, pe);
+  if (ev) cudaEventRecord(ev[2], st);
+  UpdateArgs ua;
+  memset(&ua, 0, sizeof ua);
+  ua.nx = L.nx; ua.ny = L.ny; ua.nz = L.nz; ua.nzh = L.nzh; ua.nzp = L.nzp; ua.S = L.S; ua.F = L.F;
+  ua.cd = L.d.cd_dt;
+  ua.invN = 1.0 / (double)L.N;
+  ua.core = L.core;
+  ua.mode = PASS_STEP;
+  k_inv_update_tab<T, NP><<<dim3(planes, B), NP, L.smem_update, st>>>(tab, pa, ua);
+  if (ev) cudaEventRecord(ev[3], st);
+  const bool nyq = L.imag == IMAG_NYQ;
+  k_finalize_tab<<<B, 1024, 0, st>>>(tab, planes, nyq ? L.ntiles : 0, 1.0 / (double)L.N, tol);
+  if (ev) cudaEventRecord(ev[4], st);
+}
+
+template <typename T>
+void enqueue_all_groups(pfdd_gpu *h, cudaStream_t st, double tol) {
+  for (auto &G : h->groups) enqueue_group_step<T>(*h->inst[G.members[0]], G, st, tol);
+}
+
 constexpr int kLaunchesPerStep = 4;
+
+pfdd_status ensure_stats(pfdd_gpu *h, int cap);
+pfdd_status reset_counters(pfdd_gpu *h);
+pfdd_status collect(pfdd_gpu *h, pfdd_step_stats *stats);
+template <typename T> void stress_all(pfdd_gpu *h, int mode);
 
 template <typename T>
 pfdd_status profile_impl(pfdd_gpu *h, int n_steps, double *kernel_ms) {
   cudaStream_t st = h->stream;
   for (int k = 0; k < PFDD_NKERNELS; ++k) kernel_ms[k] = 0.0;
-  for (auto &ip : h->inst) {
-    Instance &I = *ip;
-    if (I.stats_cap < n_steps) {
-      I.stats.release();
-      CUDA_TRY(h, I.stats.alloc(2 * (size_t)n_steps * sizeof(double)));
-      I.stats_cap = n_steps;
-    }
-    k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.stress, 0, I.flags());
-  }
-  std::vector<cudaEvent_t> ev(5 * (size_t)n_steps * h->inst.size());
+  pfdd_status ps;
+  if ((ps = ensure_stats(h, n_steps))) return ps;
+  if ((ps = reset_counters(h))) return ps;
+  stress_all<T>(h, 0);
+  const size_t ng = h->groups.size();
+  std::vector<cudaEvent_t> ev(5 * (size_t)n_steps * ng);
   for (auto &e : ev) CUDA_TRY(h, cudaEventCreate(&e));
   size_t q = 0;
   for (int it = 0; it < n_steps; ++it)
-    for (auto &ip : h->inst) {
-      enqueue_step<T>(*ip, st, it, 0.0, &ev[q]);
-      ip->cur ^= 1;
+    for (auto &G : h->groups) {
+      enqueue_group_step<T>(*h->inst[G.members[0]], G, st, 0.0, &ev[q]);
       q += 5;
     }
   cudaError_t e = cudaStreamSynchronize(st);
@@ -356,21 +484,82 @@ pfdd_status profile_impl(pfdd_gpu *h, int n_steps, double *kernel_ms) {
   }
   for (auto &x : ev) cudaEventDestroy(x);
   CUDA_TRY(h, e);
-  for (auto &ip : h->inst) {
-    Instance &I = *ip;
-    int fl[4];
-    CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
-    if (fl[3]) return fail(h, PFDD_ETIMEOUT, "a bounded device wait ran out");
-    if (fl[1]) return fail(h, PFDD_EDIVERGED, "non-finite order parameter");
-    I.hist.resize(2 * (size_t)fl[2]);
-    if (fl[2]) CUDA_TRY(h, cudaMemcpy(I.hist.data(), I.stats.p, 2 * (size_t)fl[2] * sizeof(double),
-                                      cudaMemcpyDeviceToHost));
-    I.hist_count = fl[2];
-    CUDA_TRY(h, cudaMemset(I.flags() + 2, 0, sizeof(int)));
-  }
-  return PFDD_OK;
+  return collect(h, nullptr);
 }
 
+// ------------------------------------------------------------ energy
+// E_elastic = 1/2 <xi, L xi> (Re and Im), E_core = sum f(Re xi),
+// E_applied = -sum tau_a Re xi_a, from one elastic pass of the current state.
+template <typename T>
+pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, double *e_app) {
+  constexpr int NP = Threads<T>::plane, NC = Threads<T>::pencil;
+  cudaStream_t st = h->stream;
+  DevBuf gpart;
+  CUDA_TRY(h, gpart.alloc(4 * (size_t)I.F * I.nx * sizeof(double)));
+  k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.stress, 0, nullptr);
+  PlaneArgs pa;
+  fill_plane_args<T>(I, pa);
+  const T *xcur = I.xi[I.cur].as<T>();
+  cx<T> *spec = I.spec.as<cx<T>>();
+  const int planes = I.F * I.nx;
+  k_fwd_planes<T, NP><<<planes, NP, I.smem_plane, st>>>(xcur, spec, pa, nullptr, I.flags() + 3);
+  PencilArgs pe;
+  memset(&pe, 0, sizeof pe);
+  pe.px = I.px;
+  pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.nzp = I.nzp; pe.M = I.M;
+  pe.S = I.S; pe.F = I.F; pe.imag = I.imag;
+  pe.ncols = I.ny * I.nzp;
+  pe.ccols = I.ccols;
+  pe.tw_x = I.tw_x.p;
+  pe.kx_of = I.kx_of; pe.ky_of = I.ky_of; pe.kz_of = I.kz_of;
+  pe.mode = PASS_ENERGY;
+  pe.fstride = I.fstride;
+  pe.aux = I.aux.p;
+  pe.sx_n = I.sx_n; pe.sy_n = I.sy_n;
+  pe.cd = I.d.cd_dt;
+  pe.partials = I.imag == IMAG_NYQ ? I.ppart.as<double>() : nullptr;
+  pe.g = I.green;
+  k_xpencil<T, NC><<<I.ntiles, NC, I.smem_pencil, st>>>(spec, pe, nullptr);
+  UpdateArgs ua;
+  memset(&ua, 0, sizeof ua);
+  ua.nx = I.nx; ua.ny = I.ny; ua.nz = I.nz; ua.nzh = I.nzh; ua.nzp = I.nzp; ua.S = I.S; ua.F = I.F;
+  ua.cd = I.d.cd_dt;
+  ua.invN = 1.0 / (double)I.N;
+  ua.core = I.core;
+  ua.tau = I.tau();
+  ua.mask = I.mask.as<uint8_t>();
+  ua.site = I.site.p;
+  ua.err = I.flags() + 3;
+  ua.mode = PASS_ENERGY;
+  ua.gpart = gpart.as<double>();
+  // xout is not written by the energy pass
+  k_inv_update<T, NP><<<planes, NP, I.smem_update, st>>>(spec, xcur, I.xi[I.cur ^ 1].as<T>(), pa, ua,
+                                                        I.partials.as<double>());
+  std::vector<double> gp(4 * (size_t)planes), pp;
+  CUDA_TRY(h, cudaMemcpyAsync(gp.data(), gpart.p, gp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (I.imag == IMAG_NYQ) {
+    pp.resize(2 * (size_t)I.ntiles);
+    CUDA_TRY(h, cudaMemcpyAsync(pp.data(), I.ppart.p, pp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  CUDA_TRY(h, cudaGetLastError());
+  // compensated (Neumaier) sums in FP64
+  auto sum = [](const double *v, size_t n, size_t stride, double scale) {
+    double s = 0.0, c = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+      const double x = v[i * stride] * scale, t = s + x;
+      c += (std::fabs(s) >= std::fabs(x)) ? (s - t) + x : (x - t) + s;
+      s = t;
+    }
+    return s + c;
+  };
+  double el = sum(gp.data(), planes, 4, 1.0);
+  if (!pp.empty()) el += sum(pp.data(), I.ntiles, 2, 1.0 / (double)I.N);
+  if (e_el) *e_el = el;
+  if (e_core) *e_core = sum(gp.data() + 1, planes, 4, 1.0);
+  if (e_app) *e_app = sum(gp.data() + 2, planes, 4, 1.0);
+  return PFDD_OK;
+}
 
 // ------------------------------------------------------------ adjoint
 // Gradient of J = sum (Re xi_N - target)^2 over the S real fields, N = n_steps
@@ -460,8 +649,9 @@ pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const dou
       k_grad_accum<<<1, 32, 0, st>>>(gpart.as<double>(), I.S, I.nx, acc.as<double>(), acc.as<double>() + 2 + PFDD_MAXS);
     }
   }
-  // hand back xi_N
+  // hand back xi_N (and make the device's buffer selector agree with the host's)
   CUDA_TRY(h, cudaMemcpyAsync(I.xi[I.cur].p, fin.p, n_all * sizeof(T), cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(h, cudaMemcpyAsync(I.flags() + 4, &I.cur, sizeof(int), cudaMemcpyHostToDevice, st));
   if (aux_bytes) CUDA_TRY(h, cudaMemcpyAsync(I.aux.p, finaux.p, aux_bytes, cudaMemcpyDeviceToDevice, st));
   double hacc[2 * (2 + PFDD_MAXS)], hl[2 * 1184];
   CUDA_TRY(h, cudaMemcpyAsync(hacc, acc.p, sizeof hacc, cudaMemcpyDeviceToHost, st));
@@ -504,66 +694,105 @@ pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const dou
   return PFDD_OK;
 }
 
+// Graph of `steps` GL iterations of every group (captured once per (steps, tol)).
 template <typename T>
-pfdd_status advance_impl(pfdd_gpu *h, int n_steps, int stress_states, double tol, pfdd_step_stats *stats) {
+pfdd_status graph_for(pfdd_gpu *h, int steps, double tol, cudaGraphExec_t *out) {
+  GraphKey key{steps, tol};
+  auto it = h->graphs.find(key);
+  if (it != h->graphs.end()) { *out = it->second; return PFDD_OK; }
   cudaStream_t st = h->stream;
+  cudaGraph_t g;
+  CUDA_TRY(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < steps; ++i) enqueue_all_groups<T>(h, st, tol);
+  CUDA_TRY(h, cudaStreamEndCapture(st, &g));
+  cudaGraphExec_t ge;
+  cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  CUDA_TRY(h, e);
+  h->graphs[key] = ge;
+  *out = ge;
+  return PFDD_OK;
+}
+
+// Grow every instance's per-step record buffer to `cap` records.
+pfdd_status ensure_stats(pfdd_gpu *h, int cap) {
+  bool changed = false;
   for (auto &ip : h->inst) {
     Instance &I = *ip;
-    if (I.stats_cap < n_steps) {
-      I.stats.release();
-      CUDA_TRY(h, I.stats.alloc(2 * (size_t)std::max(n_steps, 1) * sizeof(double)));
-      I.stats_cap = std::max(n_steps, 1);
-    }
+    if (I.stats_cap >= cap) continue;
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    I.stats.release();
+    CUDA_TRY(h, I.stats.alloc(2 * (size_t)cap * sizeof(double)));
+    I.stats_cap = cap;
+    changed = true;
   }
-  std::vector<int> done(h->inst.size(), 0), conv(h->inst.size(), 0);
-  for (int ss = 0; ss < stress_states; ++ss) {
-    for (auto &ip : h->inst) {
-      Instance &I = *ip;
-      k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.stress, 0, I.flags());
-    }
-    // interleave instances step by step so independent instances overlap
-    // their short tails on the device
-    for (int it = 0; it < n_steps; ++it) {
-      for (auto &ip : h->inst) {
-        Instance &I = *ip;
-        enqueue_step<T>(I, st, it, tol);
-        I.cur ^= 1;
-      }
-    }
-    // the stop flag freezes later steps without moving data, but the host
-    // flips buffers unconditionally: recover the true parity from steps_done
-    CUDA_TRY(h, cudaStreamSynchronize(st));
-    for (size_t i = 0; i < h->inst.size(); ++i) {
-      Instance &I = *h->inst[i];
-      int fl[4];
-      CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
-      if (fl[3]) return fail(h, PFDD_ETIMEOUT, "instance %zu: a bounded device wait ran out", i);
-      if (fl[1]) return fail(h, PFDD_EDIVERGED, "instance %zu: non-finite order parameter", i);
-      const int did = fl[2];
-      // parity: started at cur0, flipped n_steps times on the host, but only `did` real swaps
-      if ((n_steps - did) & 1) I.cur ^= 1;
-      done[i] = did;
-      conv[i] = fl[0];
-      I.hist.resize(2 * (size_t)did);
-      if (did) CUDA_TRY(h, cudaMemcpy(I.hist.data(), I.stats.p, 2 * (size_t)did * sizeof(double),
-                                      cudaMemcpyDeviceToHost));
-      I.hist_count = did;
-      k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.stress, 1, I.flags());
-      CUDA_TRY(h, cudaMemsetAsync(I.flags() + 2, 0, sizeof(int), st));
-    }
-  }
-  CUDA_TRY(h, cudaStreamSynchronize(st));
-  CUDA_TRY(h, cudaGetLastError());
-  if (stats) {
-    for (size_t i = 0; i < h->inst.size(); ++i) {
-      Instance &I = *h->inst[i];
-      stats[i].steps_done = done[i];
-      stats[i].converged = conv[i];
-      stats[i].xinorm = I.hist_count ? I.hist[2 * (I.hist_count - 1)] : 0.0;
-      stats[i].xiave = I.hist_count ? I.hist[2 * (I.hist_count - 1) + 1] : 0.0;
+  return changed ? refresh_tables(h) : PFDD_OK;
+}
+
+// Read back each instance's control words after a run; keeps the host mirror
+// of the current buffer in step with the device.
+pfdd_status collect(pfdd_gpu *h, pfdd_step_stats *stats) {
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  for (size_t i = 0; i < h->inst.size(); ++i) {
+    Instance &I = *h->inst[i];
+    int fl[5];
+    CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+    if (fl[3]) return fail(h, PFDD_ETIMEOUT, "instance %zu: a bounded device wait ran out", i);
+    if (fl[1]) return fail(h, PFDD_EDIVERGED, "instance %zu: non-finite order parameter", i);
+    I.cur = fl[4];
+    const int did = std::min(fl[2], I.stats_cap);
+    I.hist.resize(2 * (size_t)did);
+    if (did)
+      CUDA_TRY(h, cudaMemcpy(I.hist.data(), I.stats.p, 2 * (size_t)did * sizeof(double), cudaMemcpyDeviceToHost));
+    I.hist_count = did;
+    if (stats) {
+      stats[i].steps_done = fl[2];
+      stats[i].converged = fl[0];
+      stats[i].xinorm = did ? I.hist[2 * (did - 1)] : 0.0;
+      stats[i].xiave = did ? I.hist[2 * (did - 1) + 1] : 0.0;
     }
   }
   return PFDD_OK;
+}
+
+pfdd_status reset_counters(pfdd_gpu *h) {
+  for (auto &ip : h->inst) CUDA_TRY(h, cudaMemsetAsync(ip->flags() + 2, 0, sizeof(int), h->stream));
+  return PFDD_OK;
+}
+
+template <typename T>
+void stress_all(pfdd_gpu *h, int mode) {
+  for (auto &G : h->groups)
+    k_stress_state_tab<<<(unsigned)G.members.size(), 32, 0, h->stream>>>(
+        static_cast<const InstPtrs *>(G.table.p), h->inst[G.members[0]]->stress, mode);
+}
+
+template <typename T>
+pfdd_status advance_impl(pfdd_gpu *h, int n_steps, int stress_states, double tol, pfdd_step_stats *stats) {
+  cudaStream_t st = h->stream;
+  pfdd_status ps;
+  const long long total = (long long)n_steps * stress_states;
+  if ((ps = ensure_stats(h, (int)std::min<long long>(total, 1 << 24)))) return ps;
+  if ((ps = reset_counters(h))) return ps;
+  const int chunk = 32;
+  for (int ss = 0; ss < stress_states; ++ss) {
+    stress_all<T>(h, 0);
+    if (h->opt.use_graphs) {
+      int left = n_steps;
+      while (left > 0) {
+        const int k = std::min(chunk, left);
+        cudaGraphExec_t ge;
+        if ((ps = graph_for<T>(h, k, tol, &ge))) return ps;
+        CUDA_TRY(h, cudaGraphLaunch(ge, st));
+        left -= k;
+      }
+    } else {
+      for (int it = 0; it < n_steps; ++it) enqueue_all_groups<T>(h, st, tol);
+    }
+    stress_all<T>(h, 1);
+  }
+  CUDA_TRY(h, cudaGetLastError());
+  return collect(h, stats);
 }
 
 template <typename T>
@@ -779,6 +1008,11 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
   pfdd_status st = (o.precision == PFDD_FP64) ? set_smem_attrs<double>(h.get(), max_plane, max_upd, max_pen)
                                               : set_smem_attrs<float>(h.get(), max_plane, max_upd, max_pen);
   if (st != PFDD_OK) { g_create_error = h->err; return st; }
+  build_groups(h.get());
+  if ((st = ensure_stats(h.get(), 1)) != PFDD_OK || (st = refresh_tables(h.get())) != PFDD_OK) {
+    g_create_error = h->err;
+    return st;
+  }
   *out = h.release();
   return PFDD_OK;
 }
@@ -853,8 +1087,14 @@ pfdd_status pfdd_gpu_tau(pfdd_gpu *h, int inst, double *tau) {
 
 pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_core, double *e_applied) {
   if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
-  (void)inst; (void)e_elastic; (void)e_core; (void)e_applied;
-  return fail(h, PFDD_EUNSUPPORTED, "energy reduction not built yet");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  Instance &I = *h->inst[inst];
+  const int f = I.d.core_flag;
+  if (f == PFDD_CORE_EXTENDED || f == PFDD_CORE_PYRII)
+    return fail(h, PFDD_EUNSUPPORTED, "no energy density for core model %d", f);
+  cudaSetDevice(h->device);
+  return h->precision == PFDD_FP64 ? energy_impl<double>(h, I, e_elastic, e_core, e_applied)
+                                   : energy_impl<float>(h, I, e_elastic, e_core, e_applied);
 }
 
 pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every, const double *xi_target,
@@ -884,7 +1124,7 @@ pfdd_status pfdd_gpu_profile(pfdd_gpu *h, int n_steps, double *kernel_ms, int *l
   if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
   if (n_steps < 1 || !kernel_ms) return fail(h, PFDD_EINVAL, "need n_steps >= 1 and kernel_ms");
   cudaSetDevice(h->device);
-  if (launches_per_step) *launches_per_step = kLaunchesPerStep * (int)h->inst.size();
+  if (launches_per_step) *launches_per_step = kLaunchesPerStep * (int)h->groups.size();
   return h->precision == PFDD_FP64 ? profile_impl<double>(h, n_steps, kernel_ms)
                                    : profile_impl<float>(h, n_steps, kernel_ms);
 }
@@ -902,6 +1142,9 @@ void pfdd_gpu_destroy(pfdd_gpu *h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
+  h->graphs.clear();
+  h->groups.clear();
   h->inst.clear();
   h->staging.release();
   if (h->own_stream) cudaStreamDestroy(h->own_stream);

@@ -71,7 +71,7 @@ template <> __device__ __forceinline__ float core_k<float>(const Core &c, int i)
 // IMAG_NYQ:  Im xi carried as its spectrum on the Nyquist planes only, where
 //            it lives when no obstacle mask is set (updated inside P2)
 enum { IMAG_NONE = 0, IMAG_FULL = 1, IMAG_NYQ = 2 };
-enum { PASS_STEP = 0, PASS_SYNTH = 1, PASS_ADJOINT = 2 };
+enum { PASS_STEP = 0, PASS_SYNTH = 1, PASS_ADJOINT = 2, PASS_ENERGY = 3 };
 
 struct PlaneArgs {
   FftPlan py, pz;
@@ -114,6 +114,30 @@ struct UpdateArgs {
   const void *site;           // [S*N] per-site GSFE field (compute precision) or null
   const int *stop;            // device flag: skip the step when nonzero
   int *err;                   // device flag: a bounded wait ran out
+};
+
+// Per-instance device pointers of a batched group: the batched kernel entries
+// take a table of these and handle instance blockIdx.y, so one launch covers
+// every instance of a group (same grid shape and constants, own state, stress,
+// mask and per-site GSFE).  The flags word block is the instance's control
+// state on the device: [0] stop (tolerance reached), [1] non-finite, [2]
+// steps done (also the stats record index), [3] a bounded wait ran out,
+// [4] which xi buffer holds the current state.  Keeping the buffer parity on
+// the device makes a step's launches independent of how many earlier steps
+// were skipped, so they can be replayed from a CUDA graph.
+struct InstPtrs {
+  void *xi[2];
+  void *spec;
+  void *aux;
+  double *ppart;       // x-pencil partial sums (Nyquist carrier) or null
+  double *partials;    // plane partial sums
+  double *tau;         // [S]
+  double *sigma;       // [9] current stress, [9] increment per stress state
+  int *flags;
+  double *stats;       // {xinorm, xiave} per step
+  int stats_cap;
+  const uint8_t *mask;
+  const void *site;
 };
 
 // ------------------------------------------------------------ small helpers
@@ -186,16 +210,13 @@ __device__ __forceinline__ void load_plane_tables(const PlaneSmem<C> &sm, const 
   for (int i = threadIdx.x; i < a.M; i += blockDim.x) sm.pos[i] = a.posM[i];
 }
 
-// grid.x = F * nx planes
 template <typename T, int NT>
-__global__ void __launch_bounds__(NT) k_fwd_planes(const T *__restrict__ xi, cx<T> *__restrict__ spec,
-                                                   PlaneArgs a, const int *__restrict__ stop, int *err) {
+__device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> *__restrict__ spec,
+                                                const PlaneArgs &a, int *err, size_t plane) {
   using C = cx<T>;
-  if (stop && *stop) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const PlaneSmem<C> sm(smem_raw, a);
   const int ny = a.ny, nz = a.nz, nzh = a.nzh, nzp = a.nzp, M = a.M;
-  const size_t plane = blockIdx.x;
   if (threadIdx.x == 0) mbar_init(sm.bar, 1);
   __syncthreads();
   // rows of the real plane -> shared rows of stride 2*nzp reals (bulk copies)
@@ -256,6 +277,23 @@ __global__ void __launch_bounds__(NT) k_fwd_planes(const T *__restrict__ xi, cx<
     bulk_commit();
     bulk_wait_all();
   }
+}
+
+// grid.x = F * nx planes
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_fwd_planes(const T *__restrict__ xi, cx<T> *__restrict__ spec,
+                                                   PlaneArgs a, const int *__restrict__ stop, int *err) {
+  if (stop && *stop) return;
+  fwd_planes_body<T, NT>(xi, spec, a, err, blockIdx.x);
+}
+
+// grid = (F * nx planes, instances of the group)
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_fwd_planes_tab(const InstPtrs *__restrict__ tab, PlaneArgs a) {
+  const InstPtrs &ip = tab[blockIdx.y];
+  if (ip.flags[0]) return;
+  const T *xi = static_cast<const T *>(ip.xi[ip.flags[4]]);
+  fwd_planes_body<T, NT>(xi, static_cast<cx<T> *>(ip.spec), a, ip.flags + 3, blockIdx.x);
 }
 
 // ------------------------------------------------------------ B(k) operator
@@ -340,10 +378,9 @@ __device__ __forceinline__ size_t nyq_index(const PencilArgs &a, int f, int sx, 
 }
 
 template <typename T, int NT>
-__global__ void __launch_bounds__(NT) k_xpencil(cx<T> *__restrict__ spec, PencilArgs a,
-                                                const int *__restrict__ stop) {
+__device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const PencilArgs &a, void *aux_ptr,
+                                             double *ppart) {
   using C = cx<T>;
-  if (stop && *stop) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nx = a.nx, F = a.F, cc = a.ccols, S = a.S, fst = a.fstride;
   C *buf = reinterpret_cast<C *>(smem_raw);   // [F][fstride >= nx*cc]
@@ -354,8 +391,8 @@ __global__ void __launch_bounds__(NT) k_xpencil(cx<T> *__restrict__ spec, Pencil
   const int cpr = (int)(cc * sizeof(C) / 16);    // 16-byte chunks per (field, x) row
   const int nchunks = F * nx * cpr;
   const FastDiv dc(cpr), dnx(nx);
-  C *caux = reinterpret_cast<C *>(a.aux);
-  if (a.mode == PASS_STEP) {
+  C *caux = reinterpret_cast<C *>(aux_ptr);
+  if (a.mode != PASS_SYNTH) {
     for (int q = threadIdx.x; q < nchunks; q += blockDim.x) {
       const int fx = dc.div(q), ch = q - fx * cpr;
       const int f = dnx.div(fx), x = fx - f * nx;
@@ -366,11 +403,11 @@ __global__ void __launch_bounds__(NT) k_xpencil(cx<T> *__restrict__ spec, Pencil
     for (int i = threadIdx.x; i < F * fst; i += blockDim.x) buf[i] = mk<C>((T)0, (T)0);
   }
   load_table(twx, a.tw_x, nx);
-  if (a.mode == PASS_STEP) cp_async_wait_all();
+  if (a.mode != PASS_SYNTH) cp_async_wait_all();
   __syncthreads();
 
   Batch gx{F * cc, cc, 1, fst, cc, true};
-  if (a.mode == PASS_STEP) fft_forward<MaxRadix<NT>::value>(buf, twx, a.px, gx);
+  if (a.mode != PASS_SYNTH) fft_forward<MaxRadix<NT>::value>(buf, twx, a.px, gx);
 
   double dsq = 0.0;
   for (int w = threadIdx.x; w < nx * cc; w += blockDim.x) {
@@ -436,6 +473,10 @@ __global__ void __launch_bounds__(NT) k_xpencil(cx<T> *__restrict__ spec, Pencil
         const C ei = mk<C>((T)0.5 * (P.y - Q.y), (T)-0.5 * (P.x - Q.x));
         if (a.imag == IMAG_FULL) {
           pk[(S + aa) * fs] = ei;
+        } else if (a.mode == PASS_ENERGY) {
+          // 1/2 <Im xi, (L xi)_i> from the Nyquist spectrum (Parseval; 1/N on the host)
+          const C xim = caux[a0 + aa * astride];
+          dsq += 0.5 * wgt * ((double)xim.x * (double)ei.x + (double)xim.y * (double)ei.y);
         } else {
           // Nyquist point: Im xi spectrum updated in k-space (no mask, no core force on Im xi)
           const C dlt = mk<C>(-cd * ei.x, -cd * ei.y);
@@ -462,7 +503,7 @@ __global__ void __launch_bounds__(NT) k_xpencil(cx<T> *__restrict__ spec, Pencil
     }
     for (int aa = 0; aa < S; ++aa) pk[aa * fs] = green_out<T>(g, aa, sr, Tp, zp);
   }
-  if (a.partials) block_sum2(dsq, 0.0, red, a.partials + 2 * blockIdx.x);
+  if (ppart) block_sum2(dsq, 0.0, red, ppart + 2 * blockIdx.x);
   __syncthreads();
 
   fft_inverse<MaxRadix<NT>::value>(buf, twx, a.px, gx);
@@ -474,6 +515,22 @@ __global__ void __launch_bounds__(NT) k_xpencil(cx<T> *__restrict__ spec, Pencil
     *dst = *reinterpret_cast<const float4 *>(reinterpret_cast<const char *>(buf + (size_t)f * fst + (size_t)x * cc) +
                                              16 * ch);
   }
+}
+
+// grid.x = ncols / ccols tiles
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_xpencil(cx<T> *__restrict__ spec, PencilArgs a,
+                                                const int *__restrict__ stop) {
+  if (stop && *stop) return;
+  xpencil_body<T, NT>(spec, a, a.aux, a.partials);
+}
+
+// grid = (tiles, instances of the group)
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_xpencil_tab(const InstPtrs *__restrict__ tab, PencilArgs a) {
+  const InstPtrs &ip = tab[blockIdx.y];
+  if (ip.flags[0]) return;
+  xpencil_body<T, NT>(static_cast<cx<T> *>(ip.spec), a, ip.aux, ip.ppart);
 }
 
 // ------------------------------------------------------------ core force
@@ -559,6 +616,32 @@ __device__ __forceinline__ T core_derivative(const Core &cm, T x, int a, size_t 
   }
 }
 
+// ------------------------------------------------------------ core energy
+// f(x) per site-slip whose derivative core_derivative evaluates (the reference
+// accumulates E_core but never reduces it, fft_fftw_slab.cpp:1399).
+template <typename T>
+__device__ __forceinline__ T core_energy_density(const Core &cm, T x, int a, size_t r, size_t N,
+                                                 const T *__restrict__ site) {
+  const T s1 = sinpi_t<T>(x), s2 = sinpi_t<T>((T)2 * x);
+  switch (cm.flag) {
+    case 1:
+    case 6:
+      return core_k<T>(cm, 10) * s1 * s1;
+    case 3:
+      return core_k<T>(cm, 10) * s1 * s1 + core_k<T>(cm, 11) * s2 * s2;
+    case 7:
+      return site[(size_t)a * N + r] * core_k<T>(cm, 10) * s1 * s1;
+    case 103: {
+      const T m = site[(size_t)a * N + r];
+      const T isf = core_k<T>(cm, 2) * m;
+      const T cn = core_k<T>(cm, 3) * m - isf * core_k<T>(cm, 4);
+      return isf * s1 * s1 + cn * s2 * s2;
+    }
+    default:
+      return (T)0;
+  }
+}
+
 // ------------------------------------------------------------ adjoint helpers
 // f''(x) and the derivatives of f'(x) with respect to the model's parameters
 // p0, p1 (sine: isf, usf; perfect / USFE: An, -; sine field: isf, usf;
@@ -620,19 +703,16 @@ __device__ __forceinline__ T update_one(const UpdateArgs &u, bool real_field, in
   return old - cd * el;
 }
 
-// grid.x = F * nx planes
 template <typename T, int NT>
-__global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spec, const T *__restrict__ xin,
-                                                   T *__restrict__ xout, PlaneArgs a, UpdateArgs u,
-                                                   double *__restrict__ partials) {
+__device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, const T *__restrict__ xin,
+                                                T *__restrict__ xout, const PlaneArgs &a, const UpdateArgs &u,
+                                                double *__restrict__ partials, size_t plane) {
   using C = cx<T>;
   using V = typename Vec<T>::type;
   constexpr int VN = Vec<T>::n;
-  if (u.stop && *u.stop) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const PlaneSmem<C> sm(smem_raw, a);
   const int ny = a.ny, nz = a.nz, nzh = a.nzh, nzp = a.nzp, M = a.M;
-  const size_t plane = blockIdx.x;
   if (threadIdx.x == 0) {
     mbar_init(sm.bar, 1);
     const uint32_t bytes = (uint32_t)((size_t)ny * nzp * sizeof(C));
@@ -698,6 +778,31 @@ __global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spe
       for (int q = 0; q < VN; ++q) e[q] *= invN;
       *reinterpret_cast<V *>(xout + off + y * nz + zq * VN) = *reinterpret_cast<V *>(e);
     }
+    return;
+  }
+  if (u.mode == PASS_ENERGY) {
+    // 1/2 xi . (L xi), f(Re xi) and -tau Re xi, summed over the plane (FP64)
+    const T *site = reinterpret_cast<const T *>(u.site);
+    const double tau = real_field ? u.tau[sys] : 0.0;
+    double e_el = 0.0, e_core = 0.0, e_app = 0.0;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int y = dv.div(i), zq = i - y * nvec;
+      const int idx = y * nz + zq * VN;
+      T xv[VN], e[VN];
+      *reinterpret_cast<V *>(xv) = *reinterpret_cast<const V *>(xin + off + idx);
+      *reinterpret_cast<V *>(e) = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzp + zq * VN);
+#pragma unroll
+      for (int q = 0; q < VN; ++q) {
+        const double x = (double)xv[q];
+        e_el += 0.5 * x * (double)(e[q] * invN);
+        if (real_field) {
+          e_core += (double)core_energy_density<T>(u.core, xv[q], sys, rbase + idx + q, N, site);
+          e_app -= tau * x;
+        }
+      }
+    }
+    block_sum2(e_el, e_core, sm.red, u.gpart + 4 * plane);
+    block_sum2(e_app, 0.0, sm.red, u.gpart + 4 * plane + 2);
     return;
   }
   if (u.mode == PASS_ADJOINT) {
@@ -775,6 +880,30 @@ __global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spe
   block_sum2(dsq, sum, sm.red, partials + 2 * plane);
 }
 
+// grid.x = F * nx planes
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spec, const T *__restrict__ xin,
+                                                   T *__restrict__ xout, PlaneArgs a, UpdateArgs u,
+                                                   double *__restrict__ partials) {
+  if (u.stop && *u.stop) return;
+  inv_update_body<T, NT>(spec, xin, xout, a, u, partials, blockIdx.x);
+}
+
+// grid = (F * nx planes, instances of the group); per-instance stress, mask,
+// GSFE field and buffers come from the table
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_inv_update_tab(const InstPtrs *__restrict__ tab, PlaneArgs a, UpdateArgs u) {
+  const InstPtrs &ip = tab[blockIdx.y];
+  if (ip.flags[0]) return;
+  const int cur = ip.flags[4];
+  u.tau = ip.tau;
+  u.mask = ip.mask;
+  u.site = ip.site;
+  u.err = ip.flags + 3;
+  inv_update_body<T, NT>(static_cast<const cx<T> *>(ip.spec), static_cast<const T *>(ip.xi[cur]),
+                         static_cast<T *>(ip.xi[cur ^ 1]), a, u, ip.partials, blockIdx.x);
+}
+
 // ------------------------------------------------------------ reduction
 // One block: Neumaier-compensated FP64 sums of the per-plane partials.
 // stats[step] = {xinorm, xiave}; sets *stop when 0 < tol and xinorm < tol;
@@ -824,6 +953,60 @@ static __global__ void k_finalize(const double *__restrict__ partials, int npart
   }
 }
 
+// One block per instance of a group: records {xinorm, xiave} at index
+// steps_done, counts the step, flips the buffer parity and sets the stop flag
+// when 0 < tol and xinorm < tol (solve_GL.cpp:137-141).
+static __global__ void k_finalize_tab(const InstPtrs *__restrict__ tab, int nparts, int nparts2, double scale2,
+                                      double tol) {
+  const InstPtrs &ip = tab[blockIdx.x];
+  int *flags = ip.flags;
+  if (flags[0]) return;
+  __shared__ double sh[4][1024];
+  const double *partials = ip.partials, *partials2 = ip.ppart;
+  double s0 = 0, c0 = 0, s1 = 0, c1 = 0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+    double v = partials[2 * i], t = s0 + v;
+    c0 += (fabs(s0) >= fabs(v)) ? (s0 - t) + v : (v - t) + s0;
+    s0 = t;
+    v = partials[2 * i + 1];
+    t = s1 + v;
+    c1 += (fabs(s1) >= fabs(v)) ? (s1 - t) + v : (v - t) + s1;
+    s1 = t;
+  }
+  if (partials2)
+    for (int i = threadIdx.x; i < nparts2; i += blockDim.x) {
+      double v = partials2[2 * i] * scale2, t = s0 + v;
+      c0 += (fabs(s0) >= fabs(v)) ? (s0 - t) + v : (v - t) + s0;
+      s0 = t;
+    }
+  sh[0][threadIdx.x] = s0; sh[1][threadIdx.x] = c0; sh[2][threadIdx.x] = s1; sh[3][threadIdx.x] = c1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a0 = 0, e0 = 0, a1 = 0, e1 = 0;
+    for (int i = 0; i < (int)blockDim.x; ++i) {
+      double v = sh[0][i], t = a0 + v;
+      e0 += (fabs(a0) >= fabs(v)) ? (a0 - t) + v : (v - t) + a0;
+      a0 = t;
+      e0 += sh[1][i];
+      v = sh[2][i];
+      t = a1 + v;
+      e1 += (fabs(a1) >= fabs(v)) ? (a1 - t) + v : (v - t) + a1;
+      a1 = t;
+      e1 += sh[3][i];
+    }
+    const double xinorm = sqrt(a0 + e0), xiave = a1 + e1;
+    const int k = flags[2];
+    if (k < ip.stats_cap) {
+      ip.stats[2 * k] = xinorm;
+      ip.stats[2 * k + 1] = xiave;
+    }
+    flags[2] = k + 1;
+    flags[4] ^= 1;
+    if (!isfinite(xinorm) || !isfinite(xiave)) flags[1] = 1;
+    if (tol > 0.0 && xinorm < tol) flags[0] = 1;
+  }
+}
+
 // ------------------------------------------------------------ stress state
 // sigma_rot and tau in FP64 exactly as rotate_stress + resolSS_Schmid
 // (fft_fftw_slab.cpp:242-274, 737-769); then optionally sigma += dsigma
@@ -861,6 +1044,36 @@ static __global__ void k_stress_state(double *sigma /*[9]*/, double *tau, Stress
   } else {
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) sigma[3 * i + j] = sigma[3 * i + j] + s.dsig[i][j];
+  }
+}
+
+// One block per instance: mode 0 = sigma_rot and tau from the current sigma,
+// clear the stop flag; mode 1 = sigma += dsigma (stored after sigma).
+static __global__ void k_stress_state_tab(const InstPtrs *__restrict__ tab, StressArgs s, int mode) {
+  if (threadIdx.x != 0) return;
+  const InstPtrs &ip = tab[blockIdx.x];
+  double *sigma = ip.sigma;
+  if (mode == 0) {
+    double sr[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        sr[i][j] = 0.0;
+        if (s.ortho) {
+          for (int k = 0; k < 3; ++k)
+            for (int l = 0; l < 3; ++l) sr[i][j] += s.prim[i][k] * sigma[3 * k + l] * s.invprim[l][j];
+        } else {
+          sr[i][j] = sigma[3 * i + j];
+        }
+      }
+    for (int a = 0; a < s.S; ++a) {
+      double t = 0.0;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) t = t + (sr[i][j] * s.xn[a][j] * s.xb[a][i]) / s.dslip;
+      ip.tau[a] = t;
+    }
+    ip.flags[0] = 0;
+  } else {
+    for (int i = 0; i < 9; ++i) sigma[i] = sigma[i] + sigma[9 + i];
   }
 }
 

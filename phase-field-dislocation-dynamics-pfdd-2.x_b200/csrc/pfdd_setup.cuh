@@ -153,11 +153,18 @@ inline bool build_core(const pfdd_instance_desc &d, Core &c) {
     default:
       return false;
   }
-  // derivatives of f' with respect to the GSFE parameters (adjoint step)
+  // derivatives of f' with respect to the GSFE parameters (adjoint step) and
+  // the amplitudes of f itself (energy)
   if (d.core_flag != PFDD_CORE_EXTENDED && d.core_flag != PFDD_CORE_PYRII) {
     c.k[7] = M_PI / s;
     c.k[8] = M_PI / (s * s);
     c.k[9] = 2.0 * M_PI / s;
+    if (d.core_flag == PFDD_CORE_PERFECT || d.core_flag == PFDD_CORE_USFE_ANGLE) c.k[10] = d.An / s;
+    if (d.core_flag == PFDD_CORE_SINE) {
+      c.k[10] = d.isf / s;
+      c.k[11] = (d.usf - (d.isf / s) / 2.0) / s;
+    }
+    if (d.core_flag == PFDD_CORE_MPEA) c.k[10] = 1.0 / s;
   }
   for (int i = 0; i < 12; ++i) c.kf[i] = (float)c.k[i];
   return true;

@@ -142,12 +142,12 @@ def desc_from_workload(w, core_flag=None, An=None):
 class Stepper:
     """Owns one pfdd_gpu handle (one or more instances)."""
 
-    def __init__(self, descs, precision=FP64, imag_mode=IMAG_AUTO, device=0, keep=()):
+    def __init__(self, descs, precision=FP64, imag_mode=IMAG_AUTO, device=0, keep=(), use_graphs=True):
         lib = load()
         self._lib = lib
         self._keep = list(keep)   # host arrays referenced by descriptors during create
         arr = (InstanceDesc * len(descs))(*descs)
-        opt = Options(precision, imag_mode, device, 1, 1)
+        opt = Options(precision, imag_mode, device, 1 if use_graphs else 0, 1)
         h = ctypes.c_void_p()
         st = lib.pfdd_gpu_create(arr, len(descs), ctypes.byref(opt), ctypes.byref(h))
         if st != PFDD_OK:
@@ -157,7 +157,7 @@ class Stepper:
         self.n = len(descs)
 
     @classmethod
-    def from_workloads(cls, workloads, precision=FP64, imag_mode=IMAG_AUTO, device=0):
+    def from_workloads(cls, workloads, precision=FP64, imag_mode=IMAG_AUTO, device=0, use_graphs=True):
         descs, keep = [], []
         for w in workloads:
             d = desc_from_workload(w)
@@ -170,7 +170,7 @@ class Stepper:
                 keep.append(m)
                 d.xo = _dp(m)
             descs.append(d)
-        st = cls(descs, precision, imag_mode, device, keep)
+        st = cls(descs, precision, imag_mode, device, keep, use_graphs)
         st._keep = []
         return st
 

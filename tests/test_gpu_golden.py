@@ -23,7 +23,7 @@ def test_gpu_reproduces_reference_fixture(name):
     ref = fx["xi"]
     assert np.abs(re - ref.real).max() <= 1e-10
     assert np.abs(im - ref.imag).max() <= 1e-10
-    last = int(fx["steps"])
-    np.testing.assert_allclose(ha, fx["xiave"][-last:], rtol=1e-9, atol=1e-9)
+    # the history covers every stress state of the call
+    np.testing.assert_allclose(ha, fx["xiave"], rtol=1e-9, atol=1e-9)
     if w.xo is None:
-        np.testing.assert_allclose(hn, fx["xinorm"][-last:], rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(hn, fx["xinorm"], rtol=1e-9, atol=1e-12)
