@@ -51,7 +51,7 @@ template <> struct Threads<double> { static constexpr int plane = 256, pencil = 
 struct Instance {
   pfdd_instance_desc d;
   int S, F, imag;
-  int nx, ny, nz, nzh, nzp, M;
+  int nx, ny, nz, nzh, nzp, nzs, M;
   size_t N;
   FftPlan px, py, pz;
   int ccols, fstride, ntiles;
@@ -212,7 +212,7 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   }
 
   // shared-memory budgets
-  I.smem_plane = PlaneSmem<C>::bytes(I.ny, I.nzp, I.M);
+  I.smem_plane = PlaneSmem<C>::bytes(I.ny, I.nzs, I.M);
   I.smem_update = I.smem_plane;
   const size_t limit = 227 * 1024;
   if (I.smem_update > limit)
@@ -258,7 +258,7 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
 template <typename T>
 void fill_plane_args(const Instance &I, PlaneArgs &pa) {
   pa.py = I.py; pa.pz = I.pz;
-  pa.nx = I.nx; pa.ny = I.ny; pa.nz = I.nz; pa.nzh = I.nzh; pa.nzp = I.nzp; pa.M = I.M;
+  pa.nx = I.nx; pa.ny = I.ny; pa.nz = I.nz; pa.nzh = I.nzh; pa.nzp = I.nzp; pa.nzs = I.nzs; pa.M = I.M;
   pa.S = I.S; pa.F = I.F;
   pa.tw_y = I.tw_y.p; pa.tw_z = I.tw_z.p; pa.tw_r = I.tw_r.p;
   pa.posM = I.posM;
@@ -984,6 +984,15 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
     I->nzh = I->M + 1;
     // spectrum rows padded to whole 16-byte units so a plane moves in one bulk copy
     I->nzp = (o.precision == PFDD_FP32) ? ((I->nzh + 1) & ~1) : I->nzh;
+    // shared-memory row stride: consecutive rows start 8 words apart in the
+    // 32 banks (FP32: 2*nzs = 8 mod 32; FP64: nzs = 4 mod 8 16-byte units)
+    I->nzs = I->nzp;
+    if (o.precision == PFDD_FP32)
+      while ((2 * I->nzs) % 32 != 8) I->nzs += 2;
+    else
+      while (I->nzs % 8 != 4) ++I->nzs;
+    // store spectrum rows with the same stride, so a plane moves in one bulk copy
+    I->nzp = I->nzs;
     I->N = (size_t)I->nx * I->ny * I->nz;
     const int maxr = (o.precision == PFDD_FP32) ? MaxRadix<Threads<float>::plane>::value
                                                 : MaxRadix<Threads<double>::plane>::value;

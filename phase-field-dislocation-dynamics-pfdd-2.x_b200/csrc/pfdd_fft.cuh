@@ -202,8 +202,20 @@ __device__ __forceinline__ void fft_stage(C *__restrict__ x, const C *__restrict
     C *base = x + dI.mod(b) * g.bs_in + dI.div(b) * g.bs_out + (blk * L + j) * g.es;
     const int st = Lr * g.es;
     C v[R];
+    // contiguous elements (last stage along a unit-stride axis): 16-byte vectors
+    constexpr bool VEC = sizeof(C) == 8 && (R % 2 == 0);
+    const bool vec = VEC && st == 1;
+    if (vec) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = base[r * st];
+      for (int r = 0; r < R; r += 2) {
+        const float4 q = reinterpret_cast<const float4 *>(base)[r / 2];
+        v[r] = mk<C>(q.x, q.y);
+        v[r + 1] = mk<C>(q.z, q.w);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = base[r * st];
+    }
     if constexpr (!INV) {
       dft<R, -1>(v);
       if (j) apply_twiddles<R, false>(v, tw, j * twstep);
@@ -211,8 +223,14 @@ __device__ __forceinline__ void fft_stage(C *__restrict__ x, const C *__restrict
       if (j) apply_twiddles<R, true>(v, tw, j * twstep);
       dft<R, 1>(v);
     }
+    if (vec) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) base[r * st] = v[r];
+      for (int r = 0; r < R; r += 2)
+        reinterpret_cast<float4 *>(base)[r / 2] = make_float4(v[r].x, v[r].y, v[r + 1].x, v[r + 1].y);
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) base[r * st] = v[r];
+    }
   }
 }
 
@@ -292,7 +310,9 @@ __device__ __forceinline__ void bulk_s2g(void *dst_gmem, const void *src_smem, u
                : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// waits until the pending bulk stores have read their shared-memory source;
+// the global writes complete before the grid does
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }

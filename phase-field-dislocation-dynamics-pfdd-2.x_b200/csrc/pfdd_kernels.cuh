@@ -76,6 +76,7 @@ enum { PASS_STEP = 0, PASS_SYNTH = 1, PASS_ADJOINT = 2, PASS_ENERGY = 3 };
 struct PlaneArgs {
   FftPlan py, pz;
   int nx, ny, nz, nzh, nzp, M;   // nzp: complex entries per stored spectrum row (>= nzh, 16-byte rows)
+  int nzs;                       // complex entries per shared-memory row (>= nzp, chosen against bank conflicts)
   int S, F;                   // slip systems; fields in flight (S, or 2S with Im xi)
   const void *tw_y, *tw_z, *tw_r;   // W_ny^m, W_M^m, W_nz^k tables in compute precision
   const int16_t *posM;        // position of z-frequency k (< M) after the M-point transform
@@ -181,7 +182,7 @@ __device__ __forceinline__ void load_table(C *dst, const void *src, int n) {
 }
 
 // ------------------------------------------------------------ P1
-// Shared memory of a plane kernel: the ny x nzp complex plane, then the y, z
+// Shared memory of a plane kernel: the ny x nzs complex plane, then the y, z
 // and real-to-complex twiddle tables, the z position table and one mbarrier.
 template <typename C> struct PlaneSmem {
   C *buf, *twy, *twz, *twr;
@@ -190,15 +191,15 @@ template <typename C> struct PlaneSmem {
   double *red;
   __device__ PlaneSmem(unsigned char *raw, const PlaneArgs &a) {
     buf = reinterpret_cast<C *>(raw);
-    twy = buf + (size_t)a.ny * a.nzp;
+    twy = buf + (size_t)a.ny * a.nzs;
     twz = twy + a.ny;
     twr = twz + a.M;
     pos = reinterpret_cast<int *>(twr + a.M);
     bar = reinterpret_cast<uint64_t *>(pos + ((a.M + 1) & ~1));
     red = reinterpret_cast<double *>(bar + 1);
   }
-  static size_t bytes(int ny, int nzp, int M) {
-    return ((size_t)ny * nzp + ny + 2 * (size_t)M) * sizeof(C) + (size_t)((M + 1) & ~1) * 4 + 8 + 64 * 8;
+  static size_t bytes(int ny, int nzs, int M) {
+    return ((size_t)ny * nzs + ny + 2 * (size_t)M) * sizeof(C) + (size_t)((M + 1) & ~1) * 4 + 8 + 64 * 8;
   }
 };
 
@@ -216,17 +217,17 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
   using C = cx<T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const PlaneSmem<C> sm(smem_raw, a);
-  const int ny = a.ny, nz = a.nz, nzh = a.nzh, nzp = a.nzp, M = a.M;
+  const int ny = a.ny, nz = a.nz, nzh = a.nzh, nzp = a.nzp, nzs = a.nzs, M = a.M;
   if (threadIdx.x == 0) mbar_init(sm.bar, 1);
   __syncthreads();
-  // rows of the real plane -> shared rows of stride 2*nzp reals (bulk copies)
+  // rows of the real plane -> shared rows of stride 2*nzs reals (bulk copies)
   if (threadIdx.x < 32) {
     if (threadIdx.x == 0) mbar_expect_tx(sm.bar, (uint32_t)(ny * nz * sizeof(T)));
     __syncwarp();
     const T *src = xi + plane * (size_t)ny * nz;
     T *bufr = reinterpret_cast<T *>(sm.buf);
     for (int y = threadIdx.x; y < ny; y += 32)
-      bulk_g2s(bufr + (size_t)y * 2 * nzp, src + (size_t)y * nz, (uint32_t)(nz * sizeof(T)), sm.bar);
+      bulk_g2s(bufr + (size_t)y * 2 * nzs, src + (size_t)y * nz, (uint32_t)(nz * sizeof(T)), sm.bar);
   }
   load_plane_tables(sm, a);
   const bool ok = __syncthreads_and(mbar_wait(sm.bar, 0));
@@ -239,14 +240,14 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
   const int *pos = sm.pos;
 
   // z: M-point complex transform of the packed rows
-  Batch gz{ny, ny, nzp, 0, 1, false};
+  Batch gz{ny, ny, nzs, 0, 1, false};
   fft_forward<MaxRadix<NT>::value>(buf, sm.twz, a.pz, gz);
 
   // real-to-complex unpacking, pairs (k, M-k); X[M] goes to slot M
   const int half = M / 2 + 1;
   for (int w = threadIdx.x; w < ny * half; w += blockDim.x) {
     const int y = w / half, k = w - y * half;
-    C *row = buf + (size_t)y * nzp;
+    C *row = buf + (size_t)y * nzs;
     if (k == 0) {
       C z0 = row[pos[0]];
       row[pos[0]] = mk<C>(z0.x + z0.y, (T)0);
@@ -266,14 +267,22 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
   __syncthreads();
 
   // y: ny-point transforms over the nzh slot columns
-  Batch gy{nzh, nzh, 1, 0, nzp, true};
+  Batch gy{nzh, nzh, 1, 0, nzs, true};
   fft_forward<MaxRadix<NT>::value>(buf, sm.twy, a.py, gy);
 
-  // whole plane -> spectrum with one bulk store
+  // rows -> spectrum rows of nzp entries (bulk stores, one warp)
   fence_proxy_async();
   __syncthreads();
-  if (threadIdx.x == 0) {
-    bulk_s2g(spec + plane * (size_t)ny * nzp, buf, (uint32_t)((size_t)ny * nzp * sizeof(C)));
+  if (nzs == nzp) {
+    if (threadIdx.x == 0) {  // rows are contiguous in both: one bulk copy
+      bulk_s2g(spec + plane * (size_t)ny * nzp, buf, (uint32_t)((size_t)ny * nzp * sizeof(C)));
+      bulk_commit();
+      bulk_wait_all();
+    }
+  } else if (threadIdx.x < 32) {
+    C *dst = spec + plane * (size_t)ny * nzp;
+    for (int y = threadIdx.x; y < ny; y += 32)
+      bulk_s2g(dst + (size_t)y * nzp, buf + (size_t)y * nzs, (uint32_t)(nzp * sizeof(C)));
     bulk_commit();
     bulk_wait_all();
   }
@@ -703,34 +712,46 @@ __device__ __forceinline__ T update_one(const UpdateArgs &u, bool real_field, in
   return old - cd * el;
 }
 
+// Per-instance pointers travel as arguments so the constant parameter block
+// (PlaneArgs, UpdateArgs) is read in place and never copied.
 template <typename T, int NT>
 __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, const T *__restrict__ xin,
                                                 T *__restrict__ xout, const PlaneArgs &a, const UpdateArgs &u,
-                                                double *__restrict__ partials, size_t plane) {
+                                                double *__restrict__ partials, size_t plane,
+                                                const double *__restrict__ tau_p, const uint8_t *__restrict__ mask,
+                                                const void *site_p, int *err) {
   using C = cx<T>;
   using V = typename Vec<T>::type;
   constexpr int VN = Vec<T>::n;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const PlaneSmem<C> sm(smem_raw, a);
-  const int ny = a.ny, nz = a.nz, nzh = a.nzh, nzp = a.nzp, M = a.M;
-  if (threadIdx.x == 0) {
-    mbar_init(sm.bar, 1);
-    const uint32_t bytes = (uint32_t)((size_t)ny * nzp * sizeof(C));
-    mbar_expect_tx(sm.bar, bytes);
-    bulk_g2s(sm.buf, spec + plane * (size_t)ny * nzp, bytes, sm.bar);
+  const int ny = a.ny, nz = a.nz, nzh = a.nzh, nzp = a.nzp, nzs = a.nzs, M = a.M;
+  if (threadIdx.x == 0) mbar_init(sm.bar, 1);
+  __syncthreads();
+  // spectrum rows of nzp entries -> shared rows of nzs (bulk copies, one warp)
+  if (threadIdx.x < 32) {
+    if (threadIdx.x == 0) mbar_expect_tx(sm.bar, (uint32_t)((size_t)ny * nzp * sizeof(C)));
+    __syncwarp();
+    const C *src = spec + plane * (size_t)ny * nzp;
+    if (nzs == nzp) {
+      if (threadIdx.x == 0) bulk_g2s(sm.buf, src, (uint32_t)((size_t)ny * nzp * sizeof(C)), sm.bar);
+    } else {
+      for (int y = threadIdx.x; y < ny; y += 32)
+        bulk_g2s(sm.buf + (size_t)y * nzs, src + (size_t)y * nzp, (uint32_t)(nzp * sizeof(C)), sm.bar);
+    }
   }
   load_plane_tables(sm, a);
   __syncthreads();
   const bool ok = __syncthreads_and(mbar_wait(sm.bar, 0));
   if (!ok) {
-    if (threadIdx.x == 0) atomicExch(u.err, 1);
+    if (threadIdx.x == 0) atomicExch(err, 1);
     return;
   }
   C *buf = sm.buf;
   const C *twr = sm.twr;
   const int *pos = sm.pos;
 
-  Batch gy{nzh, nzh, 1, 0, nzp, true};
+  Batch gy{nzh, nzh, 1, 0, nzs, true};
   fft_inverse<MaxRadix<NT>::value>(buf, sm.twy, a.py, gy);
 
   // complex-to-real packing: Zin[k] = A + i w D, Zin[M-k] = conj(A - i w D),
@@ -738,7 +759,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   const int half = M / 2 + 1;
   for (int w = threadIdx.x; w < ny * half; w += blockDim.x) {
     const int y = w / half, k = w - y * half;
-    C *row = buf + (size_t)y * nzp;
+    C *row = buf + (size_t)y * nzs;
     const int pk = pos[k];
     const int pm = (k == 0) ? -1 : pos[M - k];
     const C xk = row[pk];
@@ -752,7 +773,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   }
   __syncthreads();
 
-  Batch gz{ny, ny, nzp, 0, 1, false};
+  Batch gz{ny, ny, nzs, 0, 1, false};
   fft_inverse<MaxRadix<NT>::value>(buf, sm.twz, a.pz, gz);
 
   // fused GSFE force + applied stress + masked explicit Euler update,
@@ -773,7 +794,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int y = dv.div(i), zq = i - y * nvec;
       T e[VN];
-      *reinterpret_cast<V *>(e) = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzp + zq * VN);
+      *reinterpret_cast<V *>(e) = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzs + zq * VN);
 #pragma unroll
       for (int q = 0; q < VN; ++q) e[q] *= invN;
       *reinterpret_cast<V *>(xout + off + y * nz + zq * VN) = *reinterpret_cast<V *>(e);
@@ -782,15 +803,15 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   }
   if (u.mode == PASS_ENERGY) {
     // 1/2 xi . (L xi), f(Re xi) and -tau Re xi, summed over the plane (FP64)
-    const T *site = reinterpret_cast<const T *>(u.site);
-    const double tau = real_field ? u.tau[sys] : 0.0;
+    const T *site = reinterpret_cast<const T *>(site_p);
+    const double tau = real_field ? tau_p[sys] : 0.0;
     double e_el = 0.0, e_core = 0.0, e_app = 0.0;
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int y = dv.div(i), zq = i - y * nvec;
       const int idx = y * nz + zq * VN;
       T xv[VN], e[VN];
       *reinterpret_cast<V *>(xv) = *reinterpret_cast<const V *>(xin + off + idx);
-      *reinterpret_cast<V *>(e) = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzp + zq * VN);
+      *reinterpret_cast<V *>(e) = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzs + zq * VN);
 #pragma unroll
       for (int q = 0; q < VN; ++q) {
         const double x = (double)xv[q];
@@ -809,7 +830,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
     // lam_n = lam_{n+1} - cd (L lam + f''(xi_n) lam_{n+1}) on unmasked sites
     // (the elastic operator is self-adjoint; tau is constant and drops out);
     // parameter gradients use lam_{n+1} and xi_n on the same sites.
-    const T *site = reinterpret_cast<const T *>(u.site);
+    const T *site = reinterpret_cast<const T *>(site_p);
     const T *xf = reinterpret_cast<const T *>(u.xfwd);
     const T cd = (T)u.cd;
     double g0 = 0.0, g1 = 0.0, gl = 0.0;
@@ -818,11 +839,11 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
       const int idx = y * nz + zq * VN;
       T lam[VN], e[VN], nv[VN];
       *reinterpret_cast<V *>(lam) = *reinterpret_cast<const V *>(xin + off + idx);
-      *reinterpret_cast<V *>(e) = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzp + zq * VN);
+      *reinterpret_cast<V *>(e) = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzs + zq * VN);
 #pragma unroll
       for (int q = 0; q < VN; ++q) {
         const size_t r = rbase + idx + q;
-        const bool frozen = u.mask && u.mask[(size_t)sys * N + r];
+        const bool frozen = mask && mask[(size_t)sys * N + r];
         if (real_field) {
           T d2, dp0, dp1;
           core_adjoint_terms<T>(u.core, xf[(size_t)sys * N + r], sys, r, N, site, d2, dp0, dp1);
@@ -843,8 +864,8 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
     return;
   }
   // update pass only: tau, mask and per-site GSFE are read from here on
-  const T tau = real_field ? (T)u.tau[sys] : (T)0;
-  const T *site = reinterpret_cast<const T *>(u.site);
+  const T tau = real_field ? (T)tau_p[sys] : (T)0;
+  const T *site = reinterpret_cast<const T *>(site_p);
   double dsq = 0.0, sum = 0.0;
   for (int i0 = threadIdx.x; i0 < total; i0 += 2 * blockDim.x) {
     V oldv[2], elv[2];
@@ -857,7 +878,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
       const int y = dv.div(on[h] ? i : 0), zq = (on[h] ? i : 0) - y * nvec;
       idx[h] = y * nz + zq * VN;
       oldv[h] = *reinterpret_cast<const V *>(xin + off + idx[h]);
-      elv[h] = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzp + zq * VN);
+      elv[h] = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzs + zq * VN);
     }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -869,7 +890,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
       for (int q = 0; q < VN; ++q) {
         const size_t r = rbase + idx[h] + q;
         nv[q] = update_one<T>(u, real_field, sys, e[q] * invN, o[q], tau, r, N, xin, site);
-        if (u.mask && u.mask[(size_t)sys * N + r]) nv[q] = o[q];
+        if (mask && mask[(size_t)sys * N + r]) nv[q] = o[q];
         const double d = (double)nv[q] - (double)o[q];
         dsq += d * d;
         if (real_field) sum += (double)nv[q];
@@ -886,7 +907,7 @@ __global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spe
                                                    T *__restrict__ xout, PlaneArgs a, UpdateArgs u,
                                                    double *__restrict__ partials) {
   if (u.stop && *u.stop) return;
-  inv_update_body<T, NT>(spec, xin, xout, a, u, partials, blockIdx.x);
+  inv_update_body<T, NT>(spec, xin, xout, a, u, partials, blockIdx.x, u.tau, u.mask, u.site, u.err);
 }
 
 // grid = (F * nx planes, instances of the group); per-instance stress, mask,
@@ -896,12 +917,9 @@ __global__ void __launch_bounds__(NT) k_inv_update_tab(const InstPtrs *__restric
   const InstPtrs &ip = tab[blockIdx.y];
   if (ip.flags[0]) return;
   const int cur = ip.flags[4];
-  u.tau = ip.tau;
-  u.mask = ip.mask;
-  u.site = ip.site;
-  u.err = ip.flags + 3;
   inv_update_body<T, NT>(static_cast<const cx<T> *>(ip.spec), static_cast<const T *>(ip.xi[cur]),
-                         static_cast<T *>(ip.xi[cur ^ 1]), a, u, ip.partials, blockIdx.x);
+                         static_cast<T *>(ip.xi[cur ^ 1]), a, u, ip.partials, blockIdx.x, ip.tau, ip.mask, ip.site,
+                         ip.flags + 3);
 }
 
 // ------------------------------------------------------------ reduction

@@ -204,7 +204,7 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   const C *tw_x = tw, *tw_y = tw + nx, *tw_z = tw + nx + ny, *tw_r = tw + nx + ny + M;
   PlaneArgs pa;
   pa.py = py; pa.pz = pz;
-  pa.nx = nx; pa.ny = ny; pa.nz = nz; pa.nzh = nzh; pa.nzp = nzp; pa.M = M;
+  pa.nx = nx; pa.ny = ny; pa.nz = nz; pa.nzh = nzh; pa.nzp = nzp; pa.nzs = nzp; pa.M = M;
   pa.S = S; pa.F = F;
   pa.tw_y = tw_y; pa.tw_z = tw_z; pa.tw_r = tw_r;
   pa.posM = t_posM - htab + tab;
