@@ -8,9 +8,11 @@
 // per (step count, buffer parity) and replayed.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -45,8 +47,9 @@ struct DevBuf {
 };
 
 template <typename T> struct Threads;
-template <> struct Threads<float> { static constexpr int plane = 512, pencil = 512; };
-template <> struct Threads<double> { static constexpr int plane = 256, pencil = 256; };
+// plane: whole-plane P1/P3 CTAs; half: each CTA of a split (2-CTA cluster) plane
+template <> struct Threads<float> { static constexpr int plane = 512, half = 256, pencil = 512; };
+template <> struct Threads<double> { static constexpr int plane = 256, half = 256, pencil = 256; };
 
 struct Instance {
   pfdd_instance_desc d;
@@ -56,6 +59,7 @@ struct Instance {
   FftPlan px, py, pz;
   int ccols, fstride, ntiles;
   int sx_n, sy_n;
+  bool split = false;  // P1/P3 planes on 2-CTA clusters, half the rows per CTA
   size_t smem_plane, smem_update, smem_pencil;
   DevBuf aux;          // Nyquist spectrum of Im xi (IMAG_NYQ)
   DevBuf ppart;        // per-tile partial sums of P2
@@ -134,9 +138,7 @@ pfdd_status fail(pfdd_gpu *h, pfdd_status code, const char *fmt, ...) {
 template <typename T> size_t csize() { return sizeof(cx<T>); }
 
 template <typename T>
-pfdd_status upload_twiddles(pfdd_gpu *h, DevBuf &dst, int n, int count) {
-  std::vector<double> tw;
-  twiddles(n, count, tw);
+pfdd_status upload_table(pfdd_gpu *h, DevBuf &dst, const std::vector<double> &tw) {
   std::vector<T> t(tw.size());
   for (size_t i = 0; i < tw.size(); ++i) t[i] = (T)tw[i];
   CUDA_TRY(h, dst.alloc(t.size() * sizeof(T)));
@@ -146,12 +148,28 @@ pfdd_status upload_twiddles(pfdd_gpu *h, DevBuf &dst, int n, int count) {
 }
 
 template <typename T>
+pfdd_status upload_twiddles(pfdd_gpu *h, DevBuf &dst, int n, int count) {
+  std::vector<double> tw;
+  twiddles(n, count, tw);
+  return upload_table<T>(h, dst, tw);
+}
+
+template <typename T>
 pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   const pfdd_instance_desc &d = I.d;
   using C = cx<T>;
   pfdd_status st;
   if ((st = upload_twiddles<T>(h, I.tw_x, I.nx, I.nx))) return st;
-  if ((st = upload_twiddles<T>(h, I.tw_y, I.ny, I.ny))) return st;
+  if (I.split) {
+    // W_ny^m (m < ny/2) of the cross-CTA stage, then W_{ny/2}^m of the local stages
+    std::vector<double> tw, twh;
+    twiddles(I.ny, I.ny / 2, tw);
+    twiddles(I.ny / 2, I.ny / 2, twh);
+    tw.insert(tw.end(), twh.begin(), twh.end());
+    if ((st = upload_table<T>(h, I.tw_y, tw))) return st;
+  } else if ((st = upload_twiddles<T>(h, I.tw_y, I.ny, I.ny))) {
+    return st;
+  }
   if ((st = upload_twiddles<T>(h, I.tw_z, I.M, I.M))) return st;
   if ((st = upload_twiddles<T>(h, I.tw_r, I.nz, I.M))) return st;
 
@@ -161,11 +179,23 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   int16_t *t_posM = tab.data(), *t_kx = t_posM + I.M, *t_ky = t_kx + I.nx, *t_kz = t_ky + I.ny;
   for (int k = 0; k < I.M; ++k) t_posM[k] = (int16_t)pz[k];
   for (int k = 0; k < I.nx; ++k) t_kx[px[k]] = (int16_t)k;
-  for (int k = 0; k < I.ny; ++k) t_ky[py[k]] = (int16_t)k;
+  if (I.split) {
+    // rank r of a split plane holds ky = r + 2 k at the slots of the ny/2 plan
+    const int nyh = I.ny / 2;
+    for (int r = 0; r < 2; ++r)
+      for (int k = 0; k < nyh; ++k) t_ky[r * nyh + py[k]] = (int16_t)(r + 2 * k);
+  } else {
+    for (int k = 0; k < I.ny; ++k) t_ky[py[k]] = (int16_t)k;
+  }
   for (int k = 0; k < I.M; ++k) t_kz[pz[k]] = (int16_t)k;
   t_kz[I.M] = (int16_t)I.M;
   I.sx_n = px[I.nx / 2];
-  I.sy_n = py[I.ny / 2];
+  if (I.split) {
+    const int r = (I.ny / 2) % 2;
+    I.sy_n = r * (I.ny / 2) + py[(I.ny / 2 - r) / 2];
+  } else {
+    I.sy_n = py[I.ny / 2];
+  }
   CUDA_TRY(h, I.tab16.alloc(tab.size() * sizeof(int16_t)));
   CUDA_TRY(h, cudaMemcpy(I.tab16.p, tab.data(), tab.size() * sizeof(int16_t), cudaMemcpyHostToDevice));
   h->device_bytes += I.tab16.bytes;
@@ -212,7 +242,7 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   }
 
   // shared-memory budgets
-  I.smem_plane = PlaneSmem<C>::bytes(I.ny, I.nzs, I.M);
+  I.smem_plane = PlaneSmem<C>::bytes(I.split ? I.ny / 2 : I.ny, I.ny, I.nzs, I.M);
   I.smem_update = I.smem_plane;
   const size_t limit = 227 * 1024;
   if (I.smem_update > limit)
@@ -266,14 +296,74 @@ void fill_plane_args(const Instance &I, PlaneArgs &pa) {
 
 template <typename T>
 pfdd_status set_smem_attrs(pfdd_gpu *h, size_t plane, size_t upd, size_t pencil) {
-  constexpr int NP = Threads<T>::plane, NC = Threads<T>::pencil;
-  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_xpencil<T, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pencil));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes_tab<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update_tab<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_xpencil_tab<T, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pencil));
+  constexpr int NP = Threads<T>::plane, NH = Threads<T>::half, NC = Threads<T>::pencil;
+  const auto A = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes<T, NP, false>, A, (int)plane));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes<T, NH, true>, A, (int)plane));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update<T, NP, false>, A, (int)upd));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update<T, NH, true>, A, (int)upd));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_xpencil<T, NC>, A, (int)pencil));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes_tab<T, NP, false>, A, (int)plane));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes_tab<T, NH, true>, A, (int)plane));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update_tab<T, NP, false>, A, (int)upd));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update_tab<T, NH, true>, A, (int)upd));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_xpencil_tab<T, NC>, A, (int)pencil));
   return PFDD_OK;
+}
+
+// Launch with an optional 2-CTA cluster (split planes).
+template <typename K, typename... Args>
+void launch_pair(K kernel, dim3 grid, int nt, size_t smem, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(nt, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// P1 of one instance (grid.x = planes) or of a group (grid.y = instances)
+template <typename T>
+void launch_fwd(const Instance &I, cudaStream_t st, const T *xin, cx<T> *spec, const PlaneArgs &pa,
+                const int *stop, int *err) {
+  constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
+  const unsigned planes = (unsigned)(I.F * I.nx);
+  if (I.split) launch_pair(k_fwd_planes<T, NH, true>, dim3(2 * planes), NH, I.smem_plane, st, xin, spec, pa, stop, err);
+  else k_fwd_planes<T, NP, false><<<planes, NP, I.smem_plane, st>>>(xin, spec, pa, stop, err);
+}
+
+template <typename T>
+void launch_fwd_tab(const Instance &L, unsigned B, cudaStream_t st, const InstPtrs *tab, const PlaneArgs &pa) {
+  constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
+  const unsigned planes = (unsigned)(L.F * L.nx);
+  if (L.split) launch_pair(k_fwd_planes_tab<T, NH, true>, dim3(2 * planes, B), NH, L.smem_plane, st, tab, pa);
+  else k_fwd_planes_tab<T, NP, false><<<dim3(planes, B), NP, L.smem_plane, st>>>(tab, pa);
+}
+
+// P3 of one instance (any pass) or of a group (GL step)
+template <typename T>
+void launch_inv(const Instance &I, unsigned planes, cudaStream_t st, const cx<T> *spec, const T *xin, T *xout,
+                const PlaneArgs &pa, const UpdateArgs &ua, double *partials) {
+  constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
+  if (I.split)
+    launch_pair(k_inv_update<T, NH, true>, dim3(2 * planes), NH, I.smem_update, st, spec, xin, xout, pa, ua, partials);
+  else k_inv_update<T, NP, false><<<planes, NP, I.smem_update, st>>>(spec, xin, xout, pa, ua, partials);
+}
+
+template <typename T>
+void launch_inv_tab(const Instance &L, unsigned B, cudaStream_t st, const InstPtrs *tab, const PlaneArgs &pa,
+                    const UpdateArgs &ua) {
+  constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
+  const unsigned planes = (unsigned)(L.F * L.nx);
+  if (L.split) launch_pair(k_inv_update_tab<T, NH, true>, dim3(2 * planes, B), NH, L.smem_update, st, tab, pa, ua);
+  else k_inv_update_tab<T, NP, false><<<dim3(planes, B), NP, L.smem_update, st>>>(tab, pa, ua);
 }
 
 // Enqueue one GL iteration of one instance; `step` indexes the stats record.
@@ -298,9 +388,9 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   T *xout = adj ? static_cast<T *>(adj->lam_out) : I.xi[I.cur ^ 1].as<T>();
   cx<T> *spec = I.spec.as<cx<T>>();
   const int planes = I.F * I.nx;
-  constexpr int NP = Threads<T>::plane, NC = Threads<T>::pencil;
+  constexpr int NC = Threads<T>::pencil;
   if (ev) cudaEventRecord(ev[0], st);
-  k_fwd_planes<T, NP><<<planes, NP, I.smem_plane, st>>>(xin, spec, pa, flags, flags + 3);
+  launch_fwd<T>(I, st, xin, spec, pa, flags, flags + 3);
   if (ev) cudaEventRecord(ev[1], st);
   PencilArgs pe;
   pe.px = I.px;
@@ -332,7 +422,7 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   ua.mode = adj ? PASS_ADJOINT : PASS_STEP;
   ua.xfwd = adj ? adj->xfwd : nullptr;
   ua.gpart = adj ? adj->gpart : nullptr;
-  k_inv_update<T, NP><<<planes, NP, I.smem_update, st>>>(spec, xin, xout, pa, ua, I.partials.as<double>());
+  launch_inv<T>(I, planes, st, spec, xin, xout, pa, ua, I.partials.as<double>());
   if (ev) cudaEventRecord(ev[3], st);
   if (adj) return;
   const bool nyq = I.imag == IMAG_NYQ;
@@ -404,14 +494,14 @@ void build_groups(pfdd_gpu *h) {
 // One GL iteration of every instance of group G (4 launches for the group).
 template <typename T>
 void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol, cudaEvent_t *ev = nullptr) {
-  constexpr int NP = Threads<T>::plane, NC = Threads<T>::pencil;
+  constexpr int NC = Threads<T>::pencil;
   const unsigned B = (unsigned)G.members.size();
   const InstPtrs *tab = static_cast<const InstPtrs *>(G.table.p);
   PlaneArgs pa;
   fill_plane_args<T>(L, pa);
   const int planes = L.F * L.nx;
   if (ev) cudaEventRecord(ev[0], st);
-  k_fwd_planes_tab<T, NP><<<dim3(planes, B), NP, L.smem_plane, st>>>(tab, pa);
+  launch_fwd_tab<T>(L, B, st, tab, pa);
   if (ev) cudaEventRecord(ev[1], st);
   PencilArgs pe;
   memset(&pe, 0, sizeof pe);
@@ -436,7 +526,7 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   ua.invN = 1.0 / (double)L.N;
   ua.core = L.core;
   ua.mode = PASS_STEP;
-  k_inv_update_tab<T, NP><<<dim3(planes, B), NP, L.smem_update, st>>>(tab, pa, ua);
+  launch_inv_tab<T>(L, B, st, tab, pa, ua);
   if (ev) cudaEventRecord(ev[3], st);
   const bool nyq = L.imag == IMAG_NYQ;
   k_finalize_tab<<<B, 1024, 0, st>>>(tab, planes, nyq ? L.ntiles : 0, 1.0 / (double)L.N, tol);
@@ -492,7 +582,7 @@ pfdd_status profile_impl(pfdd_gpu *h, int n_steps, double *kernel_ms) {
 // E_applied = -sum tau_a Re xi_a, from one elastic pass of the current state.
 template <typename T>
 pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, double *e_app) {
-  constexpr int NP = Threads<T>::plane, NC = Threads<T>::pencil;
+  constexpr int NC = Threads<T>::pencil;
   cudaStream_t st = h->stream;
   DevBuf gpart;
   CUDA_TRY(h, gpart.alloc(4 * (size_t)I.F * I.nx * sizeof(double)));
@@ -502,7 +592,7 @@ pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, 
   const T *xcur = I.xi[I.cur].as<T>();
   cx<T> *spec = I.spec.as<cx<T>>();
   const int planes = I.F * I.nx;
-  k_fwd_planes<T, NP><<<planes, NP, I.smem_plane, st>>>(xcur, spec, pa, nullptr, I.flags() + 3);
+  launch_fwd<T>(I, st, xcur, spec, pa, nullptr, I.flags() + 3);
   PencilArgs pe;
   memset(&pe, 0, sizeof pe);
   pe.px = I.px;
@@ -533,7 +623,7 @@ pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, 
   ua.mode = PASS_ENERGY;
   ua.gpart = gpart.as<double>();
   // xout is not written by the energy pass
-  k_inv_update<T, NP><<<planes, NP, I.smem_update, st>>>(spec, xcur, I.xi[I.cur ^ 1].as<T>(), pa, ua,
+  launch_inv<T>(I, planes, st, spec, xcur, I.xi[I.cur ^ 1].as<T>(), pa, ua,
                                                         I.partials.as<double>());
   std::vector<double> gp(4 * (size_t)planes), pp;
   CUDA_TRY(h, cudaMemcpyAsync(gp.data(), gpart.p, gp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -844,7 +934,7 @@ pfdd_status set_state_impl(pfdd_gpu *h, Instance &I, const double *re, const dou
 // inverse (k_inv_update PASS_SYNTH), through the spectrum buffer.
 template <typename T>
 void synth_imag(Instance &I, cudaStream_t st, T *dst) {
-  constexpr int NP = Threads<T>::plane, NC = Threads<T>::pencil;
+  constexpr int NC = Threads<T>::pencil;
   PencilArgs pe;
   memset(&pe, 0, sizeof pe);
   pe.px = I.px;
@@ -870,8 +960,7 @@ void synth_imag(Instance &I, cudaStream_t st, T *dst) {
   ua.mode = PASS_SYNTH;
   ua.err = I.flags() + 3;
   // xin is not read by the synthesis pass
-  k_inv_update<T, NP><<<I.S * I.nx, NP, I.smem_update, st>>>(spec, I.xi[I.cur].as<T>(), dst, pa, ua,
-                                                              I.partials.as<double>());
+  launch_inv<T>(I, (unsigned)(I.S * I.nx), st, spec, I.xi[I.cur].as<T>(), dst, pa, ua, I.partials.as<double>());
 }
 
 template <typename T>
@@ -913,6 +1002,10 @@ pfdd_status get_state_impl(pfdd_gpu *h, Instance &I, double *re, double *im, dou
   CUDA_TRY(h, cudaGetLastError());
   return PFDD_OK;
 }
+
+// whole-plane shared memory above which planes are split (two such CTAs
+// cannot share an SM's 228 KB)
+constexpr size_t kSplitAbove = 113 * 1024;
 
 bool valid_size(int n) {
   if (n < 2 || n > 1024 || (n & 1)) return false;
@@ -994,10 +1087,21 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
     // store spectrum rows with the same stride, so a plane moves in one bulk copy
     I->nzp = I->nzs;
     I->N = (size_t)I->nx * I->ny * I->nz;
-    const int maxr = (o.precision == PFDD_FP32) ? MaxRadix<Threads<float>::plane>::value
-                                                : MaxRadix<Threads<double>::plane>::value;
+    // Split the P1/P3 planes over 2-CTA clusters when a whole plane leaves
+    // room for one CTA per SM only (or does not fit); PFDD_PLANE_SPLIT=0|1
+    // in the environment forces the choice.
+    const size_t whole = (o.precision == PFDD_FP32) ? PlaneSmem<cx<float>>::bytes(I->ny, I->ny, I->nzs, I->M)
+                                                    : PlaneSmem<cx<double>>::bytes(I->ny, I->ny, I->nzs, I->M);
+    I->split = whole > kSplitAbove;
+    if (const char *env = getenv("PFDD_PLANE_SPLIT")) {
+      if (!strcmp(env, "0")) I->split = false;
+      else if (!strcmp(env, "1")) I->split = true;
+    }
+    const int maxr = (o.precision == PFDD_FP32)
+                         ? std::min(MaxRadix<Threads<float>::plane>::value, MaxRadix<Threads<float>::half>::value)
+                         : std::min(MaxRadix<Threads<double>::plane>::value, MaxRadix<Threads<double>::half>::value);
     make_plan(I->nx, I->px, maxr);
-    make_plan(I->ny, I->py, maxr);
+    make_plan(I->split ? I->ny / 2 : I->ny, I->py, maxr);
     make_plan(I->M, I->pz, maxr);
     pfdd_instance_desc d = descs[i];
     I->d.xo = d.xo;               // used during set-up only

@@ -20,7 +20,16 @@
 // ky and kz (z slot M = nz/2 holds the Nyquist column); P2 additionally
 // permutes kx inside shared memory only.  Frequencies are recovered through
 // slot tables, so no transform ever reorders data.
+//
+// Split planes (SPLIT = true): P1 and P3 can run each (field, x) plane on a
+// cluster of two CTAs, CTA rank r holding rows [r ny/2, (r+1) ny/2) in its
+// own shared memory; the first radix-2 stage of the y transform (rows y and
+// y + ny/2) goes through distributed shared memory and the remaining
+// ny/2-point stages are local.  Rank r then holds ky = r + 2 k' at the slots
+// of the ny/2-point plan, which the host's ky slot table encodes.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "pfdd_fft.cuh"
 
 #define PFDD_MAXS 12
@@ -175,6 +184,105 @@ __device__ __forceinline__ void block_sum2(double a, double b, double *scratch, 
   }
 }
 
+// Block-reduce NV doubles; warp 0 ends with the totals (thread 0 uses them).
+// scratch: NV*32 doubles.
+template <int NV>
+__device__ __forceinline__ void block_reduce(double (&v)[NV], double *scratch) {
+#pragma unroll
+  for (int q = 0; q < NV; ++q) v[q] = warp_sum(v[q]);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) scratch[q * 32 + wid] = v[q];
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = warp_sum(lane < nw ? scratch[q * 32 + lane] : 0.0);
+  }
+}
+
+// Sum of NV doubles over the CTA (SPLIT: over both CTAs of the plane's
+// cluster, rank 1 handing its totals to rank 0 through distributed shared
+// memory) written to out[0..NV-1] by one thread.  scratch: NV*32 + NV doubles.
+// Every thread of both CTAs must call it.
+template <bool SPLIT, int NV>
+__device__ __forceinline__ void plane_sum(double (&v)[NV], double *scratch, double *out) {
+  block_reduce<NV>(v, scratch);
+  if constexpr (!SPLIT) {
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int q = 0; q < NV; ++q) out[q] = v[q];
+    }
+  } else {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned rank = cl.block_rank();
+    double *slot = scratch + NV * 32;
+    if (rank == 1 && threadIdx.x == 0) {
+      double *peer = cl.map_shared_rank(slot, 0);
+#pragma unroll
+      for (int q = 0; q < NV; ++q) peer[q] = v[q];
+    }
+    cl.sync();
+    if (rank == 0 && threadIdx.x == 0) {
+#pragma unroll
+      for (int q = 0; q < NV; ++q) out[q] = v[q] + slot[q];
+    }
+  }
+}
+
+// The cross-CTA radix-2 stage of a split plane, over the nzh slot columns of
+// the ny/2 local rows.  Forward (decimation in frequency): lo = a + b,
+// hi = (a - b) W_ny^y with a, b rows y and y + ny/2; inverse (decimation in
+// time, unnormalised): lo = E + O conj(W_ny^y), hi = E - O conj(W_ny^y).  Each
+// pair (y, c) is read and written by one thread of one CTA (rank 0 takes the
+// first half of the pairs), so no result overwrites a value still to be read;
+// the cluster barriers before and after order it against both CTAs' own
+// passes.  twx2: W_ny^y, y < ny/2.
+template <bool INV, typename C>
+__device__ __forceinline__ void cross_stage(C *buf, const C *__restrict__ twx2, int nyh, int nzh, int nzs) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const unsigned rank = cl.block_rank();
+  C *peer = cl.map_shared_rank(buf, rank ^ 1u);
+  C *lo = rank == 0 ? buf : peer;
+  C *hi = rank == 0 ? peer : buf;
+  const int total = nyh * nzh;
+  const int begin = rank == 0 ? 0 : total / 2, end = rank == 0 ? total / 2 : total;
+  const FastDiv dz(nzh);
+  cl.sync();
+  constexpr int U = 4;   // pairs in flight per thread
+  for (int i0 = begin + threadIdx.x; i0 < end; i0 += U * blockDim.x) {
+    C a[U], b[U], w[U];
+    size_t o[U];
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+      const int i = i0 + q * blockDim.x;
+      const int ii = i < end ? i : begin;
+      const int y = dz.div(ii), c = ii - y * nzh;
+      o[q] = (size_t)y * nzs + c;
+      a[q] = lo[o[q]];
+      b[q] = hi[o[q]];
+      w[q] = twx2[y];
+    }
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+      if (i0 + q * blockDim.x >= end) continue;
+      if (!INV) {
+        lo[o[q]] = cadd(a[q], b[q]);
+        hi[o[q]] = cmul(csub(a[q], b[q]), w[q]);
+      } else {
+        const C t = cmulc(b[q], w[q]);
+        lo[o[q]] = cadd(a[q], t);
+        hi[o[q]] = csub(a[q], t);
+      }
+    }
+  }
+  cl.sync();
+}
+
 template <typename C>
 __device__ __forceinline__ void load_table(C *dst, const void *src, int n) {
   const C *s = reinterpret_cast<const C *>(src);
@@ -182,24 +290,30 @@ __device__ __forceinline__ void load_table(C *dst, const void *src, int n) {
 }
 
 // ------------------------------------------------------------ P1
-// Shared memory of a plane kernel: the ny x nzs complex plane, then the y, z
-// and real-to-complex twiddle tables, the z position table and one mbarrier.
+// Shared memory of a plane kernel: `rows` complex rows of stride nzs (ny, or
+// ny/2 for a split plane), then the y, z and real-to-complex twiddle tables,
+// the z position table, one mbarrier and the reduction scratch.  The y table
+// has ny entries: W_ny^m (m < ny), or for a split plane W_ny^m (m < ny/2)
+// followed by the W_{ny/2}^m of the local stages.
+constexpr int kPlaneRed = 136;   // doubles of reduction scratch (4 sums)
+
 template <typename C> struct PlaneSmem {
   C *buf, *twy, *twz, *twr;
   int *pos;
   uint64_t *bar;
   double *red;
-  __device__ PlaneSmem(unsigned char *raw, const PlaneArgs &a) {
+  __device__ PlaneSmem(unsigned char *raw, const PlaneArgs &a, int rows) {
     buf = reinterpret_cast<C *>(raw);
-    twy = buf + (size_t)a.ny * a.nzs;
+    twy = buf + (size_t)rows * a.nzs;
     twz = twy + a.ny;
     twr = twz + a.M;
     pos = reinterpret_cast<int *>(twr + a.M);
     bar = reinterpret_cast<uint64_t *>(pos + ((a.M + 1) & ~1));
     red = reinterpret_cast<double *>(bar + 1);
   }
-  static size_t bytes(int ny, int nzs, int M) {
-    return ((size_t)ny * nzs + ny + 2 * (size_t)M) * sizeof(C) + (size_t)((M + 1) & ~1) * 4 + 8 + 64 * 8;
+  static size_t bytes(int rows, int ny, int nzs, int M) {
+    return ((size_t)rows * nzs + ny + 2 * (size_t)M) * sizeof(C) + (size_t)((M + 1) & ~1) * 4 + 8 +
+           kPlaneRed * 8;
   }
 };
 
@@ -211,41 +325,53 @@ __device__ __forceinline__ void load_plane_tables(const PlaneSmem<C> &sm, const 
   for (int i = threadIdx.x; i < a.M; i += blockDim.x) sm.pos[i] = a.posM[i];
 }
 
-template <typename T, int NT>
+// plane index and first row of this CTA (grid.x = planes, or 2 planes for SPLIT)
+template <bool SPLIT> __device__ __forceinline__ size_t plane_of_block() {
+  return SPLIT ? (size_t)(blockIdx.x >> 1) : (size_t)blockIdx.x;
+}
+template <bool SPLIT> __device__ __forceinline__ int row0_of_block(int ny) {
+  if constexpr (SPLIT) return (int)cooperative_groups::this_cluster().block_rank() * (ny / 2);
+  return 0;
+}
+
+template <typename T, int NT, bool SPLIT>
 __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> *__restrict__ spec,
                                                 const PlaneArgs &a, int *err, size_t plane) {
   using C = cx<T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const PlaneSmem<C> sm(smem_raw, a);
   const int ny = a.ny, nz = a.nz, nzh = a.nzh, nzp = a.nzp, nzs = a.nzs, M = a.M;
+  const int rows = SPLIT ? ny / 2 : ny;
+  const int row0 = row0_of_block<SPLIT>(ny);
+  const PlaneSmem<C> sm(smem_raw, a, rows);
   if (threadIdx.x == 0) mbar_init(sm.bar, 1);
   __syncthreads();
   // rows of the real plane -> shared rows of stride 2*nzs reals (bulk copies)
   if (threadIdx.x < 32) {
-    if (threadIdx.x == 0) mbar_expect_tx(sm.bar, (uint32_t)(ny * nz * sizeof(T)));
+    if (threadIdx.x == 0) mbar_expect_tx(sm.bar, (uint32_t)(rows * nz * sizeof(T)));
     __syncwarp();
-    const T *src = xi + plane * (size_t)ny * nz;
+    const T *src = xi + (plane * (size_t)ny + row0) * nz;
     T *bufr = reinterpret_cast<T *>(sm.buf);
-    for (int y = threadIdx.x; y < ny; y += 32)
+    for (int y = threadIdx.x; y < rows; y += 32)
       bulk_g2s(bufr + (size_t)y * 2 * nzs, src + (size_t)y * nz, (uint32_t)(nz * sizeof(T)), sm.bar);
   }
   load_plane_tables(sm, a);
   const bool ok = __syncthreads_and(mbar_wait(sm.bar, 0));
   if (!ok) {
     if (threadIdx.x == 0) atomicExch(err, 1);
-    return;
+    // a split CTA carries on without storing: its peer waits at the cluster barriers
+    if constexpr (!SPLIT) return;
   }
   C *buf = sm.buf;
   const C *twr = sm.twr;
   const int *pos = sm.pos;
 
   // z: M-point complex transform of the packed rows
-  Batch gz{ny, ny, nzs, 0, 1, false};
+  Batch gz{rows, rows, nzs, 0, 1, false};
   fft_forward<MaxRadix<NT>::value>(buf, sm.twz, a.pz, gz);
 
   // real-to-complex unpacking, pairs (k, M-k); X[M] goes to slot M
   const int half = M / 2 + 1;
-  for (int w = threadIdx.x; w < ny * half; w += blockDim.x) {
+  for (int w = threadIdx.x; w < rows * half; w += blockDim.x) {
     const int y = w / half, k = w - y * half;
     C *row = buf + (size_t)y * nzs;
     if (k == 0) {
@@ -264,45 +390,47 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
       if (pm != pk) row[pm] = cconj(csub(e, wo));
     }
   }
-  __syncthreads();
+  if constexpr (SPLIT) cross_stage<false>(buf, sm.twy, rows, nzh, nzs);
+  else __syncthreads();
 
-  // y: ny-point transforms over the nzh slot columns
+  // y: (ny or ny/2)-point transforms over the nzh slot columns
   Batch gy{nzh, nzh, 1, 0, nzs, true};
-  fft_forward<MaxRadix<NT>::value>(buf, sm.twy, a.py, gy);
+  fft_forward<MaxRadix<NT>::value>(buf, SPLIT ? sm.twy + rows : sm.twy, a.py, gy);
 
-  // rows -> spectrum rows of nzp entries (bulk stores, one warp)
+  // rows -> spectrum rows of nzp entries (bulk stores)
   fence_proxy_async();
   __syncthreads();
+  if (!ok) return;
+  C *dst = spec + (plane * (size_t)ny + row0) * nzp;
   if (nzs == nzp) {
     if (threadIdx.x == 0) {  // rows are contiguous in both: one bulk copy
-      bulk_s2g(spec + plane * (size_t)ny * nzp, buf, (uint32_t)((size_t)ny * nzp * sizeof(C)));
+      bulk_s2g(dst, buf, (uint32_t)((size_t)rows * nzp * sizeof(C)));
       bulk_commit();
       bulk_wait_all();
     }
   } else if (threadIdx.x < 32) {
-    C *dst = spec + plane * (size_t)ny * nzp;
-    for (int y = threadIdx.x; y < ny; y += 32)
+    for (int y = threadIdx.x; y < rows; y += 32)
       bulk_s2g(dst + (size_t)y * nzp, buf + (size_t)y * nzs, (uint32_t)(nzp * sizeof(C)));
     bulk_commit();
     bulk_wait_all();
   }
 }
 
-// grid.x = F * nx planes
-template <typename T, int NT>
+// grid.x = F * nx planes (SPLIT: 2 F nx CTAs in clusters of 2)
+template <typename T, int NT, bool SPLIT>
 __global__ void __launch_bounds__(NT) k_fwd_planes(const T *__restrict__ xi, cx<T> *__restrict__ spec,
                                                    PlaneArgs a, const int *__restrict__ stop, int *err) {
-  if (stop && *stop) return;
-  fwd_planes_body<T, NT>(xi, spec, a, err, blockIdx.x);
+  if (stop && *stop) return;   // both CTAs of a cluster read the same flag
+  fwd_planes_body<T, NT, SPLIT>(xi, spec, a, err, plane_of_block<SPLIT>());
 }
 
-// grid = (F * nx planes, instances of the group)
-template <typename T, int NT>
+// grid = (F * nx planes [x 2 for SPLIT], instances of the group)
+template <typename T, int NT, bool SPLIT>
 __global__ void __launch_bounds__(NT) k_fwd_planes_tab(const InstPtrs *__restrict__ tab, PlaneArgs a) {
   const InstPtrs &ip = tab[blockIdx.y];
   if (ip.flags[0]) return;
   const T *xi = static_cast<const T *>(ip.xi[ip.flags[4]]);
-  fwd_planes_body<T, NT>(xi, static_cast<cx<T> *>(ip.spec), a, ip.flags + 3, blockIdx.x);
+  fwd_planes_body<T, NT, SPLIT>(xi, static_cast<cx<T> *>(ip.spec), a, ip.flags + 3, plane_of_block<SPLIT>());
 }
 
 // ------------------------------------------------------------ B(k) operator
@@ -714,7 +842,7 @@ __device__ __forceinline__ T update_one(const UpdateArgs &u, bool real_field, in
 
 // Per-instance pointers travel as arguments so the constant parameter block
 // (PlaneArgs, UpdateArgs) is read in place and never copied.
-template <typename T, int NT>
+template <typename T, int NT, bool SPLIT>
 __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, const T *__restrict__ xin,
                                                 T *__restrict__ xout, const PlaneArgs &a, const UpdateArgs &u,
                                                 double *__restrict__ partials, size_t plane,
@@ -724,19 +852,21 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   using V = typename Vec<T>::type;
   constexpr int VN = Vec<T>::n;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const PlaneSmem<C> sm(smem_raw, a);
   const int ny = a.ny, nz = a.nz, nzh = a.nzh, nzp = a.nzp, nzs = a.nzs, M = a.M;
+  const int rows = SPLIT ? ny / 2 : ny;
+  const int row0 = row0_of_block<SPLIT>(ny);
+  const PlaneSmem<C> sm(smem_raw, a, rows);
   if (threadIdx.x == 0) mbar_init(sm.bar, 1);
   __syncthreads();
   // spectrum rows of nzp entries -> shared rows of nzs (bulk copies, one warp)
   if (threadIdx.x < 32) {
-    if (threadIdx.x == 0) mbar_expect_tx(sm.bar, (uint32_t)((size_t)ny * nzp * sizeof(C)));
+    if (threadIdx.x == 0) mbar_expect_tx(sm.bar, (uint32_t)((size_t)rows * nzp * sizeof(C)));
     __syncwarp();
-    const C *src = spec + plane * (size_t)ny * nzp;
+    const C *src = spec + (plane * (size_t)ny + row0) * nzp;
     if (nzs == nzp) {
-      if (threadIdx.x == 0) bulk_g2s(sm.buf, src, (uint32_t)((size_t)ny * nzp * sizeof(C)), sm.bar);
+      if (threadIdx.x == 0) bulk_g2s(sm.buf, src, (uint32_t)((size_t)rows * nzp * sizeof(C)), sm.bar);
     } else {
-      for (int y = threadIdx.x; y < ny; y += 32)
+      for (int y = threadIdx.x; y < rows; y += 32)
         bulk_g2s(sm.buf + (size_t)y * nzs, src + (size_t)y * nzp, (uint32_t)(nzp * sizeof(C)), sm.bar);
     }
   }
@@ -745,19 +875,21 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   const bool ok = __syncthreads_and(mbar_wait(sm.bar, 0));
   if (!ok) {
     if (threadIdx.x == 0) atomicExch(err, 1);
-    return;
+    // a split CTA carries on without storing: its peer waits at the cluster barriers
+    if constexpr (!SPLIT) return;
   }
   C *buf = sm.buf;
   const C *twr = sm.twr;
   const int *pos = sm.pos;
 
   Batch gy{nzh, nzh, 1, 0, nzs, true};
-  fft_inverse<MaxRadix<NT>::value>(buf, sm.twy, a.py, gy);
+  fft_inverse<MaxRadix<NT>::value>(buf, SPLIT ? sm.twy + rows : sm.twy, a.py, gy);
+  if constexpr (SPLIT) cross_stage<true>(buf, sm.twy, rows, nzh, nzs);
 
   // complex-to-real packing: Zin[k] = A + i w D, Zin[M-k] = conj(A - i w D),
   // A = X[k] + conj X[M-k], D = X[k] - conj X[M-k], w = exp(+2 pi i k / nz)
   const int half = M / 2 + 1;
-  for (int w = threadIdx.x; w < ny * half; w += blockDim.x) {
+  for (int w = threadIdx.x; w < rows * half; w += blockDim.x) {
     const int y = w / half, k = w - y * half;
     C *row = buf + (size_t)y * nzs;
     const int pk = pos[k];
@@ -773,7 +905,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   }
   __syncthreads();
 
-  Batch gz{ny, ny, nzs, 0, 1, false};
+  Batch gz{rows, rows, nzs, 0, 1, false};
   fft_inverse<MaxRadix<NT>::value>(buf, sm.twz, a.pz, gz);
 
   // fused GSFE force + applied stress + masked explicit Euler update,
@@ -783,12 +915,12 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   const bool real_field = f < u.S;
   const int sys = real_field ? f : f - u.S;
   const size_t N = (size_t)a.nx * ny * nz;
-  const size_t off = plane * (size_t)ny * nz;
-  const size_t rbase = (size_t)x * ny * nz;
+  const size_t off = (plane * (size_t)ny + row0) * nz;   // first site of this CTA's rows
+  const size_t rbase = ((size_t)x * ny + row0) * nz;
   const T *bufr = reinterpret_cast<const T *>(buf);
   const T invN = (T)u.invN;
   const int nvec = nz / VN;
-  const int total = ny * nvec;
+  const int total = rows * nvec;
   const FastDiv dv(nvec);
   if (u.mode == PASS_SYNTH) {
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
@@ -797,7 +929,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
       *reinterpret_cast<V *>(e) = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzs + zq * VN);
 #pragma unroll
       for (int q = 0; q < VN; ++q) e[q] *= invN;
-      *reinterpret_cast<V *>(xout + off + y * nz + zq * VN) = *reinterpret_cast<V *>(e);
+      if (ok) *reinterpret_cast<V *>(xout + off + y * nz + zq * VN) = *reinterpret_cast<V *>(e);
     }
     return;
   }
@@ -822,8 +954,8 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
         }
       }
     }
-    block_sum2(e_el, e_core, sm.red, u.gpart + 4 * plane);
-    block_sum2(e_app, 0.0, sm.red, u.gpart + 4 * plane + 2);
+    double v[4] = {e_el, e_core, e_app, 0.0};
+    plane_sum<SPLIT>(v, sm.red, u.gpart + 4 * plane);
     return;
   }
   if (u.mode == PASS_ADJOINT) {
@@ -857,10 +989,10 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
           nv[q] = frozen ? lam[q] : lam[q] - cd * e[q] * invN;
         }
       }
-      *reinterpret_cast<V *>(xout + off + idx) = *reinterpret_cast<V *>(nv);
+      if (ok) *reinterpret_cast<V *>(xout + off + idx) = *reinterpret_cast<V *>(nv);
     }
-    block_sum2(g0, g1, sm.red, u.gpart + 4 * plane);
-    block_sum2(gl, 0.0, sm.red, u.gpart + 4 * plane + 2);
+    double v[4] = {g0, g1, gl, 0.0};
+    plane_sum<SPLIT>(v, sm.red, u.gpart + 4 * plane);
     return;
   }
   // update pass only: tau, mask and per-site GSFE are read from here on
@@ -895,31 +1027,33 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
         dsq += d * d;
         if (real_field) sum += (double)nv[q];
       }
-      *reinterpret_cast<V *>(xout + off + idx[h]) = *reinterpret_cast<V *>(nv);
+      if (ok) *reinterpret_cast<V *>(xout + off + idx[h]) = *reinterpret_cast<V *>(nv);
     }
   }
-  block_sum2(dsq, sum, sm.red, partials + 2 * plane);
+  double v[2] = {dsq, sum};
+  plane_sum<SPLIT>(v, sm.red, partials + 2 * plane);
 }
 
-// grid.x = F * nx planes
-template <typename T, int NT>
+// grid.x = F * nx planes (SPLIT: 2 F nx CTAs in clusters of 2)
+template <typename T, int NT, bool SPLIT>
 __global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spec, const T *__restrict__ xin,
                                                    T *__restrict__ xout, PlaneArgs a, UpdateArgs u,
                                                    double *__restrict__ partials) {
   if (u.stop && *u.stop) return;
-  inv_update_body<T, NT>(spec, xin, xout, a, u, partials, blockIdx.x, u.tau, u.mask, u.site, u.err);
+  inv_update_body<T, NT, SPLIT>(spec, xin, xout, a, u, partials, plane_of_block<SPLIT>(), u.tau, u.mask, u.site,
+                                u.err);
 }
 
 // grid = (F * nx planes, instances of the group); per-instance stress, mask,
 // GSFE field and buffers come from the table
-template <typename T, int NT>
+template <typename T, int NT, bool SPLIT>
 __global__ void __launch_bounds__(NT) k_inv_update_tab(const InstPtrs *__restrict__ tab, PlaneArgs a, UpdateArgs u) {
   const InstPtrs &ip = tab[blockIdx.y];
   if (ip.flags[0]) return;
   const int cur = ip.flags[4];
-  inv_update_body<T, NT>(static_cast<const cx<T> *>(ip.spec), static_cast<const T *>(ip.xi[cur]),
-                         static_cast<T *>(ip.xi[cur ^ 1]), a, u, ip.partials, blockIdx.x, ip.tau, ip.mask, ip.site,
-                         ip.flags + 3);
+  inv_update_body<T, NT, SPLIT>(static_cast<const cx<T> *>(ip.spec), static_cast<const T *>(ip.xi[cur]),
+                                static_cast<T *>(ip.xi[cur ^ 1]), a, u, ip.partials, plane_of_block<SPLIT>(),
+                                ip.tau, ip.mask, ip.site, ip.flags + 3);
 }
 
 // ------------------------------------------------------------ reduction

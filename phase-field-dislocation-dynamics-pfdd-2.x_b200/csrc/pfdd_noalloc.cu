@@ -70,11 +70,11 @@ pfdd_status device_setup(int dev, void **addr) {
   cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
   if (e != cudaSuccess || !p) return nerr(PFDD_ECUDA, "cudaGetSymbolAddress of the static scratch failed");
   const int lim = 227 * 1024;
-  if (cudaFuncSetAttribute(k_fwd_planes<double, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) !=
+  if (cudaFuncSetAttribute(k_fwd_planes<double, 256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) !=
           cudaSuccess ||
       cudaFuncSetAttribute(k_xpencil<double, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) !=
           cudaSuccess ||
-      cudaFuncSetAttribute(k_inv_update<double, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) !=
+      cudaFuncSetAttribute(k_inv_update<double, 256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) !=
           cudaSuccess)
     return nerr(PFDD_ECUDA, "cudaFuncSetAttribute failed during static-scratch set-up");
   g_addr[dev] = p;
@@ -115,7 +115,7 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   auto pencil_bytes = [&](int cc) { return ((size_t)F * fstride_for(cc) + nx) * sizeof(C) + 64 * sizeof(double); };
   int cc = 32;
   while (cc > 1 && (ncols % cc || pencil_bytes(cc) > 200 * 1024)) cc >>= 1;
-  const size_t smem_plane = PlaneSmem<C>::bytes(ny, nzp, M);
+  const size_t smem_plane = PlaneSmem<C>::bytes(ny, ny, nzp, M);
   if (ncols % cc || pencil_bytes(cc) > 227 * 1024 || smem_plane > 227 * 1024)
     return nerr(PFDD_EUNSUPPORTED, "grid too large for the shared-memory passes in FP64");
 
@@ -234,9 +234,9 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   ua.mode = PASS_STEP;
 
   const int planes = F * nx;
-  k_fwd_planes<double, 256><<<planes, 256, smem_plane, s>>>(d_xi_in, spec, pa, flags, flags + 3);
+  k_fwd_planes<double, 256, false><<<planes, 256, smem_plane, s>>>(d_xi_in, spec, pa, flags, flags + 3);
   k_xpencil<double, 256><<<(int)(ncols / cc), 256, pencil_bytes(cc), s>>>(spec, pe, flags);
-  k_inv_update<double, 256><<<planes, 256, smem_plane, s>>>(spec, d_xi_in, d_xi_out, pa, ua, partials);
+  k_inv_update<double, 256, false><<<planes, 256, smem_plane, s>>>(spec, d_xi_in, d_xi_out, pa, ua, partials);
   k_finalize<<<1, 1024, 0, s>>>(partials, planes, stats, 0, 0.0, flags, flags + 1, flags + 2, nullptr, 0, 0.0);
   e = cudaGetLastError();
   if (e != cudaSuccess) return nerr(PFDD_ECUDA, cudaGetErrorString(e));
