@@ -47,8 +47,23 @@ struct DevBuf {
 };
 
 template <typename T> struct Threads;
-// plane: whole-plane P1/P3 CTAs; half: each CTA of a split (2-CTA cluster) plane
-template <> struct Threads<float> { static constexpr int plane = 512, half = 256, pencil = 512; };
+// plane: whole-plane P1/P3 CTAs; half: each CTA of a split (2-CTA cluster)
+// plane; pencil: P2 CTAs.  FP32 defaults were measured on 256x256x128 with
+// 12 systems: 256-thread split-plane CTAs at three per SM (80 registers) and
+// 256-thread pencil CTAs of at most 100 KB of shared memory at two per SM
+// beat 512-thread CTAs at one per SM by 0.3 ms per step.
+#ifndef PFDD_HALF_THREADS_F32
+#define PFDD_HALF_THREADS_F32 256
+#endif
+#ifndef PFDD_PENCIL_THREADS_F32
+#define PFDD_PENCIL_THREADS_F32 256
+#endif
+#ifndef PFDD_PENCIL_SMEM_KB
+#define PFDD_PENCIL_SMEM_KB 100
+#endif
+template <> struct Threads<float> {
+  static constexpr int plane = 512, half = PFDD_HALF_THREADS_F32, pencil = PFDD_PENCIL_THREADS_F32;
+};
 template <> struct Threads<double> { static constexpr int plane = 256, half = 256, pencil = 256; };
 
 struct Instance {
@@ -263,7 +278,7 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
     return ((size_t)I.F * fstride_for(cc) + I.nx) * sizeof(C) + 64 * sizeof(double);
   };
   int cc = 32;
-  while (cc > cmin && (ncols % cc || pencil_bytes(cc) > 200 * 1024)) cc >>= 1;
+  while (cc > cmin && (ncols % cc || pencil_bytes(cc) > PFDD_PENCIL_SMEM_KB * 1024)) cc >>= 1;
   if (ncols % cc || pencil_bytes(cc) > limit)
     return fail(h, PFDD_EUNSUPPORTED, "x-pencil of %d x %d fields does not fit shared memory", I.nx, I.F);
   I.ccols = cc;
@@ -292,6 +307,7 @@ void fill_plane_args(const Instance &I, PlaneArgs &pa) {
   pa.S = I.S; pa.F = I.F;
   pa.tw_y = I.tw_y.p; pa.tw_z = I.tw_z.p; pa.tw_r = I.tw_r.p;
   pa.posM = I.posM;
+  set_plane_divisors<T>(pa, I.split ? I.ny / 2 : I.ny);
 }
 
 template <typename T>
@@ -392,7 +408,7 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   if (ev) cudaEventRecord(ev[0], st);
   launch_fwd<T>(I, st, xin, spec, pa, flags, flags + 3);
   if (ev) cudaEventRecord(ev[1], st);
-  PencilArgs pe;
+  PencilArgs pe{};
   pe.px = I.px;
   pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.nzp = I.nzp; pe.M = I.M;
   pe.S = I.S; pe.F = I.F; pe.imag = I.imag;
@@ -407,6 +423,7 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   pe.cd = I.d.cd_dt;
   pe.partials = (I.imag == IMAG_NYQ && !adj) ? I.ppart.as<double>() : nullptr;
   pe.g = I.green;
+  set_pencil_divisors<T>(pe);
   k_xpencil<T, NC><<<I.ntiles, NC, I.smem_pencil, st>>>(spec, pe, flags);
   if (ev) cudaEventRecord(ev[2], st);
   UpdateArgs ua;
@@ -504,7 +521,7 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   launch_fwd_tab<T>(L, B, st, tab, pa);
   if (ev) cudaEventRecord(ev[1], st);
   PencilArgs pe;
-  memset(&pe, 0, sizeof pe);
+  pe = PencilArgs{};
   pe.px = L.px;
   pe.nx = L.nx; pe.ny = L.ny; pe.nz = L.nz; pe.nzh = L.nzh; pe.nzp = L.nzp; pe.M = L.M;
   pe.S = L.S; pe.F = L.F; pe.imag = L.imag;
@@ -517,6 +534,7 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   pe.sx_n = L.sx_n; pe.sy_n = L.sy_n;
   pe.cd = L.d.cd_dt;
   pe.g = L.green;
+  set_pencil_divisors<T>(pe);
   k_xpencil_tab<T, NC><<<dim3(L.ntiles, B), NC, L.smem_pencil, st>>>(tab, pe);
   if (ev) cudaEventRecord(ev[2], st);
   UpdateArgs ua;
@@ -594,7 +612,7 @@ pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, 
   const int planes = I.F * I.nx;
   launch_fwd<T>(I, st, xcur, spec, pa, nullptr, I.flags() + 3);
   PencilArgs pe;
-  memset(&pe, 0, sizeof pe);
+  pe = PencilArgs{};
   pe.px = I.px;
   pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.nzp = I.nzp; pe.M = I.M;
   pe.S = I.S; pe.F = I.F; pe.imag = I.imag;
@@ -609,6 +627,7 @@ pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, 
   pe.cd = I.d.cd_dt;
   pe.partials = I.imag == IMAG_NYQ ? I.ppart.as<double>() : nullptr;
   pe.g = I.green;
+  set_pencil_divisors<T>(pe);
   k_xpencil<T, NC><<<I.ntiles, NC, I.smem_pencil, st>>>(spec, pe, nullptr);
   UpdateArgs ua;
   memset(&ua, 0, sizeof ua);
@@ -936,7 +955,7 @@ template <typename T>
 void synth_imag(Instance &I, cudaStream_t st, T *dst) {
   constexpr int NC = Threads<T>::pencil;
   PencilArgs pe;
-  memset(&pe, 0, sizeof pe);
+  pe = PencilArgs{};
   pe.px = I.px;
   pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.nzp = I.nzp; pe.M = I.M;
   pe.S = I.S; pe.F = I.S; pe.imag = IMAG_NYQ;
@@ -950,6 +969,7 @@ void synth_imag(Instance &I, cudaStream_t st, T *dst) {
   pe.sx_n = I.sx_n; pe.sy_n = I.sy_n;
   pe.g = I.green;
   cx<T> *spec = I.spec.as<cx<T>>();
+  set_pencil_divisors<T>(pe);
   k_xpencil<T, NC><<<I.ntiles, NC, I.smem_pencil, st>>>(spec, pe, nullptr);
   PlaneArgs pa;
   fill_plane_args<T>(I, pa);

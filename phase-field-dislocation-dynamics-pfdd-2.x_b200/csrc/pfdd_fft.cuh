@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "pfdd_fastdiv.h"
+
 namespace pfdd {
 
 template <typename T> struct cx_of;
@@ -126,35 +128,27 @@ template <int R, int SIGN, typename C> __device__ __forceinline__ void dft(C *v)
   else if constexpr (R == 16) dft16<SIGN>(v);
 }
 
-// Radix plan of one axis, built on the host.
+// Radix plan of one axis, built on the host, with the per-stage divisors:
+// stage s has n / R_s work items per transform (per[s]) and L_s / R_s
+// positions j per block (lr[s]); its twiddles step by n / L_s (twstep[s]).
 struct FftPlan {
   int n;
   int nst;
   int radix[8];
   int L[8];
-};
-
-// Division by a block-uniform divisor: shift when it is a power of two.
-struct FastDiv {
-  int d, sh;
-  __host__ __device__ FastDiv() : d(1), sh(0) {}
-  __host__ __device__ explicit FastDiv(int v) : d(v), sh(-1) {
-    if (v > 0 && (v & (v - 1)) == 0) {
-      sh = 0;
-      while ((1 << sh) < v) ++sh;
-    }
-  }
-  __device__ __forceinline__ int div(int x) const { return sh >= 0 ? (x >> sh) : x / d; }
-  __device__ __forceinline__ int mod(int x) const { return sh >= 0 ? (x & (d - 1)) : x % d; }
+  int twstep[8];
+  FastDiv per[8], lr[8];
 };
 
 // Batched transform geometry in shared memory: transform b (0 <= b < batch)
 // starts at (b % bin) * bs_in + (b / bin) * bs_out and its element i sits at
 // start + i * es.  If batch_fast, consecutive threads take consecutive b (use
 // when bs_in == 1); otherwise consecutive butterflies of one transform.
+// fb and fi divide by batch and bin (built by the caller, outside the stages).
 struct Batch {
   int batch, bin, bs_in, bs_out, es;
   bool batch_fast;
+  FastDiv fb, fi;
 };
 
 // multiply v[k] (k = 1..R-1) by W^(j k) (or its conjugate), W^(j k) built from
@@ -187,19 +181,21 @@ __device__ __forceinline__ void apply_twiddles(C *v, const C *__restrict__ tw, i
 }
 
 template <int R, bool INV, typename C>
-__device__ __forceinline__ void fft_stage(C *__restrict__ x, const C *__restrict__ tw, int n, int L,
+__device__ __forceinline__ void fft_stage(C *__restrict__ x, const C *__restrict__ tw, const FftPlan &p, int s,
                                           const Batch &g, int tid, int nthr) {
+  const int L = p.L[s];
   const int Lr = L / R;
-  const int per = n / R;
+  const FastDiv &dP = p.per[s], &dL = p.lr[s];
+  const int per = (int)dP.d;
   const int total = g.batch * per;
-  const int twstep = n / L;
-  const FastDiv dB(g.batch), dP(per), dL(Lr), dI(g.bin);
+  const int twstep = p.twstep[s];
   for (int w = tid; w < total; w += nthr) {
     int b, bf;
-    if (g.batch_fast) { b = dB.mod(w); bf = dB.div(w); }
-    else { bf = dP.mod(w); b = dP.div(w); }
+    if (g.batch_fast) { bf = g.fb.div(w); b = w - bf * g.batch; }
+    else { b = dP.div(w); bf = w - b * per; }
     const int blk = dL.div(bf), j = bf - blk * Lr;
-    C *base = x + dI.mod(b) * g.bs_in + dI.div(b) * g.bs_out + (blk * L + j) * g.es;
+    const int bq = g.fi.div(b), bm = b - bq * g.bin;
+    C *base = x + bm * g.bs_in + bq * g.bs_out + (blk * L + j) * g.es;
     const int st = Lr * g.es;
     C v[R];
     // contiguous elements (last stage along a unit-stride axis): 16-byte vectors
@@ -237,14 +233,14 @@ __device__ __forceinline__ void fft_stage(C *__restrict__ x, const C *__restrict
 // Radices above MAXR are compiled out (the host plans never use them for
 // such a kernel), which bounds the registers a butterfly needs.
 template <bool INV, int MAXR, typename C>
-__device__ __forceinline__ void fft_stage_dispatch(C *x, const C *tw, int n, int R, int L, const Batch &g,
+__device__ __forceinline__ void fft_stage_dispatch(C *x, const C *tw, const FftPlan &p, int s, const Batch &g,
                                                    int tid, int nthr) {
-  switch (R) {
-    case 2: fft_stage<2, INV>(x, tw, n, L, g, tid, nthr); break;
-    case 3: fft_stage<3, INV>(x, tw, n, L, g, tid, nthr); break;
-    case 4: fft_stage<4, INV>(x, tw, n, L, g, tid, nthr); break;
-    case 8: if constexpr (MAXR >= 8) fft_stage<8, INV>(x, tw, n, L, g, tid, nthr); break;
-    case 16: if constexpr (MAXR >= 16) fft_stage<16, INV>(x, tw, n, L, g, tid, nthr); break;
+  switch (p.radix[s]) {
+    case 2: fft_stage<2, INV>(x, tw, p, s, g, tid, nthr); break;
+    case 3: fft_stage<3, INV>(x, tw, p, s, g, tid, nthr); break;
+    case 4: fft_stage<4, INV>(x, tw, p, s, g, tid, nthr); break;
+    case 8: if constexpr (MAXR >= 8) fft_stage<8, INV>(x, tw, p, s, g, tid, nthr); break;
+    case 16: if constexpr (MAXR >= 16) fft_stage<16, INV>(x, tw, p, s, g, tid, nthr); break;
     default: break;
   }
 }
@@ -253,7 +249,7 @@ __device__ __forceinline__ void fft_stage_dispatch(C *x, const C *tw, int n, int
 template <int MAXR = 16, typename C>
 __device__ void fft_forward(C *x, const C *tw, const FftPlan &p, const Batch &g) {
   for (int s = 0; s < p.nst; ++s) {
-    fft_stage_dispatch<false, MAXR>(x, tw, p.n, p.radix[s], p.L[s], g, threadIdx.x, blockDim.x);
+    fft_stage_dispatch<false, MAXR>(x, tw, p, s, g, threadIdx.x, blockDim.x);
     __syncthreads();
   }
 }
@@ -262,7 +258,7 @@ __device__ void fft_forward(C *x, const C *tw, const FftPlan &p, const Batch &g)
 template <int MAXR = 16, typename C>
 __device__ void fft_inverse(C *x, const C *tw, const FftPlan &p, const Batch &g) {
   for (int s = p.nst - 1; s >= 0; --s) {
-    fft_stage_dispatch<true, MAXR>(x, tw, p.n, p.radix[s], p.L[s], g, threadIdx.x, blockDim.x);
+    fft_stage_dispatch<true, MAXR>(x, tw, p, s, g, threadIdx.x, blockDim.x);
     __syncthreads();
   }
 }

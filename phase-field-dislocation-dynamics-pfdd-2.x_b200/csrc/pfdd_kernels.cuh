@@ -41,6 +41,21 @@ namespace pfdd {
 // 1024-thread blocks must fit 64 registers per thread).
 template <int NT> struct MaxRadix { static constexpr int value = NT >= 1024 ? 8 : 16; };
 
+// Resident CTAs per SM a plane kernel is compiled for (register cap): FP32
+// split planes (half a plane of shared memory each) fit three to an SM.
+#ifndef PFDD_SPLIT_MINB_F32
+#define PFDD_SPLIT_MINB_F32 3
+#endif
+template <typename T, bool SPLIT> struct PlaneMinBlocks {
+  static constexpr int value = (SPLIT && sizeof(T) == 4) ? PFDD_SPLIT_MINB_F32 : 1;
+};
+#ifndef PFDD_PENCIL_MINB_F32
+#define PFDD_PENCIL_MINB_F32 2
+#endif
+template <typename T> struct PencilMinBlocks {
+  static constexpr int value = sizeof(T) == 4 ? PFDD_PENCIL_MINB_F32 : 1;
+};
+
 // Per-instance constants of the contraction and the update (FP64 on the host).
 // Each table is kept in FP64 (set-up, FP64 path) and rounded once to FP32
 // (FP32 path), so the kernels never convert constants in their inner loops.
@@ -89,6 +104,9 @@ struct PlaneArgs {
   int S, F;                   // slip systems; fields in flight (S, or 2S with Im xi)
   const void *tw_y, *tw_z, *tw_r;   // W_ny^m, W_M^m, W_nz^k tables in compute precision
   const int16_t *posM;        // position of z-frequency k (< M) after the M-point transform
+  // divisors built on the host: rows per CTA (ny, or ny/2 when split), nzh,
+  // M/2 + 1 (real-to-complex pairs per row), nz / vector width
+  FastDiv fd_rows, fd_nzh, fd_half, fd_nvec;
 };
 
 struct PencilArgs {
@@ -107,6 +125,9 @@ struct PencilArgs {
   int sx_n, sy_n;             // slots of kx = nx/2 and ky = ny/2
   double cd;                  // CD * timestep
   double *partials;           // per-CTA sum of |d Im xi|^2 * N (Parseval weight), or null
+  // divisors built on the host: F * ccols, ccols, nzp, 16-byte chunks per
+  // (field, x) row of a tile, nx
+  FastDiv fd_fcc, fd_cc, fd_nzp, fd_cpr, fd_nx;
   Green g;
 };
 
@@ -242,16 +263,17 @@ __device__ __forceinline__ void plane_sum(double (&v)[NV], double *scratch, doub
 // the cluster barriers before and after order it against both CTAs' own
 // passes.  twx2: W_ny^y, y < ny/2.
 template <bool INV, typename C>
-__device__ __forceinline__ void cross_stage(C *buf, const C *__restrict__ twx2, int nyh, int nzh, int nzs) {
+__device__ __forceinline__ void cross_stage(C *buf, const C *__restrict__ twx2, int nyh, const FastDiv &dz,
+                                            int nzs) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   const unsigned rank = cl.block_rank();
   C *peer = cl.map_shared_rank(buf, rank ^ 1u);
   C *lo = rank == 0 ? buf : peer;
   C *hi = rank == 0 ? peer : buf;
+  const int nzh = (int)dz.d;
   const int total = nyh * nzh;
   const int begin = rank == 0 ? 0 : total / 2, end = rank == 0 ? total / 2 : total;
-  const FastDiv dz(nzh);
   cl.sync();
   constexpr int U = 4;   // pairs in flight per thread
   for (int i0 = begin + threadIdx.x; i0 < end; i0 += U * blockDim.x) {
@@ -366,13 +388,13 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
   const int *pos = sm.pos;
 
   // z: M-point complex transform of the packed rows
-  Batch gz{rows, rows, nzs, 0, 1, false};
+  Batch gz{rows, rows, nzs, 0, 1, false, a.fd_rows, a.fd_rows};
   fft_forward<MaxRadix<NT>::value>(buf, sm.twz, a.pz, gz);
 
   // real-to-complex unpacking, pairs (k, M-k); X[M] goes to slot M
   const int half = M / 2 + 1;
   for (int w = threadIdx.x; w < rows * half; w += blockDim.x) {
-    const int y = w / half, k = w - y * half;
+    const int y = a.fd_half.div(w), k = w - y * half;
     C *row = buf + (size_t)y * nzs;
     if (k == 0) {
       C z0 = row[pos[0]];
@@ -390,11 +412,11 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
       if (pm != pk) row[pm] = cconj(csub(e, wo));
     }
   }
-  if constexpr (SPLIT) cross_stage<false>(buf, sm.twy, rows, nzh, nzs);
+  if constexpr (SPLIT) cross_stage<false>(buf, sm.twy, rows, a.fd_nzh, nzs);
   else __syncthreads();
 
   // y: (ny or ny/2)-point transforms over the nzh slot columns
-  Batch gy{nzh, nzh, 1, 0, nzs, true};
+  Batch gy{nzh, nzh, 1, 0, nzs, true, a.fd_nzh, a.fd_nzh};
   fft_forward<MaxRadix<NT>::value>(buf, SPLIT ? sm.twy + rows : sm.twy, a.py, gy);
 
   // rows -> spectrum rows of nzp entries (bulk stores)
@@ -418,7 +440,7 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
 
 // grid.x = F * nx planes (SPLIT: 2 F nx CTAs in clusters of 2)
 template <typename T, int NT, bool SPLIT>
-__global__ void __launch_bounds__(NT) k_fwd_planes(const T *__restrict__ xi, cx<T> *__restrict__ spec,
+__global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, SPLIT>::value)) k_fwd_planes(const T *__restrict__ xi, cx<T> *__restrict__ spec,
                                                    PlaneArgs a, const int *__restrict__ stop, int *err) {
   if (stop && *stop) return;   // both CTAs of a cluster read the same flag
   fwd_planes_body<T, NT, SPLIT>(xi, spec, a, err, plane_of_block<SPLIT>());
@@ -426,7 +448,7 @@ __global__ void __launch_bounds__(NT) k_fwd_planes(const T *__restrict__ xi, cx<
 
 // grid = (F * nx planes [x 2 for SPLIT], instances of the group)
 template <typename T, int NT, bool SPLIT>
-__global__ void __launch_bounds__(NT) k_fwd_planes_tab(const InstPtrs *__restrict__ tab, PlaneArgs a) {
+__global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, SPLIT>::value)) k_fwd_planes_tab(const InstPtrs *__restrict__ tab, PlaneArgs a) {
   const InstPtrs &ip = tab[blockIdx.y];
   if (ip.flags[0]) return;
   const T *xi = static_cast<const T *>(ip.xi[ip.flags[4]]);
@@ -527,7 +549,7 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
   const size_t ncols = a.ncols;
   const int cpr = (int)(cc * sizeof(C) / 16);    // 16-byte chunks per (field, x) row
   const int nchunks = F * nx * cpr;
-  const FastDiv dc(cpr), dnx(nx);
+  const FastDiv &dc = a.fd_cpr, &dnx = a.fd_nx;
   C *caux = reinterpret_cast<C *>(aux_ptr);
   if (a.mode != PASS_SYNTH) {
     for (int q = threadIdx.x; q < nchunks; q += blockDim.x) {
@@ -543,14 +565,14 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
   if (a.mode != PASS_SYNTH) cp_async_wait_all();
   __syncthreads();
 
-  Batch gx{F * cc, cc, 1, fst, cc, true};
+  Batch gx{F * cc, cc, 1, fst, cc, true, a.fd_fcc, a.fd_cc};
   if (a.mode != PASS_SYNTH) fft_forward<MaxRadix<NT>::value>(buf, twx, a.px, gx);
 
   double dsq = 0.0;
   for (int w = threadIdx.x; w < nx * cc; w += blockDim.x) {
-    const int c = w % cc, sx = w / cc;
+    const int sx = a.fd_cc.div(w), c = w - sx * cc;
     const int col = (int)(col0 + c);
-    const int sy = col / a.nzp, sz = col - sy * a.nzp;
+    const int sy = a.fd_nzp.div(col), sz = col - sy * a.nzp;
     C *pk = buf + sx * cc + c;
     if (a.mode == PASS_SYNTH) {
       bool nq;
@@ -656,7 +678,7 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
 
 // grid.x = ncols / ccols tiles
 template <typename T, int NT>
-__global__ void __launch_bounds__(NT) k_xpencil(cx<T> *__restrict__ spec, PencilArgs a,
+__global__ void __launch_bounds__(NT, (PencilMinBlocks<T>::value)) k_xpencil(cx<T> *__restrict__ spec, PencilArgs a,
                                                 const int *__restrict__ stop) {
   if (stop && *stop) return;
   xpencil_body<T, NT>(spec, a, a.aux, a.partials);
@@ -664,7 +686,7 @@ __global__ void __launch_bounds__(NT) k_xpencil(cx<T> *__restrict__ spec, Pencil
 
 // grid = (tiles, instances of the group)
 template <typename T, int NT>
-__global__ void __launch_bounds__(NT) k_xpencil_tab(const InstPtrs *__restrict__ tab, PencilArgs a) {
+__global__ void __launch_bounds__(NT, (PencilMinBlocks<T>::value)) k_xpencil_tab(const InstPtrs *__restrict__ tab, PencilArgs a) {
   const InstPtrs &ip = tab[blockIdx.y];
   if (ip.flags[0]) return;
   xpencil_body<T, NT>(static_cast<cx<T> *>(ip.spec), a, ip.aux, ip.ppart);
@@ -882,15 +904,15 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   const C *twr = sm.twr;
   const int *pos = sm.pos;
 
-  Batch gy{nzh, nzh, 1, 0, nzs, true};
+  Batch gy{nzh, nzh, 1, 0, nzs, true, a.fd_nzh, a.fd_nzh};
   fft_inverse<MaxRadix<NT>::value>(buf, SPLIT ? sm.twy + rows : sm.twy, a.py, gy);
-  if constexpr (SPLIT) cross_stage<true>(buf, sm.twy, rows, nzh, nzs);
+  if constexpr (SPLIT) cross_stage<true>(buf, sm.twy, rows, a.fd_nzh, nzs);
 
   // complex-to-real packing: Zin[k] = A + i w D, Zin[M-k] = conj(A - i w D),
   // A = X[k] + conj X[M-k], D = X[k] - conj X[M-k], w = exp(+2 pi i k / nz)
   const int half = M / 2 + 1;
   for (int w = threadIdx.x; w < rows * half; w += blockDim.x) {
-    const int y = w / half, k = w - y * half;
+    const int y = a.fd_half.div(w), k = w - y * half;
     C *row = buf + (size_t)y * nzs;
     const int pk = pos[k];
     const int pm = (k == 0) ? -1 : pos[M - k];
@@ -905,7 +927,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   }
   __syncthreads();
 
-  Batch gz{rows, rows, nzs, 0, 1, false};
+  Batch gz{rows, rows, nzs, 0, 1, false, a.fd_rows, a.fd_rows};
   fft_inverse<MaxRadix<NT>::value>(buf, sm.twz, a.pz, gz);
 
   // fused GSFE force + applied stress + masked explicit Euler update,
@@ -921,7 +943,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   const T invN = (T)u.invN;
   const int nvec = nz / VN;
   const int total = rows * nvec;
-  const FastDiv dv(nvec);
+  const FastDiv &dv = a.fd_nvec;
   if (u.mode == PASS_SYNTH) {
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int y = dv.div(i), zq = i - y * nvec;
@@ -1036,7 +1058,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
 
 // grid.x = F * nx planes (SPLIT: 2 F nx CTAs in clusters of 2)
 template <typename T, int NT, bool SPLIT>
-__global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spec, const T *__restrict__ xin,
+__global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, SPLIT>::value)) k_inv_update(const cx<T> *__restrict__ spec, const T *__restrict__ xin,
                                                    T *__restrict__ xout, PlaneArgs a, UpdateArgs u,
                                                    double *__restrict__ partials) {
   if (u.stop && *u.stop) return;
@@ -1047,7 +1069,7 @@ __global__ void __launch_bounds__(NT) k_inv_update(const cx<T> *__restrict__ spe
 // grid = (F * nx planes, instances of the group); per-instance stress, mask,
 // GSFE field and buffers come from the table
 template <typename T, int NT, bool SPLIT>
-__global__ void __launch_bounds__(NT) k_inv_update_tab(const InstPtrs *__restrict__ tab, PlaneArgs a, UpdateArgs u) {
+__global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, SPLIT>::value)) k_inv_update_tab(const InstPtrs *__restrict__ tab, PlaneArgs a, UpdateArgs u) {
   const InstPtrs &ip = tab[blockIdx.y];
   if (ip.flags[0]) return;
   const int cur = ip.flags[4];

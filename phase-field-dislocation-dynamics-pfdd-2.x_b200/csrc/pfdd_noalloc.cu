@@ -208,8 +208,9 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   pa.S = S; pa.F = F;
   pa.tw_y = tw_y; pa.tw_z = tw_z; pa.tw_r = tw_r;
   pa.posM = t_posM - htab + tab;
+  set_plane_divisors<double>(pa, ny);
   PencilArgs pe;
-  memset(&pe, 0, sizeof pe);
+  pe = PencilArgs{};
   pe.px = px;
   pe.nx = nx; pe.ny = ny; pe.nz = nz; pe.nzh = nzh; pe.nzp = nzp; pe.M = M;
   pe.S = S; pe.F = F; pe.imag = IMAG_FULL;
@@ -222,6 +223,7 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   pe.sx_n = sx_n; pe.sy_n = sy_n;
   pe.cd = d.cd_dt;
   pe.g = green;
+  set_pencil_divisors<double>(pe);
   UpdateArgs ua;
   memset(&ua, 0, sizeof ua);
   ua.nx = nx; ua.ny = ny; ua.nz = nz; ua.nzh = nzh; ua.nzp = nzp; ua.S = S; ua.F = F;

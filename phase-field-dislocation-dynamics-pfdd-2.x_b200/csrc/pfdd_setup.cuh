@@ -31,11 +31,30 @@ inline bool make_plan(int n, FftPlan &p, int maxr = 16) {
     if (p.nst >= 8) return false;
     p.radix[p.nst] = r;
     p.L[p.nst] = L;
+    p.twstep[p.nst] = n / L;
+    p.per[p.nst] = FastDiv(n / r);
+    p.lr[p.nst] = FastDiv(L / r);
     ++p.nst;
     L /= r;
     rem /= r;
   }
   return true;
+}
+
+// Host-built divisors of the plane and pencil kernels (after the integer
+// fields of the argument block are set).
+template <typename T> inline void set_plane_divisors(PlaneArgs &pa, int rows) {
+  pa.fd_rows = FastDiv(rows);
+  pa.fd_nzh = FastDiv(pa.nzh);
+  pa.fd_half = FastDiv(pa.M / 2 + 1);
+  pa.fd_nvec = FastDiv(pa.nz / (sizeof(T) == 4 ? 4 : 2));
+}
+template <typename T> inline void set_pencil_divisors(PencilArgs &pe) {
+  pe.fd_fcc = FastDiv(pe.F * pe.ccols);
+  pe.fd_cc = FastDiv(pe.ccols);
+  pe.fd_nzp = FastDiv(pe.nzp);
+  pe.fd_cpr = FastDiv((int)(pe.ccols * sizeof(cx<T>) / 16));
+  pe.fd_nx = FastDiv(pe.nx);
 }
 
 // position of frequency k after the forward (digit-reversing) transform
