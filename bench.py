@@ -51,18 +51,40 @@ def peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+WORKLOADS = ("fcc256", "loop64", "alloy64", "edge128", "frank512")
+
+
 def workload_config(name):
+    """(workloads, description, default precision) of a named configuration."""
     from pfdd_b200 import configs
     if name == "fcc256":
-        w = configs.fcc_workload()
+        ws = [configs.fcc_workload()]
         desc = ("fcc256: 256x256x128 grid, 12 FCC slip systems, 8 seeded loops r~U[8,40], "
                 "sigma_xz 300 MPa, sine GSFE 45/175 mJ/m^2")
+        prec = "fp32"
     elif name == "loop64":
-        w = configs.loop_workload()
-        desc = "loop64: 64^3 grid, 3 systems on one plane, loop r=12 + 1e-3 noise, sigma_xz 200 MPa"
+        ws = [configs.loop_workload()]
+        desc = ("loop64: 64^3 grid, 3 systems on one {111} plane, loop r=12 + U(-1e-3,1e-3) noise (seed 576), "
+                "sigma_xz 200 MPa, sine GSFE 45/175 mJ/m^2, plain FP64")
+        prec = "fp64"
+    elif name == "alloy64":
+        ws = configs.alloy_batch(64)
+        desc = ("alloy64: 64 instances, n^3 with n~U{32,48,64,96,128}, 3 systems, lognormal(0,0.15) per-site "
+                "isf/usf multiplier, sigma~U[100,400] MPa, batched groups + CUDA graphs")
+        prec = "fp32"
+    elif name == "edge128":
+        ws = [configs.edge_workload()]
+        desc = ("edge128: 128x128x32, 3 basal systems, straight edge + 10-cell seeded perturbation, "
+                "sigma_xz 250 MPa; adjoint 500 steps, checkpoint every 50")
+        prec = "fp32"
+    elif name == "frank512":
+        ws = [configs.frank_read_workload()]
+        desc = ("frank512: 512x512x64 on a 60-degree skewed grid, 2 BCC systems, 64-cell pinned segment (xo mask), "
+                "usf 300 mJ/m^2, sigma_yz ramp 0->600 MPa over 20000 one-step stress states")
+        prec = "fp32"
     else:
-        raise SystemExit("unknown workload %s" % name)
-    return w, desc
+        raise SystemExit("unknown workload %s (one of %s)" % (name, ", ".join(WORKLOADS)))
+    return ws, desc, prec
 
 
 def sample_clocks(dev_index):
@@ -72,7 +94,7 @@ def sample_clocks(dev_index):
     f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
     try:
         proc = subprocess.Popen(["nvidia-smi", "-i", str(dev_index), "--query-gpu=" + q,
-                                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=f,
+                                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=f,
                                 stderr=subprocess.DEVNULL)
     except Exception:
         proc = None
@@ -111,13 +133,21 @@ def parse_clocks(proc, path):
 
 
 def kernel_bytes(w, F, csize, rsize):
-    """Algorithmic HBM bytes per launch of each kernel (one read and one write
-    of what the pass must move): P1 reads xi and writes the half spectrum, P2
-    reads and writes it, P3 reads it plus xi and writes xi."""
+    """Algorithmic HBM bytes per launch of each kernel for one instance (one
+    read and one write of what the pass must move): P1 reads xi and writes the
+    half spectrum, P2 reads and writes it, P3 reads it plus xi (and the mask or
+    per-site GSFE field when present) and writes xi."""
     N = w.nx * w.ny * w.nz
     spec = F * w.nx * w.ny * (w.nz // 2 + 1) * csize
     field = F * N * rsize
-    return {"fwd_planes": field + spec, "xpencil": 2 * spec, "inv_update": spec + 2 * field}
+    extra = (w.S * N if w.xo is not None else 0) + (w.S * N * rsize if w.site is not None else 0)
+    return {"fwd_planes": field + spec, "xpencil": 2 * spec, "inv_update": spec + 2 * field + extra}
+
+
+def fields_carried(w):
+    """Real fields through the FFT passes: Re xi, plus Im xi when a mask forces
+    the full complex carrier (otherwise Im xi rides on the Nyquist planes)."""
+    return 2 * w.S if w.xo is not None else w.S
 
 
 def traffic_from_profiles(kernel, workload):
@@ -195,16 +225,78 @@ def reference_arm(args):
     return 0
 
 
+def timed_events(stream, fn):
+    import torch
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), out
+
+
+def fp32_vs_fp64(ws, K, stream, local, steps=2000):
+    """Plain-FP64 workload: FP32 speed (same timed profile pass) and the FP32
+    error against the FP64 GPU path after `steps` steps (relative L2 of Re xi)."""
+    import numpy as np
+    from pfdd_b200 import capi
+    w = ws[0]
+    out = {}
+    for name, prec in (("fp32", capi.FP32), ("fp64", capi.FP64)):
+        with capi.Stepper.from_workloads([w], precision=prec, device=local) as st:
+            st.set_stream(stream.cuda_stream)
+            st.set_state(0, w.xi0)
+            st.advance(5)
+            ms, _ = timed_events(stream, lambda: st.profile(K))
+            out[name + "_ms_per_step"] = ms / K
+            st.set_state(0, w.xi0)
+            st.advance(steps)
+            out[name + "_state"] = st.get_state(0)[0]
+    a, b = out.pop("fp32_state"), out.pop("fp64_state")
+    out["rel_l2_fp32_vs_fp64_after_%d" % steps] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out["fp32_speedup"] = out["fp64_ms_per_step"] / out["fp32_ms_per_step"]
+    return out
+
+
+def adjoint_ratio(st, w, prec, stream, local, steps=500, ckpt=50):
+    """Adjoint (checkpointed, one forward re-run per segment) over forward time
+    for `steps` steps; the target state comes from a forward run with
+    isf 40 / usf 160 mJ/m^2 and 250 MPa."""
+    import copy
+    from pfdd_b200 import capi, configs
+    wt = copy.deepcopy(w)
+    wt.material.isf, wt.material.usf = 0.040, 0.160
+    wt.sigma = configs._sigma("xz", 250e6 / wt.material.mu)
+    with capi.Stepper.from_workloads([wt], precision=prec, device=local) as tg:
+        tg.set_state(0, wt.xi0)
+        tg.advance(steps)
+        target = tg.get_state(0)[0]
+    st.set_state(0, w.xi0)
+    fwd_ms, _ = timed_events(stream, lambda: st.advance(steps))
+    st.set_state(0, w.xi0)
+    adj_ms, res = timed_events(stream, lambda: st.adjoint(0, steps, ckpt, target))
+    loss, dp, ds = res
+    # the adjoint call runs the checkpointed forward, then per segment the
+    # forward recomputation and the backward steps
+    return {"steps": steps, "checkpoint_every": ckpt, "forward_ms": fwd_ms, "adjoint_call_ms": adj_ms,
+            "adjoint_call_over_forward": adj_ms / fwd_ms,
+            "backward_over_forward": (adj_ms - fwd_ms) / fwd_ms, "loss": float(loss),
+            "dL_dparams": [float(x) for x in dp], "dL_dsigma": [float(x) for x in ds]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="fcc256")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--e2e-steps", type=int, default=5000)
+    ap.add_argument("--workload", default="fcc256", choices=WORKLOADS)
+    ap.add_argument("--precision", default=None, choices=["fp32", "fp64"])
+    ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -226,12 +318,17 @@ def main():
         dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = dist_mod
 
-    w, w_desc = workload_config(args.workload)
-    prec = capi.FP32 if args.precision == "fp32" else capi.FP64
-    st = capi.Stepper.from_workloads([w], precision=prec, device=local)
+    ws, w_desc, prec_name = workload_config(args.workload)
+    prec_name = args.precision or prec_name
+    prec = capi.FP32 if prec_name == "fp32" else capi.FP64
+    ramp = args.workload == "frank512"   # one GL step per stress state
+    run_len = {"fcc256": 5000, "loop64": 2000, "alloy64": 1000, "edge128": 500, "frank512": 20000}[args.workload]
+    E = args.e2e_steps or run_len
+    st = capi.Stepper.from_workloads(ws, precision=prec, device=local)
     stream = torch.cuda.current_stream()
     st.set_stream(stream.cuda_stream)
-    st.set_state(0, w.xi0)
+    for i, w in enumerate(ws):
+        st.set_state(i, w.xi0)
     st.advance(args.warmup)
 
     # timed region: K GL iterations with per-kernel events (profile pass)
@@ -254,15 +351,16 @@ def main():
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    S, N = w.S, w.N
-    per_gpu_updates = S * N * args.steps
-    value = per_gpu_updates * world / (ms / 1e3)
+    units_per_step = sum(w.S * w.N for w in ws)
+    value = units_per_step * args.steps * world / (ms / 1e3)
 
-    # roofline of the dominant kernel
-    F = st.descs[0].n_slip  # Re xi field; Im xi rides on the Nyquist planes (no mask)
+    # roofline of the dominant kernel (bytes summed over the instances of every group)
     n_inst, dev_bytes = st.info()
     csize, rsize = (8, 4) if prec == capi.FP32 else (16, 8)
-    kb = kernel_bytes(w, F, csize, rsize)
+    kb = {k: 0 for k in ("fwd_planes", "xpencil", "inv_update")}
+    for w in ws:
+        for k, v in kernel_bytes(w, fields_carried(w), csize, rsize).items():
+            kb[k] += v
     dom = max(kb, key=lambda k: kms[k])
     peak, peak_kind = peak_hbm()
     achieved = kb[dom] / (kms[dom] / 1e3) / 1e9
@@ -270,41 +368,58 @@ def main():
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": kb[dom], "mean_launch_ms": kms[dom],
                 "traffic": traffic_from_profiles(dom, args.workload),
-                "kernel_ms": kms}
+                "kernel_ms": kms,
+                "step_algorithmic_gbs": sum(kb.values()) / (ms / args.steps / 1e3) / 1e9}
 
-    # end to end through the C ABI from pinned host memory
+    # end to end through the C ABI from pinned host memory: every instance's
+    # state in (H2D), the run, every state out (D2H)
     e2e = None
     if rank == 0 or world > 1:
-        n_el = S * N
-        host_in = torch.empty(2 * n_el, dtype=torch.float64, pin_memory=True)
-        host_out = torch.empty(2 * n_el, dtype=torch.float64, pin_memory=True)
-        hin = host_in.numpy()
-        hin[0::2] = w.xi0.reshape(-1)
-        hin[1::2] = 0.0
         import ctypes
         lib = capi.load()
         DP = capi.DP
-        E = args.e2e_steps
-        torch.cuda.synchronize()
-        a0 = torch.cuda.Event(enable_timing=True)
-        a1 = torch.cuda.Event(enable_timing=True)
-        a0.record(stream)
-        rc = lib.pfdd_gpu_set_state_interleaved(st.h, 0, ctypes.cast(host_in.data_ptr(), DP))
-        stats = (capi.StepStats * 1)()
-        rc |= lib.pfdd_gpu_advance(st.h, E, 1, 0.0, stats)
-        rc |= lib.pfdd_gpu_get_state_interleaved(st.h, 0, ctypes.cast(host_out.data_ptr(), DP))
-        a1.record(stream)
-        torch.cuda.synchronize()
+        hosts = []
+        for w in ws:
+            n_el = w.S * w.N
+            hin = torch.empty(2 * n_el, dtype=torch.float64, pin_memory=True)
+            hout = torch.empty(2 * n_el, dtype=torch.float64, pin_memory=True)
+            v = hin.numpy()
+            v[0::2] = w.xi0.reshape(-1)
+            v[1::2] = 0.0
+            hosts.append((hin, hout))
+
+        def run_e2e():
+            rc = 0
+            for i, (hin, _) in enumerate(hosts):
+                rc |= lib.pfdd_gpu_set_state_interleaved(st.h, i, ctypes.cast(hin.data_ptr(), DP))
+            stats = (capi.StepStats * len(ws))()
+            if ramp:
+                rc |= lib.pfdd_gpu_advance(st.h, 1, E, 0.0, stats)
+            else:
+                rc |= lib.pfdd_gpu_advance(st.h, E, 1, 0.0, stats)
+            for i, (_, hout) in enumerate(hosts):
+                rc |= lib.pfdd_gpu_get_state_interleaved(st.h, i, ctypes.cast(hout.data_ptr(), DP))
+            return rc
+
+        ems, rc = timed_events(stream, run_e2e)
         if rc != 0:
             raise RuntimeError(lib.pfdd_gpu_last_error(st.h))
-        ems = a0.elapsed_time(a1)
         if dist:
             t = torch.tensor([ems], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ems = float(t.item())
-        e2e = {"value": S * N * E * world / (ems / 1e3), "unit": UNIT, "steps": E,
-               "h2d_bytes_per_step": 16 * n_el / E, "d2h_bytes_per_step": 16 * n_el / E + 16,
-               "note": "set_state_interleaved + advance(%d) + get_state_interleaved, pinned host buffers" % E}
+        nbytes = sum(16 * w.S * w.N for w in ws)
+        e2e = {"value": units_per_step * E * world / (ems / 1e3), "unit": UNIT, "steps": E,
+               "h2d_bytes_per_step": nbytes / E, "d2h_bytes_per_step": nbytes / E + 16 * len(ws),
+               "note": ("set_state_interleaved + advance(%s) + get_state_interleaved per instance, pinned host "
+                        "buffers" % ("1 step x %d stress states" % E if ramp else "%d" % E))}
+
+    extras = {}
+    if not args.no_extras and rank == 0:
+        if args.workload == "loop64":
+            extras["fp32_vs_fp64"] = fp32_vs_fp64(ws, args.steps, stream, local)
+        if args.workload == "edge128":
+            extras["adjoint"] = adjoint_ratio(st, ws[0], prec, stream, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -320,13 +435,17 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == capi.FP32 else "f64",
             "data": "synthetic",
-            "config": {"workload": w_desc, "grid": [w.nx, w.ny, w.nz], "slip_systems": S,
-                       "precision": args.precision, "imag_part": "Nyquist-plane spectrum carried in the x-pencil pass",
+            "config": {"workload": w_desc, "instances": len(ws),
+                       "grid": [ws[0].nx, ws[0].ny, ws[0].nz] if len(ws) == 1 else "mixed",
+                       "slip_systems": ws[0].S, "precision": prec_name,
+                       "imag_part": ("full complex carrier (obstacle mask)" if ws[0].xo is not None else
+                                     "Nyquist-plane spectrum carried in the x-pencil pass"),
                        "parallelism": "replicas x%d" % world,
                        "l2": "working set %.2f GB > 126 MB L2 (no flush)" % (dev_bytes / 1e9)},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches_per_step * args.steps + 1,
         }
+        line.update(extras)
         print(json.dumps(line))
     st.close()
     if dist:

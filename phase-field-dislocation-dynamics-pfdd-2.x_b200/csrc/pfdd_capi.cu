@@ -127,6 +127,7 @@ struct pfdd_gpu {
   DevBuf staging;                     // FP64 host<->device staging, kept across calls
   std::string err;
   size_t device_bytes = 0;
+  int nsm = 148;                      // SMs of the device (grid sizing)
 };
 
 namespace {
@@ -278,7 +279,10 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
     return ((size_t)I.F * fstride_for(cc) + I.nx) * sizeof(C) + 64 * sizeof(double);
   };
   int cc = 32;
-  while (cc > cmin && (ncols % cc || pencil_bytes(cc) > PFDD_PENCIL_SMEM_KB * 1024)) cc >>= 1;
+  // widest tile that fits the budget and still gives every SM two tiles
+  while (cc > cmin && (ncols % cc || pencil_bytes(cc) > PFDD_PENCIL_SMEM_KB * 1024 ||
+                       ncols / cc < 2 * (size_t)h->nsm))
+    cc >>= 1;
   if (ncols % cc || pencil_bytes(cc) > limit)
     return fail(h, PFDD_EUNSUPPORTED, "x-pencil of %d x %d fields does not fit shared memory", I.nx, I.F);
   I.ccols = cc;
@@ -443,7 +447,7 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   if (ev) cudaEventRecord(ev[3], st);
   if (adj) return;
   const bool nyq = I.imag == IMAG_NYQ;
-  k_finalize<<<1, 1024, 0, st>>>(I.partials.as<double>(), planes, I.stats.as<double>(), step, tol, flags,
+  k_finalize<<<1, 256, 0, st>>>(I.partials.as<double>(), planes, I.stats.as<double>(), step, tol, flags,
                                  flags + 1, flags + 2, nyq ? I.ppart.as<double>() : nullptr, nyq ? I.ntiles : 0,
                                  1.0 / (double)I.N);
   if (ev) cudaEventRecord(ev[4], st);
@@ -547,7 +551,7 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   launch_inv_tab<T>(L, B, st, tab, pa, ua);
   if (ev) cudaEventRecord(ev[3], st);
   const bool nyq = L.imag == IMAG_NYQ;
-  k_finalize_tab<<<B, 1024, 0, st>>>(tab, planes, nyq ? L.ntiles : 0, 1.0 / (double)L.N, tol);
+  k_finalize_tab<<<B, 256, 0, st>>>(tab, planes, nyq ? L.ntiles : 0, 1.0 / (double)L.N, tol);
   if (ev) cudaEventRecord(ev[4], st);
 }
 
@@ -1073,6 +1077,7 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
   h->opt = o;
   h->precision = o.precision;
   h->device = o.device;
+  h->nsm = prop.multiProcessorCount;
   if (cudaSetDevice(o.device) != cudaSuccess) return fail(nullptr, PFDD_ECUDA, "cudaSetDevice failed");
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(nullptr, PFDD_ECUDA, "stream creation failed");
@@ -1112,7 +1117,8 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
     // in the environment forces the choice.
     const size_t whole = (o.precision == PFDD_FP32) ? PlaneSmem<cx<float>>::bytes(I->ny, I->ny, I->nzs, I->M)
                                                     : PlaneSmem<cx<double>>::bytes(I->ny, I->ny, I->nzs, I->M);
-    I->split = whole > kSplitAbove;
+    // (small grids split too, so the plane passes fill the SMs twice over)
+    I->split = whole > kSplitAbove || I->F * I->nx < 2 * h->nsm;
     if (const char *env = getenv("PFDD_PLANE_SPLIT")) {
       if (!strcmp(env, "0")) I->split = false;
       else if (!strcmp(env, "1")) I->split = true;

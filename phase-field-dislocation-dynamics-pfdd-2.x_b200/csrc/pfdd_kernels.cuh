@@ -1079,46 +1079,66 @@ __global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, SPLIT>::value)) k_inv_u
 }
 
 // ------------------------------------------------------------ reduction
-// One block: Neumaier-compensated FP64 sums of the per-plane partials.
-// stats[step] = {xinorm, xiave}; sets *stop when 0 < tol and xinorm < tol;
-// flags a non-finite result in *bad.
+// Neumaier-compensated FP64 sums: each thread folds a strided share of the
+// partials into (sum, compensation) pairs; the pairs are merged by a fixed
+// shuffle tree within each warp and then across warps, so the result does
+// not depend on timing.
+__device__ __forceinline__ void neu_add(double &s, double &c, double v) {
+  const double t = s + v;
+  c += (fabs(s) >= fabs(v)) ? (s - t) + v : (v - t) + s;
+  s = t;
+}
+__device__ __forceinline__ void neu_merge(double &s, double &c, double s2, double c2) {
+  neu_add(s, c, s2);
+  c += c2;
+}
+// merge (s0, c0), (s1, c1) over the block; thread 0 ends with the totals.
+// scratch: 4 * 32 doubles.
+__device__ __forceinline__ void block_neumaier2(double &s0, double &c0, double &s1, double &c1, double *scratch) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double a = __shfl_down_sync(0xffffffffu, s0, o), b = __shfl_down_sync(0xffffffffu, c0, o);
+    const double d = __shfl_down_sync(0xffffffffu, s1, o), e = __shfl_down_sync(0xffffffffu, c1, o);
+    neu_merge(s0, c0, a, b);
+    neu_merge(s1, c1, d, e);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (lane == 0) {
+    scratch[wid] = s0; scratch[32 + wid] = c0; scratch[64 + wid] = s1; scratch[96 + wid] = c1;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    s0 = lane < nw ? scratch[lane] : 0.0;
+    c0 = lane < nw ? scratch[32 + lane] : 0.0;
+    s1 = lane < nw ? scratch[64 + lane] : 0.0;
+    c1 = lane < nw ? scratch[96 + lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double a = __shfl_down_sync(0xffffffffu, s0, o), b = __shfl_down_sync(0xffffffffu, c0, o);
+      const double d = __shfl_down_sync(0xffffffffu, s1, o), e = __shfl_down_sync(0xffffffffu, c1, o);
+      neu_merge(s0, c0, a, b);
+      neu_merge(s1, c1, d, e);
+    }
+  }
+}
+
+// One block: stats[step] = {xinorm, xiave} from the per-plane partials (and
+// the x-pencil partials of the Nyquist carrier, scaled); sets *stop when
+// 0 < tol and xinorm < tol; flags a non-finite result in *bad.
 static __global__ void k_finalize(const double *__restrict__ partials, int nparts, double *__restrict__ stats, int step,
-                           double tol, int *stop, int *bad, int *steps_done, const double *__restrict__ partials2,
-                           int nparts2, double scale2) {
+                                  double tol, int *stop, int *bad, int *steps_done, const double *__restrict__ partials2,
+                                  int nparts2, double scale2) {
   if (stop && *stop) return;
-  __shared__ double sh[4][1024];
+  __shared__ double sh[128];
   double s0 = 0, c0 = 0, s1 = 0, c1 = 0;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
-    double v = partials[2 * i], t = s0 + v;
-    c0 += (fabs(s0) >= fabs(v)) ? (s0 - t) + v : (v - t) + s0;
-    s0 = t;
-    v = partials[2 * i + 1];
-    t = s1 + v;
-    c1 += (fabs(s1) >= fabs(v)) ? (s1 - t) + v : (v - t) + s1;
-    s1 = t;
+    neu_add(s0, c0, partials[2 * i]);
+    neu_add(s1, c1, partials[2 * i + 1]);
   }
-  for (int i = threadIdx.x; i < nparts2; i += blockDim.x) {
-    double v = partials2[2 * i] * scale2, t = s0 + v;
-    c0 += (fabs(s0) >= fabs(v)) ? (s0 - t) + v : (v - t) + s0;
-    s0 = t;
-  }
-  sh[0][threadIdx.x] = s0; sh[1][threadIdx.x] = c0; sh[2][threadIdx.x] = s1; sh[3][threadIdx.x] = c1;
-  __syncthreads();
+  for (int i = threadIdx.x; i < nparts2; i += blockDim.x) neu_add(s0, c0, partials2[2 * i] * scale2);
+  block_neumaier2(s0, c0, s1, c1, sh);
   if (threadIdx.x == 0) {
-    double a0 = 0, e0 = 0, a1 = 0, e1 = 0;
-    for (int i = 0; i < (int)blockDim.x; ++i) {
-      double v = sh[0][i], t = a0 + v;
-      e0 += (fabs(a0) >= fabs(v)) ? (a0 - t) + v : (v - t) + a0;
-      a0 = t;
-      e0 += sh[1][i];
-      v = sh[2][i];
-      t = a1 + v;
-      e1 += (fabs(a1) >= fabs(v)) ? (a1 - t) + v : (v - t) + a1;
-      a1 = t;
-      e1 += sh[3][i];
-    }
-    double dsq = a0 + e0;
-    const double xinorm = sqrt(dsq), xiave = a1 + e1;
+    const double xinorm = sqrt(s0 + c0), xiave = s1 + c1;
     stats[2 * step] = xinorm;
     stats[2 * step + 1] = xiave;
     if (steps_done) *steps_done = step + 1;
@@ -1128,47 +1148,26 @@ static __global__ void k_finalize(const double *__restrict__ partials, int npart
 }
 
 // One block per instance of a group: records {xinorm, xiave} at index
-// steps_done, counts the step, flips the buffer parity and sets the stop flag
-// when 0 < tol and xinorm < tol (solve_GL.cpp:137-141).
+// flags[2] (when within the stats capacity), advances flags[2], flips the
+// buffer parity flags[4], flags non-finite results and sets the stop flag
+// when 0 < tol and xinorm < tol.
 static __global__ void k_finalize_tab(const InstPtrs *__restrict__ tab, int nparts, int nparts2, double scale2,
                                       double tol) {
   const InstPtrs &ip = tab[blockIdx.x];
   int *flags = ip.flags;
   if (flags[0]) return;
-  __shared__ double sh[4][1024];
+  __shared__ double sh[128];
   const double *partials = ip.partials, *partials2 = ip.ppart;
   double s0 = 0, c0 = 0, s1 = 0, c1 = 0;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
-    double v = partials[2 * i], t = s0 + v;
-    c0 += (fabs(s0) >= fabs(v)) ? (s0 - t) + v : (v - t) + s0;
-    s0 = t;
-    v = partials[2 * i + 1];
-    t = s1 + v;
-    c1 += (fabs(s1) >= fabs(v)) ? (s1 - t) + v : (v - t) + s1;
-    s1 = t;
+    neu_add(s0, c0, partials[2 * i]);
+    neu_add(s1, c1, partials[2 * i + 1]);
   }
   if (partials2)
-    for (int i = threadIdx.x; i < nparts2; i += blockDim.x) {
-      double v = partials2[2 * i] * scale2, t = s0 + v;
-      c0 += (fabs(s0) >= fabs(v)) ? (s0 - t) + v : (v - t) + s0;
-      s0 = t;
-    }
-  sh[0][threadIdx.x] = s0; sh[1][threadIdx.x] = c0; sh[2][threadIdx.x] = s1; sh[3][threadIdx.x] = c1;
-  __syncthreads();
+    for (int i = threadIdx.x; i < nparts2; i += blockDim.x) neu_add(s0, c0, partials2[2 * i] * scale2);
+  block_neumaier2(s0, c0, s1, c1, sh);
   if (threadIdx.x == 0) {
-    double a0 = 0, e0 = 0, a1 = 0, e1 = 0;
-    for (int i = 0; i < (int)blockDim.x; ++i) {
-      double v = sh[0][i], t = a0 + v;
-      e0 += (fabs(a0) >= fabs(v)) ? (a0 - t) + v : (v - t) + a0;
-      a0 = t;
-      e0 += sh[1][i];
-      v = sh[2][i];
-      t = a1 + v;
-      e1 += (fabs(a1) >= fabs(v)) ? (a1 - t) + v : (v - t) + a1;
-      a1 = t;
-      e1 += sh[3][i];
-    }
-    const double xinorm = sqrt(a0 + e0), xiave = a1 + e1;
+    const double xinorm = sqrt(s0 + c0), xiave = s1 + c1;
     const int k = flags[2];
     if (k < ip.stats_cap) {
       ip.stats[2 * k] = xinorm;

@@ -239,7 +239,7 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   k_fwd_planes<double, 256, false><<<planes, 256, smem_plane, s>>>(d_xi_in, spec, pa, flags, flags + 3);
   k_xpencil<double, 256><<<(int)(ncols / cc), 256, pencil_bytes(cc), s>>>(spec, pe, flags);
   k_inv_update<double, 256, false><<<planes, 256, smem_plane, s>>>(spec, d_xi_in, d_xi_out, pa, ua, partials);
-  k_finalize<<<1, 1024, 0, s>>>(partials, planes, stats, 0, 0.0, flags, flags + 1, flags + 2, nullptr, 0, 0.0);
+  k_finalize<<<1, 256, 0, s>>>(partials, planes, stats, 0, 0.0, flags, flags + 1, flags + 2, nullptr, 0, 0.0);
   e = cudaGetLastError();
   if (e != cudaSuccess) return nerr(PFDD_ECUDA, cudaGetErrorString(e));
   if (h_stats) {
