@@ -225,6 +225,23 @@ def reference_arm(args):
     return 0
 
 
+def max_over_ranks(x, dist, device="cuda"):
+    """The largest of each rank's x (every rank calls this at the same point;
+    one all-reduce).  Without a process group, x itself."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(units_per_rank, world, ms):
+    """Whole-job throughput: the units every rank processed over the slowest
+    rank's time (ms)."""
+    return units_per_rank * world / (ms / 1e3)
+
+
 def timed_events(stream, fn):
     import torch
     torch.cuda.synchronize()
@@ -346,13 +363,9 @@ def main():
     if dist:
         dist.barrier()
     clocks = parse_clocks(clk_proc, clk_path)
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
     units_per_step = sum(w.S * w.N for w in ws)
-    value = units_per_step * args.steps * world / (ms / 1e3)
+    value = aggregate_rate(units_per_step * args.steps, world, ms)
 
     # roofline of the dominant kernel (bytes summed over the instances of every group)
     n_inst, dev_bytes = st.info()
@@ -404,12 +417,9 @@ def main():
         ems, rc = timed_events(stream, run_e2e)
         if rc != 0:
             raise RuntimeError(lib.pfdd_gpu_last_error(st.h))
-        if dist:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(ems, dist)
         nbytes = sum(16 * w.S * w.N for w in ws)
-        e2e = {"value": units_per_step * E * world / (ems / 1e3), "unit": UNIT, "steps": E,
+        e2e = {"value": aggregate_rate(units_per_step * E, world, ems), "unit": UNIT, "steps": E,
                "h2d_bytes_per_step": nbytes / E, "d2h_bytes_per_step": nbytes / E + 16 * len(ws),
                "note": ("set_state_interleaved + advance(%s) + get_state_interleaved per instance, pinned host "
                         "buffers" % ("1 step x %d stress states" % E if ramp else "%d" % E))}

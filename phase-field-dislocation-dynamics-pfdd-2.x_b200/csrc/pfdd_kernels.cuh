@@ -389,7 +389,7 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
 
   // z: M-point complex transform of the packed rows
   Batch gz{rows, rows, nzs, 0, 1, false, a.fd_rows, a.fd_rows};
-  fft_forward<MaxRadix<NT>::value>(buf, sm.twz, a.pz, gz);
+  fft_forward<MaxRadix<NT>::value, GeomRows>(buf, sm.twz, a.pz, gz);
 
   // real-to-complex unpacking, pairs (k, M-k); X[M] goes to slot M
   const int half = M / 2 + 1;
@@ -417,7 +417,7 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
 
   // y: (ny or ny/2)-point transforms over the nzh slot columns
   Batch gy{nzh, nzh, 1, 0, nzs, true, a.fd_nzh, a.fd_nzh};
-  fft_forward<MaxRadix<NT>::value>(buf, SPLIT ? sm.twy + rows : sm.twy, a.py, gy);
+  fft_forward<MaxRadix<NT>::value, GeomCols>(buf, SPLIT ? sm.twy + rows : sm.twy, a.py, gy);
 
   // rows -> spectrum rows of nzp entries (bulk stores)
   fence_proxy_async();
@@ -566,7 +566,7 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
   __syncthreads();
 
   Batch gx{F * cc, cc, 1, fst, cc, true, a.fd_fcc, a.fd_cc};
-  if (a.mode != PASS_SYNTH) fft_forward<MaxRadix<NT>::value>(buf, twx, a.px, gx);
+  if (a.mode != PASS_SYNTH) fft_forward<MaxRadix<NT>::value, GeomPencil>(buf, twx, a.px, gx);
 
   double dsq = 0.0;
   for (int w = threadIdx.x; w < nx * cc; w += blockDim.x) {
@@ -665,7 +665,7 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
   if (ppart) block_sum2(dsq, 0.0, red, ppart + 2 * blockIdx.x);
   __syncthreads();
 
-  fft_inverse<MaxRadix<NT>::value>(buf, twx, a.px, gx);
+  fft_inverse<MaxRadix<NT>::value, GeomPencil>(buf, twx, a.px, gx);
 
   for (int q = threadIdx.x; q < nchunks; q += blockDim.x) {
     const int fx = dc.div(q), ch = q - fx * cpr;
@@ -905,7 +905,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   const int *pos = sm.pos;
 
   Batch gy{nzh, nzh, 1, 0, nzs, true, a.fd_nzh, a.fd_nzh};
-  fft_inverse<MaxRadix<NT>::value>(buf, SPLIT ? sm.twy + rows : sm.twy, a.py, gy);
+  fft_inverse<MaxRadix<NT>::value, GeomCols>(buf, SPLIT ? sm.twy + rows : sm.twy, a.py, gy);
   if constexpr (SPLIT) cross_stage<true>(buf, sm.twy, rows, a.fd_nzh, nzs);
 
   // complex-to-real packing: Zin[k] = A + i w D, Zin[M-k] = conj(A - i w D),
@@ -928,7 +928,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   __syncthreads();
 
   Batch gz{rows, rows, nzs, 0, 1, false, a.fd_rows, a.fd_rows};
-  fft_inverse<MaxRadix<NT>::value>(buf, sm.twz, a.pz, gz);
+  fft_inverse<MaxRadix<NT>::value, GeomRows>(buf, sm.twz, a.pz, gz);
 
   // fused GSFE force + applied stress + masked explicit Euler update,
   // VN consecutive z per thread, two vectors in flight per iteration
