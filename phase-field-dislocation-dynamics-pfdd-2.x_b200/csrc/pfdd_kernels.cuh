@@ -21,6 +21,15 @@
 // permutes kx inside shared memory only.  Frequencies are recovered through
 // slot tables, so no transform ever reorders data.
 //
+// DC / Nyquist packing: after the z real-to-complex transform the kz = 0 and
+// kz = nz/2 columns of a plane are both real, so the y transforms carry them
+// as one complex column Z = Y0 + i YM in slot 0 and run over M = nz/2 columns
+// (a multiple of the warp width) instead of nz/2 + 1.  P1 splits Z back into
+// Y0[ky] = (Z[ky] + conj Z[-ky]) / 2 and YM[ky] = (Z[ky] - conj Z[-ky]) / (2i)
+// before storing (the spectrum layout keeps the Nyquist column at slot M);
+// P3 packs Y0 + i YM before its inverse y transform, which then returns the
+// two real columns as the real and imaginary parts of slot 0.
+//
 // Split planes (SPLIT = true): P1 and P3 can run each (field, x) plane on a
 // cluster of two CTAs, CTA rank r holding rows [r ny/2, (r+1) ny/2) in its
 // own shared memory; the first radix-2 stage of the y transform (rows y and
@@ -104,9 +113,10 @@ struct PlaneArgs {
   int S, F;                   // slip systems; fields in flight (S, or 2S with Im xi)
   const void *tw_y, *tw_z, *tw_r;   // W_ny^m, W_M^m, W_nz^k tables in compute precision
   const int16_t *posM;        // position of z-frequency k (< M) after the M-point transform
-  // divisors built on the host: rows per CTA (ny, or ny/2 when split), nzh,
-  // M/2 + 1 (real-to-complex pairs per row), nz / vector width
-  FastDiv fd_rows, fd_nzh, fd_half, fd_nvec;
+  const int16_t *negy;        // slot of -ky for each local y slot (a split plane's rank r at r * rows)
+  // divisors built on the host: rows per CTA (ny, or ny/2 when split),
+  // M/2 + 1 (real-to-complex pairs per row), nz / vector width, M
+  FastDiv fd_rows, fd_half, fd_nvec, fd_m;
 };
 
 struct PencilArgs {
@@ -391,15 +401,15 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
   Batch gz{rows, rows, nzs, 0, 1, false, a.fd_rows, a.fd_rows};
   fft_forward<MaxRadix<NT>::value, GeomRows>(buf, sm.twz, a.pz, gz);
 
-  // real-to-complex unpacking, pairs (k, M-k); X[M] goes to slot M
+  // real-to-complex unpacking, pairs (k, M-k); X[M] rides in slot 0 (see the packing note)
   const int half = M / 2 + 1;
   for (int w = threadIdx.x; w < rows * half; w += blockDim.x) {
     const int y = a.fd_half.div(w), k = w - y * half;
     C *row = buf + (size_t)y * nzs;
     if (k == 0) {
+      // X[0] = z0.x + z0.y and X[M] = z0.x - z0.y are real: packed as X[0] + i X[M]
       C z0 = row[pos[0]];
-      row[pos[0]] = mk<C>(z0.x + z0.y, (T)0);
-      row[M] = mk<C>(z0.x - z0.y, (T)0);
+      row[pos[0]] = mk<C>(z0.x + z0.y, z0.x - z0.y);
       for (int q = nzh; q < nzp; ++q) row[q] = mk<C>((T)0, (T)0);
     } else {
       const int pk = pos[k], pm = pos[M - k];
@@ -412,12 +422,32 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
       if (pm != pk) row[pm] = cconj(csub(e, wo));
     }
   }
-  if constexpr (SPLIT) cross_stage<false>(buf, sm.twy, rows, a.fd_nzh, nzs);
+  if constexpr (SPLIT) cross_stage<false>(buf, sm.twy, rows, a.fd_m, nzs);
   else __syncthreads();
 
-  // y: (ny or ny/2)-point transforms over the nzh slot columns
-  Batch gy{nzh, nzh, 1, 0, nzs, true, a.fd_nzh, a.fd_nzh};
+  // y: (ny or ny/2)-point transforms over the M slot columns (Nyquist packed in slot 0)
+  Batch gy{M, M, 1, 0, nzs, true, a.fd_m, a.fd_m};
   fft_forward<MaxRadix<NT>::value, GeomCols>(buf, SPLIT ? sm.twy + rows : sm.twy, a.py, gy);
+
+  // split slot 0 into the kz = 0 (slot 0) and kz = nz/2 (slot M) spectra; the
+  // partner -ky of a local slot lies in the same CTA (ky and -ky have equal parity)
+  {
+    const int16_t *neg = a.negy + row0;
+    for (int y = threadIdx.x; y < rows; y += blockDim.x) {
+      const int t = neg[y];
+      if (t < y) continue;   // the pair is handled by the thread of its smaller slot
+      C *ps = buf + (size_t)y * nzs, *pt = buf + (size_t)t * nzs;
+      const C zs = ps[0], zt = pt[0];
+      const C y0 = mk<C>((T)0.5 * (zs.x + zt.x), (T)0.5 * (zs.y - zt.y));
+      const C ym = mk<C>((T)0.5 * (zs.y + zt.y), (T)-0.5 * (zs.x - zt.x));
+      ps[0] = y0;
+      ps[M] = ym;
+      if (t != y) {
+        pt[0] = cconj(y0);
+        pt[M] = cconj(ym);
+      }
+    }
+  }
 
   // rows -> spectrum rows of nzp entries (bulk stores)
   fence_proxy_async();
@@ -874,11 +904,15 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   using V = typename Vec<T>::type;
   constexpr int VN = Vec<T>::n;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int ny = a.ny, nz = a.nz, nzh = a.nzh, nzp = a.nzp, nzs = a.nzs, M = a.M;
+  const int ny = a.ny, nz = a.nz, nzp = a.nzp, nzs = a.nzs, M = a.M;
   const int rows = SPLIT ? ny / 2 : ny;
   const int row0 = row0_of_block<SPLIT>(ny);
   const PlaneSmem<C> sm(smem_raw, a, rows);
-  if (threadIdx.x == 0) mbar_init(sm.bar, 1);
+  if (threadIdx.x == 0) {
+    mbar_init(sm.bar, 1);
+    // the update reads this CTA's xi rows after the transforms: start them towards L2 now
+    if (u.mode != PASS_SYNTH) prefetch_l2_bulk(xin + (plane * ny + row0) * nz, (uint32_t)(rows * nz * sizeof(T)));
+  }
   __syncthreads();
   // spectrum rows of nzp entries -> shared rows of nzs (bulk copies, one warp)
   if (threadIdx.x < 32) {
@@ -904,9 +938,16 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   const C *twr = sm.twr;
   const int *pos = sm.pos;
 
-  Batch gy{nzh, nzh, 1, 0, nzs, true, a.fd_nzh, a.fd_nzh};
+  // pack the kz = 0 and kz = nz/2 columns into slot 0: Y0 + i YM
+  for (int y = threadIdx.x; y < rows; y += blockDim.x) {
+    C *row = buf + (size_t)y * nzs;
+    const C y0 = row[0], ym = row[M];
+    row[0] = mk<C>(y0.x - ym.y, y0.y + ym.x);
+  }
+  __syncthreads();
+  Batch gy{M, M, 1, 0, nzs, true, a.fd_m, a.fd_m};
   fft_inverse<MaxRadix<NT>::value, GeomCols>(buf, SPLIT ? sm.twy + rows : sm.twy, a.py, gy);
-  if constexpr (SPLIT) cross_stage<true>(buf, sm.twy, rows, a.fd_nzh, nzs);
+  if constexpr (SPLIT) cross_stage<true>(buf, sm.twy, rows, a.fd_m, nzs);
 
   // complex-to-real packing: Zin[k] = A + i w D, Zin[M-k] = conj(A - i w D),
   // A = X[k] + conj X[M-k], D = X[k] - conj X[M-k], w = exp(+2 pi i k / nz)
@@ -915,15 +956,21 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
     const int y = a.fd_half.div(w), k = w - y * half;
     C *row = buf + (size_t)y * nzs;
     const int pk = pos[k];
-    const int pm = (k == 0) ? -1 : pos[M - k];
+    if (k == 0) {
+      // slot 0 holds x0 + i xM (the real kz = 0 and kz = nz/2 columns): Zin[0] = (x0 + xM) + i (x0 - xM)
+      const C z = row[pk];
+      row[pk] = mk<C>(z.x + z.y, z.x - z.y);
+      continue;
+    }
+    const int pm = pos[M - k];
     const C xk = row[pk];
-    const C xm = (k == 0) ? row[M] : row[pm];
+    const C xm = row[pm];
     const C A = mk<C>(xk.x + xm.x, xk.y - xm.y);
     const C D = mk<C>(xk.x - xm.x, xk.y + xm.y);
     const C wd = cmulc(D, twr[k]);            // D * conj(W^k) = D * exp(+2 pi i k/nz)
     const C iwd = mk<C>(-wd.y, wd.x);
     row[pk] = cadd(A, iwd);
-    if (k != 0 && pm != pk) row[pm] = cconj(csub(A, iwd));
+    if (pm != pk) row[pm] = cconj(csub(A, iwd));
   }
   __syncthreads();
 

@@ -45,9 +45,9 @@ inline bool make_plan(int n, FftPlan &p, int maxr = 16) {
 // fields of the argument block are set).
 template <typename T> inline void set_plane_divisors(PlaneArgs &pa, int rows) {
   pa.fd_rows = FastDiv(rows);
-  pa.fd_nzh = FastDiv(pa.nzh);
   pa.fd_half = FastDiv(pa.M / 2 + 1);
   pa.fd_nvec = FastDiv(pa.nz / (sizeof(T) == 4 ? 4 : 2));
+  pa.fd_m = FastDiv(pa.M);
 }
 template <typename T> inline void set_pencil_divisors(PencilArgs &pe) {
   pe.fd_fcc = FastDiv(pe.F * pe.ccols);
@@ -55,6 +55,22 @@ template <typename T> inline void set_pencil_divisors(PencilArgs &pe) {
   pe.fd_nzp = FastDiv(pe.nzp);
   pe.fd_cpr = FastDiv((int)(pe.ccols * sizeof(cx<T>) / 16));
   pe.fd_nx = FastDiv(pe.nx);
+}
+
+// Slot of -ky for every local y slot (PlaneArgs::negy).  pos[k] is the slot
+// of frequency k under the y plan (length ny, or ny/2 for a split plane whose
+// rank r holds ky = r + 2k at the slots of the ny/2 plan); rank r's entries
+// start at r * (ny/2).  Stack storage only (ny <= 1024).
+inline void neg_slots(int ny, bool split, const int *pos, int16_t *out) {
+  const int n = split ? ny / 2 : ny;
+  int kloc[1024];
+  for (int k = 0; k < n; ++k) kloc[pos[k]] = k;
+  for (int r = 0; r < (split ? 2 : 1); ++r)
+    for (int sl = 0; sl < n; ++sl) {
+      const int ky = split ? r + 2 * kloc[sl] : kloc[sl];
+      const int nk = (ny - ky) % ny;   // same parity as ky (ny even)
+      out[r * n + sl] = (int16_t)pos[split ? (nk - r) / 2 : nk];
+    }
 }
 
 // position of frequency k after the forward (digit-reversing) transform
