@@ -196,14 +196,19 @@ pfdd_status pfdd_gpu_tau(pfdd_gpu *h, int inst, double *tau);
  * bracket it with its own events. */
 pfdd_status pfdd_gpu_set_stream(pfdd_gpu *h, void *stream);
 
-/* Kernel classes of one GL iteration, in launch order. */
-enum { PFDD_K_FWD_PLANES = 0, PFDD_K_XPENCIL = 1, PFDD_K_INV_UPDATE = 2, PFDD_K_FINALIZE = 3, PFDD_NKERNELS = 4 };
+/* Kernel classes of a run of GL iterations, in launch order: the forward
+ * plane pass that opens the run (once), then per iteration the x-pencil pass,
+ * the plane pass (inverse transforms + update, fused with the next
+ * iteration's forward transforms) and the reduction. */
+enum { PFDD_K_FWD_PLANES = 0, PFDD_K_XPENCIL = 1, PFDD_K_STEP_PLANES = 2, PFDD_K_FINALIZE = 3, PFDD_NKERNELS = 4 };
 
 /* Advance n_steps GL iterations (one stress state, no tolerance test) with a
- * CUDA event pair around every launch and return the mean device time per
- * launch of each kernel class in kernel_ms[PFDD_NKERNELS] (summed over
- * instances), and the number of kernel launches one iteration makes.  The
- * state advances exactly as with pfdd_gpu_advance. */
+ * CUDA event pair around every launch and return the device time per
+ * iteration of each kernel class in kernel_ms[PFDD_NKERNELS] (summed over
+ * instances; the opening forward pass is divided by n_steps), and the number
+ * of kernel launches one iteration makes (the run adds one stress-state and
+ * one opening launch per batched group).  The state advances exactly as with
+ * pfdd_gpu_advance. */
 pfdd_status pfdd_gpu_profile(pfdd_gpu *h, int n_steps, double *kernel_ms, int *launches_per_step);
 
 /* Number of instances, and the device bytes the handle holds. */

@@ -111,8 +111,13 @@ struct Group {
 
 struct GraphKey {
   int steps;
+  int states;   // 0: steps of the current stress state; k > 0: k whole stress states of `steps` steps
   double tol;
-  bool operator<(const GraphKey &o) const { return steps < o.steps || (steps == o.steps && tol < o.tol); }
+  bool operator<(const GraphKey &o) const {
+    if (steps != o.steps) return steps < o.steps;
+    if (states != o.states) return states < o.states;
+    return tol < o.tol;
+  }
 };
 
 struct pfdd_gpu {
@@ -331,6 +336,10 @@ pfdd_status set_smem_attrs(pfdd_gpu *h, size_t plane, size_t upd, size_t pencil)
   CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update_tab<T, NP, false>, A, (int)upd));
   CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update_tab<T, NH, true>, A, (int)upd));
   CUDA_TRY(h, cudaFuncSetAttribute(k_xpencil_tab<T, NC>, A, (int)pencil));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes<T, NP, false>, A, (int)upd));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes<T, NH, true>, A, (int)upd));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes_tab<T, NP, false>, A, (int)upd));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes_tab<T, NH, true>, A, (int)upd));
   return PFDD_OK;
 }
 
@@ -370,7 +379,7 @@ void launch_fwd_tab(const Instance &L, unsigned B, cudaStream_t st, const InstPt
   else k_fwd_planes_tab<T, NP, false><<<dim3(planes, B), NP, L.smem_plane, st>>>(tab, pa);
 }
 
-// P3 of one instance (any pass) or of a group (GL step)
+// P3 of one instance (any pass)
 template <typename T>
 void launch_inv(const Instance &I, unsigned planes, cudaStream_t st, const cx<T> *spec, const T *xin, T *xout,
                 const PlaneArgs &pa, const UpdateArgs &ua, double *partials) {
@@ -380,13 +389,16 @@ void launch_inv(const Instance &I, unsigned planes, cudaStream_t st, const cx<T>
   else k_inv_update<T, NP, false><<<planes, NP, I.smem_update, st>>>(spec, xin, xout, pa, ua, partials);
 }
 
+
+// Fused plane pass of a group (P3 of this step + P1 of the next when fwd)
 template <typename T>
-void launch_inv_tab(const Instance &L, unsigned B, cudaStream_t st, const InstPtrs *tab, const PlaneArgs &pa,
-                    const UpdateArgs &ua) {
+void launch_step_tab(const Instance &L, unsigned B, cudaStream_t st, const InstPtrs *tab, const PlaneArgs &pa,
+                     const UpdateArgs &ua, bool fwd) {
   constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
   const unsigned planes = (unsigned)(L.F * L.nx);
-  if (L.split) launch_pair(k_inv_update_tab<T, NH, true>, dim3(2 * planes, B), NH, L.smem_update, st, tab, pa, ua);
-  else k_inv_update_tab<T, NP, false><<<dim3(planes, B), NP, L.smem_update, st>>>(tab, pa, ua);
+  if (L.split)
+    launch_pair(k_step_planes_tab<T, NH, true>, dim3(2 * planes, B), NH, L.smem_update, st, tab, pa, ua, (int)fwd);
+  else k_step_planes_tab<T, NP, false><<<dim3(planes, B), NP, L.smem_update, st>>>(tab, pa, ua, (int)fwd);
 }
 
 // Enqueue one GL iteration of one instance; `step` indexes the stats record.
@@ -515,9 +527,20 @@ void build_groups(pfdd_gpu *h) {
   }
 }
 
-// One GL iteration of every instance of group G (4 launches for the group).
+// The forward pass (P1) that opens a run of steps of group G: every later
+// step's spectrum comes from the previous step's fused plane pass.
 template <typename T>
-void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol, cudaEvent_t *ev = nullptr) {
+void enqueue_group_open(Instance &L, const Group &G, cudaStream_t st) {
+  PlaneArgs pa;
+  fill_plane_args<T>(L, pa);
+  launch_fwd_tab<T>(L, (unsigned)G.members.size(), st, static_cast<const InstPtrs *>(G.table.p), pa);
+}
+
+// One GL iteration of every instance of group G whose spectrum is current
+// (3 launches: P2, the fused plane pass, finalize); fwd: the plane pass also
+// leaves the next step's spectrum.  ev[0..3] bracket the three launches.
+template <typename T>
+void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol, bool fwd, cudaEvent_t *ev = nullptr) {
   constexpr int NC = Threads<T>::pencil;
   const unsigned B = (unsigned)G.members.size();
   const InstPtrs *tab = static_cast<const InstPtrs *>(G.table.p);
@@ -525,8 +548,6 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   fill_plane_args<T>(L, pa);
   const int planes = L.F * L.nx;
   if (ev) cudaEventRecord(ev[0], st);
-  launch_fwd_tab<T>(L, B, st, tab, pa);
-  if (ev) cudaEventRecord(ev[1], st);
   PencilArgs pe;
   pe = PencilArgs{};
   pe.px = L.px;
@@ -543,7 +564,7 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   pe.g = L.green;
   set_pencil_divisors<T>(pe);
   k_xpencil_tab<T, NC><<<dim3(L.ntiles, B), NC, L.smem_pencil, st>>>(tab, pe);
-  if (ev) cudaEventRecord(ev[2], st);
+  if (ev) cudaEventRecord(ev[1], st);
   UpdateArgs ua;
   memset(&ua, 0, sizeof ua);
   ua.nx = L.nx; ua.ny = L.ny; ua.nz = L.nz; ua.nzh = L.nzh; ua.nzp = L.nzp; ua.S = L.S; ua.F = L.F;
@@ -551,19 +572,24 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   ua.invN = 1.0 / (double)L.N;
   ua.core = L.core;
   ua.mode = PASS_STEP;
-  launch_inv_tab<T>(L, B, st, tab, pa, ua);
-  if (ev) cudaEventRecord(ev[3], st);
+  launch_step_tab<T>(L, B, st, tab, pa, ua, fwd);
+  if (ev) cudaEventRecord(ev[2], st);
   const bool nyq = L.imag == IMAG_NYQ;
   k_finalize_tab<<<B, 256, 0, st>>>(tab, planes, nyq ? L.ntiles : 0, 1.0 / (double)L.N, tol);
-  if (ev) cudaEventRecord(ev[4], st);
+  if (ev) cudaEventRecord(ev[3], st);
 }
 
 template <typename T>
-void enqueue_all_groups(pfdd_gpu *h, cudaStream_t st, double tol) {
-  for (auto &G : h->groups) enqueue_group_step<T>(*h->inst[G.members[0]], G, st, tol);
+void enqueue_open_all(pfdd_gpu *h, cudaStream_t st) {
+  for (auto &G : h->groups) enqueue_group_open<T>(*h->inst[G.members[0]], G, st);
 }
 
-constexpr int kLaunchesPerStep = 4;
+template <typename T>
+void enqueue_all_groups(pfdd_gpu *h, cudaStream_t st, double tol, bool fwd) {
+  for (auto &G : h->groups) enqueue_group_step<T>(*h->inst[G.members[0]], G, st, tol, fwd);
+}
+
+constexpr int kLaunchesPerStep = 3;   // per group, plus one opening P1 per run
 
 pfdd_status ensure_stats(pfdd_gpu *h, int cap);
 pfdd_status reset_counters(pfdd_gpu *h);
@@ -579,21 +605,27 @@ pfdd_status profile_impl(pfdd_gpu *h, int n_steps, double *kernel_ms) {
   if ((ps = reset_counters(h))) return ps;
   stress_all<T>(h, 0);
   const size_t ng = h->groups.size();
-  std::vector<cudaEvent_t> ev(5 * (size_t)n_steps * ng);
+  std::vector<cudaEvent_t> ev(4 * (size_t)n_steps * ng + 2);
   for (auto &e : ev) CUDA_TRY(h, cudaEventCreate(&e));
-  size_t q = 0;
+  cudaEventRecord(ev[0], st);
+  enqueue_open_all<T>(h, st);
+  cudaEventRecord(ev[1], st);
+  size_t q = 2;
   for (int it = 0; it < n_steps; ++it)
     for (auto &G : h->groups) {
-      enqueue_group_step<T>(*h->inst[G.members[0]], G, st, 0.0, &ev[q]);
-      q += 5;
+      enqueue_group_step<T>(*h->inst[G.members[0]], G, st, 0.0, it + 1 < n_steps, &ev[q]);
+      q += 4;
     }
   cudaError_t e = cudaStreamSynchronize(st);
   if (e == cudaSuccess) {
-    for (size_t b = 0; b < q; b += 5)
-      for (int k = 0; k < PFDD_NKERNELS; ++k) {
-        float ms = 0.f;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    kernel_ms[PFDD_K_FWD_PLANES] = ms;
+    for (size_t b = 2; b < q; b += 4)
+      for (int k = 0; k < 3; ++k) {
+        ms = 0.f;
         cudaEventElapsedTime(&ms, ev[b + k], ev[b + k + 1]);
-        kernel_ms[k] += ms;
+        kernel_ms[PFDD_K_XPENCIL + k] += ms;
       }
     for (int k = 0; k < PFDD_NKERNELS; ++k) kernel_ms[k] /= (double)n_steps;
   }
@@ -810,16 +842,32 @@ pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const dou
   return PFDD_OK;
 }
 
-// Graph of `steps` GL iterations of every group (captured once per (steps, tol)).
+// Graph of `steps` GL iterations of every group (states = 0), or of `states`
+// whole stress states of `steps` iterations each (tau from sigma, the steps,
+// sigma += dsigma), captured once per key.  One opening forward pass, then
+// every plane pass but the last leaves the next step's spectrum: the forward
+// spectrum does not depend on the stress, and an instance that stopped on
+// the tolerance keeps the spectrum of its current state.
 template <typename T>
-pfdd_status graph_for(pfdd_gpu *h, int steps, double tol, cudaGraphExec_t *out) {
-  GraphKey key{steps, tol};
+pfdd_status graph_for(pfdd_gpu *h, int steps, int states, double tol, cudaGraphExec_t *out) {
+  GraphKey key{steps, states, tol};
   auto it = h->graphs.find(key);
   if (it != h->graphs.end()) { *out = it->second; return PFDD_OK; }
   cudaStream_t st = h->stream;
   cudaGraph_t g;
   CUDA_TRY(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  for (int i = 0; i < steps; ++i) enqueue_all_groups<T>(h, st, tol);
+  if (states == 0) {
+    enqueue_open_all<T>(h, st);
+    for (int i = 0; i < steps; ++i) enqueue_all_groups<T>(h, st, tol, i + 1 < steps);
+  } else {
+    for (int j = 0; j < states; ++j) {
+      stress_all<T>(h, 0);   // clears the stop flags before the opening pass reads them
+      if (j == 0) enqueue_open_all<T>(h, st);
+      for (int i = 0; i < steps; ++i)
+        enqueue_all_groups<T>(h, st, tol, !(j + 1 == states && i + 1 == steps));
+      stress_all<T>(h, 1);
+    }
+  }
   CUDA_TRY(h, cudaStreamEndCapture(st, &g));
   cudaGraphExec_t ge;
   cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
@@ -891,19 +939,33 @@ pfdd_status advance_impl(pfdd_gpu *h, int n_steps, int stress_states, double tol
   if ((ps = ensure_stats(h, (int)std::min<long long>(total, 1 << 24)))) return ps;
   if ((ps = reset_counters(h))) return ps;
   const int chunk = 32;
+  if (h->opt.use_graphs && n_steps < chunk && stress_states > 1) {
+    // short stress states (a ramp): several whole states per graph
+    const int per = chunk / n_steps;
+    for (int left = stress_states; left > 0;) {
+      const int k = std::min(per, left);
+      cudaGraphExec_t ge = nullptr;
+      if ((ps = graph_for<T>(h, n_steps, k, tol, &ge))) return ps;
+      CUDA_TRY(h, cudaGraphLaunch(ge, st));
+      left -= k;
+    }
+    CUDA_TRY(h, cudaGetLastError());
+    return collect(h, stats);
+  }
   for (int ss = 0; ss < stress_states; ++ss) {
     stress_all<T>(h, 0);
     if (h->opt.use_graphs) {
       int left = n_steps;
       while (left > 0) {
         const int k = std::min(chunk, left);
-        cudaGraphExec_t ge;
-        if ((ps = graph_for<T>(h, k, tol, &ge))) return ps;
+        cudaGraphExec_t ge = nullptr;
+        if ((ps = graph_for<T>(h, k, 0, tol, &ge))) return ps;
         CUDA_TRY(h, cudaGraphLaunch(ge, st));
         left -= k;
       }
     } else {
-      for (int it = 0; it < n_steps; ++it) enqueue_all_groups<T>(h, st, tol);
+      enqueue_open_all<T>(h, st);
+      for (int it = 0; it < n_steps; ++it) enqueue_all_groups<T>(h, st, tol, it + 1 < n_steps);
     }
     stress_all<T>(h, 1);
   }

@@ -367,11 +367,16 @@ template <bool SPLIT> __device__ __forceinline__ int row0_of_block(int ny) {
 }
 
 template <typename T, int NT, bool SPLIT>
+__device__ __forceinline__ void fwd_planes_compute(const PlaneSmem<cx<T>> &sm, const PlaneArgs &a,
+                                                   cx<T> *__restrict__ spec, size_t plane, int rows, int row0,
+                                                   bool ok);
+
+template <typename T, int NT, bool SPLIT>
 __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> *__restrict__ spec,
                                                 const PlaneArgs &a, int *err, size_t plane) {
   using C = cx<T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int ny = a.ny, nz = a.nz, nzh = a.nzh, nzp = a.nzp, nzs = a.nzs, M = a.M;
+  const int ny = a.ny, nz = a.nz, nzs = a.nzs;
   const int rows = SPLIT ? ny / 2 : ny;
   const int row0 = row0_of_block<SPLIT>(ny);
   const PlaneSmem<C> sm(smem_raw, a, rows);
@@ -393,6 +398,19 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
     // a split CTA carries on without storing: its peer waits at the cluster barriers
     if constexpr (!SPLIT) return;
   }
+  fwd_planes_compute<T, NT, SPLIT>(sm, a, spec, plane, rows, row0, ok);
+}
+
+// The forward part of P1 on the real rows already in shared memory (row
+// stride 2*nzs reals): z real-to-complex, y, DC/Nyquist split, bulk store of
+// the half-spectrum rows.  `ok` false: compute (a split peer waits at the
+// cluster barriers) but store nothing.  Every thread of the CTA calls it.
+template <typename T, int NT, bool SPLIT>
+__device__ __forceinline__ void fwd_planes_compute(const PlaneSmem<cx<T>> &sm, const PlaneArgs &a,
+                                                   cx<T> *__restrict__ spec, size_t plane, int rows, int row0,
+                                                   bool ok) {
+  using C = cx<T>;
+  const int ny = a.ny, nzh = a.nzh, nzp = a.nzp, nzs = a.nzs, M = a.M;
   C *buf = sm.buf;
   const C *twr = sm.twr;
   const int *pos = sm.pos;
@@ -894,12 +912,15 @@ __device__ __forceinline__ T update_one(const UpdateArgs &u, bool real_field, in
 
 // Per-instance pointers travel as arguments so the constant parameter block
 // (PlaneArgs, UpdateArgs) is read in place and never copied.
-template <typename T, int NT, bool SPLIT>
-__device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, const T *__restrict__ xin,
+// FUSE (PASS_STEP only): the updated plane also stays in shared memory and,
+// when `fwd`, is transformed forward (fwd_planes_compute) and stored over the
+// spectrum rows this CTA read, as the next step's P1 output.
+template <typename T, int NT, bool SPLIT, bool FUSE = false>
+__device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__restrict__ xin,
                                                 T *__restrict__ xout, const PlaneArgs &a, const UpdateArgs &u,
                                                 double *__restrict__ partials, size_t plane,
                                                 const double *__restrict__ tau_p, const uint8_t *__restrict__ mask,
-                                                const void *site_p, int *err) {
+                                                const void *site_p, int *err, bool fwd = false) {
   using C = cx<T>;
   using V = typename Vec<T>::type;
   constexpr int VN = Vec<T>::n;
@@ -1067,10 +1088,12 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
   // update pass only: tau, mask and per-site GSFE are read from here on
   const T tau = real_field ? (T)tau_p[sys] : (T)0;
   const T *site = reinterpret_cast<const T *>(site_p);
+  T *bufw = reinterpret_cast<T *>(buf);
+  const bool keep = FUSE && fwd;   // new xi also into shared memory for the forward part
   double dsq = 0.0, sum = 0.0;
   for (int i0 = threadIdx.x; i0 < total; i0 += 2 * blockDim.x) {
     V oldv[2], elv[2];
-    int idx[2];
+    int idx[2], soff[2];
     bool on[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -1078,8 +1101,9 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
       on[h] = i < total;
       const int y = dv.div(on[h] ? i : 0), zq = (on[h] ? i : 0) - y * nvec;
       idx[h] = y * nz + zq * VN;
+      soff[h] = y * 2 * nzs + zq * VN;
       oldv[h] = *reinterpret_cast<const V *>(xin + off + idx[h]);
-      elv[h] = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzs + zq * VN);
+      elv[h] = *reinterpret_cast<const V *>(bufr + soff[h]);
     }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -1097,10 +1121,17 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *__restrict__ spec, 
         if (real_field) sum += (double)nv[q];
       }
       if (ok) *reinterpret_cast<V *>(xout + off + idx[h]) = *reinterpret_cast<V *>(nv);
+      if (keep) *reinterpret_cast<V *>(bufw + soff[h]) = *reinterpret_cast<V *>(nv);
     }
   }
   double v[2] = {dsq, sum};
   plane_sum<SPLIT>(v, sm.red, partials + 2 * plane);
+  if constexpr (FUSE) {
+    if (fwd) {
+      __syncthreads();
+      fwd_planes_compute<T, NT, SPLIT>(sm, a, const_cast<cx<T> *>(spec), plane, rows, row0, ok);
+    }
+  }
 }
 
 // grid.x = F * nx planes (SPLIT: 2 F nx CTAs in clusters of 2)
@@ -1111,6 +1142,30 @@ __global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, SPLIT>::value)) k_inv_u
   if (u.stop && *u.stop) return;
   inv_update_body<T, NT, SPLIT>(spec, xin, xout, a, u, partials, plane_of_block<SPLIT>(), u.tau, u.mask, u.site,
                                 u.err);
+}
+
+// P3 of step n fused with P1 of step n + 1 (PASS_STEP): inverse transforms,
+// update, then (fwd != 0) the forward transforms of the new plane, stored
+// over the same spectrum rows.  grid.x = F * nx planes (x 2 for SPLIT).
+template <typename T, int NT, bool SPLIT>
+__global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, SPLIT>::value))
+    k_step_planes(cx<T> *spec, const T *__restrict__ xin, T *__restrict__ xout, PlaneArgs a, UpdateArgs u,
+                  double *__restrict__ partials, int fwd) {
+  if (u.stop && *u.stop) return;
+  inv_update_body<T, NT, SPLIT, true>(spec, xin, xout, a, u, partials, plane_of_block<SPLIT>(), u.tau, u.mask,
+                                      u.site, u.err, fwd != 0);
+}
+
+// grid = (F * nx planes [x 2 for SPLIT], instances of the group)
+template <typename T, int NT, bool SPLIT>
+__global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, SPLIT>::value))
+    k_step_planes_tab(const InstPtrs *__restrict__ tab, PlaneArgs a, UpdateArgs u, int fwd) {
+  const InstPtrs &ip = tab[blockIdx.y];
+  if (ip.flags[0]) return;
+  const int cur = ip.flags[4];
+  inv_update_body<T, NT, SPLIT, true>(static_cast<const cx<T> *>(ip.spec), static_cast<const T *>(ip.xi[cur]),
+                                      static_cast<T *>(ip.xi[cur ^ 1]), a, u, ip.partials,
+                                      plane_of_block<SPLIT>(), ip.tau, ip.mask, ip.site, ip.flags + 3, fwd != 0);
 }
 
 // grid = (F * nx planes, instances of the group); per-instance stress, mask,

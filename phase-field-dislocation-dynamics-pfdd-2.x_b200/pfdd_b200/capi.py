@@ -31,7 +31,7 @@ EXPORTS = [
     "pfdd_gpu_tau", "pfdd_gpu_info", "pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version",
     "pfdd_gpu_set_stream", "pfdd_gpu_profile", "pfdd_gpu_adjoint",
 ]
-KERNELS = ["fwd_planes", "xpencil", "inv_update", "finalize"]
+KERNELS = ["fwd_planes", "xpencil", "step_planes", "finalize"]
 
 D33 = ctypes.c_double * 3 * 3
 DS3 = ctypes.c_double * 3 * MAX_SLIP

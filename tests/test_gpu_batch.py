@@ -18,7 +18,7 @@ def test_group_of_alloy_instances_matches_oracle():
         st.advance(9)
         outs = [st.get_state(i) for i in range(4)]
         _, lps = st.profile(1)
-        assert lps == 4          # one group: 4 launches per step for all 4 instances
+        assert lps == 3          # one group: 3 launches per step for all 4 instances
     for w, (re, im) in zip(ws, outs):
         ref, _, _ = O.run(oracle_instance(w), w.xi0, 9)
         assert np.abs(re - ref.real).max() <= 1e-10
@@ -52,6 +52,29 @@ def test_tolerance_stops_across_stress_states(graphs):
     with capi.Stepper.from_workloads([w], precision=capi.FP64, use_graphs=graphs) as st:
         st.set_state(0, w.xi0)
         (xn, xa, done, conv), = st.advance(40, 3, 0.3)
+        re, im = st.get_state(0)
+        hn, _ = st.history(0)
+    assert done == len(nrm)
+    np.testing.assert_allclose(hn, nrm, rtol=1e-9)
+    assert np.abs(re - ref.real).max() <= 1e-10
+    assert np.abs(im - ref.imag).max() <= 1e-10
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_tolerance_stops_in_short_stress_states(graphs):
+    """Several short stress states per graph: an instance that stops on the
+    tolerance resumes in the next state from the spectrum its last plane pass
+    left (the forward spectrum does not depend on the stress)."""
+    w = small_loop(16)
+    w.dsigma = np.zeros((3, 3))
+    w.dsigma[0, 2] = w.dsigma[2, 0] = 2e-4
+    _, free = _oracle_with_tol(w, 6, 1, tol=0.0)
+    tol = float(free[3]) * (1 + 1e-6)   # the first state stops after 4 steps
+    ref, nrm = _oracle_with_tol(w, 6, 5, tol=tol)
+    assert len(nrm) < 30
+    with capi.Stepper.from_workloads([w], precision=capi.FP64, use_graphs=graphs) as st:
+        st.set_state(0, w.xi0)
+        (xn, xa, done, conv), = st.advance(6, 5, tol)
         re, im = st.get_state(0)
         hn, _ = st.history(0)
     assert done == len(nrm)
