@@ -50,7 +50,7 @@ template <typename T> struct Threads;
 // plane: whole-plane P1/P3 CTAs; half: each CTA of a split (2-CTA cluster)
 // plane; pencil: P2 CTAs.  FP32 defaults were measured on 256x256x128 with
 // 12 systems: 256-thread split-plane CTAs at three per SM (80 registers) and
-// 256-thread pencil CTAs of at most 100 KB of shared memory at two per SM
+// 256-thread pencil CTAs of at most 106 KB of shared memory at two per SM
 // beat 512-thread CTAs at one per SM by 0.3 ms per step.
 #ifndef PFDD_HALF_THREADS_F32
 #define PFDD_HALF_THREADS_F32 256
@@ -59,7 +59,7 @@ template <typename T> struct Threads;
 #define PFDD_PENCIL_THREADS_F32 256
 #endif
 #ifndef PFDD_PENCIL_SMEM_KB
-#define PFDD_PENCIL_SMEM_KB 100
+#define PFDD_PENCIL_SMEM_KB 106
 #endif
 template <> struct Threads<float> {
   static constexpr int plane = 512, half = PFDD_HALF_THREADS_F32, pencil = PFDD_PENCIL_THREADS_F32;
@@ -282,8 +282,11 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
         return I.nx * cc + pad;
     return I.nx * cc;
   };
+  // tile, x twiddles, reduction scratch, wave-vector parts (x slots and the
+  // tile's columns) and the columns' slots
   auto pencil_bytes = [&](int cc) {
-    return ((size_t)I.F * fstride_for(cc) + I.nx) * sizeof(C) + 64 * sizeof(double);
+    return ((size_t)I.F * fstride_for(cc) + (size_t)I.nx) * sizeof(C) + 64 * sizeof(double) +
+           ((size_t)I.nx + 2 * (size_t)cc) * sizeof(V4<T>) + 2 * (size_t)cc * sizeof(int);
   };
   int cc = 32;
   // widest tile that fits the budget and still gives every SM two tiles
@@ -330,17 +333,32 @@ pfdd_status set_smem_attrs(pfdd_gpu *h, size_t plane, size_t upd, size_t pencil)
   CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes<T, NH, true>, A, (int)plane));
   CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update<T, NP, false>, A, (int)upd));
   CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update<T, NH, true>, A, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_xpencil<T, NC>, A, (int)pencil));
+  cudaError_t pe_err = cudaSuccess;
+  for (int sc : {0, 2, 3})
+    with_pencil_sc(sc, [&](auto SCc) {
+      constexpr int SC = decltype(SCc)::value;
+      if (pe_err == cudaSuccess) pe_err = cudaFuncSetAttribute(k_xpencil<T, NC, SC>, A, (int)pencil);
+      if (pe_err == cudaSuccess) pe_err = cudaFuncSetAttribute(k_xpencil_tab<T, NC, SC>, A, (int)pencil);
+    });
+  CUDA_TRY(h, pe_err);
   CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes_tab<T, NP, false>, A, (int)plane));
   CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes_tab<T, NH, true>, A, (int)plane));
   CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update_tab<T, NP, false>, A, (int)upd));
   CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update_tab<T, NH, true>, A, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_xpencil_tab<T, NC>, A, (int)pencil));
   CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes<T, NP, false>, A, (int)upd));
   CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes<T, NH, true>, A, (int)upd));
   CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes_tab<T, NP, false>, A, (int)upd));
   CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes_tab<T, NH, true>, A, (int)upd));
   return PFDD_OK;
+}
+
+// P2 of one instance, with the contraction unrolled for its slip-system count
+template <typename T>
+void launch_pencil(const Instance &I, cudaStream_t st, cx<T> *spec, const PencilArgs &pe, const int *stop) {
+  constexpr int NC = Threads<T>::pencil;
+  with_pencil_sc(I.S, [&](auto SCc) {
+    k_xpencil<T, NC, decltype(SCc)::value><<<I.ntiles, NC, I.smem_pencil, st>>>(spec, pe, stop);
+  });
 }
 
 // Launch with an optional 2-CTA cluster (split planes).
@@ -423,7 +441,6 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   T *xout = adj ? static_cast<T *>(adj->lam_out) : I.xi[I.cur ^ 1].as<T>();
   cx<T> *spec = I.spec.as<cx<T>>();
   const int planes = I.F * I.nx;
-  constexpr int NC = Threads<T>::pencil;
   if (ev) cudaEventRecord(ev[0], st);
   launch_fwd<T>(I, st, xin, spec, pa, flags, flags + 3);
   if (ev) cudaEventRecord(ev[1], st);
@@ -443,7 +460,7 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   pe.partials = (I.imag == IMAG_NYQ && !adj) ? I.ppart.as<double>() : nullptr;
   pe.g = I.green;
   set_pencil_divisors<T>(pe);
-  k_xpencil<T, NC><<<I.ntiles, NC, I.smem_pencil, st>>>(spec, pe, flags);
+  launch_pencil<T>(I, st, spec, pe, flags);
   if (ev) cudaEventRecord(ev[2], st);
   UpdateArgs ua;
   ua.nx = I.nx; ua.ny = I.ny; ua.nz = I.nz; ua.nzh = I.nzh; ua.nzp = I.nzp; ua.S = I.S; ua.F = I.F;
@@ -563,7 +580,9 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   pe.cd = L.d.cd_dt;
   pe.g = L.green;
   set_pencil_divisors<T>(pe);
-  k_xpencil_tab<T, NC><<<dim3(L.ntiles, B), NC, L.smem_pencil, st>>>(tab, pe);
+  with_pencil_sc(L.S, [&](auto SCc) {
+    k_xpencil_tab<T, NC, decltype(SCc)::value><<<dim3(L.ntiles, B), NC, L.smem_pencil, st>>>(tab, pe);
+  });
   if (ev) cudaEventRecord(ev[1], st);
   UpdateArgs ua;
   memset(&ua, 0, sizeof ua);
@@ -639,7 +658,6 @@ pfdd_status profile_impl(pfdd_gpu *h, int n_steps, double *kernel_ms) {
 // E_applied = -sum tau_a Re xi_a, from one elastic pass of the current state.
 template <typename T>
 pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, double *e_app) {
-  constexpr int NC = Threads<T>::pencil;
   cudaStream_t st = h->stream;
   DevBuf gpart;
   CUDA_TRY(h, gpart.alloc(4 * (size_t)I.F * I.nx * sizeof(double)));
@@ -667,7 +685,7 @@ pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, 
   pe.partials = I.imag == IMAG_NYQ ? I.ppart.as<double>() : nullptr;
   pe.g = I.green;
   set_pencil_divisors<T>(pe);
-  k_xpencil<T, NC><<<I.ntiles, NC, I.smem_pencil, st>>>(spec, pe, nullptr);
+  launch_pencil<T>(I, st, spec, pe, nullptr);
   UpdateArgs ua;
   memset(&ua, 0, sizeof ua);
   ua.nx = I.nx; ua.ny = I.ny; ua.nz = I.nz; ua.nzh = I.nzh; ua.nzp = I.nzp; ua.S = I.S; ua.F = I.F;
@@ -1022,7 +1040,6 @@ pfdd_status set_state_impl(pfdd_gpu *h, Instance &I, const double *re, const dou
 // inverse (k_inv_update PASS_SYNTH), through the spectrum buffer.
 template <typename T>
 void synth_imag(Instance &I, cudaStream_t st, T *dst) {
-  constexpr int NC = Threads<T>::pencil;
   PencilArgs pe;
   pe = PencilArgs{};
   pe.px = I.px;
@@ -1039,7 +1056,7 @@ void synth_imag(Instance &I, cudaStream_t st, T *dst) {
   pe.g = I.green;
   cx<T> *spec = I.spec.as<cx<T>>();
   set_pencil_divisors<T>(pe);
-  k_xpencil<T, NC><<<I.ntiles, NC, I.smem_pencil, st>>>(spec, pe, nullptr);
+  launch_pencil<T>(I, st, spec, pe, nullptr);
   PlaneArgs pa;
   fill_plane_args<T>(I, pa);
   UpdateArgs ua;

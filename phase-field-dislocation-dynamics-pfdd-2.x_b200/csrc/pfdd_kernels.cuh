@@ -39,6 +39,8 @@
 #pragma once
 #include <cooperative_groups.h>
 
+#include <type_traits>
+
 #include "pfdd_fft.cuh"
 
 #define PFDD_MAXS 12
@@ -182,6 +184,13 @@ struct InstPtrs {
 };
 
 // ------------------------------------------------------------ small helpers
+template <typename T> struct __align__(16) V4 { T x, y, z, w; };
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
+// correctly rounded reciprocal
+__device__ __forceinline__ float recip_t(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double recip_t(double x) { return 1.0 / x; }
+
 template <typename T> __device__ __forceinline__ void sincospi_t(T x, T *s, T *c);
 template <> __device__ __forceinline__ void sincospi_t<double>(double x, double *s, double *c) { sincospi(x, s, c); }
 template <> __device__ __forceinline__ void sincospi_t<float>(float x, float *s, float *c) { sincospif(x, s, c); }
@@ -517,7 +526,7 @@ template <typename T, typename C>
 __device__ __forceinline__ bool green_tensor(const GreenT<T> &g, const C (&sig)[6], T kx, T ky, T kz, C (&Tq)[6]) {
   const T k2 = kx * kx + ky * ky + kz * kz;
   if (!(k2 > (T)0)) return false;
-  const T ik2 = (T)1 / k2;
+  const T ik2 = recip_t(k2);
   const T g1 = (T)2 * ik2 * g.c2;
   const T g2 = ik2 * ik2 * g.c1nu * g.c2;
   // sig order: xx yy zz xy xz yz
@@ -543,13 +552,16 @@ __device__ __forceinline__ C green_out(const GreenT<T> &g, int a, const C (&sig)
   if (!nz) return mk<C>((T)0, (T)0);
   const T *e = g.epso[a];
   const T *o = g.sigo[a];
-  C r = mk<C>((T)0, (T)0);
+  // eps^a : Sig and sigma^a : Tq as separate chains (shorter dependences)
+  T ex = (T)0, ey = (T)0, ox = (T)0, oy = (T)0;
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
-    r.x += e[q] * sig[q].x + o[q] * Tq[q].x;
-    r.y += e[q] * sig[q].y + o[q] * Tq[q].y;
+    ex = fma_t(e[q], sig[q].x, ex);
+    ey = fma_t(e[q], sig[q].y, ey);
+    ox = fma_t(o[q], Tq[q].x, ox);
+    oy = fma_t(o[q], Tq[q].y, oy);
   }
-  return r;
+  return mk<C>(ex + ox, ey + oy);
 }
 
 template <typename T, typename C>
@@ -570,7 +582,7 @@ template <typename T> __device__ __forceinline__ T freq_neg(int i, int n) {
 }
 
 // ------------------------------------------------------------ P2
-// grid.x = ncols / ccols tiles; dynamic smem = (F*nx*ccols + nx) * sizeof(C)
+// grid.x = ncols / ccols tiles; dynamic smem = (F*fstride + nx) * sizeof(C) + scratch + wave-vector parts
 template <typename T, typename C>
 __device__ __forceinline__ size_t nyq_index(const PencilArgs &a, int f, int sx, int sy, int sz, bool &is_nyq) {
   // returns the aux slot of a Nyquist point; is_nyq false for ordinary points
@@ -584,15 +596,23 @@ __device__ __forceinline__ size_t nyq_index(const PencilArgs &a, int f, int sx, 
   return 0;
 }
 
-template <typename T, int NT>
+// SC > 0: the slip-system count is the constant SC (contraction loops
+// unrolled, the per-system constants read as immediates of the parameter
+// block); 0: a.S at run time.
+template <typename T, int NT, int SC>
 __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const PencilArgs &a, void *aux_ptr,
                                              double *ppart) {
   using C = cx<T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int nx = a.nx, F = a.F, cc = a.ccols, S = a.S, fst = a.fstride;
+  const int nx = a.nx, F = a.F, cc = a.ccols, S = SC > 0 ? SC : a.S, fst = a.fstride;
   C *buf = reinterpret_cast<C *>(smem_raw);   // [F][fstride >= nx*cc]
   C *twx = buf + (size_t)F * fst;
   double *red = reinterpret_cast<double *>(twx + nx);
+  // wave vector k = fx four[0] + fy four[1] + fz four[2] in parts: kxv per x
+  // slot, cyv / czv per column of the tile (w = 1 on the axis's Nyquist index)
+  V4<T> *kxv = reinterpret_cast<V4<T> *>(red + 64);
+  V4<T> *cyv = kxv + nx, *czv = cyv + cc;
+  int *csy = reinterpret_cast<int *>(czv + cc), *csz = csy + cc;
   const size_t col0 = (size_t)blockIdx.x * cc;
   const size_t ncols = a.ncols;
   const int cpr = (int)(cc * sizeof(C) / 16);    // 16-byte chunks per (field, x) row
@@ -610,6 +630,26 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
     for (int i = threadIdx.x; i < F * fst; i += blockDim.x) buf[i] = mk<C>((T)0, (T)0);
   }
   load_table(twx, a.tw_x, nx);
+  {
+    const GreenT<T> &g = green_t<T>(a.g);
+    for (int i = threadIdx.x; i < nx + cc; i += blockDim.x) {
+      if (i < nx) {
+        const int ix = a.kx_of[i];
+        const T f = freq_of<T>(ix, nx);
+        kxv[i] = V4<T>{f * g.four[0][0], f * g.four[0][1], f * g.four[0][2], (T)(2 * ix == nx ? 1 : 0)};
+      } else {
+        const int c = i - nx;
+        const int col = (int)(col0 + c);
+        const int sy = a.fd_nzp.div(col), sz = col - sy * a.nzp;
+        const int iy = a.ky_of[sy], iz = a.kz_of[sz];
+        const T fy = freq_of<T>(iy, a.ny), fz = freq_of<T>(iz, a.nz);
+        cyv[c] = V4<T>{fy * g.four[1][0], fy * g.four[1][1], fy * g.four[1][2], (T)(2 * iy == a.ny ? 1 : 0)};
+        czv[c] = V4<T>{fz * g.four[2][0], fz * g.four[2][1], fz * g.four[2][2], (T)(2 * iz == a.nz ? 1 : 0)};
+        csy[c] = sy;
+        csz[c] = sz;
+      }
+    }
+  }
   if (a.mode != PASS_SYNTH) cp_async_wait_all();
   __syncthreads();
 
@@ -617,10 +657,11 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
   if (a.mode != PASS_SYNTH) fft_forward<MaxRadix<NT>::value, GeomPencil>(buf, twx, a.px, gx);
 
   double dsq = 0.0;
+  const GreenT<T> &g = green_t<T>(a.g);
+  const size_t fs = (size_t)fst;
   for (int w = threadIdx.x; w < nx * cc; w += blockDim.x) {
     const int sx = a.fd_cc.div(w), c = w - sx * cc;
-    const int col = (int)(col0 + c);
-    const int sy = a.fd_nzp.div(col), sz = col - sy * a.nzp;
+    const int sy = csy[c], sz = csz[c];
     C *pk = buf + sx * cc + c;
     if (a.mode == PASS_SYNTH) {
       bool nq;
@@ -630,35 +671,59 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
       }
       continue;
     }
-    const int ix = a.kx_of[sx], iy = a.ky_of[sy], iz = a.kz_of[sz];
-    const T fx = freq_of<T>(ix, a.nx), fy = freq_of<T>(iy, a.ny), fz = freq_of<T>(iz, a.nz);
-    const GreenT<T> &g = green_t<T>(a.g);
-    const T kx = fx * g.four[0][0] + fy * g.four[1][0] + fz * g.four[2][0];
-    const T ky = fx * g.four[0][1] + fy * g.four[1][1] + fz * g.four[2][1];
-    const T kz = fx * g.four[0][2] + fy * g.four[1][2] + fz * g.four[2][2];
-    // B at the index -k is B evaluated at the wave vector the reference assigns to -k
-    const T gxn = freq_neg<T>(ix, a.nx), gyn = freq_neg<T>(iy, a.ny), gzn = freq_neg<T>(iz, a.nz);
-    const T mx = gxn * g.four[0][0] + gyn * g.four[1][0] + gzn * g.four[2][0];
-    const T my = gxn * g.four[0][1] + gyn * g.four[1][1] + gzn * g.four[2][1];
-    const T mz = gxn * g.four[0][2] + gyn * g.four[1][2] + gzn * g.four[2][2];
-    const size_t fs = (size_t)fst;
+    if (sz > a.M) continue;   // row padding: nothing to contract
+    const V4<T> X = kxv[sx], Y = cyv[c], Z = czv[c];
+    const T kx = X.x + (Y.x + Z.x), ky = X.y + (Y.y + Z.y), kz = X.z + (Y.z + Z.z);
     C sr[6];
 #pragma unroll
     for (int q = 0; q < 6; ++q) sr[q] = mk<C>((T)0, (T)0);
-    for (int b = 0; b < S; ++b) green_accumulate<T>(g, b, pk[b * fs], sr);
+    {
+      // even and odd systems into separate partial sums (shorter dependences)
+      C s2[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) s2[q] = mk<C>((T)0, (T)0);
+      int b = 0;
+#pragma unroll(SC > 0 ? SC / 2 : 1)
+      for (; b + 1 < S; b += 2) {
+        const C y0 = pk[b * fs], y1 = pk[(b + 1) * fs];
+        green_accumulate<T>(g, b, y0, sr);
+        green_accumulate<T>(g, b + 1, y1, s2);
+      }
+      if (b < S) green_accumulate<T>(g, b, pk[b * fs], sr);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) sr[q] = mk<C>(sr[q].x + s2[q].x, sr[q].y + s2[q].y);
+    }
     bool nyq = false;
     size_t a0 = 0, astride = 0;
     if (a.imag == IMAG_NYQ) {
       a0 = nyq_index<T, C>(a, 0, sx, sy, sz, nyq);
       astride = (sz == a.M) ? (size_t)a.nx * a.ny : (sy == a.sy_n ? (size_t)a.nx * a.M : (size_t)a.ny * a.M);
     }
-    if (a.imag == IMAG_FULL || nyq) {
+    if (a.imag == IMAG_FULL || nyq || a.imag == IMAG_NONE) {
+      // B at the index -k is B evaluated at the wave vector the reference
+      // assigns to -k: -f on every axis except at its Nyquist index (frec)
+      const T gx = X.w != (T)0 ? (T)1 : (T)-1, gy = Y.w != (T)0 ? (T)1 : (T)-1, gz = Z.w != (T)0 ? (T)1 : (T)-1;
+      const T mx = gx * X.x + (gy * Y.x + gz * Z.x), my = gx * X.y + (gy * Y.y + gz * Z.y),
+              mz = gx * X.z + (gy * Y.z + gz * Z.z);
+      if (a.imag == IMAG_NONE) {
+        // real field only: average B over k and index -k (the Hermitian part)
+        C Tp[6], Tm[6];
+        const bool zp = green_tensor<T>(g, sr, kx, ky, kz, Tp);
+        const bool zq = green_tensor<T>(g, sr, mx, my, mz, Tm);
+#pragma unroll(SC > 0 ? SC : 1)
+        for (int aa = 0; aa < S; ++aa) {
+          const C P = green_out<T>(g, aa, sr, Tp, zp), Q = green_out<T>(g, aa, sr, Tm, zq);
+          pk[aa * fs] = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
+        }
+        continue;
+      }
       // P = B(k)(Xr + i Xi), Q = B(k')(Xr - i Xi), k' = vector of index -k;
       // Er = (P + Q)/2, Ei = (P - Q)/(2i): the real and imaginary fields of
       // IFFT(B_index X) for the complex field X = Xr + i Xi.
       C si[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) si[q] = mk<C>((T)0, (T)0);
+#pragma unroll(SC > 0 ? SC : 1)
       for (int b = 0; b < S; ++b)
         green_accumulate<T>(g, b, a.imag == IMAG_FULL ? pk[(S + b) * fs] : caux[a0 + b * astride], si);
       C sp[6], sq[6];
@@ -671,7 +736,8 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
       const bool zp = green_tensor<T>(g, sp, kx, ky, kz, Tp);
       const bool zq = green_tensor<T>(g, sq, mx, my, mz, Tm);
       const T cd = (T)a.cd;
-      const double wgt = (iz == 0 || iz == a.M) ? 1.0 : 2.0;   // k and its unstored partner -k
+      const double wgt = (sz == 0 || sz == a.M) ? 1.0 : 2.0;   // k and its unstored partner -k
+#pragma unroll 1
       for (int aa = 0; aa < S; ++aa) {
         const C P = green_out<T>(g, aa, sp, Tp, zp);
         const C Q = green_out<T>(g, aa, sq, Tm, zq);
@@ -698,17 +764,16 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
     // B(k) = B(index -k) off the Nyquist planes: Er = B Xr
     C Tp[6];
     const bool zp = green_tensor<T>(g, sr, kx, ky, kz, Tp);
-    if (a.imag == IMAG_NONE) {
-      // real field only: average B over k and index -k (the Hermitian part)
-      C Tm[6];
-      const bool zq = green_tensor<T>(g, sr, mx, my, mz, Tm);
-      for (int aa = 0; aa < S; ++aa) {
-        const C P = green_out<T>(g, aa, sr, Tp, zp), Q = green_out<T>(g, aa, sr, Tm, zq);
-        pk[aa * fs] = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
+    {
+      int aa = 0;
+#pragma unroll(SC > 0 ? SC / 2 : 1)
+      for (; aa + 1 < S; aa += 2) {   // two outputs in flight
+        const C o0 = green_out<T>(g, aa, sr, Tp, zp), o1 = green_out<T>(g, aa + 1, sr, Tp, zp);
+        pk[aa * fs] = o0;
+        pk[(aa + 1) * fs] = o1;
       }
-      continue;
+      if (aa < S) pk[aa * fs] = green_out<T>(g, aa, sr, Tp, zp);
     }
-    for (int aa = 0; aa < S; ++aa) pk[aa * fs] = green_out<T>(g, aa, sr, Tp, zp);
   }
   if (ppart) block_sum2(dsq, 0.0, red, ppart + 2 * blockIdx.x);
   __syncthreads();
@@ -724,20 +789,31 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
   }
 }
 
-// grid.x = ncols / ccols tiles
-template <typename T, int NT>
+// grid.x = ncols / ccols tiles; SC: constant slip-system count (0: a.S)
+template <typename T, int NT, int SC = 0>
 __global__ void __launch_bounds__(NT, (PencilMinBlocks<T>::value)) k_xpencil(cx<T> *__restrict__ spec, PencilArgs a,
                                                 const int *__restrict__ stop) {
   if (stop && *stop) return;
-  xpencil_body<T, NT>(spec, a, a.aux, a.partials);
+  xpencil_body<T, NT, SC>(spec, a, a.aux, a.partials);
 }
 
 // grid = (tiles, instances of the group)
-template <typename T, int NT>
+template <typename T, int NT, int SC = 0>
 __global__ void __launch_bounds__(NT, (PencilMinBlocks<T>::value)) k_xpencil_tab(const InstPtrs *__restrict__ tab, PencilArgs a) {
   const InstPtrs &ip = tab[blockIdx.y];
   if (ip.flags[0]) return;
-  xpencil_body<T, NT>(static_cast<cx<T> *>(ip.spec), a, ip.aux, ip.ppart);
+  xpencil_body<T, NT, SC>(static_cast<cx<T> *>(ip.spec), a, ip.aux, ip.ppart);
+}
+
+// Slip-system counts with an unrolled contraction (basal / {111} triples 3,
+// BCC pairs 2); others, FCC's 12 among them (fully unrolled it spills),
+// run the generic loop.
+template <typename Fn> __host__ inline void with_pencil_sc(int S, Fn f) {
+  switch (S) {
+    case 3: f(std::integral_constant<int, 3>()); break;
+    case 2: f(std::integral_constant<int, 2>()); break;
+    default: f(std::integral_constant<int, 0>()); break;
+  }
 }
 
 // ------------------------------------------------------------ core force

@@ -112,7 +112,10 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
       if ((((size_t)nx * cc + pad) * 4) % 32 == (size_t)target) return nx * cc + pad;
     return nx * cc;
   };
-  auto pencil_bytes = [&](int cc) { return ((size_t)F * fstride_for(cc) + nx) * sizeof(C) + 64 * sizeof(double); };
+  auto pencil_bytes = [&](int cc) {
+    return ((size_t)F * fstride_for(cc) + (size_t)nx) * sizeof(C) + 64 * sizeof(double) +
+           ((size_t)nx + 2 * (size_t)cc) * sizeof(V4<double>) + 2 * (size_t)cc * sizeof(int);
+  };
   int cc = 32;
   while (cc > 1 && (ncols % cc || pencil_bytes(cc) > 200 * 1024)) cc >>= 1;
   const size_t smem_plane = PlaneSmem<C>::bytes(ny, ny, nzp, M);
