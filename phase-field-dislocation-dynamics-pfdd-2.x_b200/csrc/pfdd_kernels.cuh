@@ -191,15 +191,51 @@ __device__ __forceinline__ double fma_t(double a, double b, double c) { return _
 __device__ __forceinline__ float recip_t(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double recip_t(double x) { return 1.0 / x; }
 
+// sin(pi y) and cos(pi y) of the FP32 path (this project's polynomials, not
+// a library routine): y = n/2 + t with n = rint(2y), |t| <= 1/4, then
+// sin(pi t) = t S(t^2) and cos(pi t) = C(t^2) with S of degree 3 and C of
+// degree 4 (least-squares fits, in FP64, of sin(pi t)/t and cos(pi t) over
+// 2000 Chebyshev nodes of 0 < t <= 1/4, weighted for relative error and
+// rounded to FP32), and the quadrant n mod 4 rotates (sin, cos).  Error
+// within 2 ulp of sin(pi y), cos(pi y) for |y| < 2^22
+// (tests/test_sincospi_cpu.py).
+__device__ __forceinline__ void sincospi_poly(float y, float *s, float *c) {
+  const float n = rintf(2.0f * y);
+  const float t = __fmaf_rn(n, -0.5f, y);   // exact
+  const float u = t * t;
+  float ps = __fmaf_rn(u, -0.5890104174613953f, 2.5497608184814453f);
+  ps = __fmaf_rn(u, ps, -5.167707443237305f);
+  ps = __fmaf_rn(u, ps, 3.1415927410125732f);
+  const float sv = t * ps;
+  float pc = __fmaf_rn(u, 0.23126046359539032f, -1.335035800933838f);
+  pc = __fmaf_rn(u, pc, 4.058706760406494f);
+  pc = __fmaf_rn(u, pc, -4.934802055358887f);
+  const float cv = __fmaf_rn(u, pc, 1.0f);
+  const int q = (int)n & 3;
+  float ss = (q & 1) ? cv : sv, cs = (q & 1) ? sv : cv;
+  if (q & 2) ss = -ss;
+  if ((q + 1) & 2) cs = -cs;
+  *s = ss;
+  *c = cs;
+}
+
 template <typename T> __device__ __forceinline__ void sincospi_t(T x, T *s, T *c);
 template <> __device__ __forceinline__ void sincospi_t<double>(double x, double *s, double *c) { sincospi(x, s, c); }
-template <> __device__ __forceinline__ void sincospi_t<float>(float x, float *s, float *c) { sincospif(x, s, c); }
+template <> __device__ __forceinline__ void sincospi_t<float>(float x, float *s, float *c) { sincospi_poly(x, s, c); }
 template <typename T> __device__ __forceinline__ T sinpi_t(T x);
 template <> __device__ __forceinline__ double sinpi_t<double>(double x) { return sinpi(x); }
-template <> __device__ __forceinline__ float sinpi_t<float>(float x) { return sinpif(x); }
+template <> __device__ __forceinline__ float sinpi_t<float>(float x) {
+  float s, c;
+  sincospi_poly(x, &s, &c);
+  return s;
+}
 template <typename T> __device__ __forceinline__ T cospi_t(T x);
 template <> __device__ __forceinline__ double cospi_t<double>(double x) { return cospi(x); }
-template <> __device__ __forceinline__ float cospi_t<float>(float x) { return cospif(x); }
+template <> __device__ __forceinline__ float cospi_t<float>(float x) {
+  float s, c;
+  sincospi_poly(x, &s, &c);
+  return c;
+}
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -1187,15 +1223,19 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
       T o[VN], e[VN], nv[VN];
       *reinterpret_cast<V *>(o) = oldv[h];
       *reinterpret_cast<V *>(e) = elv[h];
+      // the vector's |dxi|^2 and sum in compute precision, then FP64
+      T dq = (T)0, sq = (T)0;
 #pragma unroll
       for (int q = 0; q < VN; ++q) {
         const size_t r = rbase + idx[h] + q;
         nv[q] = update_one<T>(u, real_field, sys, e[q] * invN, o[q], tau, r, N, xin, site);
         if (mask && mask[(size_t)sys * N + r]) nv[q] = o[q];
-        const double d = (double)nv[q] - (double)o[q];
-        dsq += d * d;
-        if (real_field) sum += (double)nv[q];
+        const T d = nv[q] - o[q];
+        dq = fma_t(d, d, dq);
+        sq += nv[q];
       }
+      dsq += (double)dq;
+      if (real_field) sum += (double)sq;
       if (ok) *reinterpret_cast<V *>(xout + off + idx[h]) = *reinterpret_cast<V *>(nv);
       if (keep) *reinterpret_cast<V *>(bufw + soff[h]) = *reinterpret_cast<V *>(nv);
     }
