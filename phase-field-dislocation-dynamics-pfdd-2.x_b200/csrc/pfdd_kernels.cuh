@@ -1203,6 +1203,11 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
   T *bufw = reinterpret_cast<T *>(buf);
   const bool keep = FUSE && fwd;   // new xi also into shared memory for the forward part
   double dsq = 0.0, sum = 0.0;
+  // CF: the core model as a compile-time constant (3: sine GSFE, the common
+  // case, with its force inlined), 0: dispatch per site
+  auto update_loop = [&](auto CFc) {
+  constexpr int CF = decltype(CFc)::value;
+  const T cdt = (T)u.cd, k0 = core_k<T>(u.core, 0), k1 = core_k<T>(u.core, 1);
   for (int i0 = threadIdx.x; i0 < total; i0 += 2 * blockDim.x) {
     V oldv[2], elv[2];
     int idx[2], soff[2];
@@ -1228,7 +1233,14 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
 #pragma unroll
       for (int q = 0; q < VN; ++q) {
         const size_t r = rbase + idx[h] + q;
-        nv[q] = update_one<T>(u, real_field, sys, e[q] * invN, o[q], tau, r, N, xin, site);
+        if constexpr (CF == 3) {
+          T sv, cv;
+          sincospi_t<T>((T)2 * o[q], &sv, &cv);
+          nv[q] = real_field ? o[q] - cdt * (e[q] * invN - tau + (k0 * sv + k1 * ((T)2 * sv * cv)))
+                             : o[q] - cdt * (e[q] * invN);
+        } else {
+          nv[q] = update_one<T>(u, real_field, sys, e[q] * invN, o[q], tau, r, N, xin, site);
+        }
         if (mask && mask[(size_t)sys * N + r]) nv[q] = o[q];
         const T d = nv[q] - o[q];
         dq = fma_t(d, d, dq);
@@ -1240,6 +1252,9 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
       if (keep) *reinterpret_cast<V *>(bufw + soff[h]) = *reinterpret_cast<V *>(nv);
     }
   }
+  };
+  if (u.core.flag == 3) update_loop(std::integral_constant<int, 3>());
+  else update_loop(std::integral_constant<int, 0>());
   double v[2] = {dsq, sum};
   plane_sum<SPLIT>(v, sm.red, partials + 2 * plane);
   if constexpr (FUSE) {
