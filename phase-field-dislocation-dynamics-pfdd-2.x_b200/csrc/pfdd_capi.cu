@@ -90,7 +90,8 @@ struct Instance {
   DevBuf small;        // tau[12], sigma[9], dsigma[9], flags[8]
   DevBuf mask, site;
   DevBuf tw_x, tw_y, tw_z, tw_r, tab16;  // twiddles in compute precision, int16 tables
-  const int16_t *posM = nullptr, *kx_of = nullptr, *ky_of = nullptr, *kz_of = nullptr, *negy = nullptr;
+  const int16_t *posM = nullptr, *kx_of = nullptr, *ky_of = nullptr, *kz_of = nullptr, *negy = nullptr,
+                *kord = nullptr;
   std::vector<double> hist;  // host copy of the last advance's per-step stats
   int hist_count = 0;
   int group = -1;       // index of the batched group this instance belongs to
@@ -194,11 +195,12 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   if ((st = upload_twiddles<T>(h, I.tw_z, I.M, I.M))) return st;
   if ((st = upload_twiddles<T>(h, I.tw_r, I.nz, I.M))) return st;
 
-  // int16 tables: posM[M], kx_of[nx], ky_of[ny], kz_of[nzp], negy[ny]
+  // int16 tables: posM[M], kx_of[nx], ky_of[ny], kz_of[nzp], negy[ny], kord[M/2]
   std::vector<int> pz = positions(I.pz), px = positions(I.px), py = positions(I.py);
-  std::vector<int16_t> tab(I.M + I.nx + I.ny + I.nzp + I.ny, 0);
+  std::vector<int16_t> tab(I.M + I.nx + I.ny + I.nzp + I.ny + I.M / 2, 0);
   int16_t *t_posM = tab.data(), *t_kx = t_posM + I.M, *t_ky = t_kx + I.nx, *t_kz = t_ky + I.ny;
   neg_slots(I.ny, I.split, py.data(), t_kz + I.nzp);
+  unpack_order(pz.data(), I.M, t_kz + I.nzp + I.ny);
   for (int k = 0; k < I.M; ++k) t_posM[k] = (int16_t)pz[k];
   for (int k = 0; k < I.nx; ++k) t_kx[px[k]] = (int16_t)k;
   if (I.split) {
@@ -227,6 +229,7 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   I.ky_of = I.kx_of + I.nx;
   I.kz_of = I.ky_of + I.ny;
   I.negy = I.kz_of + I.nzp;
+  I.kord = I.negy + I.ny;
 
   const size_t fieldN = (size_t)I.F * I.N;
   for (int b = 0; b < 2; ++b) {
@@ -322,6 +325,7 @@ void fill_plane_args(const Instance &I, PlaneArgs &pa) {
   pa.tw_y = I.tw_y.p; pa.tw_z = I.tw_z.p; pa.tw_r = I.tw_r.p;
   pa.posM = I.posM;
   pa.negy = I.negy;
+  pa.kord = I.kord;
   set_plane_divisors<T>(pa, I.split ? I.ny / 2 : I.ny);
 }
 

@@ -115,10 +115,11 @@ struct PlaneArgs {
   int S, F;                   // slip systems; fields in flight (S, or 2S with Im xi)
   const void *tw_y, *tw_z, *tw_r;   // W_ny^m, W_M^m, W_nz^k tables in compute precision
   const int16_t *posM;        // position of z-frequency k (< M) after the M-point transform
+  const int16_t *kord;        // k = 1..M/2 ordered by posM[k]: real/complex (un)packing pairs in slot order
   const int16_t *negy;        // slot of -ky for each local y slot (a split plane's rank r at r * rows)
   // divisors built on the host: rows per CTA (ny, or ny/2 when split),
-  // M/2 + 1 (real-to-complex pairs per row), nz / vector width, M
-  FastDiv fd_rows, fd_half, fd_nvec, fd_m;
+  // nz / vector width, M, M/2 (real-to-complex pairs per row)
+  FastDiv fd_rows, fd_nvec, fd_m, fd_mh;
 };
 
 struct PencilArgs {
@@ -376,7 +377,7 @@ constexpr int kPlaneRed = 136;   // doubles of reduction scratch (4 sums)
 
 template <typename C> struct PlaneSmem {
   C *buf, *twy, *twz, *twr;
-  int *pos;
+  int *pos, *kord;
   uint64_t *bar;
   double *red;
   __device__ PlaneSmem(unsigned char *raw, const PlaneArgs &a, int rows) {
@@ -385,12 +386,13 @@ template <typename C> struct PlaneSmem {
     twz = twy + a.ny;
     twr = twz + a.M;
     pos = reinterpret_cast<int *>(twr + a.M);
-    bar = reinterpret_cast<uint64_t *>(pos + ((a.M + 1) & ~1));
+    kord = pos + ((a.M + 1) & ~1);
+    bar = reinterpret_cast<uint64_t *>(kord + ((a.M / 2 + 1) & ~1));
     red = reinterpret_cast<double *>(bar + 1);
   }
   static size_t bytes(int rows, int ny, int nzs, int M) {
-    return ((size_t)rows * nzs + ny + 2 * (size_t)M) * sizeof(C) + (size_t)((M + 1) & ~1) * 4 + 8 +
-           kPlaneRed * 8;
+    return ((size_t)rows * nzs + ny + 2 * (size_t)M) * sizeof(C) + (size_t)((M + 1) & ~1) * 4 +
+           (size_t)((M / 2 + 1) & ~1) * 4 + 8 + kPlaneRed * 8;
   }
 };
 
@@ -400,6 +402,7 @@ __device__ __forceinline__ void load_plane_tables(const PlaneSmem<C> &sm, const 
   load_table(sm.twz, a.tw_z, a.M);
   load_table(sm.twr, a.tw_r, a.M);
   for (int i = threadIdx.x; i < a.M; i += blockDim.x) sm.pos[i] = a.posM[i];
+  for (int i = threadIdx.x; i < a.M / 2; i += blockDim.x) sm.kord[i] = a.kord[i];
 }
 
 // plane index and first row of this CTA (grid.x = planes, or 2 planes for SPLIT)
@@ -465,16 +468,21 @@ __device__ __forceinline__ void fwd_planes_compute(const PlaneSmem<cx<T>> &sm, c
   fft_forward<MaxRadix<NT>::value, GeomRows>(buf, sm.twz, a.pz, gz);
 
   // real-to-complex unpacking, pairs (k, M-k); X[M] rides in slot 0 (see the packing note)
-  const int half = M / 2 + 1;
-  for (int w = threadIdx.x; w < rows * half; w += blockDim.x) {
-    const int y = a.fd_half.div(w), k = w - y * half;
+  // k = 0 and the row padding, one row per thread: X[0] = z0.x + z0.y and
+  // X[M] = z0.x - z0.y are real, packed as X[0] + i X[M]
+  for (int y = threadIdx.x; y < rows; y += blockDim.x) {
     C *row = buf + (size_t)y * nzs;
-    if (k == 0) {
-      // X[0] = z0.x + z0.y and X[M] = z0.x - z0.y are real: packed as X[0] + i X[M]
-      C z0 = row[pos[0]];
-      row[pos[0]] = mk<C>(z0.x + z0.y, z0.x - z0.y);
-      for (int q = nzh; q < nzp; ++q) row[q] = mk<C>((T)0, (T)0);
-    } else {
+    C z0 = row[pos[0]];
+    row[pos[0]] = mk<C>(z0.x + z0.y, z0.x - z0.y);
+    for (int q = nzh; q < nzp; ++q) row[q] = mk<C>((T)0, (T)0);
+  }
+  // pairs (k, M-k), k = 1..M/2 taken in slot order (few bank conflicts)
+  const int mh = M / 2;
+  const int *kord = sm.kord;
+  for (int w = threadIdx.x; w < rows * mh; w += blockDim.x) {
+    const int y = a.fd_mh.div(w), k = kord[w - y * mh];
+    C *row = buf + (size_t)y * nzs;
+    {
       const int pk = pos[k], pm = pos[M - k];
       C zk = row[pk], zm = row[pm];
       // E = (Zk + conj Zm)/2, O = (Zk - conj Zm)/(2i), X[k] = E + W^k O, X[M-k] = conj(E - W^k O)
@@ -1084,17 +1092,20 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
 
   // complex-to-real packing: Zin[k] = A + i w D, Zin[M-k] = conj(A - i w D),
   // A = X[k] + conj X[M-k], D = X[k] - conj X[M-k], w = exp(+2 pi i k / nz)
-  const int half = M / 2 + 1;
-  for (int w = threadIdx.x; w < rows * half; w += blockDim.x) {
-    const int y = a.fd_half.div(w), k = w - y * half;
+  // k = 0, one row per thread: slot 0 holds x0 + i xM (the real kz = 0 and
+  // kz = nz/2 columns), so Zin[0] = (x0 + xM) + i (x0 - xM)
+  for (int y = threadIdx.x; y < rows; y += blockDim.x) {
+    C *row = buf + (size_t)y * nzs;
+    const C z = row[pos[0]];
+    row[pos[0]] = mk<C>(z.x + z.y, z.x - z.y);
+  }
+  // pairs (k, M-k), k = 1..M/2 taken in slot order (few bank conflicts)
+  const int mh = M / 2;
+  const int *kord = sm.kord;
+  for (int w = threadIdx.x; w < rows * mh; w += blockDim.x) {
+    const int y = a.fd_mh.div(w), k = kord[w - y * mh];
     C *row = buf + (size_t)y * nzs;
     const int pk = pos[k];
-    if (k == 0) {
-      // slot 0 holds x0 + i xM (the real kz = 0 and kz = nz/2 columns): Zin[0] = (x0 + xM) + i (x0 - xM)
-      const C z = row[pk];
-      row[pk] = mk<C>(z.x + z.y, z.x - z.y);
-      continue;
-    }
     const int pm = pos[M - k];
     const C xk = row[pk];
     const C xm = row[pm];

@@ -127,7 +127,7 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   const size_t b_part = up256(2 * (size_t)F * nx * sizeof(double));
   const size_t b_small = up256((PFDD_MAXS + 9 + 8 + 2) * sizeof(double));
   const size_t b_tw = up256((size_t)(nx + ny + 2 * M) * sizeof(C));
-  const size_t b_tab = up256((size_t)(M + nx + 2 * ny + nzp) * sizeof(int16_t));
+  const size_t b_tab = up256((size_t)(M + nx + 2 * ny + nzp + M / 2) * sizeof(int16_t));
   const size_t need = b_spec + b_part + b_small + b_tw + b_tab;
   if (need > PFDD_STATIC_SCRATCH_BYTES)
     return nerr(PFDD_EINVAL, "grid needs more scratch than the static array holds; use pfdd_gpu_create");
@@ -155,11 +155,13 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   twiddles_into(M, M, htw + nx + ny);
   twiddles_into(nz, M, htw + nx + ny + M);
   int pos[1024];
-  int16_t htab[512 + 1024 + 1024 + 513 + 1024];
+  int16_t htab[512 + 1024 + 1024 + 513 + 1024 + 256];
   memset(htab, 0, sizeof htab);
   int16_t *t_posM = htab, *t_kx = t_posM + M, *t_ky = t_kx + nx, *t_kz = t_ky + ny;
   positions_into(pz, pos);
   for (int k = 0; k < M; ++k) { t_posM[k] = (int16_t)pos[k]; t_kz[pos[k]] = (int16_t)k; }
+  int16_t *t_kord = t_kz + nzp + ny;
+  unpack_order(pos, M, t_kord);
   t_kz[M] = (int16_t)M;
   positions_into(px, pos);
   for (int k = 0; k < nx; ++k) t_kx[pos[k]] = (int16_t)k;
@@ -201,7 +203,7 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   cudaError_t e = cudaSuccess;
   e = cudaMemcpyAsync(tw, htw, (size_t)(nx + ny + 2 * M) * sizeof(C), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(tab, htab, (size_t)(M + nx + 2 * ny + nzp) * sizeof(int16_t), cudaMemcpyHostToDevice, s);
+    e = cudaMemcpyAsync(tab, htab, (size_t)(M + nx + 2 * ny + nzp + M / 2) * sizeof(int16_t), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(tau, htau, S * sizeof(double), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(flags, 0, 8 * sizeof(int), s);
   if (e != cudaSuccess) return nerr(PFDD_ECUDA, cudaGetErrorString(e));
@@ -214,6 +216,7 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   pa.tw_y = tw_y; pa.tw_z = tw_z; pa.tw_r = tw_r;
   pa.posM = t_posM - htab + tab;
   pa.negy = t_neg - htab + tab;
+  pa.kord = t_kord - htab + tab;
   set_plane_divisors<double>(pa, ny);
   PencilArgs pe;
   pe = PencilArgs{};

@@ -45,9 +45,9 @@ inline bool make_plan(int n, FftPlan &p, int maxr = 16) {
 // fields of the argument block are set).
 template <typename T> inline void set_plane_divisors(PlaneArgs &pa, int rows) {
   pa.fd_rows = FastDiv(rows);
-  pa.fd_half = FastDiv(pa.M / 2 + 1);
   pa.fd_nvec = FastDiv(pa.nz / (sizeof(T) == 4 ? 4 : 2));
   pa.fd_m = FastDiv(pa.M);
+  pa.fd_mh = FastDiv(pa.M / 2);
 }
 template <typename T> inline void set_pencil_divisors(PencilArgs &pe) {
   pe.fd_fcc = FastDiv(pe.F * pe.ccols);
@@ -70,6 +70,19 @@ inline void neg_slots(int ny, bool split, const int *pos, int16_t *out) {
       const int ky = split ? r + 2 * kloc[sl] : kloc[sl];
       const int nk = (ny - ky) % ny;   // same parity as ky (ny even)
       out[r * n + sl] = (int16_t)pos[split ? (nk - r) / 2 : nk];
+    }
+}
+
+// k = 1..M/2 sorted by the slot pos[k] (PlaneArgs::kord), so consecutive
+// threads of the (un)packing loops touch neighbouring slots.  Stack only.
+inline void unpack_order(const int *pos, int M, int16_t *out) {
+  const int mh = M / 2;
+  for (int i = 0; i < mh; ++i) out[i] = (int16_t)(i + 1);
+  for (int i = 1; i < mh; ++i)   // insertion sort by slot (M <= 512)
+    for (int j = i; j > 0 && pos[out[j]] < pos[out[j - 1]]; --j) {
+      const int16_t t = out[j];
+      out[j] = out[j - 1];
+      out[j - 1] = t;
     }
 }
 
