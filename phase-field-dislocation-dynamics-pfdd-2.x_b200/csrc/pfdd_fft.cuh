@@ -38,6 +38,15 @@ template <typename C> __device__ __forceinline__ C cmulc(C a, C b) {
   return mk<C>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 template <typename C> __device__ __forceinline__ C cconj(C a) { return mk<C>(a.x, -a.y); }
+#ifndef PFDD_NO_F32X2
+// FP32 complex add / subtract as one packed f32x2 add (sm_100 FADD2; same
+// rounding as two scalar adds).  A packed complex multiply measured slower
+// (its operand shuffles cost more than the packing saves), so cmul stays scalar.
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+  return __fadd2_rn(a, make_float2(-b.x, -b.y));
+}
+#endif
 template <typename C, typename T> __device__ __forceinline__ C cscale(C a, T s) { return mk<C>(a.x * s, a.y * s); }
 // multiply by SIGN * i
 template <int SIGN, typename C> __device__ __forceinline__ C mul_si(C a) {

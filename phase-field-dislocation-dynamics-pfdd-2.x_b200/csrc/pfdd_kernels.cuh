@@ -331,7 +331,10 @@ __device__ __forceinline__ void cross_stage(C *buf, const C *__restrict__ twx2, 
   const int total = nyh * nzh;
   const int begin = rank == 0 ? 0 : total / 2, end = rank == 0 ? total / 2 : total;
   cl.sync();
-  constexpr int U = 4;   // pairs in flight per thread
+#ifndef PFDD_CROSS_U
+#define PFDD_CROSS_U 4
+#endif
+  constexpr int U = PFDD_CROSS_U;   // pairs in flight per thread
   for (int i0 = begin + threadIdx.x; i0 < end; i0 += U * blockDim.x) {
     C a[U], b[U], w[U];
     size_t o[U];
