@@ -50,7 +50,7 @@ template <typename T> struct Threads;
 // plane: whole-plane P1/P3 CTAs; half: each CTA of a split (2-CTA cluster)
 // plane; pencil: P2 CTAs.  FP32 defaults were measured on 256x256x128 with
 // 12 systems: 256-thread split-plane CTAs at three per SM (80 registers) and
-// 256-thread pencil CTAs of at most 106 KB of shared memory at two per SM
+// 256-thread pencil CTAs of at most 107 KB of shared memory at two per SM
 // beat 512-thread CTAs at one per SM by 0.3 ms per step.
 #ifndef PFDD_HALF_THREADS_F32
 #define PFDD_HALF_THREADS_F32 256
@@ -59,7 +59,7 @@ template <typename T> struct Threads;
 #define PFDD_PENCIL_THREADS_F32 256
 #endif
 #ifndef PFDD_PENCIL_SMEM_KB
-#define PFDD_PENCIL_SMEM_KB 106
+#define PFDD_PENCIL_SMEM_KB 107
 #endif
 template <> struct Threads<float> {
   static constexpr int plane = 512, half = PFDD_HALF_THREADS_F32, pencil = PFDD_PENCIL_THREADS_F32;
@@ -289,7 +289,8 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   // tile's columns) and the columns' slots
   auto pencil_bytes = [&](int cc) {
     return ((size_t)I.F * fstride_for(cc) + (size_t)I.nx) * sizeof(C) + 64 * sizeof(double) +
-           ((size_t)I.nx + 2 * (size_t)cc) * sizeof(V4<T>) + 2 * (size_t)cc * sizeof(int);
+           ((size_t)I.nx + 2 * (size_t)cc) * sizeof(V4<T>) + 2 * (size_t)((cc + 3) & ~3) * sizeof(int) +
+           (size_t)cc * I.S * sizeof(C);
   };
   int cc = 32;
   // widest tile that fits the budget and still gives every SM two tiles

@@ -659,7 +659,11 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
   // slot, cyv / czv per column of the tile (w = 1 on the axis's Nyquist index)
   V4<T> *kxv = reinterpret_cast<V4<T> *>(red + 64);
   V4<T> *cyv = kxv + nx, *czv = cyv + cc;
-  int *csy = reinterpret_cast<int *>(czv + cc), *csz = csy + cc;
+  int *csy = reinterpret_cast<int *>(czv + cc), *csz = csy + ((cc + 3) & ~3);
+  // Im xi spectrum at this tile's kx = nx/2 points (cc columns x S systems),
+  // read once at CTA start: those few points would otherwise make one warp
+  // wait on S dependent global loads while the CTA waits for it
+  C *nqs = reinterpret_cast<C *>(csz + ((cc + 3) & ~3));
   const size_t col0 = (size_t)blockIdx.x * cc;
   const size_t ncols = a.ncols;
   const int cpr = (int)(cc * sizeof(C) / 16);    // 16-byte chunks per (field, x) row
@@ -696,6 +700,15 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
         csz[c] = sz;
       }
     }
+    if (a.imag == IMAG_NYQ && a.mode != PASS_SYNTH)
+      for (int i = threadIdx.x; i < cc * S; i += blockDim.x) {
+        const int c = i / S, f = i - c * S;
+        const int col = (int)(col0 + c);
+        const int sy = a.fd_nzp.div(col), sz = col - sy * a.nzp;
+        bool nq;
+        const size_t ai = nyq_index<T, C>(a, f, a.sx_n, sy, sz, nq);
+        nqs[i] = nq ? caux[ai] : mk<C>((T)0, (T)0);
+      }
   }
   if (a.mode != PASS_SYNTH) cp_async_wait_all();
   __syncthreads();
@@ -767,12 +780,29 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
       // P = B(k)(Xr + i Xi), Q = B(k')(Xr - i Xi), k' = vector of index -k;
       // Er = (P + Q)/2, Ei = (P - Q)/(2i): the real and imaginary fields of
       // IFFT(B_index X) for the complex field X = Xr + i Xi.
+      // Im xi of the point for system b: the second field (full carrier), the
+      // tile's kx = nx/2 snapshot, or the Nyquist spectrum (loads batched by 4)
+      const bool snap = a.imag == IMAG_NYQ && sx == a.sx_n;
+      const int s0 = c * S;
       C si[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) si[q] = mk<C>((T)0, (T)0);
-#pragma unroll(SC > 0 ? SC : 1)
-      for (int b = 0; b < S; ++b)
-        green_accumulate<T>(g, b, a.imag == IMAG_FULL ? pk[(S + b) * fs] : caux[a0 + b * astride], si);
+      for (int b0 = 0; b0 < S; b0 += 4) {
+        C xv[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int b = b0 + q;
+          xv[q] = mk<C>((T)0, (T)0);
+          if (b < S) {
+            if (a.imag == IMAG_FULL) xv[q] = pk[(S + b) * fs];
+            else if (snap) xv[q] = nqs[s0 + b];
+            else xv[q] = caux[a0 + b * astride];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (b0 + q < S) green_accumulate<T>(g, b0 + q, xv[q], si);
+      }
       C sp[6], sq[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
@@ -801,7 +831,9 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
           // Nyquist point: Im xi spectrum updated in k-space (no mask, no core force on Im xi)
           const C dlt = mk<C>(-cd * ei.x, -cd * ei.y);
           C *ap = caux + a0 + aa * astride;
-          const C old = *ap;
+          C old;
+          if (snap) old = nqs[s0 + aa];
+          else old = *ap;
           *ap = mk<C>(old.x + dlt.x, old.y + dlt.y);
           dsq += wgt * ((double)dlt.x * (double)dlt.x + (double)dlt.y * (double)dlt.y);
         }

@@ -114,7 +114,8 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   };
   auto pencil_bytes = [&](int cc) {
     return ((size_t)F * fstride_for(cc) + (size_t)nx) * sizeof(C) + 64 * sizeof(double) +
-           ((size_t)nx + 2 * (size_t)cc) * sizeof(V4<double>) + 2 * (size_t)cc * sizeof(int);
+           ((size_t)nx + 2 * (size_t)cc) * sizeof(V4<double>) + 2 * (size_t)((cc + 3) & ~3) * sizeof(int) +
+           (size_t)cc * S * sizeof(C);
   };
   int cc = 32;
   while (cc > 1 && (ncols % cc || pencil_bytes(cc) > 200 * 1024)) cc >>= 1;
