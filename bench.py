@@ -281,25 +281,28 @@ def fp32_vs_fp64(ws, K, stream, local, steps=2000):
 def cufft_comparison(w, F, prec, stream, reps=10):
     """cuFFT (torch.fft) real-to-complex and complex-to-real 3-D transforms of
     the same F fields on the same grid and precision, timed alone with CUDA
-    events: what a library FFT pair costs before any contraction or update."""
+    events (median of `reps` single calls into preallocated outputs): what a
+    library FFT pair costs before any contraction or update."""
     import torch
     dt = torch.float32 if prec == "fp32" else torch.float64
     x = torch.randn(F, w.nx, w.ny, w.nz, device="cuda", dtype=dt)
     y = torch.fft.rfftn(x, dim=(1, 2, 3))
+    z = torch.empty_like(x)
 
     def t(fn):
         with torch.cuda.stream(stream):
             for _ in range(3):
                 fn()
-            ms, _ = timed_events(stream, lambda: [fn() for _ in range(reps)])
-        return ms / reps
+            ms = [timed_events(stream, fn)[0] for _ in range(reps)]
+        return statistics.median(ms)
 
-    r = t(lambda: torch.fft.rfftn(x, dim=(1, 2, 3)))
-    i = t(lambda: torch.fft.irfftn(y, s=(w.nx, w.ny, w.nz), dim=(1, 2, 3)))
-    del x, y
+    r = t(lambda: torch.fft.rfftn(x, dim=(1, 2, 3), out=y))
+    i = t(lambda: torch.fft.irfftn(y, s=(w.nx, w.ny, w.nz), dim=(1, 2, 3), out=z))
+    del x, y, z
     torch.cuda.empty_cache()
     return {"rfftn_ms": r, "irfftn_ms": i, "pair_ms": r + i,
-            "note": "torch.fft (cuFFT) on [%d,%d,%d,%d] %s, transforms only" % (F, w.nx, w.ny, w.nz, prec)}
+            "note": "torch.fft (cuFFT) on [%d,%d,%d,%d] %s, transforms only, median of %d calls"
+                    % (F, w.nx, w.ny, w.nz, prec, reps)}
 
 
 def adjoint_ratio(st, w, prec, stream, local, steps=500, ckpt=50):

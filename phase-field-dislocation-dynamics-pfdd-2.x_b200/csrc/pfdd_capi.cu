@@ -95,6 +95,9 @@ struct Instance {
   std::vector<double> hist;  // host copy of the last advance's per-step stats
   int hist_count = 0;
   int group = -1;       // index of the batched group this instance belongs to
+  // adjoint scratch, kept between calls (checkpoints, segment states,
+  // lambda pair, target, Nyquist carrier of lambda, partial sums, final state)
+  DevBuf adj_ck, adj_seg, adj_lam[2], adj_tgt, adj_aux, adj_gpart, adj_acc, adj_lpart, adj_fin, adj_finaux;
   double *tau() const { return small.as<double>(); }
   double *sigma() const { return small.as<double>() + PFDD_MAXS; }   // sigma[9] then dsigma[9]
   int *flags() const { return reinterpret_cast<int *>(small.as<double>() + PFDD_MAXS + 18); }
@@ -353,6 +356,8 @@ pfdd_status set_smem_attrs(pfdd_gpu *h, size_t plane, size_t upd, size_t pencil)
   CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes<T, NP, false>, A, (int)upd));
   CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes<T, NH, true>, A, (int)upd));
   CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes_tab<T, NP, false>, A, (int)upd));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_adj_planes<T, NP, false>, A, (int)upd));
+  CUDA_TRY(h, cudaFuncSetAttribute(k_adj_planes<T, NH, true>, A, (int)upd));
   CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes_tab<T, NH, true>, A, (int)upd));
   return PFDD_OK;
 }
@@ -424,11 +429,10 @@ void launch_step_tab(const Instance &L, unsigned B, cudaStream_t st, const InstP
   else k_step_planes_tab<T, NP, false><<<dim3(planes, B), NP, L.smem_update, st>>>(tab, pa, ua, (int)fwd);
 }
 
-// Enqueue one GL iteration of one instance; `step` indexes the stats record.
-// One GL iteration (PASS_STEP) of instance I from xi[cur] into xi[cur^1];
-// with `adj`, one adjoint iteration of the fields in adj->lam[cur] into
-// adj->lam[cur^1] at forward state adj->xfwd (P1 and P2 unchanged: the
-// elastic operator is self-adjoint).
+// Buffers of one adjoint iteration: lambda in and out, the forward state it
+// linearises about, the Nyquist carrier of lambda and the gradient partials
+// (P1 and P2 are those of the forward step: the elastic operator is
+// self-adjoint).
 struct AdjointPass {
   void *lam_in, *lam_out;
   const void *xfwd;
@@ -436,9 +440,13 @@ struct AdjointPass {
   double *gpart;
 };
 
+// One GL iteration (or, with adj, one adjoint iteration) of instance I whose
+// spectrum is current, i.e. opened by launch_fwd or left by the previous fused
+// plane pass: P2, the fused plane pass (fwd: also the next iteration's
+// spectrum) and, for forward steps, the reduction.
 template <typename T>
-void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_t *ev = nullptr,
-                  const AdjointPass *adj = nullptr) {
+void enqueue_step_fused(Instance &I, cudaStream_t st, bool fwd, const AdjointPass *adj = nullptr) {
+  constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
   PlaneArgs pa;
   fill_plane_args<T>(I, pa);
   int *flags = I.flags();
@@ -446,9 +454,6 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   T *xout = adj ? static_cast<T *>(adj->lam_out) : I.xi[I.cur ^ 1].as<T>();
   cx<T> *spec = I.spec.as<cx<T>>();
   const int planes = I.F * I.nx;
-  if (ev) cudaEventRecord(ev[0], st);
-  launch_fwd<T>(I, st, xin, spec, pa, flags, flags + 3);
-  if (ev) cudaEventRecord(ev[1], st);
   PencilArgs pe{};
   pe.px = I.px;
   pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.nzp = I.nzp; pe.M = I.M;
@@ -466,8 +471,8 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   pe.g = I.green;
   set_pencil_divisors<T>(pe);
   launch_pencil<T>(I, st, spec, pe, flags);
-  if (ev) cudaEventRecord(ev[2], st);
   UpdateArgs ua;
+  memset(&ua, 0, sizeof ua);
   ua.nx = I.nx; ua.ny = I.ny; ua.nz = I.nz; ua.nzh = I.nzh; ua.nzp = I.nzp; ua.S = I.S; ua.F = I.F;
   ua.cd = I.d.cd_dt;
   ua.invN = 1.0 / (double)I.N;
@@ -480,16 +485,22 @@ void enqueue_step(Instance &I, cudaStream_t st, int step, double tol, cudaEvent_
   ua.mode = adj ? PASS_ADJOINT : PASS_STEP;
   ua.xfwd = adj ? adj->xfwd : nullptr;
   ua.gpart = adj ? adj->gpart : nullptr;
-  launch_inv<T>(I, planes, st, spec, xin, xout, pa, ua, I.partials.as<double>());
-  if (ev) cudaEventRecord(ev[3], st);
-  if (adj) return;
+  double *partials = I.partials.as<double>();
+  if (adj) {
+    if (I.split)
+      launch_pair(k_adj_planes<T, NH, true>, dim3(2 * planes), NH, I.smem_update, st, spec, xin, xout, pa, ua,
+                  partials, (int)fwd);
+    else k_adj_planes<T, NP, false><<<planes, NP, I.smem_update, st>>>(spec, xin, xout, pa, ua, partials, (int)fwd);
+    return;
+  }
+  if (I.split)
+    launch_pair(k_step_planes<T, NH, true>, dim3(2 * planes), NH, I.smem_update, st, spec, xin, xout, pa, ua,
+                partials, (int)fwd);
+  else k_step_planes<T, NP, false><<<planes, NP, I.smem_update, st>>>(spec, xin, xout, pa, ua, partials, (int)fwd);
   const bool nyq = I.imag == IMAG_NYQ;
-  k_finalize<<<1, 256, 0, st>>>(I.partials.as<double>(), planes, I.stats.as<double>(), step, tol, flags,
-                                 flags + 1, flags + 2, nyq ? I.ppart.as<double>() : nullptr, nyq ? I.ntiles : 0,
-                                 1.0 / (double)I.N);
-  if (ev) cudaEventRecord(ev[4], st);
+  k_finalize<<<1, 256, 0, st>>>(partials, planes, I.stats.as<double>(), 0, 0.0, flags, flags + 1, flags + 2,
+                                 nyq ? I.ppart.as<double>() : nullptr, nyq ? I.ntiles : 0, 1.0 / (double)I.N);
 }
-
 
 // ------------------------------------------------------------ batched groups
 bool same_group(const Instance &a, const Instance &b) {
@@ -746,15 +757,25 @@ pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const dou
   const size_t n_all = (size_t)I.F * I.N;
   const size_t aux_bytes = I.aux.bytes;
   const int nck = (n_steps + K - 1) / K;
-  DevBuf ck, seg, lam[2], tgt, auxa, gpart, acc, lpart;
-  CUDA_TRY(h, ck.alloc((size_t)nck * (n_all * sizeof(T) + aux_bytes)));
-  CUDA_TRY(h, seg.alloc((size_t)K * n_re * sizeof(T)));
-  for (int b = 0; b < 2; ++b) CUDA_TRY(h, lam[b].alloc(n_all * sizeof(T)));
-  CUDA_TRY(h, tgt.alloc(n_re * sizeof(T)));
-  if (aux_bytes) CUDA_TRY(h, auxa.alloc(aux_bytes));
-  CUDA_TRY(h, gpart.alloc(4 * (size_t)I.F * I.nx * sizeof(double)));
-  CUDA_TRY(h, acc.alloc(2 * (2 + PFDD_MAXS) * sizeof(double)));
-  CUDA_TRY(h, lpart.alloc(2 * 1184 * sizeof(double)));
+  // scratch kept in the instance and grown on demand (no allocation per call)
+  auto need = [&](DevBuf &b, size_t bytes) -> cudaError_t {
+    if (b.bytes >= bytes && b.p) return cudaSuccess;
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    b.release();
+    return b.alloc(bytes);
+  };
+  DevBuf &ck = I.adj_ck, &seg = I.adj_seg, &tgt = I.adj_tgt, &auxa = I.adj_aux, &gpart = I.adj_gpart,
+         &acc = I.adj_acc, &lpart = I.adj_lpart;
+  DevBuf *lam = I.adj_lam;
+  CUDA_TRY(h, need(ck, (size_t)nck * (n_all * sizeof(T) + aux_bytes)));
+  CUDA_TRY(h, need(seg, (size_t)K * n_re * sizeof(T)));
+  for (int b = 0; b < 2; ++b) CUDA_TRY(h, need(lam[b], n_all * sizeof(T)));
+  CUDA_TRY(h, need(tgt, n_re * sizeof(T)));
+  if (aux_bytes) CUDA_TRY(h, need(auxa, aux_bytes));
+  CUDA_TRY(h, need(gpart, 4 * (size_t)I.F * I.nx * sizeof(double)));
+  CUDA_TRY(h, need(acc, 2 * (2 + PFDD_MAXS) * sizeof(double)));
+  CUDA_TRY(h, need(lpart, 2 * 1184 * sizeof(double)));
   CUDA_TRY(h, cudaMemsetAsync(acc.p, 0, acc.bytes, st));
   if (I.stats_cap < 1) {  // the forward steps record their stats at index 0
     CUDA_TRY(h, I.stats.alloc(2 * sizeof(double)));
@@ -783,18 +804,21 @@ pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const dou
     return e;
   };
   k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.stress, 0, I.flags());
-  // forward with checkpoints
+  PlaneArgs pa;
+  fill_plane_args<T>(I, pa);
+  // forward with checkpoints: one opening transform, then fused steps
+  launch_fwd<T>(I, st, I.xi[I.cur].as<T>(), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
   for (int n = 0; n < n_steps; ++n) {
     if (n % K == 0) CUDA_TRY(h, save(n / K));
-    enqueue_step<T>(I, st, 0, 0.0);
+    enqueue_step_fused<T>(I, st, n + 1 < n_steps);
     I.cur ^= 1;
   }
   // keep the final state to hand back; seed lambda = 2 (Re xi_N - target), mu = 0
-  DevBuf fin, finaux;
-  CUDA_TRY(h, fin.alloc(n_all * sizeof(T)));
+  DevBuf &fin = I.adj_fin, &finaux = I.adj_finaux;
+  CUDA_TRY(h, need(fin, n_all * sizeof(T)));
   CUDA_TRY(h, cudaMemcpyAsync(fin.p, I.xi[I.cur].p, n_all * sizeof(T), cudaMemcpyDeviceToDevice, st));
   if (aux_bytes) {
-    CUDA_TRY(h, finaux.alloc(aux_bytes));
+    CUDA_TRY(h, need(finaux, aux_bytes));
     CUDA_TRY(h, cudaMemcpyAsync(finaux.p, I.aux.p, aux_bytes, cudaMemcpyDeviceToDevice, st));
     CUDA_TRY(h, cudaMemsetAsync(auxa.p, 0, aux_bytes, st));
   }
@@ -805,17 +829,21 @@ pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const dou
   for (int j = nck - 1; j >= 0; --j) {
     const int n0 = j * K, n1 = std::min(n_steps, n0 + K);
     CUDA_TRY(h, restore(j));
+    // recompute the segment's states (fused steps after one opening transform)
+    if (n1 - n0 > 1) launch_fwd<T>(I, st, I.xi[I.cur].as<T>(), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
     for (int n = n0; n < n1; ++n) {
       CUDA_TRY(h, cudaMemcpyAsync(seg.as<T>() + (size_t)(n - n0) * n_re, I.xi[I.cur].p, n_re * sizeof(T),
                                   cudaMemcpyDeviceToDevice, st));
       if (n + 1 < n1) {
-        enqueue_step<T>(I, st, 0, 0.0);
+        enqueue_step_fused<T>(I, st, n + 2 < n1);
         I.cur ^= 1;
       }
     }
+    // backward steps: the plane pass of each also transforms the new lambda
+    launch_fwd<T>(I, st, lam[lc].as<T>(), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
     for (int n = n1 - 1; n >= n0; --n) {
       AdjointPass ap{lam[lc].p, lam[lc ^ 1].p, seg.as<T>() + (size_t)(n - n0) * n_re, auxa.p, gpart.as<double>()};
-      enqueue_step<T>(I, st, 0, 0.0, nullptr, &ap);
+      enqueue_step_fused<T>(I, st, n > n0, &ap);
       lc ^= 1;
       k_grad_accum<<<1, 32, 0, st>>>(gpart.as<double>(), I.S, I.nx, acc.as<double>(), acc.as<double>() + 2 + PFDD_MAXS);
     }

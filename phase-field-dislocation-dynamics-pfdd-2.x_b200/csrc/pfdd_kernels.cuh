@@ -1067,10 +1067,11 @@ __device__ __forceinline__ T update_one(const UpdateArgs &u, bool real_field, in
 
 // Per-instance pointers travel as arguments so the constant parameter block
 // (PlaneArgs, UpdateArgs) is read in place and never copied.
-// FUSE (PASS_STEP only): the updated plane also stays in shared memory and,
+// FUSE 1 (PASS_STEP) / 2 (PASS_ADJOINT): only that pass is compiled, and the
+// updated plane also stays in shared memory and,
 // when `fwd`, is transformed forward (fwd_planes_compute) and stored over the
 // spectrum rows this CTA read, as the next step's P1 output.
-template <typename T, int NT, bool SPLIT, bool FUSE = false>
+template <typename T, int NT, bool SPLIT, int FUSE = 0>
 __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__restrict__ xin,
                                                 T *__restrict__ xout, const PlaneArgs &a, const UpdateArgs &u,
                                                 double *__restrict__ partials, size_t plane,
@@ -1170,7 +1171,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
   const int nvec = nz / VN;
   const int total = rows * nvec;
   const FastDiv &dv = a.fd_nvec;
-  if (u.mode == PASS_SYNTH) {
+  if (FUSE == 0 && u.mode == PASS_SYNTH) {
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int y = dv.div(i), zq = i - y * nvec;
       T e[VN];
@@ -1181,7 +1182,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
     }
     return;
   }
-  if (u.mode == PASS_ENERGY) {
+  if (FUSE == 0 && u.mode == PASS_ENERGY) {
     // 1/2 xi . (L xi), f(Re xi) and -tau Re xi, summed over the plane (FP64)
     const T *site = reinterpret_cast<const T *>(site_p);
     const double tau = real_field ? tau_p[sys] : 0.0;
@@ -1206,7 +1207,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
     plane_sum<SPLIT>(v, sm.red, u.gpart + 4 * plane);
     return;
   }
-  if (u.mode == PASS_ADJOINT) {
+  if (FUSE != 1 && u.mode == PASS_ADJOINT) {
     // lam_n = lam_{n+1} - cd (L lam + f''(xi_n) lam_{n+1}) on unmasked sites
     // (the elastic operator is self-adjoint; tau is constant and drops out);
     // parameter gradients use lam_{n+1} and xi_n on the same sites.
@@ -1238,16 +1239,27 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
         }
       }
       if (ok) *reinterpret_cast<V *>(xout + off + idx) = *reinterpret_cast<V *>(nv);
+      if (FUSE == 2 && fwd)
+        *reinterpret_cast<V *>(reinterpret_cast<T *>(buf) + (size_t)y * 2 * nzs + zq * VN) =
+            *reinterpret_cast<V *>(nv);
     }
     double v[4] = {g0, g1, gl, 0.0};
     plane_sum<SPLIT>(v, sm.red, u.gpart + 4 * plane);
+    if constexpr (FUSE == 2) {
+      if (fwd) {   // the next backward step's spectrum of the new lambda
+        __syncthreads();
+        fwd_planes_compute<T, NT, SPLIT>(sm, a, const_cast<cx<T> *>(spec), plane, rows, row0, ok);
+      }
+    }
     return;
   }
+  if constexpr (FUSE == 2) return;
+  else {
   // update pass only: tau, mask and per-site GSFE are read from here on
   const T tau = real_field ? (T)tau_p[sys] : (T)0;
   const T *site = reinterpret_cast<const T *>(site_p);
   T *bufw = reinterpret_cast<T *>(buf);
-  const bool keep = FUSE && fwd;   // new xi also into shared memory for the forward part
+  const bool keep = FUSE == 1 && fwd;   // new xi also into shared memory for the forward part
   double dsq = 0.0, sum = 0.0;
   // CF: the core model as a compile-time constant (3: sine GSFE, the common
   // case, with its force inlined), 0: dispatch per site
@@ -1303,11 +1315,12 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
   else update_loop(std::integral_constant<int, 0>());
   double v[2] = {dsq, sum};
   plane_sum<SPLIT>(v, sm.red, partials + 2 * plane);
-  if constexpr (FUSE) {
+  if constexpr (FUSE == 1) {
     if (fwd) {
       __syncthreads();
       fwd_planes_compute<T, NT, SPLIT>(sm, a, const_cast<cx<T> *>(spec), plane, rows, row0, ok);
     }
+  }
   }
 }
 
@@ -1329,8 +1342,19 @@ __global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, SPLIT>::value))
     k_step_planes(cx<T> *spec, const T *__restrict__ xin, T *__restrict__ xout, PlaneArgs a, UpdateArgs u,
                   double *__restrict__ partials, int fwd) {
   if (u.stop && *u.stop) return;
-  inv_update_body<T, NT, SPLIT, true>(spec, xin, xout, a, u, partials, plane_of_block<SPLIT>(), u.tau, u.mask,
+  inv_update_body<T, NT, SPLIT, 1>(spec, xin, xout, a, u, partials, plane_of_block<SPLIT>(), u.tau, u.mask,
                                       u.site, u.err, fwd != 0);
+}
+
+// One adjoint iteration (PASS_ADJOINT) fused with the forward transforms of
+// the new lambda (fwd != 0), for the next backward iteration.
+template <typename T, int NT, bool SPLIT>
+__global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, SPLIT>::value))
+    k_adj_planes(cx<T> *spec, const T *__restrict__ xin, T *__restrict__ xout, PlaneArgs a, UpdateArgs u,
+                 double *__restrict__ partials, int fwd) {
+  if (u.stop && *u.stop) return;
+  inv_update_body<T, NT, SPLIT, 2>(spec, xin, xout, a, u, partials, plane_of_block<SPLIT>(), u.tau, u.mask,
+                                   u.site, u.err, fwd != 0);
 }
 
 // grid = (F * nx planes [x 2 for SPLIT], instances of the group)
@@ -1340,7 +1364,7 @@ __global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, SPLIT>::value))
   const InstPtrs &ip = tab[blockIdx.y];
   if (ip.flags[0]) return;
   const int cur = ip.flags[4];
-  inv_update_body<T, NT, SPLIT, true>(static_cast<const cx<T> *>(ip.spec), static_cast<const T *>(ip.xi[cur]),
+  inv_update_body<T, NT, SPLIT, 1>(static_cast<const cx<T> *>(ip.spec), static_cast<const T *>(ip.xi[cur]),
                                       static_cast<T *>(ip.xi[cur ^ 1]), a, u, ip.partials,
                                       plane_of_block<SPLIT>(), ip.tau, ip.mask, ip.site, ip.flags + 3, fwd != 0);
 }
