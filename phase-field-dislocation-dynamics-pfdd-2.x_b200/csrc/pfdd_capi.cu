@@ -498,7 +498,7 @@ void enqueue_step_fused(Instance &I, cudaStream_t st, bool fwd, const AdjointPas
                 partials, (int)fwd);
   else k_step_planes<T, NP, false><<<planes, NP, I.smem_update, st>>>(spec, xin, xout, pa, ua, partials, (int)fwd);
   const bool nyq = I.imag == IMAG_NYQ;
-  k_finalize<<<1, 256, 0, st>>>(partials, planes, I.stats.as<double>(), 0, 0.0, flags, flags + 1, flags + 2,
+  k_finalize<<<1, 1024, 0, st>>>(partials, planes, I.stats.as<double>(), 0, 0.0, flags, flags + 1, flags + 2,
                                  nyq ? I.ppart.as<double>() : nullptr, nyq ? I.ntiles : 0, 1.0 / (double)I.N);
 }
 
@@ -610,7 +610,7 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   launch_step_tab<T>(L, B, st, tab, pa, ua, fwd);
   if (ev) cudaEventRecord(ev[2], st);
   const bool nyq = L.imag == IMAG_NYQ;
-  k_finalize_tab<<<B, 256, 0, st>>>(tab, planes, nyq ? L.ntiles : 0, 1.0 / (double)L.N, tol);
+  k_finalize_tab<<<B, 1024, 0, st>>>(tab, planes, nyq ? L.ntiles : 0, 1.0 / (double)L.N, tol);
   if (ev) cudaEventRecord(ev[3], st);
 }
 
