@@ -129,6 +129,62 @@ def resolved_shear(sigma_rot, xn, xb, dslip):
     return np.einsum("ij,aj,ai->a", np.asarray(sigma_rot), np.asarray(xn), np.asarray(xb)) / dslip
 
 
+# ---------------------------------------------------------------- strain / stress diagnostics
+def strain_stress(nx, ny, nz, four, xn, xb, dslip, C44, C12, C11, sigma_rot, xi):
+    """The reference's strain and stress diagnostics of state xi, computed as
+    DiagStress does (diag_stress.cpp:43-62) when data_fftw holds the forward
+    transform of xi: Fmatrix (fft_fftw_slab.cpp:644-732), strain (:3370-3469)
+    with stressfree_strain (:3252-3326), total_average_strain (:3331-3365) and
+    stress (:3474-3553).
+
+    F[s,i,j](k) = sum_klmn C_klmn G_jk eps^s_mn k_i k_l with
+    G = (2 I / k^2 - k k^T / ((1 - nu) k^4)) / (2 mu) (Voigt mu, nu), F(0) = 0;
+    strain_ij = IFFT(sum_s F[s,i,j] FFT(xi_s)) / N, plus avepst_ij on the real
+    part; eps = (strain + strain^T) / 2; sigma_ij = C_ijml (Re strain_ml -
+    eps0_ml - avepsts_ml) + sigma_rot_ij mu with eps0 = sum_s eps^s Re xi_s;
+    avepsts = S : sigma_rot mu (S the isotropic compliance of material.cpp:
+    154-156, here from the Voigt young and nu, identical for isotropic C),
+    avepst = avepsts + <eps0>.
+
+    Returns eps [3,3,nx,ny,nz] complex (data_eps), sigma [3,3,nx,ny,nz] real,
+    ave_eps [3,3], ave_sigma [3,3], avepst [3,3].
+    """
+    xi = np.asarray(xi)
+    C = stiffness(C44, C12)
+    mu, ll, young, xnu = voigt_constants(C44, C12, C11)
+    S11, S12 = 1.0 / young, -xnu / young
+    S44 = 2.0 * (S11 - S12)
+    d = np.eye(3)
+    Sc = (S44 / 4.0 * (np.einsum("ik,jl->ijkl", d, d) + np.einsum("il,jk->ijkl", d, d))
+          + S12 * np.einsum("ij,kl->ijkl", d, d))
+    eps = slip_eigenstrain(np.asarray(xn, float), np.asarray(xb, float), dslip)
+    sig = np.einsum("klmn,smn->skl", C, eps)
+    fx, fy, fz = frequencies(nx, ny, nz, four)
+    k = np.stack([fx, fy, fz], axis=0)                                  # [3, ...]
+    k2 = np.einsum("i...,i...->...", k, k)
+    nzm = k2 > 0
+    k2s = np.where(nzm, k2, 1.0)
+    G = (2.0 * d[:, :, None, None, None] / k2s
+         - (1.0 / (1.0 - xnu)) * np.einsum("j...,k...->jk...", k, k) / k2s ** 2) / (2.0 * mu)
+    X = np.fft.fftn(xi, axes=(1, 2, 3))
+    Y = np.einsum("skl,l...,s...->k...", sig, k, X)                     # sum_s (sigma^s k) X_s
+    GU = np.einsum("jk...,k...->j...", G, Y)
+    Fx = np.einsum("i...,j...->ij...", k, GU) * nzm
+    strain = np.fft.ifftn(Fx, axes=(2, 3, 4))
+    N = nx * ny * nz
+    ave_epsd = np.einsum("sij,s->ij", eps, xi.real.reshape(len(eps), -1).sum(axis=1)) / N
+    avepsts = np.einsum("ijkl,kl->ij", Sc, np.asarray(sigma_rot, float)) * mu
+    avepst = avepsts + ave_epsd
+    strain = strain + avepst[:, :, None, None, None]
+    eps_out = 0.5 * (strain + strain.transpose(1, 0, 2, 3, 4))
+    ave_eps = eps_out.real.reshape(3, 3, -1).mean(axis=2)
+    eps0 = np.einsum("sij,s...->ij...", eps, xi.real)
+    sigma = (np.einsum("ijml,ml...->ij...", C, strain.real - eps0 - avepsts[:, :, None, None, None])
+             + (np.asarray(sigma_rot, float) * mu)[:, :, None, None, None])
+    ave_sigma = sigma.reshape(3, 3, -1).mean(axis=2)
+    return eps_out, sigma, ave_eps, ave_sigma, avepst
+
+
 # ---------------------------------------------------------------- core energy
 @dataclass
 class CoreModel:

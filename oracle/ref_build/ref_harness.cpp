@@ -4,7 +4,7 @@
 //
 //   pfdd_ref_harness -deck in.deck [-steps N] [-state_in xi0.bin] [-xo_in xo.bin]
 //       [-mpea_in a.bin] [-set key value]... [-state_out xi.bin] [-stats_out s.txt]
-//       [-setup_out setup.txt] [-B_out bb.bin] [-timing]
+//       [-setup_out setup.txt] [-B_out bb.bin] [-stress_out st.bin] [-timing]
 //
 // Sequence (mirrors App::run, app.cpp:127-205, with the `run` command taken
 // out of the deck so state can be injected between init and setup):
@@ -13,6 +13,11 @@
 //   [inject]  xi, data_fftw, xo, material scalars, per-site GSFE amplitude
 //   timer->init(); app->setup(); app->iterate()  (SolveGL::iterate)
 //   [dump]    xi[0] (2*S*N doubles, reference layout), per-step xinorm/xiave
+//   [stress]  the strain/stress diagnostics of the final state as DiagStress
+//             computes them (diag_stress.cpp:43-62: averages reset, strain,
+//             total_average_strain, stress), after prep_forward() so data_fftw
+//             holds the transform of that state: data_eps (2*9*N), data_sigma
+//             (2*9*N), ave_eps[3][3], ave_sigma[3][3], avepst[3][3]
 //
 // Injection targets are the reference's own public members: FFT::xi/xo
 // (fft.h:48-50), FFTW_Slab::data_fftw (fft_fftw_slab.h), Material scalars
@@ -109,7 +114,8 @@ static double *material_field(Material *m, const std::string &k) {
 
 int main(int argc, char **argv) {
   const char *deck = nullptr, *state_in = nullptr, *xo_in = nullptr, *mpea_in = nullptr;
-  const char *state_out = nullptr, *stats_out = nullptr, *setup_out = nullptr, *B_out = nullptr;
+  const char *state_out = nullptr, *stats_out = nullptr, *setup_out = nullptr, *B_out = nullptr,
+             *stress_out = nullptr;
   long steps_override = -1;
   bool timing = false;
   std::vector<std::pair<std::string, double>> sets;
@@ -127,6 +133,7 @@ int main(int argc, char **argv) {
     else if (a == "-stats_out") { need(1); stats_out = argv[++i]; }
     else if (a == "-setup_out") { need(1); setup_out = argv[++i]; }
     else if (a == "-B_out") { need(1); B_out = argv[++i]; }
+    else if (a == "-stress_out") { need(1); stress_out = argv[++i]; }
     else if (a == "-set") { need(2); sets.emplace_back(argv[i + 1], atof(argv[i + 2])); i += 2; }
     else if (a == "-timing") { timing = true; }
     else { fprintf(stderr, "harness: unknown option %s\n", a.c_str()); return 2; }
@@ -249,6 +256,27 @@ int main(int argc, char **argv) {
   }
   if (state_out) write_bin(state_out, fft->xi[0], 2 * (size_t)S * N);
   if (B_out) write_bin(B_out, fft->BB, (size_t)S * S * N);
+  if (stress_out) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        fft->local_sigma[i][j] = fft->avepst[i][j] = fft->avepsts[i][j] = fft->avepsd[i][j] = 0.0;
+        fft->aveps[i][j] = fft->ave_eps[i][j] = fft->ave_sigma[i][j] = 0.0;
+      }
+    fft->prep_forward();
+    fft->strain();
+    fft->total_average_strain();
+    fft->stress();
+    std::vector<double> out;
+    out.insert(out.end(), fft->data_eps, fft->data_eps + 2 * 9 * (size_t)N);
+    out.insert(out.end(), fft->data_sigma, fft->data_sigma + 2 * 9 * (size_t)N);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) out.push_back(fft->ave_eps[i][j]);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) out.push_back(fft->ave_sigma[i][j]);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) out.push_back(fft->avepst[i][j]);
+    write_bin(stress_out, out.data(), out.size());
+  }
   if (stats_out) {
     FILE *f = fopen(stats_out, "w");
     for (size_t i = 0; i < fft->step_xinorm.size(); ++i)

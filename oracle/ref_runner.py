@@ -53,26 +53,30 @@ def _raise_stack():
 
 
 def run_reference(workload, steps, state=None, xo=None, mpea=None, sets=(), want_B=False,
-                  timing=False, workdir=None, timeout=3600, set_b=True, stress_states=None):
+                  timing=False, workdir=None, timeout=3600, set_b=True, stress_states=None, want_stress=False):
     """Run `steps` GL iterations of the reference on `workload`.
 
     state: complex or real array [S, nx, ny, nz] (default workload.xi0).
     Returns dict with xi (complex [S,nx,ny,nz]), xinorm, xiave, setup, and
-    optionally BB [S,S,nx,ny,nz] and the timing record.
+    optionally BB [S,S,nx,ny,nz], the timing record and (want_stress) the
+    strain/stress diagnostics of the final state: eps and sigma [3,3,nx,ny,nz]
+    complex (data_eps, data_sigma), ave_eps, ave_sigma, avepst [3,3].
     """
     if not available():
         raise RuntimeError("reference oracle not built: make -C oracle/ref_build")
     own_tmp = workdir is None
     tmp = workdir or tempfile.mkdtemp(prefix="pfdd_ref_")
     try:
-        return _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, set_b, stress_states)
+        return _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, set_b, stress_states,
+                    want_stress)
     finally:
         if own_tmp:
             import shutil
             shutil.rmtree(tmp, ignore_errors=True)
 
 
-def _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, set_b, stress_states):
+def _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, set_b, stress_states,
+         want_stress=False):
     S, nx, ny, nz = workload.S, workload.nx, workload.ny, workload.nz
     deck = os.path.join(tmp, "in.deck")
     with open(deck, "w") as f:
@@ -102,6 +106,8 @@ def _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, s
     args += ["-set", "CD", repr(float(workload.cd_dt))]
     if want_B:
         args += ["-B_out", os.path.join(tmp, "B.bin")]
+    if want_stress:
+        args += ["-stress_out", os.path.join(tmp, "stress.bin")]
     if timing:
         args += ["-timing"]
     env = dict(os.environ)
@@ -121,6 +127,16 @@ def _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, s
     }
     if want_B:
         out["BB"] = np.fromfile(os.path.join(tmp, "B.bin")).reshape(S, S, nx, ny, nz)
+    if want_stress:
+        raw = np.fromfile(os.path.join(tmp, "stress.bin"))
+        n = 2 * 9 * nx * ny * nz
+        # layout of data_eps / data_sigma: 2*(r + ida N + idb 3N) (fft_fftw_slab.cpp:3455-3459)
+        to_field = lambda a: (a[0::2] + 1j * a[1::2]).reshape(3, 3, nx, ny, nz).transpose(1, 0, 2, 3, 4)
+        out["eps"] = to_field(raw[:n])
+        out["sigma"] = to_field(raw[n:2 * n])
+        out["ave_eps"] = raw[2 * n:2 * n + 9].reshape(3, 3)
+        out["ave_sigma"] = raw[2 * n + 9:2 * n + 18].reshape(3, 3)
+        out["avepst"] = raw[2 * n + 18:2 * n + 27].reshape(3, 3)
     if timing:
         import json
         for line in proc.stdout.splitlines()[::-1]:

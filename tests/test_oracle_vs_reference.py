@@ -53,3 +53,30 @@ def test_fftw_api_stand_in_matches_numpy(shape):
             lib.pfdd_shim_fft3d(b.ctypes.data, *shape, h, sign)
             ref = np.fft.fftn(a, axes=(0, 1, 2)) if sign < 0 else np.fft.ifftn(a, axes=(0, 1, 2)) * np.prod(shape)
             assert np.abs(b - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+@needs_ref
+@pytest.mark.parametrize("make", ["loop", "fcc", "skew"])
+def test_strain_stress_restatement_equals_reference(make):
+    """Strain and stress diagnostics (Fmatrix, strain, stressfree_strain,
+    total_average_strain, stress) of the state after 3 GL steps."""
+    if make == "loop":
+        w = configs.loop_workload(n=16, nz=8, radius=4.0, seed=5, sigma_mpa=250.0)
+    elif make == "fcc":
+        w = configs.fcc_workload(8, 6, 4, n_loops=1, seed=3)
+    else:
+        w = configs.frank_read_workload(nx=16, ny=16, nz=8, seg=4)
+    r = ref_runner.run_reference(w, 3, want_stress=True)
+    su = r["setup"]
+    C44, C12, C11 = su["C44"], su["C12"], su["C11"]
+    eps, sigma, ave_eps, ave_sigma, avepst = O.strain_stress(
+        w.nx, w.ny, w.nz, su["four"], su["xn"], su["xb"], su["dslip"], C44, C12, C11, su["sigma_rot"], r["xi"])
+    scale_e = max(1e-30, np.abs(r["eps"]).max())
+    scale_s = max(1e-30, np.abs(r["sigma"].real).max())
+    assert np.abs(eps - r["eps"]).max() <= 1e-12 * scale_e
+    assert np.abs(sigma - r["sigma"].real).max() <= 1e-12 * scale_s
+    assert np.abs(r["sigma"].imag).max() == 0.0
+    np.testing.assert_allclose(avepst, r["avepst"], rtol=1e-12, atol=1e-12 * np.abs(avepst).max())
+    # the averages are means of fields of either sign: compare on the fields' scale
+    assert np.abs(ave_eps - r["ave_eps"]).max() <= 1e-12 * scale_e
+    assert np.abs(ave_sigma - r["ave_sigma"]).max() <= 1e-12 * scale_s
