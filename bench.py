@@ -461,6 +461,10 @@ def main():
     extras = {}
     if not args.no_extras and rank == 0 and len(ws) == 1:
         extras["cufft_comparison"] = cufft_comparison(ws[0], fields_carried(ws[0]), prec_name, stream)
+        # strain / stress diagnostics of the current state (averages only, no field copy-out)
+        st.strain_stress(0, fields=False)
+        dms = [timed_events(stream, lambda: st.strain_stress(0, fields=False))[0] for _ in range(3)]
+        extras["strain_stress_ms"] = statistics.median(dms)
     if not args.no_extras and rank == 0:
         if args.workload == "loop64":
             extras["fp32_vs_fp64"] = fp32_vs_fp64(ws, args.steps, stream, local)

@@ -170,6 +170,22 @@ pfdd_status pfdd_gpu_step_history(pfdd_gpu *h, int inst, double *xinorm, double 
 pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_core,
                             double *e_applied);
 
+/* Strain and stress fields of instance `inst`'s current state, as the
+ * reference's strain/stress diagnostics compute them when data_fftw holds the
+ * forward transform of that state: FFTW_Slab::strain with Fmatrix,
+ * stressfree_strain, total_average_strain and stress
+ * (src/fft_fftw_slab.cpp:644-732, 3252-3553; called by DiagStress::compute,
+ * src/diag_stress.cpp:43-62, and DumpText, src/dump_text.cpp:296-324).
+ * eps and sigma (each 9*N doubles or NULL) receive component (i, j) at
+ * (3 i + j) * N in the z-fastest site order: the real parts of data_eps and
+ * data_sigma.  ave_eps[9] and ave_sigma[9] (or NULL) receive the box averages
+ * (FFT::ave_eps, FFT::ave_sigma).  The applied stress is that of the stress
+ * state the last pfdd_gpu_advance stepped with (the reference outputs inside
+ * its GL loop, before sigma += dsigma).  The spectrum buffer is reused, so the
+ * next pfdd_gpu_advance opens with a fresh forward transform. */
+pfdd_status pfdd_gpu_strain_stress(pfdd_gpu *h, int inst, double *eps, double *sigma, double *ave_eps,
+                                   double *ave_sigma);
+
 /* No counterpart in the reference (a hand-written adjoint of the GL step).
  * Gradient of J = sum over sites and systems of (Re xi_N - target)^2, where
  * xi_N is instance `inst` after n_steps GL iterations from its current state

@@ -95,6 +95,7 @@ struct Instance {
   std::vector<double> hist;  // host copy of the last advance's per-step stats
   int hist_count = 0;
   int group = -1;       // index of the batched group this instance belongs to
+  bool advanced = false;  // an advance ran: the device sigma is one increment past its last stress state
   // adjoint scratch, kept between calls (checkpoints, segment states,
   // lambda pair, target, Nyquist carrier of lambda, partial sums, final state)
   DevBuf adj_ck, adj_seg, adj_lam[2], adj_tgt, adj_aux, adj_gpart, adj_acc, adj_lpart, adj_fin, adj_finaux;
@@ -670,6 +671,168 @@ pfdd_status profile_impl(pfdd_gpu *h, int n_steps, double *kernel_ms) {
 }
 
 // ------------------------------------------------------------ energy
+// ------------------------------------------------------------ strain / stress
+// The strain and stress diagnostics of the current state (see the header):
+// forward planes of xi, the strain pencil pass (six symmetric components),
+// the inverse planes of those six fields, then the pointwise stress.  The
+// constants follow the reference: Voigt mu and nu for G and the stress
+// (fft_fftw_slab.cpp:483-495, 3489-3494), the isotropic compliance S11 = 1/E,
+// S12 = -nu/E, S44 = 2 (S11 - S12) (material.cpp:154-156; Voigt E and nu,
+// equal to the deck's for the isotropic C the material builds), sigma_rot as
+// rotate_stress, <eps0> from the per-system means of Re xi (stressfree_strain).
+template <typename T>
+pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *sigma, double *ave_eps,
+                               double *ave_sigma) {
+  using C = cx<T>;
+  constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
+  cudaStream_t st = h->stream;
+  const size_t N = I.N;
+  const int S = I.S;
+  // sigma_rot (rotate_stress, fft_fftw_slab.cpp:242-274) of the stress state
+  // the current xi was stepped with: the reference outputs inside its GL loop,
+  // before sigma += dsigma (solve_GL.cpp:110-155), while pfdd_gpu_advance has
+  // already added the increment when it returns
+  double sig[9], sr[3][3];
+  CUDA_TRY(h, cudaMemcpyAsync(sig, I.sigma(), sizeof sig, cudaMemcpyDeviceToHost, st));
+  // per-system sums of Re xi of the current state
+  const int nb = 296;
+  DevBuf part, spec6, strain6, e9, s9, fpart;
+  CUDA_TRY(h, part.alloc((size_t)nb * S * sizeof(double)));
+  k_field_sums<T><<<nb, 256, 0, st>>>(I.xi[I.cur].as<T>(), S, N, part.as<double>());
+  std::vector<double> hp((size_t)nb * S);
+  CUDA_TRY(h, cudaMemcpyAsync(hp.data(), part.p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  const StressArgs &sa = I.stress;
+  if (I.advanced)
+    for (int i = 0; i < 9; ++i) sig[i] -= I.d.dsigma[i / 3][i % 3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double v = 0.0;
+      if (sa.ortho) {
+        for (int k = 0; k < 3; ++k)
+          for (int l = 0; l < 3; ++l) v += sa.prim[i][k] * sig[3 * k + l] * sa.invprim[l][j];
+      } else {
+        v = sig[3 * i + j];
+      }
+      sr[i][j] = v;
+    }
+  const double C44 = I.d.C44, C12 = I.d.C12, C11 = I.d.C11;
+  const double mu = C44 - (2.0 * C44 + C12 - C11) / 5.0, ll = C12 - (2.0 * C44 + C12 - C11) / 5.0;
+  const double young = mu * (3 * ll + 2 * mu) / (ll + mu), xnu = young / 2.0 / mu - 1.0;
+  const double S11 = 1.0 / young, S12 = -xnu / young, S44 = 2.0 * (S11 - S12);
+  double epsm[PFDD_MAXS][3][3], mean[PFDD_MAXS];
+  for (int a = 0; a < S; ++a) {
+    double t = 0.0;
+    for (int b = 0; b < nb; ++b) t += hp[(size_t)b * S + a];
+    mean[a] = t / (double)N;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) epsm[a][i][j] = I.d.xb[a][i] * I.d.xn[a][j] / I.d.dslip;
+  }
+  double avepsts[3][3], avepst[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < 3; ++k)
+        for (int l = 0; l < 3; ++l) {
+          const double Sijkl = S44 / 4.0 * ((i == k && j == l) + (i == l && j == k)) + S12 * (i == j && k == l);
+          v += Sijkl * sr[k][l] * mu;
+        }
+      avepsts[i][j] = v;
+      double e0 = 0.0;
+      for (int a = 0; a < S; ++a) e0 += epsm[a][i][j] * mean[a];
+      avepst[i][j] = v + e0;
+    }
+  StressFieldArgs sp;
+  memset(&sp, 0, sizeof sp);
+  const int qi[6] = {0, 1, 2, 0, 0, 1}, qj[6] = {0, 1, 2, 1, 2, 2};
+  for (int q = 0; q < 6; ++q) {
+    const int i = qi[q], j = qj[q];
+    for (int a = 0; a < S; ++a) sp.e6[a][q] = 0.5 * (epsm[a][i][j] + epsm[a][j][i]);
+    sp.avepst6[q] = 0.5 * (avepst[i][j] + avepst[j][i]);
+    sp.avepsts6[q] = 0.5 * (avepsts[i][j] + avepsts[j][i]);
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) sp.sigmu[3 * i + j] = sr[i][j] * mu;
+  sp.C44 = C44;
+  sp.C12 = C12;
+  sp.S = S;
+
+  // forward planes of the current state into the spectrum buffer
+  PlaneArgs pa;
+  fill_plane_args<T>(I, pa);
+  launch_fwd<T>(I, st, I.xi[I.cur].as<T>(), I.spec.as<C>(), pa, nullptr, I.flags() + 3);
+  // strain pencils: tile width reduced until max(F, 6) fields fit
+  const size_t ncols = (size_t)I.ny * I.nzp;
+  const int FB = std::max(I.F, 6);
+  int cc = I.ccols;
+  auto bytes = [&](int c) { return ((size_t)FB * I.nx * c + I.nx) * sizeof(C); };
+  while (cc > 1 && bytes(cc) > 227 * 1024) cc >>= 1;
+  if (bytes(cc) > 227 * 1024 || ncols % cc)
+    return fail(h, PFDD_EUNSUPPORTED, "strain pencil of %d x %d fields does not fit shared memory", I.nx, FB);
+  CUDA_TRY(h, cudaFuncSetAttribute(k_strain_pencil<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)bytes(cc)));
+  PencilArgs pe{};
+  pe.px = I.px;
+  pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.nzp = I.nzp; pe.M = I.M;
+  pe.S = I.S; pe.F = I.F; pe.imag = I.imag;
+  pe.ncols = (int)ncols;
+  pe.ccols = cc;
+  pe.tw_x = I.tw_x.p;
+  pe.kx_of = I.kx_of; pe.ky_of = I.ky_of; pe.kz_of = I.kz_of;
+  pe.mode = PASS_STEP;
+  pe.fstride = I.nx * cc;
+  pe.aux = I.aux.p;
+  pe.sx_n = I.sx_n; pe.sy_n = I.sy_n;
+  pe.g = I.green;
+  set_pencil_divisors<T>(pe);
+  pe.fd_6cc = FastDiv(6 * cc);
+  pe.inv2mu = 0.5 / mu;
+  CUDA_TRY(h, spec6.alloc(6 * (size_t)I.nx * ncols * sizeof(C)));
+  k_strain_pencil<T, 256><<<(unsigned)(ncols / cc), 256, bytes(cc), st>>>(I.spec.as<C>(), spec6.as<C>(), pe);
+  // inverse planes of the six strain spectra (the Im-synthesis pass: IFFT / N)
+  CUDA_TRY(h, strain6.alloc(6 * N * sizeof(T)));
+  UpdateArgs ua;
+  memset(&ua, 0, sizeof ua);
+  ua.nx = I.nx; ua.ny = I.ny; ua.nz = I.nz; ua.nzh = I.nzh; ua.nzp = I.nzp; ua.S = I.S; ua.F = 6;
+  ua.invN = 1.0 / (double)N;
+  ua.core = I.core;
+  ua.err = I.flags() + 3;
+  ua.mode = PASS_SYNTH;
+  const unsigned planes6 = (unsigned)(6 * I.nx);
+  if (I.split)
+    launch_pair(k_inv_update<T, NH, true>, dim3(2 * planes6), NH, I.smem_update, st, spec6.as<C>(),
+                I.xi[I.cur].as<T>(), strain6.as<T>(), pa, ua, I.partials.as<double>());
+  else
+    k_inv_update<T, NP, false><<<planes6, NP, I.smem_update, st>>>(spec6.as<C>(), I.xi[I.cur].as<T>(),
+                                                                     strain6.as<T>(), pa, ua, I.partials.as<double>());
+  // pointwise strain and stress, FP64 sums of both
+  if (eps) CUDA_TRY(h, e9.alloc(9 * N * sizeof(double)));
+  if (sigma) CUDA_TRY(h, s9.alloc(9 * N * sizeof(double)));
+  CUDA_TRY(h, fpart.alloc((size_t)nb * 18 * sizeof(double)));
+  k_stress_fields<T><<<nb, 256, 0, st>>>(strain6.as<T>(), I.xi[I.cur].as<T>(), N, sp, e9.as<double>(),
+                                          s9.as<double>(), fpart.as<double>());
+  std::vector<double> hf((size_t)nb * 18);
+  CUDA_TRY(h, cudaMemcpyAsync(hf.data(), fpart.p, hf.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (eps) CUDA_TRY(h, cudaMemcpyAsync(eps, e9.p, 9 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (sigma) CUDA_TRY(h, cudaMemcpyAsync(sigma, s9.p, 9 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  int fl[4];
+  CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+  if (fl[3]) return fail(h, PFDD_ETIMEOUT, "a bounded device wait ran out");
+  for (int q = 0; q < 18; ++q) {
+    double t = 0.0, c = 0.0;
+    for (int b = 0; b < nb; ++b) {   // Neumaier-compensated
+      const double v = hf[(size_t)b * 18 + q], u = t + v;
+      c += (std::fabs(t) >= std::fabs(v)) ? (t - u) + v : (v - u) + t;
+      t = u;
+    }
+    const double m = (t + c) / (double)N;
+    if (q < 9 && ave_eps) ave_eps[q] = m;
+    if (q >= 9 && ave_sigma) ave_sigma[q - 9] = m;
+  }
+  return PFDD_OK;
+}
+
 // E_elastic = 1/2 <xi, L xi> (Re and Im), E_core = sum f(Re xi),
 // E_applied = -sum tau_a Re xi_a, from one elastic pass of the current state.
 template <typename T>
@@ -1000,6 +1163,7 @@ pfdd_status advance_impl(pfdd_gpu *h, int n_steps, int stress_states, double tol
       CUDA_TRY(h, cudaGraphLaunch(ge, st));
       left -= k;
     }
+    for (auto &ip : h->inst) ip->advanced = true;
     CUDA_TRY(h, cudaGetLastError());
     return collect(h, stats);
   }
@@ -1020,6 +1184,7 @@ pfdd_status advance_impl(pfdd_gpu *h, int n_steps, int stress_states, double tol
     }
     stress_all<T>(h, 1);
   }
+  for (auto &ip : h->inst) ip->advanced = true;
   CUDA_TRY(h, cudaGetLastError());
   return collect(h, stats);
 }
@@ -1349,6 +1514,15 @@ pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_
   cudaSetDevice(h->device);
   return h->precision == PFDD_FP64 ? energy_impl<double>(h, I, e_elastic, e_core, e_applied)
                                    : energy_impl<float>(h, I, e_elastic, e_core, e_applied);
+}
+
+pfdd_status pfdd_gpu_strain_stress(pfdd_gpu *h, int inst, double *eps, double *sigma, double *ave_eps,
+                                   double *ave_sigma) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  cudaSetDevice(h->device);
+  return h->precision == PFDD_FP64 ? strain_stress_impl<double>(h, *h->inst[inst], eps, sigma, ave_eps, ave_sigma)
+                                   : strain_stress_impl<float>(h, *h->inst[inst], eps, sigma, ave_eps, ave_sigma);
 }
 
 pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every, const double *xi_target,

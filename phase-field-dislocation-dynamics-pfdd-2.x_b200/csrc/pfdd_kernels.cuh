@@ -141,6 +141,8 @@ struct PencilArgs {
   // divisors built on the host: F * ccols, ccols, nzp, 16-byte chunks per
   // (field, x) row of a tile, nx
   FastDiv fd_fcc, fd_cc, fd_nzp, fd_cpr, fd_nx;
+  FastDiv fd_6cc;             // strain diagnostics: 6 * ccols
+  double inv2mu;              // strain diagnostics: 1 / (2 mu), Voigt mu (Fmatrix, fft_fftw_slab.cpp:657)
   Green g;
 };
 
@@ -1586,6 +1588,197 @@ __global__ void k_loss_seed(const T *__restrict__ xr, const T *__restrict__ targ
     acc += (double)d * (double)d;
   }
   block_sum2(acc, 0.0, red, partial + 2 * blockIdx.x);
+}
+
+// ------------------------------------------------------------ strain / stress diagnostics
+// The strain field of the current state as FFTW_Slab::strain computes it with
+// Fmatrix (fft_fftw_slab.cpp:644-732, 3370-3469):
+//   strain_ij(k) = sum_s F[s,i,j](k) Z_s(k),  F[s,i,j] = k_i (G sigma^s k)_j,
+//   G = (2 I / k^2 - k k^T / ((1 - nu) k^4)) / (2 mu)   (Voigt mu and nu),
+// i.e. with Sig = sum_s sigma^s Z_s and U = Sig k:  strain = k w^T, w = G U,
+// of which the diagnostics keep the symmetric part (data_eps).  Its real part
+// follows the Im-carrier rule of the contraction: F(k) Xr off the Nyquist
+// planes, (F(k)(Xr + i Xi) + F(k')(Xr - i Xi)) / 2 on them (or everywhere
+// with the full carrier), k' the reference's vector of index -k.
+template <typename T, typename C>
+__device__ __forceinline__ void strain_of(const C (&sig)[6], T kx, T ky, T kz, T c1nu, T inv2mu, C (&o)[6]) {
+  const T k2 = kx * kx + ky * ky + kz * kz;
+  if (!(k2 > (T)0)) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) o[q] = mk<C>((T)0, (T)0);
+    return;
+  }
+  const T ik2 = (T)1 / k2;
+  const C U0 = mk<C>(sig[0].x * kx + sig[3].x * ky + sig[4].x * kz, sig[0].y * kx + sig[3].y * ky + sig[4].y * kz);
+  const C U1 = mk<C>(sig[3].x * kx + sig[1].x * ky + sig[5].x * kz, sig[3].y * kx + sig[1].y * ky + sig[5].y * kz);
+  const C U2 = mk<C>(sig[4].x * kx + sig[5].x * ky + sig[2].x * kz, sig[4].y * kx + sig[5].y * ky + sig[2].y * kz);
+  const C kU = mk<C>(kx * U0.x + ky * U1.x + kz * U2.x, kx * U0.y + ky * U1.y + kz * U2.y);
+  const T a = (T)2 * ik2 * inv2mu, b = c1nu * ik2 * ik2 * inv2mu;
+  const C w0 = mk<C>(a * U0.x - b * kx * kU.x, a * U0.y - b * kx * kU.y);
+  const C w1 = mk<C>(a * U1.x - b * ky * kU.x, a * U1.y - b * ky * kU.y);
+  const C w2 = mk<C>(a * U2.x - b * kz * kU.x, a * U2.y - b * kz * kU.y);
+  const T h = (T)0.5;
+  o[0] = mk<C>(kx * w0.x, kx * w0.y);
+  o[1] = mk<C>(ky * w1.x, ky * w1.y);
+  o[2] = mk<C>(kz * w2.x, kz * w2.y);
+  o[3] = mk<C>(h * (kx * w1.x + ky * w0.x), h * (kx * w1.y + ky * w0.y));
+  o[4] = mk<C>(h * (kx * w2.x + kz * w0.x), h * (kx * w2.y + kz * w0.y));
+  o[5] = mk<C>(h * (ky * w2.x + kz * w1.x), h * (ky * w2.y + kz * w1.y));
+}
+
+// x pencils of the current state's half spectrum (F fields in) -> the six
+// symmetric strain components (xx yy zz xy xz yz) after the inverse x FFT.
+// grid.x = ncols / ccols; smem = (max(F, 6) * fstride + nx) * sizeof(C).
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, 1) k_strain_pencil(const cx<T> *__restrict__ spec, cx<T> *__restrict__ out6,
+                                                         PencilArgs a) {
+  using C = cx<T>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int nx = a.nx, F = a.F, cc = a.ccols, S = a.S, fst = a.fstride;
+  const int FB = F > 6 ? F : 6;
+  C *buf = reinterpret_cast<C *>(smem_raw);
+  C *twx = buf + (size_t)FB * fst;
+  const size_t col0 = (size_t)blockIdx.x * cc, ncols = a.ncols;
+  const int per = nx * cc;
+  for (int i = threadIdx.x; i < F * per; i += blockDim.x) {
+    const int f = i / per, rem = i - f * per, x = rem / cc, c = rem - x * cc;
+    buf[(size_t)f * fst + rem] = spec[((size_t)f * nx + x) * ncols + col0 + c];
+  }
+  load_table(twx, a.tw_x, nx);
+  __syncthreads();
+  Batch gx{F * cc, cc, 1, fst, cc, true, a.fd_fcc, a.fd_cc};
+  fft_forward<MaxRadix<NT>::value, GeomPencil>(buf, twx, a.px, gx);
+  const GreenT<T> &g = green_t<T>(a.g);
+  const C *caux = reinterpret_cast<const C *>(a.aux);
+  const T c1nu = g.c1nu, inv2mu = (T)a.inv2mu;
+  for (int w = threadIdx.x; w < per; w += blockDim.x) {
+    const int sx = a.fd_cc.div(w), c = w - sx * cc;
+    const int col = (int)(col0 + c);
+    const int sy = a.fd_nzp.div(col), sz = col - sy * a.nzp;
+    C *pk = buf + sx * cc + c;
+    C o[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) o[q] = mk<C>((T)0, (T)0);
+    if (sz <= a.M) {
+      const int ix = a.kx_of[sx], iy = a.ky_of[sy], iz = a.kz_of[sz];
+      const T fx = freq_of<T>(ix, a.nx), fy = freq_of<T>(iy, a.ny), fz = freq_of<T>(iz, a.nz);
+      const T kx = fx * g.four[0][0] + fy * g.four[1][0] + fz * g.four[2][0];
+      const T ky = fx * g.four[0][1] + fy * g.four[1][1] + fz * g.four[2][1];
+      const T kz = fx * g.four[0][2] + fy * g.four[1][2] + fz * g.four[2][2];
+      C sr[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) sr[q] = mk<C>((T)0, (T)0);
+      for (int b = 0; b < S; ++b) green_accumulate<T>(g, b, pk[(size_t)b * fst], sr);
+      bool nyq = false;
+      size_t a0 = 0, astride = 0;
+      if (a.imag == IMAG_NYQ) {
+        a0 = nyq_index<T, C>(a, 0, sx, sy, sz, nyq);
+        astride = (sz == a.M) ? (size_t)a.nx * a.ny : (sy == a.sy_n ? (size_t)a.nx * a.M : (size_t)a.ny * a.M);
+      }
+      if (a.imag == IMAG_FULL || nyq) {
+        C si[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) si[q] = mk<C>((T)0, (T)0);
+        for (int b = 0; b < S; ++b) {
+          C y;
+          if (a.imag == IMAG_FULL) y = pk[(size_t)(S + b) * fst];
+          else y = caux[a0 + b * astride];
+          green_accumulate<T>(g, b, y, si);
+        }
+        C sp[6], sq[6], op[6], oq[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          sp[q] = mk<C>(sr[q].x - si[q].y, sr[q].y + si[q].x);
+          sq[q] = mk<C>(sr[q].x + si[q].y, sr[q].y - si[q].x);
+        }
+        const T gxn = freq_neg<T>(ix, a.nx), gyn = freq_neg<T>(iy, a.ny), gzn = freq_neg<T>(iz, a.nz);
+        const T mx = gxn * g.four[0][0] + gyn * g.four[1][0] + gzn * g.four[2][0];
+        const T my = gxn * g.four[0][1] + gyn * g.four[1][1] + gzn * g.four[2][1];
+        const T mz = gxn * g.four[0][2] + gyn * g.four[1][2] + gzn * g.four[2][2];
+        strain_of<T>(sp, kx, ky, kz, c1nu, inv2mu, op);
+        strain_of<T>(sq, mx, my, mz, c1nu, inv2mu, oq);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) o[q] = mk<C>((T)0.5 * (op[q].x + oq[q].x), (T)0.5 * (op[q].y + oq[q].y));
+      } else {
+        strain_of<T>(sr, kx, ky, kz, c1nu, inv2mu, o);
+      }
+    }
+    // every input of this point has been read: its six outputs take slots 0..5
+#pragma unroll
+    for (int q = 0; q < 6; ++q) pk[(size_t)q * fst] = o[q];
+  }
+  __syncthreads();
+  Batch g6{6 * cc, cc, 1, fst, cc, true, a.fd_6cc, a.fd_cc};
+  fft_inverse<MaxRadix<NT>::value, GeomPencil>(buf, twx, a.px, g6);
+  for (int i = threadIdx.x; i < 6 * per; i += blockDim.x) {
+    const int f = i / per, rem = i - f * per, x = rem / cc, c = rem - x * cc;
+    out6[((size_t)f * nx + x) * ncols + col0 + c] = buf[(size_t)f * fst + rem];
+  }
+}
+
+// Per-system sums of Re xi ([S][N], compute precision) in FP64: part[blk * S + s].
+template <typename T>
+__global__ void k_field_sums(const T *__restrict__ xr, int S, size_t N, double *__restrict__ part) {
+  __shared__ double red[64];
+  for (int s0 = 0; s0 < S; ++s0) {
+    double acc = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x)
+      acc += (double)xr[(size_t)s0 * N + i];
+    double out[2];
+    block_sum2(acc, 0.0, red, out);
+    if (threadIdx.x == 0) part[(size_t)blockIdx.x * S + s0] = out[0];
+    __syncthreads();
+  }
+}
+
+// Constants of the stress field (stress, fft_fftw_slab.cpp:3474-3553), FP64.
+struct StressFieldArgs {
+  double e6[PFDD_MAXS][6];   // sym(eps^s): xx yy zz xy xz yz
+  double avepst6[6];         // sym(avepst) = sym(S : sigma_rot mu + <eps0>)
+  double avepsts6[6];        // sym(S : sigma_rot mu)
+  double sigmu[9];           // sigma_rot * mu, row major
+  double C44, C12;
+  int S;
+};
+
+// Per site: eps = strain + avepst (symmetric), eps0 = sum_s eps^s Re xi_s,
+// X = eps - eps0 - avepsts, sigma = C : X + sigma_rot mu = 2 C44 X + C12 tr(X) I
+// + sigma_rot mu (C isotropic, X symmetric).  Writes eps9 / sig9 ([3][3][N],
+// FP64, either may be null) and per-block FP64 sums of their 18 components.
+template <typename T>
+__global__ void k_stress_fields(const T *__restrict__ strain6, const T *__restrict__ xr, size_t N,
+                                StressFieldArgs p, double *__restrict__ eps9, double *__restrict__ sig9,
+                                double *__restrict__ part) {
+  __shared__ double red[18 * 32 + 18];
+  double acc[18];
+#pragma unroll
+  for (int q = 0; q < 18; ++q) acc[q] = 0.0;
+  const int map[9] = {0, 3, 4, 3, 1, 5, 4, 5, 2};   // (i, j) -> xx yy zz xy xz yz
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < N; r += (size_t)gridDim.x * blockDim.x) {
+    double e[6], x[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) e[q] = (double)strain6[(size_t)q * N + r] + p.avepst6[q];
+    double d[6] = {0, 0, 0, 0, 0, 0};
+    for (int s0 = 0; s0 < p.S; ++s0) {
+      const double v = (double)xr[(size_t)s0 * N + r];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) d[q] += p.e6[s0][q] * v;
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) x[q] = e[q] - d[q] - p.avepsts6[q];
+    const double tr = x[0] + x[1] + x[2];
+#pragma unroll
+    for (int ij = 0; ij < 9; ++ij) {
+      const int i = ij / 3, j = ij - 3 * i, q = map[ij];
+      const double ev = e[q];
+      const double sv = 2.0 * p.C44 * x[q] + (i == j ? p.C12 * tr : 0.0) + p.sigmu[ij];
+      if (eps9) eps9[(size_t)ij * N + r] = ev;
+      if (sig9) sig9[(size_t)ij * N + r] = sv;
+      acc[ij] += ev;
+      acc[9 + ij] += sv;
+    }
+  }
+  plane_sum<false, 18>(acc, red, part + 18 * (size_t)blockIdx.x);
 }
 
 // ------------------------------------------------------------ layout helpers

@@ -29,7 +29,7 @@ EXPORTS = [
     "pfdd_gpu_create", "pfdd_gpu_set_state", "pfdd_gpu_set_state_interleaved", "pfdd_gpu_get_state",
     "pfdd_gpu_get_state_interleaved", "pfdd_gpu_advance", "pfdd_gpu_step_history", "pfdd_gpu_energy",
     "pfdd_gpu_tau", "pfdd_gpu_info", "pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version",
-    "pfdd_gpu_set_stream", "pfdd_gpu_profile", "pfdd_gpu_adjoint",
+    "pfdd_gpu_set_stream", "pfdd_gpu_profile", "pfdd_gpu_adjoint", "pfdd_gpu_strain_stress",
 ]
 KERNELS = ["fwd_planes", "xpencil", "step_planes", "finalize"]
 
@@ -89,6 +89,7 @@ def load(path: str = LIB_PATH):
     lib.pfdd_gpu_advance.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(StepStats)]
     lib.pfdd_gpu_step_history.argtypes = [vp, ctypes.c_int, DP, DP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.pfdd_gpu_energy.argtypes = [vp, ctypes.c_int, DP, DP, DP]
+    lib.pfdd_gpu_strain_stress.argtypes = [vp, ctypes.c_int, DP, DP, DP, DP]
     lib.pfdd_gpu_tau.argtypes = [vp, ctypes.c_int, DP]
     lib.pfdd_gpu_adjoint.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, DP, DP, DP, DP]
     lib.pfdd_gpu_set_stream.argtypes = [vp, vp]
@@ -215,6 +216,23 @@ class Stepper:
         e = np.empty(3)
         self._check(self._lib.pfdd_gpu_energy(self.h, inst, _dp(e[0:1]), _dp(e[1:2]), _dp(e[2:3])))
         return tuple(e)
+
+    def strain_stress(self, inst, fields=True):
+        """Strain and stress of the current state (the reference's data_eps /
+        data_sigma real parts and ave_eps / ave_sigma): eps, sigma
+        [3, 3, nx, ny, nz] (None unless fields) and ave_eps, ave_sigma [3, 3]."""
+        d = self.descs[inst]
+        nx, ny, nz = d.nx, d.ny, d.nz
+        n = nx * ny * nz
+        e = np.empty(9 * n) if fields else None
+        s = np.empty(9 * n) if fields else None
+        ae, asg = np.empty(9), np.empty(9)
+        null = ctypes.cast(None, DP)
+        self._check(self._lib.pfdd_gpu_strain_stress(self.h, inst, _dp(e) if fields else null,
+                                                     _dp(s) if fields else null, _dp(ae), _dp(asg)))
+        shape = (3, 3, nx, ny, nz)
+        return (e.reshape(shape) if fields else None, s.reshape(shape) if fields else None,
+                ae.reshape(3, 3), asg.reshape(3, 3))
 
     def adjoint(self, inst, n_steps, ckpt_every, target):
         """(loss, dJ/d(p0, p1), dJ/dsigma[6]) of J = sum (Re xi_N - target)^2."""
