@@ -75,6 +75,8 @@ enum {
   PFDD_CORE_EXTENDED = 2,    /* core_energy_extended  src/fft_fftw_slab.cpp:1243-1354 */
   PFDD_CORE_SINE = 3,        /* core_energy_sine      src/fft_fftw_slab.cpp:1360-1418 */
   PFDD_CORE_PYRII = 4,       /* core_energy_pyrII     src/fft_fftw_slab.cpp:1429-1493 */
+  PFDD_CORE_BCC_PERFECT = 5, /* core_energy_bcc_perfect src/fft_fftw_slab.cpp:1070-1125, with the
+                                edge/screw angle from FFTW_Slab::gradient :869-1065 */
   PFDD_CORE_USFE_ANGLE = 6,  /* core_energy_USFE_angle_tau src/fft_fftw_slab.cpp:1500-1545;
                                 the caller passes the resulting amplitude in `An` */
   PFDD_CORE_MPEA = 7,        /* core_energy_mpea      src/fft_fftw_slab.cpp:1196-1235 */

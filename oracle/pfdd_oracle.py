@@ -191,7 +191,9 @@ class CoreModel:
     """GSFE core model; constants in the reference's SI units (J/m^2, Pa, m).
 
     flag: 1 perfect (fft_fftw_slab.cpp:1130-1191), 2 extended (:1243-1354),
-    3 sine (:1360-1418), 4 pyrII (:1429-1493), 6 USFE(angle, tau)
+    3 sine (:1360-1418), 4 pyrII (:1429-1493), 5 BCC perfect with the
+    edge/screw angle of FFTW_Slab::gradient (:1070-1125, :869-1065; needs
+    geom = (four, xn, xb)), 6 USFE(angle, tau)
     (:1500-1545, An supplied by the caller), 7 mpea (:1196-1235), and
     103 = sine with a per-site multiplier on isf and usf (random-alloy GSFE;
     no reference counterpart, reduces to flag 3 when the multiplier is 1).
@@ -207,6 +209,7 @@ class CoreModel:
     aa: tuple = (0.0,) * 5         # aa0..aa4
     bb: tuple = (0.0,) * 4         # bb1..bb4
     site: np.ndarray | None = field(default=None, repr=False)  # A_mpea or multiplier, [S, nx, ny, nz]
+    geom: tuple | None = field(default=None, repr=False)       # (four, xn, xb) for flag 5
 
     def scale(self):
         return self.mu * self.dslip * self.b
@@ -229,6 +232,8 @@ class CoreModel:
             return isf * PI * np.sin(2 * PI * xr) + Cn * 2 * PI * np.sin(4 * PI * xr)
         if f == 7:
             return self.site / s * PI * np.sin(2.0 * PI * xr)
+        if f == 5:
+            return self.usf / s * self._bcc_cof(xr) * PI * np.sin(2.0 * PI * xr)
         if f == 4:
             aa = np.asarray(self.aa, dtype=float) / s
             bb = np.asarray(self.bb, dtype=float) / s
@@ -243,6 +248,35 @@ class CoreModel:
         if f == 2:
             return self._extended_derivative(xr)
         raise ValueError("core model %d not restated" % f)
+
+    def _bcc_cof(self, xr):
+        """cof(theta) of core_energy_bcc_perfect (fft_fftw_slab.cpp:1108-1117) with
+        theta from FFTW_Slab::gradient (:869-1065): periodic central
+        differences, the in-place transform by `four` (later rows use the
+        already transformed components), t = grad x n, theta = acos(t.b/|t|),
+        pi - theta where (b x t).n < 0, theta = -1 where |t| <= 0.1."""
+        four, xn, xb = (np.asarray(v, float) for v in self.geom)
+        g = [(np.roll(xr, -1, axis=ax) - np.roll(xr, 1, axis=ax)) / 2 for ax in (1, 2, 3)]
+        gx, gy, gz = g
+        gx = gx * four[0, 0] + gy * four[1, 0] + gz * four[2, 0]
+        gy = gx * four[0, 1] + gy * four[1, 1] + gz * four[2, 1]
+        gz = gx * four[0, 2] + gy * four[1, 2] + gz * four[2, 2]
+        n = xn[:, :, None, None, None]
+        b = xb[:, :, None, None, None]
+        t0 = gy * n[:, 2] - gz * n[:, 1]
+        t1 = gz * n[:, 0] - gx * n[:, 2]
+        t2 = gx * n[:, 1] - gy * n[:, 0]
+        mag = np.sqrt(t0 * t0 + t1 * t1 + t2 * t2)
+        small = mag <= 0.1
+        m = np.where(small, 1.0, mag)
+        t0, t1, t2 = t0 / m, t1 / m, t2 / m
+        th = np.arccos(np.clip(t0 * b[:, 0] + t1 * b[:, 1] + t2 * b[:, 2], -1.0, 1.0))
+        dirv = (b[:, 1] * t2 - b[:, 2] * t1) * n[:, 0] + (b[:, 2] * t0 - b[:, 0] * t2) * n[:, 1] + \
+               (b[:, 0] * t1 - b[:, 1] * t0) * n[:, 2]
+        th = np.where(dirv < 0.0, np.arccos(-1.0) - th, th)
+        th = np.where(small, -1.0, th)
+        return np.where(th < 0.0, 1.0, np.where(th < 1.23, 1.1603 * th * th - 2.0431 * th + 1,
+                                                   0.5473 * th * th - 2.0035 * th + 1.8923))
 
     def _extended_derivative(self, xr):
         c0, c1, c2, c3, c4, a1, a3 = (v / self.mu for v in self.c)

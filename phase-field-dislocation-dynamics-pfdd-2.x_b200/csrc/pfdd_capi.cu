@@ -1509,7 +1509,7 @@ pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_
   if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
   Instance &I = *h->inst[inst];
   const int f = I.d.core_flag;
-  if (f == PFDD_CORE_EXTENDED || f == PFDD_CORE_PYRII)
+  if (f == PFDD_CORE_EXTENDED || f == PFDD_CORE_PYRII || f == PFDD_CORE_BCC_PERFECT)
     return fail(h, PFDD_EUNSUPPORTED, "no energy density for core model %d", f);
   cudaSetDevice(h->device);
   return h->precision == PFDD_FP64 ? energy_impl<double>(h, I, e_elastic, e_core, e_applied)
@@ -1532,7 +1532,7 @@ pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every,
   if (n_steps < 1 || ckpt_every < 1 || !xi_target) return fail(h, PFDD_EINVAL, "need n_steps, ckpt_every >= 1, target");
   Instance &I = *h->inst[inst];
   const int f = I.d.core_flag;
-  if (f == PFDD_CORE_EXTENDED || f == PFDD_CORE_PYRII)
+  if (f == PFDD_CORE_EXTENDED || f == PFDD_CORE_PYRII || f == PFDD_CORE_BCC_PERFECT)
     return fail(h, PFDD_EUNSUPPORTED, "no adjoint for core model %d", f);
   cudaSetDevice(h->device);
   return h->precision == PFDD_FP64

@@ -96,6 +96,11 @@ struct Core {
   int flag;
   double k[12];               // scaled constants, see core_derivative
   float kf[12];               // the same, rounded once for the FP32 path
+  // core model 5 (the angle between the line direction and b): grid, `four`
+  // and the slip normals / Burgers vectors
+  int nx, ny, nz;
+  double four[3][3];
+  double xn[PFDD_MAXS][3], xb[PFDD_MAXS][3];
 };
 template <typename T> __device__ __forceinline__ T core_k(const Core &c, int i);
 template <> __device__ __forceinline__ double core_k<double>(const Core &c, int i) { return c.k[i]; }
@@ -901,10 +906,50 @@ template <typename Fn> __host__ inline void with_pencil_sc(int S, Fn f) {
 // dE_core for field a at site r from Re xi (App::core_energy dispatch,
 // app.cpp:663-672).  k[] holds constants already divided by mu*dslip*b
 // (or mu) on the host, in the reference's order of operations.
+// Core model 5's coefficient cof(theta) at site r of system a
+// (core_energy_bcc_perfect, fft_fftw_slab.cpp:1108-1117), theta from
+// FFTW_Slab::gradient (:869-1065): periodic central differences of Re xi_a,
+// taken to the global frame through `four` in place (the y and z rows use the
+// already transformed x and y components, as the reference does), the line
+// direction t = grad x n normalised, theta = acos(t . b), pi - theta when
+// (b x t) . n < 0, and theta = -1 (cof = 1) where |t| <= 0.1.
+template <typename T>
+__device__ __forceinline__ T bcc_cof(const Core &cm, int a, size_t r, size_t N, const T *__restrict__ xin) {
+  const int nx = cm.nx, ny = cm.ny, nz = cm.nz;
+  const int k = (int)(r % nz), j = (int)((r / nz) % ny), i = (int)(r / ((size_t)nz * ny));
+  const T *f = xin + (size_t)a * N;
+  auto at = [&](int ii, int jj, int kk) { return f[((size_t)ii * ny + jj) * nz + kk]; };
+  const int ip = i + 1 == nx ? 0 : i + 1, im = i == 0 ? nx - 1 : i - 1;
+  const int jp = j + 1 == ny ? 0 : j + 1, jm = j == 0 ? ny - 1 : j - 1;
+  const int kp = k + 1 == nz ? 0 : k + 1, km = k == 0 ? nz - 1 : k - 1;
+  T gx = (at(ip, j, k) - at(im, j, k)) / (T)2;
+  T gy = (at(i, jp, k) - at(i, jm, k)) / (T)2;
+  T gz = (at(i, j, kp) - at(i, j, km)) / (T)2;
+  const double(*F)[3] = cm.four;
+  gx = gx * (T)F[0][0] + gy * (T)F[1][0] + gz * (T)F[2][0];
+  gy = gx * (T)F[0][1] + gy * (T)F[1][1] + gz * (T)F[2][1];
+  gz = gx * (T)F[0][2] + gy * (T)F[1][2] + gz * (T)F[2][2];
+  const T n0 = (T)cm.xn[a][0], n1 = (T)cm.xn[a][1], n2 = (T)cm.xn[a][2];
+  const T b0 = (T)cm.xb[a][0], b1 = (T)cm.xb[a][1], b2 = (T)cm.xb[a][2];
+  T t0 = gy * n2 - gz * n1, t1 = gz * n0 - gx * n2, t2 = gx * n1 - gy * n0;
+  const T mag = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+  if (mag <= (T)0.1) return (T)1;
+  t0 /= mag;
+  t1 /= mag;
+  t2 /= mag;
+  T th = acos(t0 * b0 + t1 * b1 + t2 * b2);
+  const T dir = (b1 * t2 - b2 * t1) * n0 + (b2 * t0 - b0 * t2) * n1 + (b0 * t1 - b1 * t0) * n2;
+  if (dir < (T)0) th = acos((T)-1) - th;
+  return th < (T)1.23 ? (T)1.1603 * th * th - (T)2.0431 * th + (T)1
+                      : (T)0.5473 * th * th - (T)2.0035 * th + (T)1.8923;
+}
+
 template <typename T>
 __device__ __forceinline__ T core_derivative(const Core &cm, T x, int a, size_t r, size_t N, const T *__restrict__ xin,
                                              const T *__restrict__ site) {
   switch (cm.flag) {
+    case 5:   // BCC perfect: usf' cof(theta) pi sin(2 pi x) (fft_fftw_slab.cpp:1120)
+      return core_k<T>(cm, 0) * bcc_cof<T>(cm, a, r, N, xin) * sinpi_t<T>((T)2 * x);
     case 1:   // perfect / USFE(angle,tau): An' pi sin(2 pi x)
     case 6:
       return core_k<T>(cm, 0) * sinpi_t<T>((T)2 * x);

@@ -186,6 +186,19 @@ inline bool build_core(const pfdd_instance_desc &d, Core &c) {
     case PFDD_CORE_MPEA:
       c.k[0] = M_PI / s;   // A(r)/(mu dslip b) pi, fft_fftw_slab.cpp:1231
       break;
+    case PFDD_CORE_BCC_PERFECT:
+      c.k[0] = d.usf / s * M_PI;   // usf' pi, fft_fftw_slab.cpp:1096,1120
+      c.nx = d.nx;
+      c.ny = d.ny;
+      c.nz = d.nz;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) c.four[i][j] = d.four[i][j];
+      for (int a = 0; a < d.n_slip; ++a)
+        for (int i = 0; i < 3; ++i) {
+          c.xn[a][i] = d.xn[a][i];
+          c.xb[a][i] = d.xb[a][i];
+        }
+      break;
     case PFDD_CORE_PYRII:
       for (int n = 1; n <= 4; ++n) {
         c.k[n] = d.aa[n] / s;
@@ -203,7 +216,7 @@ inline bool build_core(const pfdd_instance_desc &d, Core &c) {
   }
   // derivatives of f' with respect to the GSFE parameters (adjoint step) and
   // the amplitudes of f itself (energy)
-  if (d.core_flag != PFDD_CORE_EXTENDED && d.core_flag != PFDD_CORE_PYRII) {
+  if (d.core_flag != PFDD_CORE_EXTENDED && d.core_flag != PFDD_CORE_PYRII && d.core_flag != PFDD_CORE_BCC_PERFECT) {
     c.k[7] = M_PI / s;
     c.k[8] = M_PI / (s * s);
     c.k[9] = 2.0 * M_PI / s;

@@ -23,6 +23,7 @@ ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "EUNSUPPORTED", -5: "EDIV
 FP64, FP32 = 0, 1
 IMAG_AUTO, IMAG_FULL, IMAG_NYQUIST = 0, 1, 2
 CORE_PERFECT, CORE_EXTENDED, CORE_SINE, CORE_PYRII, CORE_USFE_ANGLE, CORE_MPEA, CORE_SINE_FIELD = 1, 2, 3, 4, 6, 7, 103
+CORE_BCC_PERFECT = 5
 
 # every symbol include/pfdd_b200.h declares
 EXPORTS = [

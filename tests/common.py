@@ -17,7 +17,8 @@ def oracle_instance(w, core_flag=None, An=None, extra=None):
             kw[key] = tuple(float(v) for v in ce[key])
     if extra:
         kw.update(extra)
-    core = O.CoreModel(flag, mu, w.material.dslip, w.material.b, site=w.site, **kw)
+    geom = (w.four, w.xn, w.xb) if flag == 5 else None
+    core = O.CoreModel(flag, mu, w.material.dslip, w.material.b, site=w.site, geom=geom, **kw)
     invprim = np.linalg.inv(w.prim)
     sr = O.rotate_stress(w.sigma, w.prim, invprim, np.linalg.det(w.prim))
     tau = O.resolved_shear(sr, w.xn, w.xb, w.material.dslip)

@@ -66,6 +66,23 @@ def test_fp64_core_models(flag):
     assert np.abs(im - ref.imag).max() <= 1e-10
 
 
+@pytest.mark.parametrize("make", ["loop", "skew"])
+def test_bcc_perfect_core(make):
+    """Core model 5: angle-weighted core force from the gradient of Re xi,
+    on an orthogonal grid and on the 60-degree masked grid."""
+    if make == "loop":
+        w = configs.loop_workload(n=16, nz=8, radius=4.0, seed=8, sigma_mpa=250.0)
+    else:
+        w = configs.frank_read_workload(nx=16, ny=16, nz=8, seg=4)
+    w.core_flag = capi.CORE_BCC_PERFECT
+    ref, _, _ = O.run(oracle_instance(w), w.xi0, 10)
+    (re, im), _ = [x[0] for x in _run_gpu([w], 10)]
+    assert np.abs(re - ref.real).max() <= 1e-10
+    assert np.abs(im - ref.imag).max() <= 1e-10
+    (r32, _), _ = [x[0] for x in _run_gpu([w], 10, precision=capi.FP32)]
+    assert np.linalg.norm(r32 - ref.real) / np.linalg.norm(ref.real) <= 2e-5
+
+
 def test_fp64_mask_and_complex_state():
     w = small_loop(16)
     rng = np.random.default_rng(5)

@@ -80,3 +80,20 @@ def test_strain_stress_restatement_equals_reference(make):
     # the averages are means of fields of either sign: compare on the fields' scale
     assert np.abs(ave_eps - r["ave_eps"]).max() <= 1e-12 * scale_e
     assert np.abs(ave_sigma - r["ave_sigma"]).max() <= 1e-12 * scale_s
+
+
+@needs_ref
+@pytest.mark.parametrize("make", ["loop", "skew"])
+def test_bcc_perfect_core_equals_reference(make):
+    """Core model 5: the core force weighted by the edge/screw angle of the
+    gradient of Re xi (orthogonal grid, and the 60-degree grid where the
+    in-place `four` transform of the gradient matters)."""
+    if make == "loop":
+        w = configs.loop_workload(n=16, nz=8, radius=4.0, seed=8, sigma_mpa=250.0)
+    else:
+        w = configs.frank_read_workload(nx=16, ny=16, nz=8, seg=4)
+    w.core_flag = 5
+    r = ref_runner.run_reference(w, 4)
+    xi, nrm, ave = O.run(oracle_instance(w), w.xi0, 4)
+    assert np.abs(xi - r["xi"]).max() <= 1e-12
+    np.testing.assert_allclose(nrm, r["xinorm"], rtol=1e-10)
