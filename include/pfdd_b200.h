@@ -77,8 +77,9 @@ enum {
   PFDD_CORE_PYRII = 4,       /* core_energy_pyrII     src/fft_fftw_slab.cpp:1429-1493 */
   PFDD_CORE_BCC_PERFECT = 5, /* core_energy_bcc_perfect src/fft_fftw_slab.cpp:1070-1125, with the
                                 edge/screw angle from FFTW_Slab::gradient :869-1065 */
-  PFDD_CORE_USFE_ANGLE = 6,  /* core_energy_USFE_angle_tau src/fft_fftw_slab.cpp:1500-1545;
-                                the caller passes the resulting amplitude in `An` */
+  PFDD_CORE_USFE_ANGLE = 6,  /* core_energy_USFE_angle_tau src/fft_fftw_slab.cpp:1500-1545: the
+                                amplitude follows sigma_rot[2][1] of each stress state through
+                                `usfe_fit` and `angle_to_110`; the `An` field is not read */
   PFDD_CORE_MPEA = 7,        /* core_energy_mpea      src/fft_fftw_slab.cpp:1196-1235 */
   PFDD_CORE_SINE_FIELD = 103 /* sine GSFE with a per-site multiplier on isf and usf
                                 (random-alloy fields); no reference counterpart,
@@ -106,6 +107,16 @@ typedef struct {
   const double *xo;            /* obstacle mask [S*N] (nonzero = frozen), or NULL. Copied. */
   double sigma[3][3];          /* App::sigma at the first stress state (units of mu) */
   double dsigma[3][3];         /* App::deltasig added after each stress state */
+  /* Non-Schmid resolved shear stress: App::set_nonSchmid (src/app.cpp:446-459)
+   * selects FFTW_Slab::resolSS_non_Schmid (src/fft_fftw_slab.cpp:774-840)
+   * over resolSS_Schmid (:737-769) through App::resolSS (src/app.cpp:654-658).
+   * The reference sizes its projection tables for three systems, so
+   * non_schmid = 1 needs n_slip <= 3. */
+  int non_schmid;              /* App::non_Schmid: 0 = Schmid, 1 = non-Schmid */
+  double angle_to_110;         /* App::angle_to_110, degrees (also read by core model 6) */
+  double w1, w2, w3;           /* App::w1, w2, w3 */
+  double usfe_fit[5];          /* Material::a_slope, a_b, b_b, c_slope, c_b (core model 6;
+                                  the Ta and Fe presets, src/material.cpp:713-717, :766-770) */
 } pfdd_instance_desc;
 
 typedef struct {

@@ -129,6 +129,45 @@ def resolved_shear(sigma_rot, xn, xb, dslip):
     return np.einsum("ij,aj,ai->a", np.asarray(sigma_rot), np.asarray(xn), np.asarray(xb)) / dslip
 
 
+def non_schmid_projections(xb, angle_to_110, w1, w2, w3):
+    """S_tot[a, i, j] of resolSS_non_Schmid (fft_fftw_slab.cpp:774-840): the
+    maximum resolved shear stress plane n at angle_to_110 + 120 a degrees
+    (rotation about y), the plane n' 60 degrees from it, and
+    S_tot_ij = n_j b_i + w1 n'_j b_i + w2 n_j (n x b)_i + w3 n'_j (n' x b)_i.
+    The reference's tables hold three systems."""
+    xb = np.asarray(xb, float)
+    S = xb.shape[0]
+    if S > 3:
+        raise ValueError("resolSS_non_Schmid holds at most three systems")
+    out = np.zeros((S, 3, 3))
+    for a in range(S):
+        th = 120.0 * a
+        n = np.array([-math.sin((th + angle_to_110) * PI / 180.0), 0.0, math.cos((th + angle_to_110) * PI / 180.0)])
+        npl = np.array([-math.sin((th + angle_to_110 + 60) * PI / 180.0), 0.0,
+                        math.cos((th + angle_to_110 + 60) * PI / 180.0)])
+        b = xb[a]
+        nb, npb = np.cross(n, b), np.cross(npl, b)
+        out[a] = (np.outer(b, n) + w1 * np.outer(b, npl) + w2 * np.outer(nb, n) + w3 * np.outer(npb, npl))
+    return out
+
+
+def resolved_shear_non_schmid(sigma_rot, xb, dslip, angle_to_110, w1, w2, w3):
+    """tau_a = sum_ij sigma_rot_ij S_tot[a, i, j] / dslip (fft_fftw_slab.cpp:812-827)."""
+    P = non_schmid_projections(xb, angle_to_110, w1, w2, w3)
+    return np.einsum("ij,aij->a", np.asarray(sigma_rot), P) / dslip
+
+
+def usfe_angle_tau(sigma_rot, mu, fit, angle_to_110):
+    """Core model 6 amplitude An (J/m^2) of core_energy_USFE_angle_tau
+    (fft_fftw_slab.cpp:1517-1528): the fitted USFE in mJ/m^2 at the MRSSP angle
+    and the shear stress sigma_rot[2][1] mu (in GPa through the 1e-9), times 1e-3.
+    fit = (a_slope, a_b, b_b, c_slope, c_b)."""
+    a_slope, a_b, b_b, c_slope, c_b = (float(v) for v in fit)
+    t = float(np.asarray(sigma_rot)[2, 1]) * mu * 1.0E-9
+    gsfe = (a_slope * t + a_b) * math.sin(b_b * angle_to_110 * PI / 180.0) + (c_slope * t + c_b)
+    return gsfe * 1.0E-3
+
+
 # ---------------------------------------------------------------- strain / stress diagnostics
 def strain_stress(nx, ny, nz, four, xn, xb, dslip, C44, C12, C11, sigma_rot, xi):
     """The reference's strain and stress diagnostics of state xi, computed as
@@ -194,7 +233,7 @@ class CoreModel:
     3 sine (:1360-1418), 4 pyrII (:1429-1493), 5 BCC perfect with the
     edge/screw angle of FFTW_Slab::gradient (:1070-1125, :869-1065; needs
     geom = (four, xn, xb)), 6 USFE(angle, tau)
-    (:1500-1545, An supplied by the caller), 7 mpea (:1196-1235), and
+    (:1500-1545, An = usfe_angle_tau(...) of the stress state), 7 mpea (:1196-1235), and
     103 = sine with a per-site multiplier on isf and usf (random-alloy GSFE;
     no reference counterpart, reduces to flag 3 when the multiplier is 1).
     """

@@ -251,6 +251,9 @@ int main(int argc, char **argv) {
     for (int i = 0; i < 3; ++i)
       fprintf(f, "sigma_rot %d %.17g %.17g %.17g\n", i, fft->sigma_rot[i][0], fft->sigma_rot[i][1],
               fft->sigma_rot[i][2]);
+    fprintf(f, "usfe_fit %.17g %.17g %.17g %.17g %.17g\n", mat->a_slope, mat->a_b, mat->b_b, mat->c_slope, mat->c_b);
+    fprintf(f, "non_schmid %d %.17g %.17g %.17g %.17g\n", app->non_Schmid, app->angle_to_110, app->w1, app->w2,
+            app->w3);
     fprintf(f, "iterations %zu\n", fft->step_xinorm.size());
     fclose(f);
   }

@@ -27,7 +27,11 @@ def parse_setup(path):
             w = line.split()
             if not w:
                 continue
-            if w[0] in ("slip", "four", "sigma_rot", "tau"):
+            if w[0] == "usfe_fit":
+                out["usfe_fit"] = [float(v) for v in w[1:]]
+            elif w[0] == "non_schmid":
+                out["non_schmid"] = (int(w[1]), [float(v) for v in w[2:]])
+            elif w[0] in ("slip", "four", "sigma_rot", "tau"):
                 out[w[0]][int(w[1])] = [float(v) for v in w[2:]]
             elif w[0] in ("nx", "ny", "nz", "S", "core_flag", "iterations"):
                 out[w[0]] = int(w[1])

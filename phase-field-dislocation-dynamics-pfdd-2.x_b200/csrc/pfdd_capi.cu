@@ -103,6 +103,8 @@ struct Instance {
   double *sigma() const { return small.as<double>() + PFDD_MAXS; }   // sigma[9] then dsigma[9]
   int *flags() const { return reinterpret_cast<int *>(small.as<double>() + PFDD_MAXS + 18); }
   // flags: [0] stop, [1] bad, [2] steps_done, [3] a bounded wait ran out, [4] current xi buffer
+  double *an() const { return small.as<double>() + PFDD_MAXS + 22; }  // core model 6 amplitude [4]
+  const void *site_arg = nullptr;  // `site` argument of the update kernels
 };
 
 }  // namespace
@@ -245,8 +247,8 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   h->device_bytes += I.spec.bytes;
   CUDA_TRY(h, I.partials.alloc(2 * (size_t)I.F * I.nx * sizeof(double)));
   h->device_bytes += I.partials.bytes;
-  CUDA_TRY(h, I.small.alloc((PFDD_MAXS + 18 + 4) * sizeof(double)));
-  CUDA_TRY(h, cudaMemset(I.small.p, 0, (PFDD_MAXS + 18 + 4) * sizeof(double)));
+  CUDA_TRY(h, I.small.alloc((PFDD_MAXS + 26) * sizeof(double)));
+  CUDA_TRY(h, cudaMemset(I.small.p, 0, (PFDD_MAXS + 26) * sizeof(double)));
   double sig18[18];
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) {
@@ -270,6 +272,13 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
     CUDA_TRY(h, cudaMemcpy(I.site.p, sv.data(), sv.size() * sizeof(T), cudaMemcpyHostToDevice));
     h->device_bytes += I.site.bytes;
   }
+  // core model 6 reads its per-state amplitude (An' pi, An') where the
+  // per-site models read their field: FP64 at an(), FP32 after them
+  I.site_arg = I.site.p;
+  if (d.core_flag == PFDD_CORE_USFE_ANGLE)
+    I.site_arg = sizeof(T) == 8 ? (const void *)I.an() : (const void *)(I.an() + 2);
+  if (d.non_schmid && I.S > 3)
+    return fail(h, PFDD_EINVAL, "non-Schmid stress needs n_slip <= 3 (resolSS_non_Schmid tables)");
 
   // shared-memory budgets
   I.smem_plane = PlaneSmem<C>::bytes(I.split ? I.ny / 2 : I.ny, I.ny, I.nzs, I.M);
@@ -337,29 +346,28 @@ void fill_plane_args(const Instance &I, PlaneArgs &pa) {
 template <typename T>
 pfdd_status set_smem_attrs(pfdd_gpu *h, size_t plane, size_t upd, size_t pencil) {
   constexpr int NP = Threads<T>::plane, NH = Threads<T>::half, NC = Threads<T>::pencil;
-  const auto A = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes<T, NP, false>, A, (int)plane));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes<T, NH, true>, A, (int)plane));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update<T, NP, false>, A, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update<T, NH, true>, A, (int)upd));
+  CUDA_TRY(h, raise_smem_limit(k_fwd_planes<T, NP, false>, plane));
+  CUDA_TRY(h, raise_smem_limit(k_fwd_planes<T, NH, true>, plane));
+  CUDA_TRY(h, raise_smem_limit(k_inv_update<T, NP, false>, upd));
+  CUDA_TRY(h, raise_smem_limit(k_inv_update<T, NH, true>, upd));
   cudaError_t pe_err = cudaSuccess;
   for (int sc : {0, 2, 3})
     with_pencil_sc(sc, [&](auto SCc) {
       constexpr int SC = decltype(SCc)::value;
-      if (pe_err == cudaSuccess) pe_err = cudaFuncSetAttribute(k_xpencil<T, NC, SC>, A, (int)pencil);
-      if (pe_err == cudaSuccess) pe_err = cudaFuncSetAttribute(k_xpencil_tab<T, NC, SC>, A, (int)pencil);
+      if (pe_err == cudaSuccess) pe_err = raise_smem_limit(k_xpencil<T, NC, SC>, pencil);
+      if (pe_err == cudaSuccess) pe_err = raise_smem_limit(k_xpencil_tab<T, NC, SC>, pencil);
     });
   CUDA_TRY(h, pe_err);
-  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes_tab<T, NP, false>, A, (int)plane));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_fwd_planes_tab<T, NH, true>, A, (int)plane));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update_tab<T, NP, false>, A, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_inv_update_tab<T, NH, true>, A, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes<T, NP, false>, A, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes<T, NH, true>, A, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes_tab<T, NP, false>, A, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_adj_planes<T, NP, false>, A, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_adj_planes<T, NH, true>, A, (int)upd));
-  CUDA_TRY(h, cudaFuncSetAttribute(k_step_planes_tab<T, NH, true>, A, (int)upd));
+  CUDA_TRY(h, raise_smem_limit(k_fwd_planes_tab<T, NP, false>, plane));
+  CUDA_TRY(h, raise_smem_limit(k_fwd_planes_tab<T, NH, true>, plane));
+  CUDA_TRY(h, raise_smem_limit(k_inv_update_tab<T, NP, false>, upd));
+  CUDA_TRY(h, raise_smem_limit(k_inv_update_tab<T, NH, true>, upd));
+  CUDA_TRY(h, raise_smem_limit(k_step_planes<T, NP, false>, upd));
+  CUDA_TRY(h, raise_smem_limit(k_step_planes<T, NH, true>, upd));
+  CUDA_TRY(h, raise_smem_limit(k_step_planes_tab<T, NP, false>, upd));
+  CUDA_TRY(h, raise_smem_limit(k_adj_planes<T, NP, false>, upd));
+  CUDA_TRY(h, raise_smem_limit(k_adj_planes<T, NH, true>, upd));
+  CUDA_TRY(h, raise_smem_limit(k_step_planes_tab<T, NH, true>, upd));
   return PFDD_OK;
 }
 
@@ -480,7 +488,7 @@ void enqueue_step_fused(Instance &I, cudaStream_t st, bool fwd, const AdjointPas
   ua.core = I.core;
   ua.tau = I.tau();
   ua.mask = I.mask.as<uint8_t>();
-  ua.site = I.site.p;
+  ua.site = I.site_arg;
   ua.stop = flags;
   ua.err = flags + 3;
   ua.mode = adj ? PASS_ADJOINT : PASS_STEP;
@@ -514,6 +522,10 @@ bool same_group(const Instance &a, const Instance &b) {
       memcmp(x.xn, y.xn, sizeof(double) * 3 * a.S) || memcmp(x.xb, y.xb, sizeof(double) * 3 * a.S) ||
       memcmp(x.c, y.c, sizeof x.c) || memcmp(x.aa, y.aa, sizeof x.aa) || memcmp(x.bb, y.bb, sizeof x.bb))
     return false;
+  // one StressArgs serves the whole group
+  if ((x.non_schmid != 0) != (y.non_schmid != 0) || x.angle_to_110 != y.angle_to_110 || x.w1 != y.w1 ||
+      x.w2 != y.w2 || x.w3 != y.w3 || memcmp(x.usfe_fit, y.usfe_fit, sizeof x.usfe_fit))
+    return false;
   if ((a.mask.p == nullptr) != (b.mask.p == nullptr) || (a.site.p == nullptr) != (b.site.p == nullptr)) return false;
   return true;
 }
@@ -537,7 +549,8 @@ pfdd_status refresh_tables(pfdd_gpu *h) {
       p.stats = I.stats.as<double>();
       p.stats_cap = I.stats_cap;
       p.mask = I.mask.as<uint8_t>();
-      p.site = I.site.p;
+      p.site = I.site_arg;
+      p.an = I.an();
     }
     if (!G.table.p) CUDA_TRY(h, G.table.alloc(t.size() * sizeof(InstPtrs)));
     CUDA_TRY(h, cudaMemcpy(G.table.p, t.data(), t.size() * sizeof(InstPtrs), cudaMemcpyHostToDevice));
@@ -769,8 +782,7 @@ pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *si
   while (cc > 1 && bytes(cc) > 227 * 1024) cc >>= 1;
   if (bytes(cc) > 227 * 1024 || ncols % cc)
     return fail(h, PFDD_EUNSUPPORTED, "strain pencil of %d x %d fields does not fit shared memory", I.nx, FB);
-  CUDA_TRY(h, cudaFuncSetAttribute(k_strain_pencil<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)bytes(cc)));
+  CUDA_TRY(h, raise_smem_limit(k_strain_pencil<T, 256>, bytes(cc)));
   PencilArgs pe{};
   pe.px = I.px;
   pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.nzp = I.nzp; pe.M = I.M;
@@ -840,7 +852,7 @@ pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, 
   cudaStream_t st = h->stream;
   DevBuf gpart;
   CUDA_TRY(h, gpart.alloc(4 * (size_t)I.F * I.nx * sizeof(double)));
-  k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.stress, 0, nullptr);
+  k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.an(), I.stress, 0, nullptr);
   PlaneArgs pa;
   fill_plane_args<T>(I, pa);
   const T *xcur = I.xi[I.cur].as<T>();
@@ -873,7 +885,7 @@ pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, 
   ua.core = I.core;
   ua.tau = I.tau();
   ua.mask = I.mask.as<uint8_t>();
-  ua.site = I.site.p;
+  ua.site = I.site_arg;
   ua.err = I.flags() + 3;
   ua.mode = PASS_ENERGY;
   ua.gpart = gpart.as<double>();
@@ -966,7 +978,7 @@ pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const dou
       e = cudaMemcpyAsync(I.aux.p, ck_state(j) + n_all * sizeof(T), aux_bytes, cudaMemcpyDeviceToDevice, st);
     return e;
   };
-  k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.stress, 0, I.flags());
+  k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.an(), I.stress, 0, I.flags());
   PlaneArgs pa;
   fill_plane_args<T>(I, pa);
   // forward with checkpoints: one opening transform, then fused steps
@@ -1033,8 +1045,13 @@ pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const dou
     dparams[1] = -cd * A[1];
   }
   if (dsigma) {
-    // dJ/dtau_a = cd * sum lambda_a; tau_a = sum_ij sigma_rot_ij xn_aj xb_ai / dslip
+    // dJ/dtau_a = cd * sum lambda_a; tau_a = sum_ij sigma_rot_ij P_a,ij / dslip with
+    // P_a,ij = xb_ai xn_aj (Schmid) or S_tot (non-Schmid).  Core model 6 adds
+    // dJ/dAn dAn/dsigma_rot[2][1], An = 1e-3 gsfe(sigma_rot[2][1]).
     const StressArgs &sa = I.stress;
+    const double dAn_dsr21 =
+        sa.usfe ? 1.0E-3 * (sa.fit[0] * sa.mu * 1.0E-9 * sa.fit_sin + sa.fit[3] * sa.mu * 1.0E-9) : 0.0;
+    const double dJ_dAn = -cd * A[0];
     const int comp[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
     for (int c = 0; c < 6; ++c) {
       double g = 0.0;
@@ -1045,10 +1062,18 @@ pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const dou
           for (int i = 0; i < 3; ++i)
             for (int jj = 0; jj < 3; ++jj) {
               const double dr = sa.ortho ? sa.prim[i][k] * sa.invprim[l][jj] : ((i == k && jj == l) ? 1.0 : 0.0);
-              dt += dr * sa.xn[a][jj] * sa.xb[a][i] / sa.dslip;
+              dt += dr * (sa.ns ? sa.proj[a][i][jj] : sa.xn[a][jj] * sa.xb[a][i]) / sa.dslip;
             }
         }
         g += cd * A[2 + a] * dt;
+      }
+      if (sa.usfe) {
+        double d21 = 0.0;
+        for (int pass = 0; pass < (comp[c][0] == comp[c][1] ? 1 : 2); ++pass) {
+          const int k = pass ? comp[c][1] : comp[c][0], l = pass ? comp[c][0] : comp[c][1];
+          d21 += sa.ortho ? sa.prim[2][k] * sa.invprim[l][1] : ((k == 2 && l == 1) ? 1.0 : 0.0);
+        }
+        g += dJ_dAn * dAn_dsr21 * d21;
       }
       dsigma[c] = g;
     }
@@ -1498,7 +1523,7 @@ pfdd_status pfdd_gpu_tau(pfdd_gpu *h, int inst, double *tau) {
   if (inst < 0 || inst >= (int)h->inst.size() || !tau) return fail(h, PFDD_EINVAL, "bad arguments");
   Instance &I = *h->inst[inst];
   cudaSetDevice(h->device);
-  k_stress_state<<<1, 32, 0, h->stream>>>(I.sigma(), I.tau(), I.stress, 0, nullptr);
+  k_stress_state<<<1, 32, 0, h->stream>>>(I.sigma(), I.tau(), I.an(), I.stress, 0, nullptr);
   CUDA_TRY(h, cudaMemcpyAsync(tau, I.tau(), I.S * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return PFDD_OK;

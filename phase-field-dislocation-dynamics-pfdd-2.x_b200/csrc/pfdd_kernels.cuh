@@ -189,6 +189,7 @@ struct InstPtrs {
   int stats_cap;
   const uint8_t *mask;
   const void *site;
+  double *an;          // core model 6 amplitude slots (resolve_state), or null
 };
 
 // ------------------------------------------------------------ small helpers
@@ -950,9 +951,10 @@ __device__ __forceinline__ T core_derivative(const Core &cm, T x, int a, size_t 
   switch (cm.flag) {
     case 5:   // BCC perfect: usf' cof(theta) pi sin(2 pi x) (fft_fftw_slab.cpp:1120)
       return core_k<T>(cm, 0) * bcc_cof<T>(cm, a, r, N, xin) * sinpi_t<T>((T)2 * x);
-    case 1:   // perfect / USFE(angle,tau): An' pi sin(2 pi x)
-    case 6:
+    case 1:   // perfect: An' pi sin(2 pi x)
       return core_k<T>(cm, 0) * sinpi_t<T>((T)2 * x);
+    case 6:   // USFE(angle,tau): site[0] = An' pi of the current stress state
+      return site[0] * sinpi_t<T>((T)2 * x);
     case 3: { // sine: isf' pi sin(2 pi x) + Cn' 2 pi sin(4 pi x)
       T s, c;
       sincospi_t<T>((T)2 * x, &s, &c);
@@ -1034,8 +1036,9 @@ __device__ __forceinline__ T core_energy_density(const Core &cm, T x, int a, siz
   const T s1 = sinpi_t<T>(x), s2 = sinpi_t<T>((T)2 * x);
   switch (cm.flag) {
     case 1:
-    case 6:
       return core_k<T>(cm, 10) * s1 * s1;
+    case 6:
+      return site[1] * s1 * s1;
     case 3:
       return core_k<T>(cm, 10) * s1 * s1 + core_k<T>(cm, 11) * s2 * s2;
     case 7:
@@ -1067,10 +1070,12 @@ __device__ __forceinline__ void core_adjoint_terms(const Core &cm, T x, int a, s
   dp1 = (T)0;
   switch (cm.flag) {
     case 1:
-    case 6:  // k0 = An' pi ; f' = k0 sin(2 pi x); d/dAn = (pi/s) sin(2 pi x)
-      d2 = core_k<T>(cm, 0) * (T)2 * pi * c2;
+    case 6: {  // k0 = An' pi (site[0] for model 6); f' = k0 sin(2 pi x); d/dAn = (pi/s) sin(2 pi x)
+      const T k0 = cm.flag == 6 ? site[0] : core_k<T>(cm, 0);
+      d2 = k0 * (T)2 * pi * c2;
       dp0 = core_k<T>(cm, 7) * s2;
       return;
+    }
     case 3:  // k0 = isf' pi, k1 = Cn' 2 pi
       d2 = core_k<T>(cm, 0) * (T)2 * pi * c2 + core_k<T>(cm, 1) * (T)4 * pi * c4;
       dp0 = core_k<T>(cm, 7) * s2 - core_k<T>(cm, 8) * s4;   // (pi/s) sin2 - (pi/s^2) sin4
@@ -1541,9 +1546,45 @@ struct StressArgs {
   double xn[PFDD_MAXS][3], xb[PFDD_MAXS][3];
   double dslip;
   double dsig[3][3];
+  int ns;                          // 1: tau from the non-Schmid projections proj
+  double proj[PFDD_MAXS][3][3];    // S_tot[a][i][j] of resolSS_non_Schmid
+  int usfe;                        // 1: core model 6 amplitude from sigma_rot[2][1]
+  double fit[5];                   // a_slope, a_b, b_b, c_slope, c_b
+  double fit_sin;                  // sin(b_b angle_to_110 pi / 180)
+  double mu, s;                    // Material::mu, mu dslip b
 };
 
-static __global__ void k_stress_state(double *sigma /*[9]*/, double *tau, StressArgs s, int mode, int *stop) {
+// tau_a from sigma_rot: resolSS_Schmid (fft_fftw_slab.cpp:744-749) or
+// resolSS_non_Schmid (:812-827), in the reference's order of operations; the
+// core model 6 amplitude (core_energy_USFE_angle_tau :1517-1528) into an[]:
+// an[0] = An' pi, an[1] = An', and the same two as floats after them.
+__device__ __forceinline__ void resolve_state(const StressArgs &s, const double (&sr)[3][3], double *tau, double *an) {
+  for (int a = 0; a < s.S; ++a) {
+    double t = 0.0;
+    if (s.ns) {
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) t = t + __ddiv_rn(__dmul_rn(sr[i][j], s.proj[a][i][j]), s.dslip);
+    } else {
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) t = t + (sr[i][j] * s.xn[a][j] * s.xb[a][i]) / s.dslip;
+    }
+    tau[a] = t;
+  }
+  if (s.usfe && an) {
+    const double m9 = 1.0E-9;
+    const double ga = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(s.fit[0], sr[2][1]), s.mu), m9), s.fit[1]);
+    const double gc = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(s.fit[3], sr[2][1]), s.mu), m9), s.fit[4]);
+    const double gsfe = __dmul_rn(__dadd_rn(__dmul_rn(ga, s.fit_sin), gc), 1.0E-3);
+    const double A = __ddiv_rn(gsfe, s.s);
+    an[0] = __dmul_rn(A, PFDD_PI_T);
+    an[1] = A;
+    float *af = reinterpret_cast<float *>(an + 2);
+    af[0] = (float)an[0];
+    af[1] = (float)A;
+  }
+}
+
+static __global__ void k_stress_state(double *sigma /*[9]*/, double *tau, double *an, StressArgs s, int mode, int *stop) {
   if (threadIdx.x != 0) return;
   if (mode == 0) {
     double sr[3][3];
@@ -1557,12 +1598,7 @@ static __global__ void k_stress_state(double *sigma /*[9]*/, double *tau, Stress
           sr[i][j] = sigma[3 * i + j];
         }
       }
-    for (int a = 0; a < s.S; ++a) {
-      double t = 0.0;
-      for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) t = t + (sr[i][j] * s.xn[a][j] * s.xb[a][i]) / s.dslip;
-      tau[a] = t;
-    }
+    resolve_state(s, sr, tau, an);
     if (stop) *stop = 0;
   } else {
     for (int i = 0; i < 3; ++i)
@@ -1588,12 +1624,7 @@ static __global__ void k_stress_state_tab(const InstPtrs *__restrict__ tab, Stre
           sr[i][j] = sigma[3 * i + j];
         }
       }
-    for (int a = 0; a < s.S; ++a) {
-      double t = 0.0;
-      for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) t = t + (sr[i][j] * s.xn[a][j] * s.xb[a][i]) / s.dslip;
-      ip.tau[a] = t;
-    }
+    resolve_state(s, sr, ip.tau, ip.an);
     ip.flags[0] = 0;
   } else {
     for (int i = 0; i < 9; ++i) sigma[i] = sigma[i] + sigma[9 + i];

@@ -69,14 +69,6 @@ pfdd_status device_setup(int dev, void **addr) {
   void *p = nullptr;
   cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
   if (e != cudaSuccess || !p) return nerr(PFDD_ECUDA, "cudaGetSymbolAddress of the static scratch failed");
-  const int lim = 227 * 1024;
-  if (cudaFuncSetAttribute(k_fwd_planes<double, 256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(k_xpencil<double, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(k_inv_update<double, 256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim) !=
-          cudaSuccess)
-    return nerr(PFDD_ECUDA, "cudaFuncSetAttribute failed during static-scratch set-up");
   g_addr[dev] = p;
   *addr = p;
   return PFDD_OK;
@@ -126,7 +118,7 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   // scratch layout
   const size_t b_spec = up256((size_t)F * nx * ny * nzp * sizeof(C));
   const size_t b_part = up256(2 * (size_t)F * nx * sizeof(double));
-  const size_t b_small = up256((PFDD_MAXS + 9 + 8 + 2) * sizeof(double));
+  const size_t b_small = up256((PFDD_MAXS + 9 + 8 + 2 + 2) * sizeof(double));
   const size_t b_tw = up256((size_t)(nx + ny + 2 * M) * sizeof(C));
   const size_t b_tab = up256((size_t)(M + nx + 2 * ny + nzp + M / 2) * sizeof(int16_t));
   const size_t need = b_spec + b_part + b_small + b_tw + b_tab;
@@ -138,6 +130,12 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   void *base = nullptr;
   pfdd_status st = device_setup(dev, &base);
   if (st != PFDD_OK) return st;
+  // every call: a handle created since the last call may have set these
+  // kernels' limits for its own sizes (raise_smem_limit never lowers them)
+  if (raise_smem_limit(k_fwd_planes<double, 256, false>, smem_plane) != cudaSuccess ||
+      raise_smem_limit(k_xpencil<double, 256>, pencil_bytes(cc)) != cudaSuccess ||
+      raise_smem_limit(k_inv_update<double, 256, false>, smem_plane) != cudaSuccess)
+    return nerr(PFDD_ECUDA, "raising the kernels' shared-memory limits failed");
   unsigned char *p = static_cast<unsigned char *>(base);
   C *spec = reinterpret_cast<C *>(p);
   double *partials = reinterpret_cast<double *>(p + b_spec);
@@ -145,6 +143,7 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   double *tau = small;                                   // [PFDD_MAXS]
   int *flags = reinterpret_cast<int *>(small + PFDD_MAXS + 9);  // stop, bad, steps, timeout
   double *stats = small + PFDD_MAXS + 9 + 8;            // xinorm, xiave
+  double *an = small + PFDD_MAXS + 9 + 8 + 2;           // core model 6: An' pi, An'
   C *tw = reinterpret_cast<C *>(p + b_spec + b_part + b_small);
   int16_t *tab = reinterpret_cast<int16_t *>(p + b_spec + b_part + b_small + b_tw);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -179,33 +178,18 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   if (!build_core(d, core)) return nerr(PFDD_EUNSUPPORTED, "core model not supported");
   StressArgs sa;
   build_stress(d, sa);
-  // tau at the descriptor's stress state: rotate_stress + resolSS_Schmid
-  double htau[PFDD_MAXS];
-  {
-    double sr[3][3];
-    for (int i = 0; i < 3; ++i)
-      for (int j = 0; j < 3; ++j) {
-        sr[i][j] = 0.0;
-        if (sa.ortho) {
-          for (int k = 0; k < 3; ++k)
-            for (int l = 0; l < 3; ++l) sr[i][j] += sa.prim[i][k] * d.sigma[k][l] * sa.invprim[l][j];
-        } else {
-          sr[i][j] = d.sigma[i][j];
-        }
-      }
-    for (int a = 0; a < S; ++a) {
-      double t = 0.0;
-      for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) t = t + (sr[i][j] * d.xn[a][j] * d.xb[a][i]) / d.dslip;
-      htau[a] = t;
-    }
-  }
+  if (d.non_schmid && S > 3) return nerr(PFDD_EINVAL, "non-Schmid stress needs n_slip <= 3");
+  // tau (Schmid or non-Schmid) and the core model 6 amplitude at the
+  // descriptor's stress state
+  double htau[PFDD_MAXS], han[2];
+  resolve_state_host(sa, d.sigma, htau, han);
 
   cudaError_t e = cudaSuccess;
   e = cudaMemcpyAsync(tw, htw, (size_t)(nx + ny + 2 * M) * sizeof(C), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(tab, htab, (size_t)(M + nx + 2 * ny + nzp + M / 2) * sizeof(int16_t), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(tau, htau, S * sizeof(double), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(an, han, sizeof han, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(flags, 0, 8 * sizeof(int), s);
   if (e != cudaSuccess) return nerr(PFDD_ECUDA, cudaGetErrorString(e));
 
@@ -241,6 +225,7 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   ua.invN = 1.0 / (double)N;
   ua.core = core;
   ua.tau = tau;
+  ua.site = d.core_flag == PFDD_CORE_USFE_ANGLE ? an : nullptr;
   ua.stop = flags;
   ua.err = flags + 3;
   ua.mode = PASS_STEP;

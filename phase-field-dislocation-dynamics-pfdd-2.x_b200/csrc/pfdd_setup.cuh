@@ -15,6 +15,19 @@
 namespace pfdd {
 namespace host {
 
+// A kernel's dynamic shared-memory limit is one value per process and device,
+// shared by every handle and by the allocation-free entry point: raise it to
+// what a caller needs, never lower it under another caller's launches.
+template <typename K>
+inline cudaError_t raise_smem_limit(K *kernel, size_t bytes) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, reinterpret_cast<const void *>(kernel));
+  if (e != cudaSuccess) return e;
+  if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(reinterpret_cast<const void *>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)bytes);
+}
+
 // Radix plan: greedy 16, 8, 4, 2, 3 factors; sub-lengths L_s.
 inline bool make_plan(int n, FftPlan &p, int maxr = 16) {
   p.n = n;
@@ -258,6 +271,64 @@ inline void build_stress(const pfdd_instance_desc &d, StressArgs &s) {
   s.dslip = d.dslip;
   for (int a = 0; a < d.n_slip; ++a)
     for (int i = 0; i < 3; ++i) { s.xn[a][i] = d.xn[a][i]; s.xb[a][i] = d.xb[a][i]; }
+  s.ns = d.non_schmid ? 1 : 0;
+  if (s.ns) {
+    // resolSS_non_Schmid (fft_fftw_slab.cpp:793-828): the maximum resolved
+    // shear stress plane at angle_to_110 + 120 a degrees about y, the plane
+    // 60 degrees from it, their cross products with b, and the projection
+    // S_tot_ij = n_j b_i + w1 n'_j b_i + w2 n_j (n x b)_i + w3 n'_j (n' x b)_i
+    double theta = 0.0;
+    for (int a = 0; a < d.n_slip && a < 3; ++a) {
+      const double n[3] = {-std::sin((theta + d.angle_to_110) * M_PI / 180.), 0.0,
+                           std::cos((theta + d.angle_to_110) * M_PI / 180.)};
+      const double np[3] = {-std::sin((theta + d.angle_to_110 + 60) * M_PI / 180.), 0.0,
+                            std::cos((theta + d.angle_to_110 + 60) * M_PI / 180.)};
+      theta += 120.;
+      const double *b = d.xb[a];
+      const double nb[3] = {n[1] * b[2] - n[2] * b[1], -n[0] * b[2] + n[2] * b[0], n[0] * b[1] - n[1] * b[0]};
+      const double npb[3] = {np[1] * b[2] - np[2] * b[1], -np[0] * b[2] + np[2] * b[0], np[0] * b[1] - np[1] * b[0]};
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          s.proj[a][i][j] = n[j] * b[i] + d.w1 * np[j] * b[i] + d.w2 * n[j] * nb[i] + d.w3 * np[j] * npb[i];
+    }
+  }
+  s.usfe = d.core_flag == PFDD_CORE_USFE_ANGLE ? 1 : 0;
+  const double mu = d.C44 - (2.0 * d.C44 + d.C12 - d.C11) / 5.0;
+  s.mu = mu;
+  s.s = mu * d.dslip * d.b;
+  for (int i = 0; i < 5; ++i) s.fit[i] = d.usfe_fit[i];
+  s.fit_sin = std::sin(d.usfe_fit[2] * d.angle_to_110 * M_PI / 180.);
+}
+
+// Host twin of the device stress-state step: sigma_rot (rotate_stress,
+// fft_fftw_slab.cpp:242-274), tau (resolSS_Schmid / resolSS_non_Schmid) and
+// the core model 6 amplitude an[0] = An' pi, an[1] = An' (an may be null).
+inline void resolve_state_host(const StressArgs &s, const double (&sigma)[3][3], double *tau, double *an) {
+  double sr[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      sr[i][j] = 0.0;
+      if (s.ortho) {
+        for (int k = 0; k < 3; ++k)
+          for (int l = 0; l < 3; ++l) sr[i][j] += s.prim[i][k] * sigma[k][l] * s.invprim[l][j];
+      } else {
+        sr[i][j] = sigma[i][j];
+      }
+    }
+  for (int a = 0; a < s.S; ++a) {
+    double t = 0.0;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        t = t + (s.ns ? (sr[i][j] * s.proj[a][i][j]) / s.dslip : (sr[i][j] * s.xn[a][j] * s.xb[a][i]) / s.dslip);
+    tau[a] = t;
+  }
+  if (an) {
+    const double ga = s.fit[0] * sr[2][1] * s.mu * 1.0E-9 + s.fit[1];
+    const double gc = s.fit[3] * sr[2][1] * s.mu * 1.0E-9 + s.fit[4];
+    const double A = ((ga * s.fit_sin + gc) * 1.0E-3) / s.s;
+    an[0] = s.usfe ? A * M_PI : 0.0;
+    an[1] = s.usfe ? A : 0.0;
+  }
 }
 
 }  // namespace host

@@ -50,6 +50,9 @@ class InstanceDesc(ctypes.Structure):
         ("c", ctypes.c_double * 7), ("aa", ctypes.c_double * 5), ("bb", ctypes.c_double * 4),
         ("site_gsfe", DP), ("xo", DP),
         ("sigma", D33), ("dsigma", D33),
+        ("non_schmid", ctypes.c_int), ("angle_to_110", ctypes.c_double),
+        ("w1", ctypes.c_double), ("w2", ctypes.c_double), ("w3", ctypes.c_double),
+        ("usfe_fit", ctypes.c_double * 5),
     ]
 
 
@@ -132,6 +135,14 @@ def desc_from_workload(w, core_flag=None, An=None):
     d.core_flag = w.core_flag if core_flag is None else core_flag
     d.isf, d.usf = w.material.isf, w.material.usf
     d.An = w.material.An if An is None else An
+    ns = getattr(w, "non_schmid", None)
+    if ns is not None:
+        d.non_schmid = 1
+        d.angle_to_110, d.w1, d.w2, d.w3 = (float(v) for v in ns)
+    fit = getattr(w.material, "usfe_fit", None)
+    if fit is not None:
+        for i in range(5):
+            d.usfe_fit[i] = float(fit[i])
     extra = getattr(w, "core_extra", None) or {}
     for key, n in (("c", 7), ("aa", 5), ("bb", 4)):
         if key in extra:

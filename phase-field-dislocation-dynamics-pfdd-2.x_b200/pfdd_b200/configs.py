@@ -102,6 +102,7 @@ class Material:
     dslip: float = 0.8165
     deck_line: str | None = None   # verbatim `material ...` deck line (preset constants as they are)
     elastic_override: tuple | None = None  # (C44, C12, C11) exactly as a deck produced them
+    usfe_fit: tuple | None = None  # a_slope, a_b, b_b, c_slope, c_b of the preset (core model 6)
 
     def elastic(self):
         if self.elastic_override is not None:
@@ -133,6 +134,7 @@ class Workload:
     site: np.ndarray | None = None  # per-site GSFE amplitude/multiplier [S, nx, ny, nz]
     dsigma: np.ndarray = field(default_factory=lambda: np.zeros((3, 3)))
     core_extra: dict | None = None  # c (7), aa (5), bb (4) GSFE constants for the extended / pyrII cores
+    non_schmid: tuple | None = None  # (angle_to_110 degrees, w1, w2, w3): deck `non_Schmid` (app.cpp:446-459)
 
     @property
     def S(self):
@@ -156,6 +158,8 @@ class Workload:
         lines = [
             "seed 576",
             "app_style %s core_energy %d" % (self.app, self.core_flag),
+        ] + ([] if self.non_schmid is None else ["non_Schmid %r %r %r %r" % tuple(
+            float(v) for v in self.non_schmid)]) + [
             "fft_style %s pbc 1 1 1 mode 1%s" % (fft_style, prim_txt),
             "dimension 3",
             "lattice sc/6n 1",
@@ -188,6 +192,44 @@ def _disc(nx, ny, cx, cy, r):
     x = np.arange(nx)[:, None] - cx
     y = np.arange(ny)[None, :] - cy
     return (x * x + y * y) <= r * r
+
+
+# USFE(MRSSP angle, tau) fits of the Ta and Fe presets (Material::set_constants,
+# material.cpp:713-717 and :766-770): a_slope, a_b, b_b, c_slope, c_b
+TA_USFE_FIT = (51.59816407, -2.27173784, 0.9979452, -4.16536, 1133.961364)
+FE_USFE_FIT = (15.524609942496577, 0.004388435835439675, 0.9934680885709689, -0.9065590784654822,
+               944.0633238797747)
+
+
+def ta_material() -> Material:
+    """The Ta preset (material.cpp:697-718): a = 3.3058e-10 m, b = sqrt(3) a / 2."""
+    a = 3.3058E-10
+    return Material(preset="Ta", mu=70.67E9, young=189.24E9, b=math.sqrt(3.0) * a / 2.0, isf=0.0,
+                    usf=950.21E-3, An=0.0, usfe_fit=TA_USFE_FIT)
+
+
+def bcc_screw_workload(n=16, nz=8, seed=11, sigma_mpa=300.0, angle=10.0, w=(0.3, 0.2, 0.1), core_flag=6,
+                       name="bcc_screw"):
+    """One BCC system (app 1SBCC: n = (0.7071, 0.7071, 0), b = (-0.57735,
+    0.57735, 0.57735) as set_slip writes them, CD = 0.25) in Ta with the
+    non-Schmid resolved shear stress and, for core model 6, the USFE(angle,
+    tau) amplitude; xi = 1 on a band of the (110) plane through the centre
+    plus seeded noise.  sigma_yz and sigma_xz carry the load."""
+    m = ta_material()
+    prim = np.eye(3)
+    four, _ = reciprocal_basis(prim)
+    xn = np.array([[0.7071, 0.7071, 0.0]])
+    xb = np.array([[-0.57735, 0.57735, 0.57735]])
+    rng = np.random.default_rng(seed)
+    xi0 = rng.uniform(-1e-3, 1e-3, size=(1, n, n, nz))
+    x = np.arange(n)[:, None, None]
+    y = np.arange(n)[None, :, None]
+    z = np.arange(nz)[None, None, :]
+    band = (x + y == n) & (np.abs(z - nz // 2) < max(1, nz // 4))
+    xi0[0][np.broadcast_to(band, (n, n, nz))] = 1.0
+    sig = _sigma("yz", sigma_mpa * 1e6 / m.mu) + _sigma("xz", 0.5 * sigma_mpa * 1e6 / m.mu)
+    return Workload(name, n, n, nz, "1SBCC", xn, xb, four, prim, m, core_flag, sig, 0.25, xi0,
+                    non_schmid=(float(angle),) + tuple(float(v) for v in w))
 
 
 def loop_workload(n=64, radius=12.0, noise=1e-3, seed=576, sigma_mpa=200.0, name="loop64",

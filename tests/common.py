@@ -1,4 +1,6 @@
 """Shared test helpers: build oracle instances for configs.Workload objects."""
+import dataclasses
+
 import numpy as np
 
 import pfdd_oracle as O
@@ -18,10 +20,16 @@ def oracle_instance(w, core_flag=None, An=None, extra=None):
     if extra:
         kw.update(extra)
     geom = (w.four, w.xn, w.xb) if flag == 5 else None
-    core = O.CoreModel(flag, mu, w.material.dslip, w.material.b, site=w.site, geom=geom, **kw)
     invprim = np.linalg.inv(w.prim)
     sr = O.rotate_stress(w.sigma, w.prim, invprim, np.linalg.det(w.prim))
-    tau = O.resolved_shear(sr, w.xn, w.xb, w.material.dslip)
+    ns = getattr(w, "non_schmid", None)
+    if flag == 6:
+        kw["An"] = O.usfe_angle_tau(sr, mu, w.material.usfe_fit, ns[0] if ns else 0.0)
+    core = O.CoreModel(flag, mu, w.material.dslip, w.material.b, site=w.site, geom=geom, **kw)
+    if ns is not None:
+        tau = O.resolved_shear_non_schmid(sr, w.xb, w.material.dslip, *ns)
+    else:
+        tau = O.resolved_shear(sr, w.xn, w.xb, w.material.dslip)
     return O.Instance(w.nx, w.ny, w.nz, BB, tau, w.cd_dt, core, xo=w.xo)
 
 
@@ -43,11 +51,13 @@ def load_golden(name):
     fx = dict(np.load(os.path.join(here, name + ".npz")))
     m = configs.Material(b=float(fx["b"]), dslip=float(fx["dslip"]), isf=float(fx["isf"]),
                          usf=float(fx["usf"]), An=float(fx["An"]), mu=float(fx["C44"]),
-                         elastic_override=(float(fx["C44"]), float(fx["C12"]), float(fx["C11"])))
+                         elastic_override=(float(fx["C44"]), float(fx["C12"]), float(fx["C11"])),
+                         usfe_fit=tuple(fx["usfe_fit"]) if "usfe_fit" in fx else None)
     w = configs.Workload(name, int(fx["nx"]), int(fx["ny"]), int(fx["nz"]), str(fx["app"]), fx["xn"], fx["xb"],
                          fx["four"], fx["prim"], m, int(fx["core_flag"]), fx["sigma"], float(fx["cd_dt"]),
                          fx["xi0"], xo=fx.get("xo"), site=fx.get("site"), dsigma=fx["dsigma"],
-                         core_extra={"c": fx["c"], "aa": fx["aa"], "bb": fx["bb"]})
+                         core_extra={"c": fx["c"], "aa": fx["aa"], "bb": fx["bb"]},
+                         non_schmid=tuple(fx["non_schmid"]) if "non_schmid" in fx else None)
     return w, fx
 
 
@@ -57,8 +67,7 @@ def oracle_run_golden(w, fx):
     sig = np.array(fx["sigma"], dtype=float)
     norms, aves = [], []
     for _ in range(int(fx["stress_states"])):
-        w2 = configs.Workload(w.name, w.nx, w.ny, w.nz, w.app, w.xn, w.xb, w.four, w.prim, w.material, w.core_flag,
-                              sig.copy(), w.cd_dt, w.xi0, xo=w.xo, site=w.site, core_extra=w.core_extra)
+        w2 = dataclasses.replace(w, sigma=sig.copy())
         xi, n, a = O.run(oracle_instance(w2), xi, int(fx["steps"]))
         norms += list(n)
         aves += list(a)

@@ -79,6 +79,14 @@ def case_ramp():
     return w, 2, {"stress_states": 3}
 
 
+def case_bcc_non_schmid():
+    # Ta, one BCC system, non-Schmid tau and the USFE(angle, tau) core over a
+    # ramp of sigma_yz: the core amplitude changes with every stress state
+    w = C.bcc_screw_workload(n=16, nz=8, core_flag=6)
+    w.dsigma = C._sigma("yz", 4e-3)
+    return w, 3, {"stress_states": 3}
+
+
 CASES = {
     "loop_sine": case_loop_sine,
     "fcc12_sine": case_fcc12_sine,
@@ -88,6 +96,7 @@ CASES = {
     "fcc12_extended": case_fcc12_extended,
     "pyrII": case_pyrII,
     "ramp": case_ramp,
+    "bcc_non_schmid": case_bcc_non_schmid,
 }
 
 
@@ -110,6 +119,10 @@ def run_case(name):
         out["xo"] = w.xo
     if w.site is not None:
         out["site"] = w.site
+    if w.non_schmid is not None:
+        out["non_schmid"] = np.asarray(su["non_schmid"][1])
+    if w.core_flag == 6:
+        out["usfe_fit"] = np.asarray(su["usfe_fit"])
     return out
 
 

@@ -124,3 +124,21 @@ def test_energy_gradient_is_the_drift():
         (xn, _, _, _), = [(*s,) for s in [st.advance(1)[0]]]
         e2 = sum(st.energy(0))
     assert e2 < e0
+
+
+def test_two_live_handles_of_different_sizes():
+    """A handle created for a small grid while a large-grid handle is alive
+    leaves the large one's kernels launchable (per-kernel shared-memory limits
+    are process-wide and only ever raised)."""
+    big = configs.loop_workload(n=32, radius=6.0, seed=2, sigma_mpa=350.0)
+    small = configs.bcc_screw_workload(n=16, nz=8, core_flag=6)
+    with capi.Stepper.from_workloads([big], precision=capi.FP64) as sa:
+        sa.set_state(0, big.xi0)
+        with capi.Stepper.from_workloads([small], precision=capi.FP64) as sb:
+            sb.set_state(0, small.xi0)
+            sb.advance(2)
+            sa.advance(3)
+            re, im = sa.get_state(0)
+    ref, _, _ = O.run(oracle_instance(big), big.xi0, 3)
+    assert np.abs(re - ref.real).max() <= 1e-10
+    assert np.abs(im - ref.imag).max() <= 1e-10

@@ -97,3 +97,40 @@ def test_bcc_perfect_core_equals_reference(make):
     xi, nrm, ave = O.run(oracle_instance(w), w.xi0, 4)
     assert np.abs(xi - r["xi"]).max() <= 1e-12
     np.testing.assert_allclose(nrm, r["xinorm"], rtol=1e-10)
+
+
+@needs_ref
+@pytest.mark.parametrize("flag", [1, 6])
+def test_non_schmid_and_usfe_angle_tau_equal_reference(flag):
+    """resolSS_non_Schmid (the projections on the MRSSP at angle_to_110 and
+    the plane 60 degrees from it, weights w1..w3) with the perfect core and
+    with the USFE(angle, tau) core whose amplitude follows sigma_rot[2][1]."""
+    w = configs.bcc_screw_workload(n=16, nz=8, core_flag=flag)
+    r = ref_runner.run_reference(w, 4)
+    su = r["setup"]
+    assert su["non_schmid"][0] == 1
+    np.testing.assert_array_equal(su["non_schmid"][1], w.non_schmid)
+    np.testing.assert_array_equal(su["usfe_fit"], configs.TA_USFE_FIT)
+    inst = oracle_instance(w)
+    np.testing.assert_allclose(inst.tau, su["tau"], rtol=1e-13)
+    sr = O.rotate_stress(w.sigma, w.prim, np.linalg.inv(w.prim), 1.0)
+    schmid = O.resolved_shear(sr, w.xn, w.xb, w.material.dslip)
+    assert abs(schmid[0] - inst.tau[0]) > 0.1 * abs(schmid[0])
+    xi, nrm, ave = O.run(inst, w.xi0, 4)
+    assert np.abs(xi - r["xi"]).max() <= 1e-12
+    np.testing.assert_allclose(nrm, r["xinorm"], rtol=1e-11)
+    np.testing.assert_allclose(ave, r["xiave"], rtol=1e-11)
+
+
+@needs_ref
+def test_usfe_angle_tau_follows_each_stress_state():
+    """Core model 6 over three stress states of a sigma_yz ramp: the amplitude
+    is re-evaluated from each state's sigma_rot[2][1]."""
+    from common import oracle_run_golden
+    w = configs.bcc_screw_workload(n=12, nz=8, core_flag=6, seed=4, angle=-15.0)
+    w.dsigma = configs._sigma("yz", 6e-3)
+    r = ref_runner.run_reference(w, 2, stress_states=3)
+    xi, nrm, ave = oracle_run_golden(w, {"xi0": w.xi0, "sigma": w.sigma, "dsigma": w.dsigma,
+                                         "stress_states": 3, "steps": 2})
+    assert np.abs(xi - r["xi"]).max() <= 1e-12
+    np.testing.assert_allclose(ave, r["xiave"], rtol=1e-11)

@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from common import small_loop
-from pfdd_b200 import capi
+from pfdd_b200 import capi, configs
 
 pytestmark = pytest.mark.gpu
 
@@ -34,13 +34,15 @@ def _handle_steps(w, xi0, n):
     return out
 
 
-def test_noalloc_matches_handle_path_two_calls():
+@pytest.mark.parametrize("make", ["loop", "bcc_non_schmid"])
+def test_noalloc_matches_handle_path_two_calls(make):
     import torch
     lib = capi.load()
     lib.pfdd_gl_step_noalloc.argtypes = [ctypes.POINTER(capi.InstanceDesc), ctypes.c_void_p, ctypes.c_void_p,
                                          capi.DP, ctypes.c_void_p]
     lib.pfdd_gl_step_noalloc.restype = ctypes.c_int
-    w = small_loop(32)
+    # the second deck: non-Schmid tau and the USFE(angle, tau) core (model 6)
+    w = small_loop(32) if make == "loop" else configs.bcc_screw_workload(n=16, nz=8, core_flag=6)
     rng = np.random.default_rng(17)
     xi0 = w.xi0 + 1j * rng.uniform(-1e-3, 1e-3, size=w.xi0.shape)
     expect = _handle_steps(w, xi0, 2)
