@@ -199,6 +199,17 @@ pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_
 pfdd_status pfdd_gpu_strain_stress(pfdd_gpu *h, int inst, double *eps, double *sigma, double *ave_eps,
                                    double *ave_sigma);
 
+/* FFTW_Slab::project_core_energy (src/fft_fftw_slab.cpp:1550-1624; called
+ * after each GL iteration when non_Schmid is set, src/solve_GL.cpp:121-122)
+ * on instance `inst`'s current state.  delta ([n_planes*N], z-fastest site
+ * order) receives Re xi_p for one or two slip systems, else the projection
+ * sum_c (Re xi_3p b_0c + Re xi_3p+1 b_1c + Re xi_3p+2 b_2c) b_1c.  ddelta
+ * ([n_planes*nx] or NULL) receives the forward difference along x of delta on
+ * the line j = ny/2, k = nz/2, zero at the last x (dx = 1, one rank).
+ * n_planes is App::num_planes: at most n_slip for one or two systems, at most
+ * n_slip/3 otherwise (beyond that the reference reads past its array). */
+pfdd_status pfdd_gpu_core_profile(pfdd_gpu *h, int inst, int n_planes, double *delta, double *ddelta);
+
 /* No counterpart in the reference (a hand-written adjoint of the GL step).
  * Gradient of J = sum over sites and systems of (Re xi_N - target)^2, where
  * xi_N is instance `inst` after n_steps GL iterations from its current state

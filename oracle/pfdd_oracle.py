@@ -168,6 +168,32 @@ def usfe_angle_tau(sigma_rot, mu, fit, angle_to_110):
     return gsfe * 1.0E-3
 
 
+def core_profile(xr, xb, n_planes):
+    """project_core_energy (fft_fftw_slab.cpp:1550-1624) on Re xi [S, nx, ny, nz]:
+    delta_p = Re xi_p for one or two systems, else the projection
+    sum_c (xi_3p b_0c + xi_3p+1 b_1c + xi_3p+2 b_2c) b_1c (the reference reads
+    systems 3p..3p+2 with the Burgers vectors of systems 0..2; planes with
+    3p + 2 >= S read past its array and are not defined).  ddelta_p is the
+    forward difference along x on the line j = ny/2, k = nz/2 (dx = 1, zero at
+    the last x of a single-rank run).  Returns delta [NP, nx, ny, nz], ddelta [NP, nx]."""
+    xr = np.asarray(xr, float)
+    xb = np.asarray(xb, float)
+    S, nx, ny, nz = xr.shape
+    delta = np.zeros((n_planes, nx, ny, nz))
+    for p in range(n_planes):
+        if S <= 2:
+            delta[p] = xr[p]
+        else:
+            x0, x1, x2 = xr[3 * p], xr[3 * p + 1], xr[3 * p + 2]
+            delta[p] = ((x0 * xb[0, 0] + x1 * xb[1, 0] + x2 * xb[2, 0]) * xb[1, 0]
+                        + (x0 * xb[0, 1] + x1 * xb[1, 1] + x2 * xb[2, 1]) * xb[1, 1]
+                        + (x0 * xb[0, 2] + x1 * xb[1, 2] + x2 * xb[2, 2]) * xb[1, 2])
+    line = delta[:, :, ny // 2, nz // 2]
+    ddelta = np.zeros((n_planes, nx))
+    ddelta[:, :-1] = (line[:, 1:] - line[:, :-1]) / 1.0
+    return delta, ddelta
+
+
 # ---------------------------------------------------------------- strain / stress diagnostics
 def strain_stress(nx, ny, nz, four, xn, xb, dslip, C44, C12, C11, sigma_rot, xi):
     """The reference's strain and stress diagnostics of state xi, computed as

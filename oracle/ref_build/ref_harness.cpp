@@ -4,7 +4,7 @@
 //
 //   pfdd_ref_harness -deck in.deck [-steps N] [-state_in xi0.bin] [-xo_in xo.bin]
 //       [-mpea_in a.bin] [-set key value]... [-state_out xi.bin] [-stats_out s.txt]
-//       [-setup_out setup.txt] [-B_out bb.bin] [-stress_out st.bin] [-timing]
+//       [-setup_out setup.txt] [-B_out bb.bin] [-stress_out st.bin] [-profile_out pr.bin] [-timing]
 //
 // Sequence (mirrors App::run, app.cpp:127-205, with the `run` command taken
 // out of the deck so state can be injected between init and setup):
@@ -115,7 +115,7 @@ static double *material_field(Material *m, const std::string &k) {
 int main(int argc, char **argv) {
   const char *deck = nullptr, *state_in = nullptr, *xo_in = nullptr, *mpea_in = nullptr;
   const char *state_out = nullptr, *stats_out = nullptr, *setup_out = nullptr, *B_out = nullptr,
-             *stress_out = nullptr;
+             *stress_out = nullptr, *profile_out = nullptr;
   long steps_override = -1;
   bool timing = false;
   std::vector<std::pair<std::string, double>> sets;
@@ -134,6 +134,7 @@ int main(int argc, char **argv) {
     else if (a == "-setup_out") { need(1); setup_out = argv[++i]; }
     else if (a == "-B_out") { need(1); B_out = argv[++i]; }
     else if (a == "-stress_out") { need(1); stress_out = argv[++i]; }
+    else if (a == "-profile_out") { need(1); profile_out = argv[++i]; }
     else if (a == "-set") { need(2); sets.emplace_back(argv[i + 1], atof(argv[i + 2])); i += 2; }
     else if (a == "-timing") { timing = true; }
     else { fprintf(stderr, "harness: unknown option %s\n", a.c_str()); return 2; }
@@ -279,6 +280,21 @@ int main(int argc, char **argv) {
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) out.push_back(fft->avepst[i][j]);
     write_bin(stress_out, out.data(), out.size());
+  }
+  if (profile_out) {
+    // FFTW_Slab::project_core_energy on the final state (data_fftw = xi after
+    // prepare_next_itr): num_planes, delta [NP*N], then ddelta on the
+    // j = ny/2, k = nz/2 line of each plane [NP*nx]
+    fft->project_core_energy();
+    const int NP = app->num_planes;
+    const int n2 = fft->local_y, n3 = fft->local_z;
+    std::vector<double> out;
+    out.push_back((double)NP);
+    out.insert(out.end(), fft->delta, fft->delta + (size_t)NP * N);
+    for (int p = 0; p < NP; ++p)
+      for (int i = 0; i < fft->nx; ++i)
+        out.push_back(fft->ddelta[(size_t)p * N + (size_t)i * n2 * n3 + (size_t)(n2 / 2) * n3 + n3 / 2]);
+    write_bin(profile_out, out.data(), out.size());
   }
   if (stats_out) {
     FILE *f = fopen(stats_out, "w");

@@ -57,12 +57,15 @@ def _raise_stack():
 
 
 def run_reference(workload, steps, state=None, xo=None, mpea=None, sets=(), want_B=False,
-                  timing=False, workdir=None, timeout=3600, set_b=True, stress_states=None, want_stress=False):
+                  timing=False, workdir=None, timeout=3600, set_b=True, stress_states=None, want_stress=False,
+                  want_profile=False):
     """Run `steps` GL iterations of the reference on `workload`.
 
     state: complex or real array [S, nx, ny, nz] (default workload.xi0).
     Returns dict with xi (complex [S,nx,ny,nz]), xinorm, xiave, setup, and
-    optionally BB [S,S,nx,ny,nz], the timing record and (want_stress) the
+    optionally BB [S,S,nx,ny,nz], the timing record, (want_profile) the
+    project_core_energy arrays delta [NP,nx,ny,nz] and the ddelta line [NP,nx]
+    at j = ny/2, k = nz/2 of the final state, and (want_stress) the
     strain/stress diagnostics of the final state: eps and sigma [3,3,nx,ny,nz]
     complex (data_eps, data_sigma), ave_eps, ave_sigma, avepst [3,3].
     """
@@ -72,7 +75,7 @@ def run_reference(workload, steps, state=None, xo=None, mpea=None, sets=(), want
     tmp = workdir or tempfile.mkdtemp(prefix="pfdd_ref_")
     try:
         return _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, set_b, stress_states,
-                    want_stress)
+                    want_stress, want_profile)
     finally:
         if own_tmp:
             import shutil
@@ -80,7 +83,7 @@ def run_reference(workload, steps, state=None, xo=None, mpea=None, sets=(), want
 
 
 def _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, set_b, stress_states,
-         want_stress=False):
+         want_stress=False, want_profile=False):
     S, nx, ny, nz = workload.S, workload.nx, workload.ny, workload.nz
     deck = os.path.join(tmp, "in.deck")
     with open(deck, "w") as f:
@@ -112,6 +115,8 @@ def _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, s
         args += ["-B_out", os.path.join(tmp, "B.bin")]
     if want_stress:
         args += ["-stress_out", os.path.join(tmp, "stress.bin")]
+    if want_profile:
+        args += ["-profile_out", os.path.join(tmp, "profile.bin")]
     if timing:
         args += ["-timing"]
     env = dict(os.environ)
@@ -141,6 +146,12 @@ def _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, s
         out["ave_eps"] = raw[2 * n:2 * n + 9].reshape(3, 3)
         out["ave_sigma"] = raw[2 * n + 9:2 * n + 18].reshape(3, 3)
         out["avepst"] = raw[2 * n + 18:2 * n + 27].reshape(3, 3)
+    if want_profile:
+        raw = np.fromfile(os.path.join(tmp, "profile.bin"))
+        NP = int(raw[0])
+        n = nx * ny * nz
+        out["delta"] = raw[1:1 + NP * n].reshape(NP, nx, ny, nz)
+        out["ddelta"] = raw[1 + NP * n:1 + NP * n + NP * nx].reshape(NP, nx)
     if timing:
         import json
         for line in proc.stdout.splitlines()[::-1]:

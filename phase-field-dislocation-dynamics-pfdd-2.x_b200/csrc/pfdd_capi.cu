@@ -1550,6 +1550,42 @@ pfdd_status pfdd_gpu_strain_stress(pfdd_gpu *h, int inst, double *eps, double *s
                                    : strain_stress_impl<float>(h, *h->inst[inst], eps, sigma, ave_eps, ave_sigma);
 }
 
+pfdd_status pfdd_gpu_core_profile(pfdd_gpu *h, int inst, int n_planes, double *delta, double *ddelta) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  Instance &I = *h->inst[inst];
+  if (!delta || n_planes < 1 || (I.S <= 2 ? n_planes > I.S : 3 * n_planes > I.S))
+    return fail(h, PFDD_EINVAL, "need delta and 1 <= n_planes <= %d", I.S <= 2 ? I.S : I.S / 3);
+  cudaSetDevice(h->device);
+  cudaStream_t st = h->stream;
+  const size_t n = (size_t)n_planes * I.N;
+  DevBuf out;
+  CUDA_TRY(h, out.alloc(n * sizeof(double)));
+  ProfileArgs pa;
+  memset(&pa, 0, sizeof pa);
+  for (int a = 0; a < 3 && a < I.S; ++a)
+    for (int c = 0; c < 3; ++c) pa.xb[a][c] = I.d.xb[a][c];
+  const int blocks = 4 * h->nsm;
+  if (h->precision == PFDD_FP64)
+    k_core_profile<double><<<blocks, 256, 0, st>>>(I.xi[I.cur].as<double>(), I.S, I.N, n_planes, pa, out.as<double>());
+  else
+    k_core_profile<float><<<blocks, 256, 0, st>>>(I.xi[I.cur].as<float>(), I.S, I.N, n_planes, pa, out.as<double>());
+  CUDA_TRY(h, cudaGetLastError());
+  CUDA_TRY(h, cudaMemcpyAsync(delta, out.p, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  if (ddelta) {
+    // the line j = ny/2, k = nz/2: forward difference with dx = nx/nx = 1 (fft_fftw_slab.cpp:1597-1620)
+    const size_t line = (size_t)(I.ny / 2) * I.nz + I.nz / 2, sx = (size_t)I.ny * I.nz;
+    for (int p = 0; p < n_planes; ++p)
+      for (int i = 0; i < I.nx; ++i) {
+        const double *d = delta + (size_t)p * I.N + line;
+        const double here = d[(size_t)i * sx], next = (i + 1 < I.nx) ? d[(size_t)(i + 1) * sx] : here;
+        ddelta[(size_t)p * I.nx + i] = (next - here) / 1.0;
+      }
+  }
+  return PFDD_OK;
+}
+
 pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every, const double *xi_target,
                              double *loss, double *dL_dparams, double *dL_dsigma) {
   if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");

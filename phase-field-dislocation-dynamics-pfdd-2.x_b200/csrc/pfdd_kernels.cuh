@@ -1539,6 +1539,34 @@ static __global__ void k_finalize_tab(const InstPtrs *__restrict__ tab, int npar
 // sigma_rot and tau in FP64 exactly as rotate_stress + resolSS_Schmid
 // (fft_fftw_slab.cpp:242-274, 737-769); then optionally sigma += dsigma
 // (solve_GL.cpp:151-155) and clear the stop flag.
+// project_core_energy (fft_fftw_slab.cpp:1572-1595): delta of planes 0..np-1
+// in FP64, Re xi_p for S <= 2, else the projection of systems 3p..3p+2 on b_1
+// in the reference's order of operations.
+struct ProfileArgs {
+  double xb[3][3];
+};
+
+template <typename T>
+static __global__ void k_core_profile(const T *__restrict__ xi, int S, size_t N, int np, ProfileArgs pa,
+                                      double *__restrict__ delta) {
+  const size_t total = (size_t)np * N;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t p = q / N, r = q - p * N;
+    if (S <= 2) {
+      delta[q] = (double)xi[q];
+    } else {
+      const double x0 = (double)xi[(3 * p) * N + r], x1 = (double)xi[(3 * p + 1) * N + r],
+                   x2 = (double)xi[(3 * p + 2) * N + r];
+      double v = 0.0;
+      for (int c = 0; c < 3; ++c)
+        v = __dadd_rn(v, __dmul_rn(__dadd_rn(__dadd_rn(__dmul_rn(x0, pa.xb[0][c]), __dmul_rn(x1, pa.xb[1][c])),
+                                             __dmul_rn(x2, pa.xb[2][c])),
+                                   pa.xb[1][c]));
+      delta[q] = v;
+    }
+  }
+}
+
 struct StressArgs {
   double prim[3][3], invprim[3][3];
   int ortho;

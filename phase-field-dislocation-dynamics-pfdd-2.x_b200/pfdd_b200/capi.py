@@ -31,6 +31,7 @@ EXPORTS = [
     "pfdd_gpu_get_state_interleaved", "pfdd_gpu_advance", "pfdd_gpu_step_history", "pfdd_gpu_energy",
     "pfdd_gpu_tau", "pfdd_gpu_info", "pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version",
     "pfdd_gpu_set_stream", "pfdd_gpu_profile", "pfdd_gpu_adjoint", "pfdd_gpu_strain_stress",
+    "pfdd_gpu_core_profile",
 ]
 KERNELS = ["fwd_planes", "xpencil", "step_planes", "finalize"]
 
@@ -94,6 +95,7 @@ def load(path: str = LIB_PATH):
     lib.pfdd_gpu_step_history.argtypes = [vp, ctypes.c_int, DP, DP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.pfdd_gpu_energy.argtypes = [vp, ctypes.c_int, DP, DP, DP]
     lib.pfdd_gpu_strain_stress.argtypes = [vp, ctypes.c_int, DP, DP, DP, DP]
+    lib.pfdd_gpu_core_profile.argtypes = [vp, ctypes.c_int, ctypes.c_int, DP, DP]
     lib.pfdd_gpu_tau.argtypes = [vp, ctypes.c_int, DP]
     lib.pfdd_gpu_adjoint.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, DP, DP, DP, DP]
     lib.pfdd_gpu_set_stream.argtypes = [vp, vp]
@@ -228,6 +230,15 @@ class Stepper:
         e = np.empty(3)
         self._check(self._lib.pfdd_gpu_energy(self.h, inst, _dp(e[0:1]), _dp(e[1:2]), _dp(e[2:3])))
         return tuple(e)
+
+    def core_profile(self, inst, n_planes):
+        """project_core_energy of the current state: delta [n_planes, nx, ny, nz]
+        and the ddelta line [n_planes, nx] at j = ny/2, k = nz/2."""
+        nx, ny, nz = self._dims[inst]
+        d = np.zeros(n_planes * nx * ny * nz)
+        dd = np.zeros(n_planes * nx)
+        self._check(self._lib.pfdd_gpu_core_profile(self.h, inst, n_planes, _dp(d), _dp(dd)))
+        return d.reshape(n_planes, nx, ny, nz), dd.reshape(n_planes, nx)
 
     def strain_stress(self, inst, fields=True):
         """Strain and stress of the current state (the reference's data_eps /

@@ -94,3 +94,26 @@ def test_adjoint_stress_gradient_non_schmid_usfe():
     for c in (4, 5):   # sigma_xz, sigma_yz (sigma_yz moves the amplitude)
         fd = (_loss_oracle(w, target, c, h) - _loss_oracle(w, target, c, -h)) / (2 * h)
         assert abs(ds[c] - fd) <= 2e-6 * abs(fd), (c, ds[c], fd)
+
+
+@pytest.mark.parametrize("make,planes", [("bcc", 1), ("frank_read", 2), ("fcc", 4)])
+def test_core_profile_matches_oracle(make, planes):
+    """pfdd_gpu_core_profile (project_core_energy) after 4 steps: Re xi for
+    one and two systems, the projection on b_1 for twelve FCC systems."""
+    if make == "bcc":
+        w = configs.bcc_screw_workload(n=16, nz=8, core_flag=6)
+    elif make == "frank_read":
+        w = configs.frank_read_workload(nx=16, ny=16, nz=8, seg=4)
+        w.non_schmid = (5.0, 0.1, 0.2, 0.3)
+    else:
+        w = configs.fcc_workload(16, 12, 8, n_loops=3, seed=5)
+    xi, _, _ = O.run(oracle_instance(w), w.xi0, 4)
+    d_ref, dd_ref = O.core_profile(xi.real, w.xb, planes)
+    for prec, tol in ((capi.FP64, 1e-10), (capi.FP32, 2e-4)):
+        with capi.Stepper.from_workloads([w], precision=prec) as st:
+            st.set_state(0, w.xi0)
+            st.advance(4)
+            d, dd = st.core_profile(0, planes)
+        scale = max(1.0, np.abs(d_ref).max())
+        assert np.abs(d - d_ref).max() <= tol * scale
+        assert np.abs(dd - dd_ref).max() <= 2 * tol * scale

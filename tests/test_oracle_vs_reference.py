@@ -134,3 +134,21 @@ def test_usfe_angle_tau_follows_each_stress_state():
                                          "stress_states": 3, "steps": 2})
     assert np.abs(xi - r["xi"]).max() <= 1e-12
     np.testing.assert_allclose(ave, r["xiave"], rtol=1e-11)
+
+
+@needs_ref
+@pytest.mark.parametrize("make", ["bcc", "frank_read"])
+def test_core_profile_equals_reference(make):
+    """project_core_energy (delta and the ddelta line) of the state after
+    three steps, for one system (app 1SBCC) and two (Frank-Read, 60-degree grid)."""
+    if make == "bcc":
+        w = configs.bcc_screw_workload(n=16, nz=8, core_flag=1)
+    else:
+        w = configs.frank_read_workload(nx=16, ny=16, nz=8, seg=4)
+        w.non_schmid = (5.0, 0.1, 0.2, 0.3)
+    r = ref_runner.run_reference(w, 3, want_profile=True)
+    xi, _, _ = O.run(oracle_instance(w), w.xi0, 3)
+    np.testing.assert_allclose(xi, r["xi"], rtol=0, atol=1e-12)
+    d, dd = O.core_profile(xi.real, w.xb, r["delta"].shape[0])
+    assert np.abs(d - r["delta"]).max() <= 1e-12
+    assert np.abs(dd - r["ddelta"]).max() <= 1e-12
