@@ -210,6 +210,65 @@ pfdd_status pfdd_gpu_strain_stress(pfdd_gpu *h, int inst, double *eps, double *s
  * n_slip/3 otherwise (beyond that the reference reads past its array). */
 pfdd_status pfdd_gpu_core_profile(pfdd_gpu *h, int inst, int n_planes, double *delta, double *ddelta);
 
+/* ---- Conductivity sub-problem (SolveGLCond, src/solve_GL+cond.cpp:70-150) ----
+ * A complex scalar order parameter condxi relaxed by its own GL iteration:
+ * forwardcond, divcurrent (a = i k_y/k^2 c, b = k_y^2/k^2 c),
+ * backwardcond (unnormalised inverse transforms of a and b, then
+ * j_y = sigma(y) (E_y - a/eps0) and the assembly of the driving term with
+ * the y-derivative of the layer conductivity) and update_conduct_order_param
+ * (src/fft_fftw_slab.cpp:1699-1741, 1795-1834, 1999-2186).  It reads none of
+ * the dislocation fields.  SolveGLCond's loop leaves after its first
+ * iteration in every stress state (the `break` after the unbraced `if` at
+ * src/solve_GL+cond.cpp:132-140), so a binding calls pfdd_gpu_cond_step with
+ * n_iters = 1 once per stress state, beside pfdd_gpu_advance(h, 1, 1, ...). */
+
+/* Members of one layer material (Material, src/material.h:44-56). */
+typedef struct {
+  double condsigma;          /* S/m at 300 K */
+  double alpha_resistivity;  /* 1/K */
+  double mfpel;              /* electron mean free path, m */
+  double alpha_mfpel;        /* 1/K */
+  double dlayer;             /* layer thickness, m */
+  double Rgrain;             /* grain-boundary reflection */
+  double beta_disloc;        /* resistivity per dislocation density, Ohm m^3 */
+  double rho_disloc;         /* dislocation density, 1/m^2 */
+  int Ngrains;               /* grains per layer */
+  int Nlayers;               /* read from material A only */
+  double pinterface;         /* read from material A only */
+} pfdd_cond_material;
+
+/* The per-y conductivity backwardcond builds (src/fft_fftw_slab.cpp:2064-2156):
+ * A and B layers alternate along y (A.Nlayers periods of thicknesses from the
+ * dlayer volume fraction, with the reference's integer division of ny by
+ * Nlayers); sigma_layer[ny] is the temperature-corrected layer conductivity,
+ * sigma_eff[ny] adds interface, grain-boundary and dislocation resistivity.
+ * Host-only; PFDD_EINVAL when the layer period rounds to zero cells. */
+pfdd_status pfdd_cond_layers(const pfdd_cond_material *A, const pfdd_cond_material *B, int ny,
+                             double temperature, double *sigma_eff, double *sigma_layer);
+
+typedef struct {
+  const double *sigma_eff;     /* [ny], copied */
+  const double *sigma_layer;   /* [ny], copied (needs ny >= 2) */
+  double El_y;                 /* Material::El[1] of material A, V/m */
+  double epsilonzero;          /* Material::epsilonzero */
+  double timestep;             /* App::timestep (the update uses 1e-22 * timestep) */
+} pfdd_cond_desc;
+
+typedef struct {
+  double condxinorm;    /* FFT::condxinorm of the iteration */
+  double condxiave;     /* FFT::condxiave */
+  double conductivity;  /* <j_y> / El_y of the iteration's backwardcond */
+} pfdd_cond_stats;
+
+/* Give instance `inst` a conductivity field (condxi = 0, FFTW_Slab::allocate
+ * :162-173) on its grid; calling it again replaces the tables and zeroes condxi. */
+pfdd_status pfdd_gpu_cond_enable(pfdd_gpu *h, int inst, const pfdd_cond_desc *d);
+/* condxi from / to host planes [N] each (im may be NULL = 0 on set, skipped on get). */
+pfdd_status pfdd_gpu_cond_set_state(pfdd_gpu *h, int inst, const double *re, const double *im);
+pfdd_status pfdd_gpu_cond_get_state(pfdd_gpu *h, int inst, double *re, double *im);
+/* n_iters iterations of the conductivity sub-problem; stats[n_iters] or NULL. */
+pfdd_status pfdd_gpu_cond_step(pfdd_gpu *h, int inst, int n_iters, pfdd_cond_stats *stats);
+
 /* No counterpart in the reference (a hand-written adjoint of the GL step).
  * Gradient of J = sum over sites and systems of (Re xi_N - target)^2, where
  * xi_N is instance `inst` after n_steps GL iterations from its current state

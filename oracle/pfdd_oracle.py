@@ -504,3 +504,115 @@ def total_energy(inst: Instance, xi: np.ndarray):
     core = float(np.sum(inst.core.energy_density(xr)))
     app = -float(np.sum(inst.tau[:, None, None, None] * xr))
     return el, core, app
+
+
+# ---------------------------------------------------------------- conductivity sub-problem
+@dataclass
+class CondMaterial:
+    """Material members the conductivity solver reads (material.h:44-56, the
+    preset values of material.cpp:260-275 and siblings, deck keywords
+    material.cpp:98-135)."""
+    condsigma: float
+    alpha_resistivity: float = 0.0
+    mfpel: float = 1e-9
+    alpha_mfpel: float = 0.0
+    dlayer: float = 100e-9
+    Rgrain: float = 0.0
+    beta_disloc: float = 0.0
+    rho_disloc: float = 0.0
+    Ngrains: int = 1
+    Nlayers: int = 1
+    pinterface: float = 0.5
+
+
+def cond_layers(A: CondMaterial, B: CondMaterial, ny: int, temperature: float):
+    """Per-y conductivity of FFTW_Slab::backwardcond (fft_fftw_slab.cpp:2064-2156):
+    alternating A/B layers along y (A.Nlayers periods, thicknesses from the
+    dlayer volume fraction, integer division of ny by Nlayers as the reference
+    does), temperature-corrected layer conductivity sigma_layer and the
+    effective sigma_eff with interface, grain-boundary and dislocation
+    resistivities.  Returns sigma_eff [ny], sigma_layer [ny]."""
+    Vf = B.dlayer / (A.dlayer + B.dlayer)
+    Nl = int(A.Nlayers)
+    prob = 1.0 - A.pinterface
+    per = ny // Nl
+    dB = int(round(per * Vf))
+    dA = int(round(per * (1.0 - Vf)))
+    dT = temperature - 300
+    eff = np.zeros(ny)
+    lay = np.zeros(ny)
+    for j in range(ny):
+        M = B if (j % (dA + dB)) >= dA else A
+        lay[j] = M.condsigma / (1.0 + M.alpha_resistivity * dT)
+        ps = 2 * prob / M.dlayer
+        lam = M.mfpel / (1.0 + M.alpha_mfpel * dT)
+        ag = (lam * M.Ngrains / M.dlayer) * M.Rgrain / (1 - M.Rgrain)
+        rd = M.beta_disloc * M.rho_disloc
+        if ps > 0.0:
+            ri = (1 / lay[j]) * ((3.0 / 16.0) * lam * ps)
+            if M.Ngrains > 1:
+                rg = (1 / lay[j]) * (1.0 / (1.0 - 3.0 * ag / 2.0 + 3.0 * ag * ag
+                                          - 3.0 * ag ** 3.0 * math.log(1.0 + 1.0 / ag)) - 1.0)
+                eff[j] = 1 / ((1 / lay[j]) + (2 * ri + (M.Ngrains - 1) * rg) / (M.Ngrains + 1) + rd)
+            else:
+                eff[j] = 1 / ((1 / lay[j]) + ri + rd)
+        else:
+            eff[j] = lay[j]
+    return eff, lay
+
+
+def cond_fields(condxi, four, sigma_eff, El_y, epsilonzero):
+    """forwardcond + divcurrent + backwardcond's transforms and current
+    (fft_fftw_slab.cpp:1699-1741, 2157-2168): the unnormalised inverse
+    transforms a = IFFT(i k_y/k^2 c), b = IFFT(k_y^2/k^2 c), the current
+    j = sigma_eff(y) (E_y - a/eps0) (complex, as jcurrent) and <j_y>/E_y."""
+    c = np.asarray(condxi, dtype=np.complex128)
+    nx, ny, nz = c.shape
+    N = nx * ny * nz
+    fx, fy, fz = frequencies(nx, ny, nz, four)
+    k2 = fx * fx + fy * fy + fz * fz
+    ch = np.fft.fftn(c)
+    pos = k2 > 0.0
+    safe = np.where(pos, k2, 1.0)
+    jre = np.where(pos, 0.0 - ch.imag * fy / safe, 0.0)
+    jim = np.where(pos, 0.0 + ch.real * fy / safe, 0.0)
+    bre = np.where(pos, 0.0 + ch.real * fy * fy / safe, 0.0)
+    bim = np.where(pos, 0.0 + ch.imag * fy * fy / safe, 0.0)
+    a = np.fft.ifftn(jre + 1j * jim) * N
+    b = np.fft.ifftn(bre + 1j * bim) * N
+    cs = np.asarray(sigma_eff)[None, :, None]
+    j = cs * (El_y - a.real / epsilonzero) + 1j * (-cs * a.imag / epsilonzero)
+    return a, b, j, float(np.sum(j.real / N)) / El_y
+
+
+def cond_step(condxi, four, sigma_eff, sigma_layer, El_y, epsilonzero, timestep):
+    """One iteration of the conductivity order parameter as SolveGLCond runs it
+    (solve_GL+cond.cpp:96-122): forwardcond, divcurrent (fft_fftw_slab.cpp:1699-1741:
+    a = i k_y/k^2 c, b = k_y^2/k^2 c, zero at k = 0), backwardcond's two
+    unnormalised inverse transforms and real-space assembly (:2157-2186), and
+    update_conduct_order_param (:1795-1834).  Returns the new condxi, condxinorm,
+    condxiave and the conductivity <j_y>/El_y of that backwardcond.
+
+    The y-derivative of the layer conductivity is taken on the finished
+    profile, (s[j+1] - s[j-1])/2 inside and one-sided at the ends.  The
+    reference reads s[j+1] of its stack array before its loop writes it
+    (:2108 vs :2176-2181), so its driving term, and condxi from the first
+    update on, are undefined; a, b, j and the conductivity of a given state
+    are defined and pinned (cond_fields)."""
+    c = np.asarray(condxi, dtype=np.complex128)
+    nx, ny, nz = c.shape
+    N = nx * ny * nz
+    jr, br, _, cond = cond_fields(c, four, sigma_eff, El_y, epsilonzero)
+    cs = np.asarray(sigma_eff)[None, :, None]
+    lay = np.asarray(sigma_layer)
+    d = np.empty(ny)
+    d[0] = lay[1] - lay[0]
+    d[-1] = lay[-1] - lay[-2]
+    d[1:-1] = (lay[2:] - lay[:-2]) / 2.0
+    d = d[None, :, None]
+    cre = (cs / epsilonzero) * br.real + (jr.real / epsilonzero - El_y) * d
+    cim = (cs / epsilonzero) * br.imag + (jr.imag / epsilonzero) * d
+    new = (c.real - (1e-22 * timestep * (cre / N))) + 1j * (c.imag - (1e-22 * timestep * (cim / N)))
+    dn = new - c
+    norm = math.sqrt(float(np.sum(dn.real ** 2 + dn.imag ** 2)))
+    return new, norm, float(np.sum(new.real)), cond

@@ -5,6 +5,7 @@
 //   pfdd_ref_harness -deck in.deck [-steps N] [-state_in xi0.bin] [-xo_in xo.bin]
 //       [-mpea_in a.bin] [-set key value]... [-state_out xi.bin] [-stats_out s.txt]
 //       [-setup_out setup.txt] [-B_out bb.bin] [-stress_out st.bin] [-profile_out pr.bin] [-timing]
+//       [-cond_steps n -cond_out cond.bin [-cond_in c0.bin]]
 //
 // Sequence (mirrors App::run, app.cpp:127-205, with the `run` command taken
 // out of the deck so state can be injected between init and setup):
@@ -115,7 +116,8 @@ static double *material_field(Material *m, const std::string &k) {
 int main(int argc, char **argv) {
   const char *deck = nullptr, *state_in = nullptr, *xo_in = nullptr, *mpea_in = nullptr;
   const char *state_out = nullptr, *stats_out = nullptr, *setup_out = nullptr, *B_out = nullptr,
-             *stress_out = nullptr, *profile_out = nullptr;
+             *stress_out = nullptr, *profile_out = nullptr, *cond_out = nullptr, *cond_in = nullptr;
+  long cond_steps = 0;
   long steps_override = -1;
   bool timing = false;
   std::vector<std::pair<std::string, double>> sets;
@@ -135,6 +137,9 @@ int main(int argc, char **argv) {
     else if (a == "-B_out") { need(1); B_out = argv[++i]; }
     else if (a == "-stress_out") { need(1); stress_out = argv[++i]; }
     else if (a == "-profile_out") { need(1); profile_out = argv[++i]; }
+    else if (a == "-cond_steps") { need(1); cond_steps = atol(argv[++i]); }
+    else if (a == "-cond_out") { need(1); cond_out = argv[++i]; }
+    else if (a == "-cond_in") { need(1); cond_in = argv[++i]; }
     else if (a == "-set") { need(2); sets.emplace_back(argv[i + 1], atof(argv[i + 2])); i += 2; }
     else if (a == "-timing") { timing = true; }
     else { fprintf(stderr, "harness: unknown option %s\n", a.c_str()); return 2; }
@@ -222,6 +227,52 @@ int main(int argc, char **argv) {
 
   pfdd->timer->init();
   app->setup();
+  if (cond_steps > 0) {
+    // The conductivity sub-problem alone, in SolveGLCond's order
+    // (solve_GL+cond.cpp:96-122): it reads none of the dislocation fields.
+    // condxi's imaginary half and conddata_fftw are never initialised by the
+    // reference (fft_fftw_slab.cpp:146, :170-173): start both from cond_in or 0.
+    std::vector<double> c0 = cond_in ? read_bin(cond_in, 2 * N) : std::vector<double>(2 * N, 0.0);
+    for (size_t i = 0; i < N; ++i) {
+      fft->condxi[0][2 * i] = c0[2 * i];
+      fft->condxi[0][2 * i + 1] = c0[2 * i + 1];
+      fft->conddata_fftw[i].re = c0[2 * i];
+      fft->conddata_fftw[i].im = c0[2 * i + 1];
+    }
+    std::vector<double> rec, fields;
+    for (long it = 0; it < cond_steps; ++it) {
+      fft->forwardcond();
+      fft->divcurrent();
+      fft->backwardcond();
+      rec.push_back(fft->conductivity);
+      if (it == 0) {
+        // the parts of the first iteration the reference defines: the
+        // unnormalised inverse transforms a (jcurrent_fftw), b (conddata_bpart)
+        // and j (jcurrent).  Its conddata_real also reads condsigma_array[j+1]
+        // before writing it (fft_fftw_slab.cpp:2108 vs :2176-2181).
+        for (size_t i = 0; i < N; ++i) {
+          fields.push_back(fft->jcurrent_fftw[i].re); fields.push_back(fft->jcurrent_fftw[i].im);
+        }
+        for (size_t i = 0; i < N; ++i) {
+          fields.push_back(fft->conddata_bpart[i].re); fields.push_back(fft->conddata_bpart[i].im);
+        }
+        for (size_t i = 0; i < N; ++i) {
+          fields.push_back(fft->jcurrent[i].re); fields.push_back(fft->jcurrent[i].im);
+        }
+      }
+      fft->update_conduct_order_param();
+      rec.push_back(fft->condxinorm);
+      rec.push_back(fft->condxiave);
+      fft->prepare_next_conditr();
+    }
+    std::vector<double> out(fft->condxi[0], fft->condxi[0] + 2 * N);
+    out.insert(out.end(), rec.begin(), rec.end());
+    out.insert(out.end(), fields.begin(), fields.end());
+    write_bin(cond_out, out.data(), out.size());
+    fflush(stdout);
+    MPI_Finalize();
+    return 0;
+  }
   double flops0 = pfdd_shim_fft_flops();
   auto t0 = std::chrono::steady_clock::now();
   app->iterate();

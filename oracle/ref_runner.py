@@ -159,3 +159,42 @@ def _run(workload, steps, state, xo, mpea, sets, want_B, timing, tmp, timeout, s
                 out["timing"] = json.loads(line)
                 break
     return out
+
+
+def run_reference_cond(deck_text, nx, ny, nz, steps, state=None, timeout=600):
+    """Run `steps` iterations of the reference's conductivity sub-problem
+    (forwardcond, divcurrent, backwardcond, update_conduct_order_param,
+    prepare_next_conditr) on a cond100B deck.  Returns condxi (complex
+    [nx, ny, nz]), per-iteration conductivity, condxinorm, condxiave, and the
+    first iteration's unnormalised inverse transforms a, b and current j."""
+    if not available():
+        raise RuntimeError("reference oracle not built: make -C oracle/ref_build")
+    tmp = tempfile.mkdtemp(prefix="pfdd_cond_")
+    try:
+        deck = os.path.join(tmp, "in.deck")
+        with open(deck, "w") as f:
+            f.write(deck_text)
+        N = nx * ny * nz
+        args = [HARNESS, "-deck", deck, "-cond_steps", str(steps), "-cond_out", os.path.join(tmp, "cond.bin")]
+        if state is not None:
+            st = np.asarray(state, dtype=np.complex128).reshape(-1)
+            inter = np.empty((N, 2))
+            inter[:, 0] = st.real
+            inter[:, 1] = st.imag
+            inter.tofile(os.path.join(tmp, "c0.bin"))
+            args += ["-cond_in", os.path.join(tmp, "c0.bin")]
+        proc = subprocess.run(args, cwd=tmp, capture_output=True, text=True, timeout=timeout,
+                              preexec_fn=_raise_stack)
+        if proc.returncode != 0:
+            raise RuntimeError("reference harness failed (%d):\n%s\n%s" % (
+                proc.returncode, proc.stdout[-3000:], proc.stderr[-3000:]))
+        raw = np.fromfile(os.path.join(tmp, "cond.bin"))
+        c = raw[:2 * N].reshape(nx, ny, nz, 2)
+        rec = raw[2 * N:2 * N + 3 * steps].reshape(steps, 3)
+        f = raw[2 * N + 3 * steps:].reshape(3, nx, ny, nz, 2)
+        cplx = f[..., 0] + 1j * f[..., 1]
+        return {"condxi": c[..., 0] + 1j * c[..., 1], "conductivity": rec[:, 0], "condxinorm": rec[:, 1],
+                "condxiave": rec[:, 2], "a": cplx[0], "b": cplx[1], "j": cplx[2], "stdout": proc.stdout}
+    finally:
+        import shutil
+        shutil.rmtree(tmp, ignore_errors=True)

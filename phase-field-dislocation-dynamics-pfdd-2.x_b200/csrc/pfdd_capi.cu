@@ -104,6 +104,12 @@ struct Instance {
   int *flags() const { return reinterpret_cast<int *>(small.as<double>() + PFDD_MAXS + 18); }
   // flags: [0] stop, [1] bad, [2] steps_done, [3] a bounded wait ran out, [4] current xi buffer
   double *an() const { return small.as<double>() + PFDD_MAXS + 22; }  // core model 6 amplitude [4]
+  // conductivity sub-problem (pfdd_gpu_cond_*): condxi [2][N], its spectrum
+  // [2 fields], the four output spectra, their real fields [4][N], the
+  // per-y tables [2][ny] and per-iteration partial sums
+  bool cond_on = false;
+  DevBuf cond_xi, cond_in, cond_out, cond_real, cond_tab, cond_part;
+  double cond_El = 0.0, cond_eps0 = 0.0, cond_dt = 0.0;
   const void *site_arg = nullptr;  // `site` argument of the update kernels
 };
 
@@ -1344,6 +1350,102 @@ bool valid_size(int n) {
 
 }  // namespace
 
+template <typename T>
+pfdd_status cond_step_impl(pfdd_gpu *h, Instance &I, int n_iters, pfdd_cond_stats *stats) {
+  using C = cx<T>;
+  constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
+  cudaStream_t st = h->stream;
+  const size_t N = I.N, ncols = (size_t)I.ny * I.nzp;
+  const int nb = 2 * h->nsm;
+  if (I.cond_part.bytes < (size_t)n_iters * nb * 3 * sizeof(double)) {
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    I.cond_part.release();
+    CUDA_TRY(h, I.cond_part.alloc((size_t)n_iters * nb * 3 * sizeof(double)));
+  }
+  // pencil tile: the widest that holds four fields in shared memory
+  int cc = I.ccols;
+  auto bytes = [&](int c) { return ((size_t)4 * I.nx * c + I.nx) * sizeof(C); };
+  while (cc > 1 && bytes(cc) > 227 * 1024) cc >>= 1;
+  if (bytes(cc) > 227 * 1024 || ncols % cc)
+    return fail(h, PFDD_EUNSUPPORTED, "conductivity pencil of %d x 4 fields does not fit shared memory", I.nx);
+  CUDA_TRY(h, raise_smem_limit(k_cond_pencil<T, 256>, bytes(cc)));
+  PlaneArgs pa;
+  fill_plane_args<T>(I, pa);
+  PencilArgs pe{};
+  pe.px = I.px;
+  pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.nzp = I.nzp; pe.M = I.M;
+  pe.S = 1; pe.F = 2; pe.imag = IMAG_FULL;
+  pe.ncols = (int)ncols;
+  pe.ccols = cc;
+  pe.tw_x = I.tw_x.p;
+  pe.kx_of = I.kx_of; pe.ky_of = I.ky_of; pe.kz_of = I.kz_of;
+  pe.mode = PASS_STEP;
+  pe.fstride = I.nx * cc;
+  pe.sx_n = I.sx_n; pe.sy_n = I.sy_n;
+  pe.g = I.green;
+  set_pencil_divisors<T>(pe);
+  pe.fd_6cc = FastDiv(4 * cc);
+  UpdateArgs ua;
+  memset(&ua, 0, sizeof ua);
+  ua.nx = I.nx; ua.ny = I.ny; ua.nz = I.nz; ua.nzh = I.nzh; ua.nzp = I.nzp; ua.S = I.S; ua.F = 4;
+  ua.invN = 1.0;   // backwardcond's transforms are unnormalised
+  ua.core = I.core;
+  ua.err = I.flags() + 3;
+  ua.mode = PASS_SYNTH;
+  CondArgs ca;
+  ca.El = I.cond_El;
+  ca.eps0 = I.cond_eps0;
+  ca.dt = I.cond_dt;
+  ca.ny = I.ny;
+  ca.nz = I.nz;
+  const unsigned planes2 = (unsigned)(2 * I.nx), planes4 = (unsigned)(4 * I.nx);
+  T *cxi = I.cond_xi.as<T>();
+  for (int it = 0; it < n_iters; ++it) {
+    pa.F = 2;
+    if (I.split)
+      launch_pair(k_fwd_planes<T, NH, true>, dim3(2 * planes2), NH, I.smem_plane, st, (const T *)cxi,
+                  I.cond_in.as<C>(), pa, (const int *)nullptr, I.flags() + 3);
+    else
+      k_fwd_planes<T, NP, false><<<planes2, NP, I.smem_plane, st>>>(cxi, I.cond_in.as<C>(), pa, nullptr,
+                                                                     I.flags() + 3);
+    k_cond_pencil<T, 256><<<(unsigned)(ncols / cc), 256, bytes(cc), st>>>(I.cond_in.as<C>(), I.cond_out.as<C>(), pe);
+    pa.F = 4;
+    if (I.split)
+      launch_pair(k_inv_update<T, NH, true>, dim3(2 * planes4), NH, I.smem_update, st,
+                  (const C *)I.cond_out.as<C>(), (const T *)cxi, I.cond_real.as<T>(), pa, ua, I.partials.as<double>());
+    else
+      k_inv_update<T, NP, false><<<planes4, NP, I.smem_update, st>>>(I.cond_out.as<C>(), cxi, I.cond_real.as<T>(),
+                                                                     pa, ua, I.partials.as<double>());
+    k_cond_update<T><<<nb, 256, 0, st>>>(cxi, I.cond_real.as<T>(), I.cond_tab.as<double>(), ca, N,
+                                          I.cond_part.as<double>() + (size_t)it * nb * 3);
+    CUDA_TRY(h, cudaGetLastError());
+  }
+  std::vector<double> hp((size_t)n_iters * nb * 3);
+  CUDA_TRY(h, cudaMemcpyAsync(hp.data(), I.cond_part.p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  int fl[4];
+  CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+  if (fl[3]) return fail(h, PFDD_ETIMEOUT, "a bounded device wait ran out");
+  if (stats) {
+    for (int it = 0; it < n_iters; ++it) {
+      double tot[3];
+      for (int q = 0; q < 3; ++q) {
+        double t = 0.0, c = 0.0;
+        for (int b = 0; b < nb; ++b) {   // Neumaier-compensated
+          const double v = hp[((size_t)it * nb + b) * 3 + q], u = t + v;
+          c += (std::fabs(t) >= std::fabs(v)) ? (t - u) + v : (v - u) + t;
+          t = u;
+        }
+        tot[q] = t + c;
+      }
+      stats[it].condxinorm = std::sqrt(tot[0]);
+      stats[it].condxiave = tot[1];
+      stats[it].conductivity = tot[2] / (1.0 * I.cond_El);
+    }
+  }
+  return PFDD_OK;
+}
+
 extern "C" {
 
 const char *pfdd_gpu_version(void) { return "pfdd_b200 0.1 (sm_100a)"; }
@@ -1584,6 +1686,130 @@ pfdd_status pfdd_gpu_core_profile(pfdd_gpu *h, int inst, int n_planes, double *d
       }
   }
   return PFDD_OK;
+}
+
+pfdd_status pfdd_cond_layers(const pfdd_cond_material *A, const pfdd_cond_material *B, int ny, double temperature,
+                             double *sigma_eff, double *sigma_layer) {
+  if (!A || !B || !sigma_eff || !sigma_layer || ny < 1 || A->Nlayers < 1)
+    return fail(nullptr, PFDD_EINVAL, "need A, B, outputs, ny >= 1 and A->Nlayers >= 1");
+  // backwardcond (fft_fftw_slab.cpp:2089-2156), in its order of operations
+  const double Vf = B->dlayer / (A->dlayer + B->dlayer);
+  const double prob = 1.0 - A->pinterface;
+  const int per = ny / A->Nlayers;
+  const int dB = (int)std::round(per * Vf), dA = (int)std::round(per * (1. - Vf));
+  if (dA + dB < 1) return fail(nullptr, PFDD_EINVAL, "layer period of zero cells (ny / Nlayers too small)");
+  const double dT = temperature - 300;
+  for (int j = 0; j < ny; ++j) {
+    const pfdd_cond_material &M = (j % (dA + dB) >= dA) ? *B : *A;
+    const double lay = M.condsigma / (1. + M.alpha_resistivity * dT);
+    const double ps = 2 * prob / M.dlayer;
+    const double lam = M.mfpel / (1. + M.alpha_mfpel * dT);
+    const double ag = (lam * M.Ngrains / M.dlayer) * M.Rgrain / (1 - M.Rgrain);
+    const double rd = M.beta_disloc * M.rho_disloc;
+    double cs;
+    if (ps > 0.) {
+      const double ri = ((1 / lay) * ((3. / 16.) * lam * ps));
+      if (M.Ngrains > 1) {
+        const double rg =
+            (1 / lay) * (1. / (1. - 3. * ag / 2. + 3. * ag * ag - 3. * std::pow(ag, 3.) * std::log(1. + 1. / ag)) - 1.);
+        cs = 1 / ((1 / lay) + (2 * ri + (M.Ngrains - 1) * rg) / (M.Ngrains + 1) + rd);
+      } else {
+        cs = 1 / ((1 / lay) + ri + rd);
+      }
+    } else {
+      cs = lay;
+    }
+    sigma_eff[j] = cs;
+    sigma_layer[j] = lay;
+  }
+  return PFDD_OK;
+}
+
+pfdd_status pfdd_gpu_cond_enable(pfdd_gpu *h, int inst, const pfdd_cond_desc *d) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  Instance &I = *h->inst[inst];
+  if (!d || !d->sigma_eff || !d->sigma_layer) return fail(h, PFDD_EINVAL, "need the per-y conductivity tables");
+  if (I.ny < 2) return fail(h, PFDD_EINVAL, "the conductivity gradient needs ny >= 2");
+  cudaSetDevice(h->device);
+  const size_t TB = h->precision == PFDD_FP64 ? sizeof(double) : sizeof(float);
+  const size_t CB = 2 * TB, ncols = (size_t)I.ny * I.nzp;
+  if (!I.cond_on) {
+    CUDA_TRY(h, I.cond_xi.alloc(2 * I.N * TB));
+    CUDA_TRY(h, I.cond_in.alloc(2 * (size_t)I.nx * ncols * CB));
+    CUDA_TRY(h, I.cond_out.alloc(4 * (size_t)I.nx * ncols * CB));
+    CUDA_TRY(h, I.cond_real.alloc(4 * I.N * TB));
+    CUDA_TRY(h, I.cond_tab.alloc(2 * (size_t)I.ny * sizeof(double)));
+    h->device_bytes += I.cond_xi.bytes + I.cond_in.bytes + I.cond_out.bytes + I.cond_real.bytes + I.cond_tab.bytes;
+  }
+  // d sigma_layer / dy as backwardcond takes it (one-sided at the ends, :2170-2183)
+  std::vector<double> tab(2 * (size_t)I.ny);
+  const double *L = d->sigma_layer;
+  for (int j = 0; j < I.ny; ++j) {
+    tab[j] = d->sigma_eff[j];
+    tab[I.ny + j] = (j == 0) ? (L[j + 1] - L[j]) : (j == I.ny - 1) ? (L[j] - L[j - 1]) : (L[j + 1] - L[j - 1]) / 2.;
+  }
+  CUDA_TRY(h, cudaMemcpy(I.cond_tab.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(h, cudaMemset(I.cond_xi.p, 0, I.cond_xi.bytes));
+  I.cond_El = d->El_y;
+  I.cond_eps0 = d->epsilonzero;
+  I.cond_dt = d->timestep;
+  I.cond_on = true;
+  return PFDD_OK;
+}
+
+pfdd_status pfdd_gpu_cond_set_state(pfdd_gpu *h, int inst, const double *re, const double *im) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  Instance &I = *h->inst[inst];
+  if (!I.cond_on) return fail(h, PFDD_ESTATE, "pfdd_gpu_cond_enable has not been called for instance %d", inst);
+  if (!re) return fail(h, PFDD_EINVAL, "re is required");
+  cudaSetDevice(h->device);
+  if (h->precision == PFDD_FP64) {
+    CUDA_TRY(h, cudaMemcpy(I.cond_xi.p, re, I.N * sizeof(double), cudaMemcpyHostToDevice));
+    if (im) CUDA_TRY(h, cudaMemcpy(I.cond_xi.as<double>() + I.N, im, I.N * sizeof(double), cudaMemcpyHostToDevice));
+    else CUDA_TRY(h, cudaMemset(I.cond_xi.as<double>() + I.N, 0, I.N * sizeof(double)));
+  } else {
+    std::vector<float> v(2 * I.N, 0.0f);
+    for (size_t i = 0; i < I.N; ++i) {
+      v[i] = (float)re[i];
+      if (im) v[I.N + i] = (float)im[i];
+    }
+    CUDA_TRY(h, cudaMemcpy(I.cond_xi.p, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  return PFDD_OK;
+}
+
+pfdd_status pfdd_gpu_cond_get_state(pfdd_gpu *h, int inst, double *re, double *im) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  Instance &I = *h->inst[inst];
+  if (!I.cond_on) return fail(h, PFDD_ESTATE, "pfdd_gpu_cond_enable has not been called for instance %d", inst);
+  cudaSetDevice(h->device);
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (h->precision == PFDD_FP64) {
+    if (re) CUDA_TRY(h, cudaMemcpy(re, I.cond_xi.p, I.N * sizeof(double), cudaMemcpyDeviceToHost));
+    if (im) CUDA_TRY(h, cudaMemcpy(im, I.cond_xi.as<double>() + I.N, I.N * sizeof(double), cudaMemcpyDeviceToHost));
+  } else {
+    std::vector<float> v(2 * I.N);
+    CUDA_TRY(h, cudaMemcpy(v.data(), I.cond_xi.p, v.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < I.N; ++i) {
+      if (re) re[i] = v[i];
+      if (im) im[i] = v[I.N + i];
+    }
+  }
+  return PFDD_OK;
+}
+
+pfdd_status pfdd_gpu_cond_step(pfdd_gpu *h, int inst, int n_iters, pfdd_cond_stats *stats) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  Instance &I = *h->inst[inst];
+  if (!I.cond_on) return fail(h, PFDD_ESTATE, "pfdd_gpu_cond_enable has not been called for instance %d", inst);
+  if (n_iters < 1) return fail(h, PFDD_EINVAL, "n_iters must be >= 1");
+  cudaSetDevice(h->device);
+  return h->precision == PFDD_FP64 ? cond_step_impl<double>(h, I, n_iters, stats)
+                                   : cond_step_impl<float>(h, I, n_iters, stats);
 }
 
 pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every, const double *xi_target,

@@ -146,7 +146,7 @@ struct PencilArgs {
   // divisors built on the host: F * ccols, ccols, nzp, 16-byte chunks per
   // (field, x) row of a tile, nx
   FastDiv fd_fcc, fd_cc, fd_nzp, fd_cpr, fd_nx;
-  FastDiv fd_6cc;             // strain diagnostics: 6 * ccols
+  FastDiv fd_6cc;             // strain diagnostics: 6 * ccols (conductivity pencil: 4 * ccols)
   double inv2mu;              // strain diagnostics: 1 / (2 mu), Voigt mu (Fmatrix, fft_fftw_slab.cpp:657)
   Green g;
 };
@@ -1817,6 +1817,128 @@ __global__ void __launch_bounds__(NT, 1) k_strain_pencil(const cx<T> *__restrict
   for (int i = threadIdx.x; i < 6 * per; i += blockDim.x) {
     const int f = i / per, rem = i - f * per, x = rem / cc, c = rem - x * cc;
     out6[((size_t)f * nx + x) * ncols + col0 + c] = buf[(size_t)f * fst + rem];
+  }
+}
+
+// ------------------------------------------------------------ conductivity
+// divcurrent's two operators on the conductivity field c = X + iY (X, Y the
+// spectra of Re and Im condxi, fft_fftw_slab.cpp:1699-1741): a = i (k_y/k^2) c
+// and b = (k_y^2/k^2) c, zero at k = 0.  The reference's complex transforms
+// index -k with its own frequency table (k' differs from -k on the Nyquist
+// planes), so the spectra of the real and imaginary parts of each output are
+//   Re: (M(k)(X+iY) + conj M'(X-iY)) / 2,   Im: (M(k)(X+iY) - conj M'(X-iY)) / 2i
+// with M' the operator at k'.  Slots 0..3 out: Re a, Im a, Re b, Im b.
+template <typename T, typename C>
+__device__ __forceinline__ void cond_point(C x, C y, T ky, T k2, T kyn, T k2n, C (&o)[4]) {
+  // M(k) c with c = X + iY
+  const C c = mk<C>(x.x - y.y, x.y + y.x);
+  const C d = mk<C>(x.x + y.y, x.y - y.x);   // X - iY
+  const T ra = ky / k2, rb = ky * ky / k2;    // a: i ra c ; b: rb c
+  const T rna = kyn / k2n, rnb = kyn * kyn / k2n;
+  // a: p = i ra c, q = conj(i rna) d = -i rna d
+  const C pa = mk<C>(-ra * c.y, ra * c.x), qa = mk<C>(rna * d.y, -rna * d.x);
+  const C pb = mk<C>(rb * c.x, rb * c.y), qb = mk<C>(rnb * d.x, rnb * d.y);
+  const T h = (T)0.5;
+  o[0] = mk<C>(h * (pa.x + qa.x), h * (pa.y + qa.y));
+  o[1] = mk<C>(h * (pa.y - qa.y), -h * (pa.x - qa.x));   // (p - q) / 2i
+  o[2] = mk<C>(h * (pb.x + qb.x), h * (pb.y + qb.y));
+  o[3] = mk<C>(h * (pb.y - qb.y), -h * (pb.x - qb.x));
+}
+
+// Per tile of (ky, kz) columns: x FFT of the two fields of condxi's spectrum,
+// the four output spectra per point, inverse x FFT of the four.
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, 1) k_cond_pencil(const cx<T> *__restrict__ spec, cx<T> *__restrict__ out4,
+                                                       PencilArgs a) {
+  using C = cx<T>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int nx = a.nx, cc = a.ccols, fst = a.fstride;
+  C *buf = reinterpret_cast<C *>(smem_raw);   // [4][fstride]
+  C *twx = buf + (size_t)4 * fst;
+  const size_t col0 = (size_t)blockIdx.x * cc, ncols = a.ncols;
+  const int per = nx * cc;
+  for (int i = threadIdx.x; i < 2 * per; i += blockDim.x) {
+    const int f = i / per, rem = i - f * per, x = rem / cc, c = rem - x * cc;
+    buf[(size_t)f * fst + rem] = spec[((size_t)f * nx + x) * ncols + col0 + c];
+  }
+  load_table(twx, a.tw_x, nx);
+  __syncthreads();
+  Batch gx{2 * cc, cc, 1, fst, cc, true, a.fd_fcc, a.fd_cc};
+  fft_forward<MaxRadix<NT>::value, GeomPencil>(buf, twx, a.px, gx);
+  const GreenT<T> &g = green_t<T>(a.g);
+  for (int w = threadIdx.x; w < per; w += blockDim.x) {
+    const int sx = a.fd_cc.div(w), c = w - sx * cc;
+    const int col = (int)(col0 + c);
+    const int sy = a.fd_nzp.div(col), sz = col - sy * a.nzp;
+    C *pk = buf + sx * cc + c;
+    C o[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) o[q] = mk<C>((T)0, (T)0);
+    if (sz <= a.M) {
+      const int ix = a.kx_of[sx], iy = a.ky_of[sy], iz = a.kz_of[sz];
+      const T fx = freq_of<T>(ix, a.nx), fy = freq_of<T>(iy, a.ny), fz = freq_of<T>(iz, a.nz);
+      const T kx = fx * g.four[0][0] + fy * g.four[1][0] + fz * g.four[2][0];
+      const T ky = fx * g.four[0][1] + fy * g.four[1][1] + fz * g.four[2][1];
+      const T kz = fx * g.four[0][2] + fy * g.four[1][2] + fz * g.four[2][2];
+      const T k2 = kx * kx + ky * ky + kz * kz;
+      if (k2 > (T)0) {
+        const T gxn = freq_neg<T>(ix, a.nx), gyn = freq_neg<T>(iy, a.ny), gzn = freq_neg<T>(iz, a.nz);
+        const T mx = gxn * g.four[0][0] + gyn * g.four[1][0] + gzn * g.four[2][0];
+        const T my = gxn * g.four[0][1] + gyn * g.four[1][1] + gzn * g.four[2][1];
+        const T mz = gxn * g.four[0][2] + gyn * g.four[1][2] + gzn * g.four[2][2];
+        cond_point<T, C>(pk[0], pk[(size_t)fst], ky, k2, my, mx * mx + my * my + mz * mz, o);
+      }
+    }
+    // both inputs of this point have been read: its four outputs take slots 0..3
+#pragma unroll
+    for (int q = 0; q < 4; ++q) pk[(size_t)q * fst] = o[q];
+  }
+  __syncthreads();
+  Batch g4{4 * cc, cc, 1, fst, cc, true, a.fd_6cc, a.fd_cc};
+  fft_inverse<MaxRadix<NT>::value, GeomPencil>(buf, twx, a.px, g4);
+  for (int i = threadIdx.x; i < 4 * per; i += blockDim.x) {
+    const int f = i / per, rem = i - f * per, x = rem / cc, c = rem - x * cc;
+    out4[((size_t)f * nx + x) * ncols + col0 + c] = buf[(size_t)f * fst + rem];
+  }
+}
+
+// backwardcond's real-space assembly and update_conduct_order_param
+// (fft_fftw_slab.cpp:2157-2186, 1816-1829) per site, in FP64: fr holds the
+// unnormalised inverse transforms Re a, Im a, Re b, Im b; tab the effective
+// conductivity [ny] and the y-derivative of the layer conductivity [ny].
+// part[blk * 3 + {0,1,2}] = sum |dcondxi|^2, sum Re condxi, sum j_y / N.
+struct CondArgs {
+  double El, eps0, dt;
+  int ny, nz;
+};
+
+template <typename T>
+__global__ void k_cond_update(T *__restrict__ cxi, const T *__restrict__ fr, const double *__restrict__ tab,
+                              CondArgs c, size_t N, double *__restrict__ part) {
+  __shared__ double red[3 * 32];
+  double v[3] = {0.0, 0.0, 0.0};
+  const double nsz = (double)N, kdt = 1e-22 * c.dt;
+  for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)((r / (size_t)c.nz) % (size_t)c.ny);
+    const double cs = tab[j], dcs = tab[c.ny + j];
+    const double jr = (double)fr[r], ji = (double)fr[N + r], br = (double)fr[2 * N + r], bi = (double)fr[3 * N + r];
+    const double jcur = cs * (c.El - jr / c.eps0);
+    v[2] += jcur / nsz;
+    const double cre = (cs / c.eps0) * br + (jr / c.eps0 - c.El) * dcs;
+    const double cim = (cs / c.eps0) * bi + (ji / c.eps0) * dcs;
+    const double xr = (double)cxi[r], xi = (double)cxi[N + r];
+    const T nr = (T)(xr - kdt * (cre / nsz)), ni = (T)(xi - kdt * (cim / nsz));
+    cxi[r] = nr;
+    cxi[N + r] = ni;
+    const double dr = (double)nr - xr, di = (double)ni - xi;
+    v[0] += dr * dr + di * di;
+    v[1] += (double)nr;
+  }
+  block_reduce<3>(v, red);
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x] = v[0];
+    part[3 * blockIdx.x + 1] = v[1];
+    part[3 * blockIdx.x + 2] = v[2];
   }
 }
 

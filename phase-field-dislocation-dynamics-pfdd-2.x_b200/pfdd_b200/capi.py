@@ -31,7 +31,8 @@ EXPORTS = [
     "pfdd_gpu_get_state_interleaved", "pfdd_gpu_advance", "pfdd_gpu_step_history", "pfdd_gpu_energy",
     "pfdd_gpu_tau", "pfdd_gpu_info", "pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version",
     "pfdd_gpu_set_stream", "pfdd_gpu_profile", "pfdd_gpu_adjoint", "pfdd_gpu_strain_stress",
-    "pfdd_gpu_core_profile",
+    "pfdd_gpu_core_profile", "pfdd_cond_layers", "pfdd_gpu_cond_enable", "pfdd_gpu_cond_set_state",
+    "pfdd_gpu_cond_get_state", "pfdd_gpu_cond_step",
 ]
 KERNELS = ["fwd_planes", "xpencil", "step_planes", "finalize"]
 
@@ -55,6 +56,21 @@ class InstanceDesc(ctypes.Structure):
         ("w1", ctypes.c_double), ("w2", ctypes.c_double), ("w3", ctypes.c_double),
         ("usfe_fit", ctypes.c_double * 5),
     ]
+
+
+class CondMaterial(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("condsigma", "alpha_resistivity", "mfpel", "alpha_mfpel", "dlayer",
+                                               "Rgrain", "beta_disloc", "rho_disloc")] + [
+        ("Ngrains", ctypes.c_int), ("Nlayers", ctypes.c_int), ("pinterface", ctypes.c_double)]
+
+
+class CondDesc(ctypes.Structure):
+    _fields_ = [("sigma_eff", DP), ("sigma_layer", DP), ("El_y", ctypes.c_double),
+                ("epsilonzero", ctypes.c_double), ("timestep", ctypes.c_double)]
+
+
+class CondStats(ctypes.Structure):
+    _fields_ = [("condxinorm", ctypes.c_double), ("condxiave", ctypes.c_double), ("conductivity", ctypes.c_double)]
 
 
 class Options(ctypes.Structure):
@@ -96,6 +112,12 @@ def load(path: str = LIB_PATH):
     lib.pfdd_gpu_energy.argtypes = [vp, ctypes.c_int, DP, DP, DP]
     lib.pfdd_gpu_strain_stress.argtypes = [vp, ctypes.c_int, DP, DP, DP, DP]
     lib.pfdd_gpu_core_profile.argtypes = [vp, ctypes.c_int, ctypes.c_int, DP, DP]
+    lib.pfdd_cond_layers.argtypes = [ctypes.POINTER(CondMaterial), ctypes.POINTER(CondMaterial), ctypes.c_int,
+                                     ctypes.c_double, DP, DP]
+    lib.pfdd_gpu_cond_enable.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CondDesc)]
+    lib.pfdd_gpu_cond_set_state.argtypes = [vp, ctypes.c_int, DP, DP]
+    lib.pfdd_gpu_cond_get_state.argtypes = [vp, ctypes.c_int, DP, DP]
+    lib.pfdd_gpu_cond_step.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(CondStats)]
     lib.pfdd_gpu_tau.argtypes = [vp, ctypes.c_int, DP]
     lib.pfdd_gpu_adjoint.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, DP, DP, DP, DP]
     lib.pfdd_gpu_set_stream.argtypes = [vp, vp]
@@ -152,6 +174,24 @@ def desc_from_workload(w, core_flag=None, An=None):
             for i in range(n):
                 arr[i] = float(extra[key][i])
     return d
+
+
+def cond_material(d):
+    m = CondMaterial()
+    for name, _ in CondMaterial._fields_:
+        setattr(m, name, d.get(name, 0) if name not in ("Ngrains", "Nlayers") else int(d.get(name, 1)))
+    return m
+
+
+def cond_layers(A, B, ny, temperature):
+    """pfdd_cond_layers (host): per-y effective and layer conductivity [ny] each."""
+    lib = load()
+    eff, lay = np.zeros(ny), np.zeros(ny)
+    a, b = cond_material(A), cond_material(B)
+    st = lib.pfdd_cond_layers(ctypes.byref(a), ctypes.byref(b), ny, float(temperature), _dp(eff), _dp(lay))
+    if st != 0:
+        raise PfddError(st, "pfdd_cond_layers")
+    return eff, lay
 
 
 class Stepper:
@@ -231,10 +271,37 @@ class Stepper:
         self._check(self._lib.pfdd_gpu_energy(self.h, inst, _dp(e[0:1]), _dp(e[1:2]), _dp(e[2:3])))
         return tuple(e)
 
+    def cond_enable(self, inst, sigma_eff, sigma_layer, El_y, epsilonzero, timestep=1.0):
+        eff = np.ascontiguousarray(sigma_eff, dtype=np.float64)
+        lay = np.ascontiguousarray(sigma_layer, dtype=np.float64)
+        d = CondDesc(_dp(eff), _dp(lay), float(El_y), float(epsilonzero), float(timestep))
+        self._check(self._lib.pfdd_gpu_cond_enable(self.h, inst, ctypes.byref(d)))
+
+    def cond_set_state(self, inst, c):
+        c = np.asarray(c)
+        re = np.ascontiguousarray(np.real(c), dtype=np.float64).reshape(-1)
+        im = np.ascontiguousarray(np.imag(c), dtype=np.float64).reshape(-1)
+        self._check(self._lib.pfdd_gpu_cond_set_state(self.h, inst, _dp(re), _dp(im)))
+
+    def cond_get_state(self, inst):
+        ds = self.descs[inst]
+        n = ds.nx * ds.ny * ds.nz
+        re, im = np.zeros(n), np.zeros(n)
+        self._check(self._lib.pfdd_gpu_cond_get_state(self.h, inst, _dp(re), _dp(im)))
+        return (re + 1j * im).reshape(ds.nx, ds.ny, ds.nz)
+
+    def cond_step(self, inst, n_iters=1):
+        """n_iters conductivity iterations: array [n_iters, 3] of
+        (condxinorm, condxiave, conductivity)."""
+        st = (CondStats * n_iters)()
+        self._check(self._lib.pfdd_gpu_cond_step(self.h, inst, n_iters, st))
+        return np.array([[s.condxinorm, s.condxiave, s.conductivity] for s in st])
+
     def core_profile(self, inst, n_planes):
         """project_core_energy of the current state: delta [n_planes, nx, ny, nz]
         and the ddelta line [n_planes, nx] at j = ny/2, k = nz/2."""
-        nx, ny, nz = self._dims[inst]
+        ds = self.descs[inst]
+        nx, ny, nz = ds.nx, ds.ny, ds.nz
         d = np.zeros(n_planes * nx * ny * nz)
         dd = np.zeros(n_planes * nx)
         self._check(self._lib.pfdd_gpu_core_profile(self.h, inst, n_planes, _dp(d), _dp(dd)))

@@ -232,6 +232,68 @@ def bcc_screw_workload(n=16, nz=8, seed=11, sigma_mpa=300.0, angle=10.0, w=(0.3,
                     non_schmid=(float(angle),) + tuple(float(v) for v in w))
 
 
+# Electrical members of the Cu and W presets (Material::set_constants,
+# material.cpp:269-274 and :726-731) that the conductivity solver reads
+CU_COND = dict(condsigma=5.95e7, alpha_resistivity=0.00385, mfpel=39.9e-9, alpha_mfpel=0.00385, Rgrain=0.24,
+               beta_disloc=1.3e-25)
+W_COND = dict(condsigma=1.855e7, alpha_resistivity=0.0042, mfpel=15.5e-9, alpha_mfpel=0.0042, Rgrain=0.42,
+              beta_disloc=7.5e-25)
+EPSILON_ZERO = 8.8541878128e-12   # Material::epsilonzero (material.h:53)
+
+
+@dataclass
+class CondCase:
+    """A conductivity deck (app cond100B, two layer materials Cu/W alternating
+    along y): the Workload of its dislocation field, the two materials as
+    pfdd_cond_material values, temperature and E_y."""
+    workload: Workload
+    A: dict
+    B: dict
+    temperature: float
+    El_y: float
+
+    def deck(self) -> str:
+        w = self.workload
+        A, B = self.A, self.B
+        lines = [
+            "seed 576",
+            "app_style cond100B core_energy 1",
+            "fft_style fftw_slab pbc 1 1 1 mode 1",
+            "dimension 3",
+            "lattice sc/6n 1",
+            "region box block 0 %d 0 %d 0 %d" % (w.nx, w.ny, w.nz),
+            "create_box box",
+            "create_sites box",
+            "material preset Cu El 0.0 %r 0.0 dlayer %r Nlayers %d Ngrains %d pinterface %r rho_disloc %r" % (
+                self.El_y, A["dlayer"], A["Nlayers"], A["Ngrains"], A["pinterface"], A["rho_disloc"]),
+            "material preset W dlayer %r Ngrains %d rho_disloc %r" % (B["dlayer"], B["Ngrains"], B["rho_disloc"]),
+            "solve_style GLCond max_iter 1 tol 0",
+            "temperature %r" % self.temperature,
+            "scale 1.0 1.0 1.0",
+            "sigma initial 0 0 0 0 0 0 delta 0 0 0 0 0 0",
+            "stats 1e12",
+            "run 1",
+        ]
+        return "\n".join(lines) + "\n"
+
+
+def cond_case(nx=8, ny=32, nz=8, n_layers=4, temperature=350.0, El_y=1.0, grains=(3, 2), seed=3):
+    """Cu/W multilayer along y on an nx x ny x nz grid (one slip system of app
+    cond100B: n = z, b = x, CD = 0.5); the dislocation field is a seeded loop
+    that the conductivity sub-problem never reads."""
+    m = Material(preset="Cu", mu=48.0e9, young=128.64e9)
+    prim = np.eye(3)
+    four, _ = reciprocal_basis(prim)
+    xn = np.array([[0.0, 0.0, 1.0]])
+    xb = np.array([[1.0, 0.0, 0.0]])
+    rng = np.random.default_rng(seed)
+    xi0 = rng.uniform(-1e-3, 1e-3, size=(1, nx, ny, nz))
+    w = Workload("cond", nx, ny, nz, "cond100B", xn, xb, four, prim, m, 1, np.zeros((3, 3)), 0.5, xi0)
+    A = dict(CU_COND, dlayer=2e-9, Nlayers=n_layers, Ngrains=grains[0], pinterface=0.4, rho_disloc=1e15)
+    B = dict(W_COND, dlayer=1e-9, Nlayers=1, Ngrains=grains[1], pinterface=0.5, rho_disloc=5e14)
+    return CondCase(w, A, B, temperature, El_y)
+
+
 def loop_workload(n=64, radius=12.0, noise=1e-3, seed=576, sigma_mpa=200.0, name="loop64",
                   material: Material | None = None, nz: int | None = None):
     """Circular loop on system 0 in the z = nz/2 plane of an n x n x nz grid

@@ -152,3 +152,24 @@ def test_core_profile_equals_reference(make):
     d, dd = O.core_profile(xi.real, w.xb, r["delta"].shape[0])
     assert np.abs(d - r["delta"]).max() <= 1e-12
     assert np.abs(dd - r["ddelta"]).max() <= 1e-12
+
+
+@needs_ref
+def test_conductivity_fields_equal_reference():
+    """The defined part of the conductivity iteration (forwardcond, divcurrent,
+    backwardcond's transforms, current and conductivity) of a seeded complex
+    state on a Cu/W multilayer.  (The reference's driving term reads its layer
+    table before writing it, so condxi after an update is not comparable.)"""
+    cc = configs.cond_case()
+    w = cc.workload
+    A, B = O.CondMaterial(**cc.A), O.CondMaterial(**cc.B)
+    eff, lay = O.cond_layers(A, B, w.ny, cc.temperature)
+    rng = np.random.default_rng(1)
+    c0 = (rng.standard_normal((w.nx, w.ny, w.nz)) + 1j * rng.standard_normal((w.nx, w.ny, w.nz))) * 1e-16
+    r = ref_runner.run_reference_cond(cc.deck(), w.nx, w.ny, w.nz, 1, state=c0)
+    a, b, j, cond = O.cond_fields(c0, w.four, eff, cc.El_y, configs.EPSILON_ZERO)
+    assert np.abs(a - r["a"]).max() <= 1e-13 * np.abs(r["a"]).max()
+    assert np.abs(b - r["b"]).max() <= 1e-13 * np.abs(r["b"]).max()
+    # sigma_eff carries the cancellation of the grain-boundary series
+    assert np.abs(j - r["j"]).max() <= 1e-10 * np.abs(r["j"]).max()
+    assert abs(cond / r["conductivity"][0] - 1.0) <= 1e-10
