@@ -210,6 +210,18 @@ pfdd_status pfdd_gpu_strain_stress(pfdd_gpu *h, int inst, double *eps, double *s
  * n_slip/3 otherwise (beyond that the reference reads past its array). */
 pfdd_status pfdd_gpu_core_profile(pfdd_gpu *h, int inst, int n_planes, double *delta, double *ddelta);
 
+/* Asynchronous snapshot of instance `inst`'s order parameter for output
+ * (the reference's dumps and diagnostics read fft->xi between GL iterations,
+ * src/output.cpp:79-188, src/dump_text.cpp:296-324): the state is converted
+ * to FP64 planes in device memory on the stepping stream, then copied to re
+ * and im ([S*N] each, either may be NULL) on a second stream, so the next
+ * pfdd_gpu_advance overlaps the copy.  Host buffers stay untouched by the
+ * caller until pfdd_gpu_snapshot_wait; they must be page-locked
+ * (cudaHostAlloc / cudaHostRegister) for the copy to overlap (pageable memory
+ * works, with the copy finishing inside begin). */
+pfdd_status pfdd_gpu_snapshot_begin(pfdd_gpu *h, int inst, double *re, double *im);
+pfdd_status pfdd_gpu_snapshot_wait(pfdd_gpu *h, int inst);
+
 /* ---- Conductivity sub-problem (SolveGLCond, src/solve_GL+cond.cpp:70-150) ----
  * A complex scalar order parameter condxi relaxed by its own GL iteration:
  * forwardcond, divcurrent (a = i k_y/k^2 c, b = k_y^2/k^2 c),

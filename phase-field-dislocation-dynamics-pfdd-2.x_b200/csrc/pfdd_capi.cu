@@ -107,6 +107,11 @@ struct Instance {
   // conductivity sub-problem (pfdd_gpu_cond_*): condxi [2][N], its spectrum
   // [2 fields], the four output spectra, their real fields [4][N], the
   // per-y tables [2][ny] and per-iteration partial sums
+  // asynchronous state snapshot (pfdd_gpu_snapshot_begin / _wait): FP64
+  // planes on the device, copied to the host on the handle's copy stream
+  DevBuf snap;
+  cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
+  bool snap_pending = false;
   bool cond_on = false;
   DevBuf cond_xi, cond_in, cond_out, cond_real, cond_tab, cond_part;
   double cond_El = 0.0, cond_eps0 = 0.0, cond_dt = 0.0;
@@ -143,6 +148,7 @@ struct pfdd_gpu {
   cudaStream_t stream = nullptr;      // stream in use
   cudaStream_t own_stream = nullptr;  // stream created by the handle
   DevBuf staging;                     // FP64 host<->device staging, kept across calls
+  cudaStream_t copy_stream = nullptr; // device-to-host snapshots, beside the stepping stream
   std::string err;
   size_t device_bytes = 0;
   int nsm = 148;                      // SMs of the device (grid sizing)
@@ -1351,6 +1357,41 @@ bool valid_size(int n) {
 }  // namespace
 
 template <typename T>
+pfdd_status snapshot_begin_impl(pfdd_gpu *h, Instance &I, double *re, double *im) {
+  const size_t n = (size_t)I.S * I.N;
+  if (!h->copy_stream) CUDA_TRY(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+  if (!I.snap.p) {
+    CUDA_TRY(h, I.snap.alloc(2 * n * sizeof(double)));
+    h->device_bytes += I.snap.bytes;
+    CUDA_TRY(h, cudaEventCreateWithFlags(&I.snap_ready, cudaEventDisableTiming));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&I.snap_done, cudaEventDisableTiming));
+  }
+  // the previous snapshot's copies read I.snap: the conversion waits for them
+  if (I.snap_pending) CUDA_TRY(h, cudaStreamWaitEvent(h->stream, I.snap_done, 0));
+  const T *dre = I.xi[I.cur].as<T>();
+  const T *dim = I.F > I.S ? dre + n : nullptr;
+  if (I.imag == IMAG_NYQ && im) {
+    T *scratch = I.xi[I.cur ^ 1].as<T>();   // free between steps
+    synth_imag<T>(I, h->stream, scratch);
+    dim = scratch;
+  }
+  double *d = I.snap.as<double>();
+  k_to_planar<T><<<1184, 256, 0, h->stream>>>(dre, d, n);
+  if (im) {
+    if (dim) k_to_planar<T><<<1184, 256, 0, h->stream>>>(dim, d + n, n);
+    else CUDA_TRY(h, cudaMemsetAsync(d + n, 0, n * sizeof(double), h->stream));
+  }
+  CUDA_TRY(h, cudaGetLastError());
+  CUDA_TRY(h, cudaEventRecord(I.snap_ready, h->stream));
+  CUDA_TRY(h, cudaStreamWaitEvent(h->copy_stream, I.snap_ready, 0));
+  if (re) CUDA_TRY(h, cudaMemcpyAsync(re, d, n * sizeof(double), cudaMemcpyDeviceToHost, h->copy_stream));
+  if (im) CUDA_TRY(h, cudaMemcpyAsync(im, d + n, n * sizeof(double), cudaMemcpyDeviceToHost, h->copy_stream));
+  CUDA_TRY(h, cudaEventRecord(I.snap_done, h->copy_stream));
+  I.snap_pending = true;
+  return PFDD_OK;
+}
+
+template <typename T>
 pfdd_status cond_step_impl(pfdd_gpu *h, Instance &I, int n_iters, pfdd_cond_stats *stats) {
   using C = cx<T>;
   constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
@@ -1801,6 +1842,28 @@ pfdd_status pfdd_gpu_cond_get_state(pfdd_gpu *h, int inst, double *re, double *i
   return PFDD_OK;
 }
 
+pfdd_status pfdd_gpu_snapshot_begin(pfdd_gpu *h, int inst, double *re, double *im) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  if (!re && !im) return fail(h, PFDD_EINVAL, "need re or im");
+  cudaSetDevice(h->device);
+  Instance &I = *h->inst[inst];
+  return h->precision == PFDD_FP64 ? snapshot_begin_impl<double>(h, I, re, im)
+                                   : snapshot_begin_impl<float>(h, I, re, im);
+}
+
+pfdd_status pfdd_gpu_snapshot_wait(pfdd_gpu *h, int inst) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
+  cudaSetDevice(h->device);
+  Instance &I = *h->inst[inst];
+  if (!I.snap_pending) return PFDD_OK;
+  CUDA_TRY(h, cudaEventSynchronize(I.snap_done));
+  I.snap_pending = false;
+  CUDA_TRY(h, cudaGetLastError());
+  return PFDD_OK;
+}
+
 pfdd_status pfdd_gpu_cond_step(pfdd_gpu *h, int inst, int n_iters, pfdd_cond_stats *stats) {
   if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
   if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
@@ -1857,10 +1920,16 @@ void pfdd_gpu_destroy(pfdd_gpu *h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
   for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
   h->graphs.clear();
   h->groups.clear();
+  for (auto &ip : h->inst) {
+    if (ip->snap_ready) cudaEventDestroy(ip->snap_ready);
+    if (ip->snap_done) cudaEventDestroy(ip->snap_done);
+  }
   h->inst.clear();
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   h->staging.release();
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;

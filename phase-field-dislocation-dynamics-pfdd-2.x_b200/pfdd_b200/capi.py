@@ -31,7 +31,7 @@ EXPORTS = [
     "pfdd_gpu_get_state_interleaved", "pfdd_gpu_advance", "pfdd_gpu_step_history", "pfdd_gpu_energy",
     "pfdd_gpu_tau", "pfdd_gpu_info", "pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version",
     "pfdd_gpu_set_stream", "pfdd_gpu_profile", "pfdd_gpu_adjoint", "pfdd_gpu_strain_stress",
-    "pfdd_gpu_core_profile", "pfdd_cond_layers", "pfdd_gpu_cond_enable", "pfdd_gpu_cond_set_state",
+    "pfdd_gpu_core_profile", "pfdd_gpu_snapshot_begin", "pfdd_gpu_snapshot_wait", "pfdd_cond_layers", "pfdd_gpu_cond_enable", "pfdd_gpu_cond_set_state",
     "pfdd_gpu_cond_get_state", "pfdd_gpu_cond_step",
 ]
 KERNELS = ["fwd_planes", "xpencil", "step_planes", "finalize"]
@@ -112,6 +112,8 @@ def load(path: str = LIB_PATH):
     lib.pfdd_gpu_energy.argtypes = [vp, ctypes.c_int, DP, DP, DP]
     lib.pfdd_gpu_strain_stress.argtypes = [vp, ctypes.c_int, DP, DP, DP, DP]
     lib.pfdd_gpu_core_profile.argtypes = [vp, ctypes.c_int, ctypes.c_int, DP, DP]
+    lib.pfdd_gpu_snapshot_begin.argtypes = [vp, ctypes.c_int, DP, DP]
+    lib.pfdd_gpu_snapshot_wait.argtypes = [vp, ctypes.c_int]
     lib.pfdd_cond_layers.argtypes = [ctypes.POINTER(CondMaterial), ctypes.POINTER(CondMaterial), ctypes.c_int,
                                      ctypes.c_double, DP, DP]
     lib.pfdd_gpu_cond_enable.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CondDesc)]
@@ -270,6 +272,15 @@ class Stepper:
         e = np.empty(3)
         self._check(self._lib.pfdd_gpu_energy(self.h, inst, _dp(e[0:1]), _dp(e[1:2]), _dp(e[2:3])))
         return tuple(e)
+
+    def snapshot_begin(self, inst, re, im=None):
+        """Start copying the current state into re / im (float64 arrays of
+        S*N, ideally page-locked); they are filled when snapshot_wait returns."""
+        self._snap = (re, im)   # keep the buffers alive until the wait
+        self._check(self._lib.pfdd_gpu_snapshot_begin(self.h, inst, _dp(re), _dp(im) if im is not None else None))
+
+    def snapshot_wait(self, inst):
+        self._check(self._lib.pfdd_gpu_snapshot_wait(self.h, inst))
 
     def cond_enable(self, inst, sigma_eff, sigma_layer, El_y, epsilonzero, timestep=1.0):
         eff = np.ascontiguousarray(sigma_eff, dtype=np.float64)

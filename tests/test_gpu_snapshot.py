@@ -1,0 +1,46 @@
+"""Asynchronous state snapshots (pfdd_gpu_snapshot_begin / _wait): the copy
+of the state after step 3 runs beside steps 4..7 and equals the oracle's
+state after 3 steps (FP64, 1e-10); the stepping itself is unchanged."""
+import numpy as np
+import pytest
+
+import pfdd_oracle as O
+from common import oracle_instance, small_loop
+from pfdd_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("imag,pinned", [(capi.IMAG_FULL, True), (capi.IMAG_NYQUIST, True),
+                                         (capi.IMAG_NYQUIST, False)])
+def test_snapshot_beside_the_next_steps(imag, pinned):
+    import torch
+    w = small_loop(16)
+    n = w.S * w.N
+    if pinned:
+        re = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+        im = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    else:
+        re, im = np.empty(n), np.empty(n)
+    inst = oracle_instance(w)
+    ref3, _, _ = O.run(inst, w.xi0, 3)
+    ref7, _, _ = O.run(inst, ref3, 4)
+    with capi.Stepper.from_workloads([w], precision=capi.FP64, imag_mode=imag) as st:
+        st.set_state(0, w.xi0)
+        st.advance(3)
+        st.snapshot_begin(0, re, im)
+        st.advance(4)
+        st.snapshot_wait(0)
+        first = re.copy()
+        r7, i7 = st.get_state(0)
+        # a second snapshot into the same device buffer
+        st.snapshot_begin(0, re, None)
+        st.snapshot_wait(0)
+        second = re.copy()
+    shape = (w.S, w.nx, w.ny, w.nz)
+    assert np.abs(first.reshape(shape) - ref3.real).max() <= 1e-10
+    assert np.abs(second.reshape(shape) - ref7.real).max() <= 1e-10
+    assert np.abs(r7 - ref7.real).max() <= 1e-10
+    assert np.abs(i7 - ref7.imag).max() <= 1e-10
+    # the first snapshot's imaginary part was not overwritten by the second call
+    assert np.abs(im.reshape(shape) - ref3.imag).max() <= 1e-10
