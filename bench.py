@@ -19,6 +19,10 @@ whole grid; the metric is site-slip updates per second (S * N per step).
   cpu_baseline  the reference sources compiled as a CPU oracle (oracle/_ref),
             timed on a bounded sample on this host (rank 0, N = 1 only)
 
+Before the warm-up the x-pencil tile width of every batched group is chosen
+by timing (pfdd_gpu_autotune, outside the timed region, like a planner);
+--no-autotune keeps the set-up's rule.
+
 Multi-GPU (torchrun): every rank advances its own replica (no data-path
 collective; scaling "weak"); the time is the max over ranks.
 --impl reference times the reference's own CPU code on this host's cores
@@ -266,6 +270,7 @@ def fp32_vs_fp64(ws, K, stream, local, steps=2000):
         with capi.Stepper.from_workloads([w], precision=prec, device=local) as st:
             st.set_stream(stream.cuda_stream)
             st.set_state(0, w.xi0)
+            st.autotune(reps=5)
             st.advance(5)
             ms, _ = timed_events(stream, lambda: st.profile(K))
             out[name + "_ms_per_step"] = ms / K
@@ -346,6 +351,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the set-up's x-pencil tile widths instead of timing them (pfdd_gpu_autotune)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -378,6 +385,8 @@ def main():
     st.set_stream(stream.cuda_stream)
     for i, w in enumerate(ws):
         st.set_state(i, w.xi0)
+    # measured x-pencil tile widths (a planner step before the clock starts)
+    tile_widths = None if args.no_autotune else sorted(set(st.autotune(reps=5)))
     st.advance(args.warmup)
 
     # timed region: K GL iterations with per-kernel events (profile pass)
@@ -491,6 +500,7 @@ def main():
                        "imag_part": ("full complex carrier (obstacle mask)" if ws[0].xo is not None else
                                      "Nyquist-plane spectrum carried in the x-pencil pass"),
                        "parallelism": "replicas x%d" % world,
+                       "pencil_tile_widths": tile_widths if tile_widths is not None else "set-up rule",
                        "l2": "working set %.2f GB > 126 MB L2 (no flush)" % (dev_bytes / 1e9)},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches_per_step * args.steps + 2 * (launches_per_step // 3),

@@ -210,6 +210,14 @@ pfdd_status pfdd_gpu_strain_stress(pfdd_gpu *h, int inst, double *eps, double *s
  * n_slip/3 otherwise (beyond that the reference reads past its array). */
 pfdd_status pfdd_gpu_core_profile(pfdd_gpu *h, int inst, int n_planes, double *delta, double *ddelta);
 
+/* Pick each batched group's x-pencil tile width (the number of (ky, kz)
+ * columns a CTA transforms along x) by timing every width the grid divides
+ * into and shared memory holds, `reps` launches each, on this device; the
+ * fastest is kept (chosen[n_instances] receives it, or NULL).  No counterpart
+ * in the reference (FFTW's planner measures its own plans,
+ * src/fft_fftw_slab.cpp:125-134).  Valid between calls; the state is kept. */
+pfdd_status pfdd_gpu_autotune(pfdd_gpu *h, int reps, int *chosen);
+
 /* Asynchronous snapshot of instance `inst`'s order parameter for output
  * (the reference's dumps and diagnostics read fft->xi between GL iterations,
  * src/output.cpp:79-188, src/dump_text.cpp:296-324): the state is converted

@@ -194,6 +194,31 @@ pfdd_status upload_twiddles(pfdd_gpu *h, DevBuf &dst, int n, int count) {
   return upload_table<T>(h, dst, tw);
 }
 
+// x-pencil tile of cc (ky, kz) columns: narrowest width is one 16-byte row
+// chunk; the field stride is padded so consecutive fields start cc columns
+// apart in the 32 shared-memory banks (the x FFT walks columns, then fields,
+// across a warp); the tile's shared memory holds the fields, the x twiddles,
+// reduction scratch, wave-vector parts (x slots and the tile's columns), the
+// columns' slots and the Nyquist snapshot.
+template <typename T> int pencil_cmin() { return (int)(16 / sizeof(cx<T>)) > 1 ? (int)(16 / sizeof(cx<T>)) : 1; }
+
+template <typename T> int pencil_fstride(const Instance &I, int cc) {
+  using C = cx<T>;
+  const int wpc = (int)(sizeof(C) / 4);
+  const int target = (cc * wpc) % 32;
+  for (int pad = 0; pad < 64; ++pad)
+    if ((pad * sizeof(C)) % 16 == 0 && (((size_t)I.nx * cc + pad) * wpc) % 32 == (size_t)target)
+      return I.nx * cc + pad;
+  return I.nx * cc;
+}
+
+template <typename T> size_t pencil_smem(const Instance &I, int cc) {
+  using C = cx<T>;
+  return ((size_t)I.F * pencil_fstride<T>(I, cc) + (size_t)I.nx) * sizeof(C) + 64 * sizeof(double) +
+         ((size_t)I.nx + 2 * (size_t)cc) * sizeof(V4<T>) + 2 * (size_t)((cc + 3) & ~3) * sizeof(int) +
+         (size_t)cc * I.S * sizeof(C);
+}
+
 template <typename T>
 pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   const pfdd_instance_desc &d = I.d;
@@ -299,24 +324,9 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   if (I.smem_update > limit)
     return fail(h, PFDD_EUNSUPPORTED, "x-plane of %dx%d does not fit shared memory in this precision", I.ny, I.nz);
   const size_t ncols = (size_t)I.ny * I.nzp;
-  const int cmin = (int)(16 / sizeof(C)) > 1 ? (int)(16 / sizeof(C)) : 1;  // 16-byte row chunks
-  // field stride padded so consecutive fields start cc columns apart in the
-  // 32 shared-memory banks (the x-FFT walks columns, then fields, across a warp)
-  auto fstride_for = [&](int cc) {
-    const int wpc = (int)(sizeof(C) / 4);
-    const int target = (cc * wpc) % 32;
-    for (int pad = 0; pad < 64; ++pad)
-      if ((pad * sizeof(C)) % 16 == 0 && (((size_t)I.nx * cc + pad) * wpc) % 32 == (size_t)target)
-        return I.nx * cc + pad;
-    return I.nx * cc;
-  };
-  // tile, x twiddles, reduction scratch, wave-vector parts (x slots and the
-  // tile's columns) and the columns' slots
-  auto pencil_bytes = [&](int cc) {
-    return ((size_t)I.F * fstride_for(cc) + (size_t)I.nx) * sizeof(C) + 64 * sizeof(double) +
-           ((size_t)I.nx + 2 * (size_t)cc) * sizeof(V4<T>) + 2 * (size_t)((cc + 3) & ~3) * sizeof(int) +
-           (size_t)cc * I.S * sizeof(C);
-  };
+  const int cmin = pencil_cmin<T>();
+  auto fstride_for = [&](int cc) { return pencil_fstride<T>(I, cc); };
+  auto pencil_bytes = [&](int cc) { return pencil_smem<T>(I, cc); };
   int cc = 32;
   // widest tile that fits the budget and still gives every SM two tiles
   while (cc > cmin && (ncols % cc || pencil_bytes(cc) > PFDD_PENCIL_SMEM_KB * 1024 ||
@@ -598,15 +608,12 @@ void enqueue_group_open(Instance &L, const Group &G, cudaStream_t st) {
 // One GL iteration of every instance of group G whose spectrum is current
 // (3 launches: P2, the fused plane pass, finalize); fwd: the plane pass also
 // leaves the next step's spectrum.  ev[0..3] bracket the three launches.
+// P2 of every member of a group (one launch, grid.y = members)
 template <typename T>
-void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol, bool fwd, cudaEvent_t *ev = nullptr) {
+void launch_group_pencil(const Instance &L, const Group &G, cudaStream_t st) {
   constexpr int NC = Threads<T>::pencil;
   const unsigned B = (unsigned)G.members.size();
   const InstPtrs *tab = static_cast<const InstPtrs *>(G.table.p);
-  PlaneArgs pa;
-  fill_plane_args<T>(L, pa);
-  const int planes = L.F * L.nx;
-  if (ev) cudaEventRecord(ev[0], st);
   PencilArgs pe;
   pe = PencilArgs{};
   pe.px = L.px;
@@ -625,6 +632,18 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   with_pencil_sc(L.S, [&](auto SCc) {
     k_xpencil_tab<T, NC, decltype(SCc)::value><<<dim3(L.ntiles, B), NC, L.smem_pencil, st>>>(tab, pe);
   });
+}
+
+template <typename T>
+void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol, bool fwd, cudaEvent_t *ev = nullptr) {
+  constexpr int NC = Threads<T>::pencil;
+  const unsigned B = (unsigned)G.members.size();
+  const InstPtrs *tab = static_cast<const InstPtrs *>(G.table.p);
+  PlaneArgs pa;
+  fill_plane_args<T>(L, pa);
+  const int planes = L.F * L.nx;
+  if (ev) cudaEventRecord(ev[0], st);
+  launch_group_pencil<T>(L, G, st);
   if (ev) cudaEventRecord(ev[1], st);
   UpdateArgs ua;
   memset(&ua, 0, sizeof ua);
@@ -1356,6 +1375,96 @@ bool valid_size(int n) {
 
 }  // namespace
 
+// Measured choice of the x-pencil tile width per group: every width the
+// group's grid divides into and shared memory holds is timed on the device
+// (CUDA events, `reps` launches after one warm-up) and the fastest kept.  The
+// trial launches overwrite the spectrum buffer, which holds no state between
+// calls (every advance opens with a forward pass), and the Nyquist carriers
+// and stop flags, which are saved and restored.  Captured graphs are dropped.
+template <typename T>
+pfdd_status autotune_impl(pfdd_gpu *h, int reps, int *chosen) {
+  constexpr int NC = Threads<T>::pencil;
+  cudaStream_t st = h->stream;
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
+  h->graphs.clear();
+  cudaEvent_t e0, e1;
+  CUDA_TRY(h, cudaEventCreate(&e0));
+  CUDA_TRY(h, cudaEventCreate(&e1));
+  struct Ev {
+    cudaEvent_t a, b;
+    ~Ev() { cudaEventDestroy(a); cudaEventDestroy(b); }
+  } guard{e0, e1};
+  auto apply = [&](const Group &G, int cc) -> pfdd_status {
+    for (int m : G.members) {
+      Instance &I = *h->inst[m];
+      const size_t ncols = (size_t)I.ny * I.nzp;
+      I.ccols = cc;
+      I.fstride = pencil_fstride<T>(I, cc);
+      I.ntiles = (int)(ncols / cc);
+      I.smem_pencil = pencil_smem<T>(I, cc);
+      if (I.imag == IMAG_NYQ && I.ppart.bytes < 2 * (size_t)I.ntiles * sizeof(double)) {
+        I.ppart.release();
+        CUDA_TRY(h, I.ppart.alloc(2 * (size_t)I.ntiles * sizeof(double)));
+      }
+    }
+    cudaError_t e = cudaSuccess;
+    with_pencil_sc(h->inst[G.members[0]]->S, [&](auto SCc) {
+      constexpr int SC = decltype(SCc)::value;
+      const size_t b = h->inst[G.members[0]]->smem_pencil;
+      if (e == cudaSuccess) e = raise_smem_limit(k_xpencil<T, NC, SC>, b);
+      if (e == cudaSuccess) e = raise_smem_limit(k_xpencil_tab<T, NC, SC>, b);
+    });
+    CUDA_TRY(h, e);
+    return refresh_tables(h);
+  };
+  for (size_t gi = 0; gi < h->groups.size(); ++gi) {
+    const Group &G = h->groups[gi];
+    Instance &L = *h->inst[G.members[0]];
+    // live state the trial launches touch
+    std::vector<std::vector<unsigned char>> aux(G.members.size());
+    std::vector<int> stop(G.members.size());
+    for (size_t k = 0; k < G.members.size(); ++k) {
+      Instance &I = *h->inst[G.members[k]];
+      if (I.aux.bytes) {
+        aux[k].resize(I.aux.bytes);
+        CUDA_TRY(h, cudaMemcpy(aux[k].data(), I.aux.p, I.aux.bytes, cudaMemcpyDeviceToHost));
+      }
+      CUDA_TRY(h, cudaMemcpy(&stop[k], I.flags(), sizeof(int), cudaMemcpyDeviceToHost));
+      CUDA_TRY(h, cudaMemset(I.flags(), 0, sizeof(int)));
+    }
+    const size_t ncols = (size_t)L.ny * L.nzp;
+    int best = L.ccols;
+    float best_ms = 0.0f;
+    for (int cc = 32; cc >= pencil_cmin<T>(); cc >>= 1) {
+      if (ncols % cc || pencil_smem<T>(L, cc) > 227 * 1024) continue;
+      pfdd_status ps = apply(G, cc);
+      if (ps != PFDD_OK) return ps;
+      launch_group_pencil<T>(L, G, st);
+      CUDA_TRY(h, cudaEventRecord(e0, st));
+      for (int r = 0; r < reps; ++r) launch_group_pencil<T>(L, G, st);
+      CUDA_TRY(h, cudaEventRecord(e1, st));
+      CUDA_TRY(h, cudaEventSynchronize(e1));
+      CUDA_TRY(h, cudaGetLastError());
+      float ms = 0.0f;
+      CUDA_TRY(h, cudaEventElapsedTime(&ms, e0, e1));
+      if (best_ms == 0.0f || ms < best_ms) {
+        best_ms = ms;
+        best = cc;
+      }
+    }
+    pfdd_status ps = apply(G, best);
+    if (ps != PFDD_OK) return ps;
+    for (size_t k = 0; k < G.members.size(); ++k) {
+      Instance &I = *h->inst[G.members[k]];
+      if (I.aux.bytes) CUDA_TRY(h, cudaMemcpy(I.aux.p, aux[k].data(), I.aux.bytes, cudaMemcpyHostToDevice));
+      CUDA_TRY(h, cudaMemcpy(I.flags(), &stop[k], sizeof(int), cudaMemcpyHostToDevice));
+      if (chosen) chosen[G.members[k]] = best;
+    }
+  }
+  return PFDD_OK;
+}
+
 template <typename T>
 pfdd_status snapshot_begin_impl(pfdd_gpu *h, Instance &I, double *re, double *im) {
   const size_t n = (size_t)I.S * I.N;
@@ -1840,6 +1949,13 @@ pfdd_status pfdd_gpu_cond_get_state(pfdd_gpu *h, int inst, double *re, double *i
     }
   }
   return PFDD_OK;
+}
+
+pfdd_status pfdd_gpu_autotune(pfdd_gpu *h, int reps, int *chosen) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (reps < 1) return fail(h, PFDD_EINVAL, "reps must be >= 1");
+  cudaSetDevice(h->device);
+  return h->precision == PFDD_FP64 ? autotune_impl<double>(h, reps, chosen) : autotune_impl<float>(h, reps, chosen);
 }
 
 pfdd_status pfdd_gpu_snapshot_begin(pfdd_gpu *h, int inst, double *re, double *im) {

@@ -31,7 +31,7 @@ EXPORTS = [
     "pfdd_gpu_get_state_interleaved", "pfdd_gpu_advance", "pfdd_gpu_step_history", "pfdd_gpu_energy",
     "pfdd_gpu_tau", "pfdd_gpu_info", "pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version",
     "pfdd_gpu_set_stream", "pfdd_gpu_profile", "pfdd_gpu_adjoint", "pfdd_gpu_strain_stress",
-    "pfdd_gpu_core_profile", "pfdd_gpu_snapshot_begin", "pfdd_gpu_snapshot_wait", "pfdd_cond_layers", "pfdd_gpu_cond_enable", "pfdd_gpu_cond_set_state",
+    "pfdd_gpu_core_profile", "pfdd_gpu_autotune", "pfdd_gpu_snapshot_begin", "pfdd_gpu_snapshot_wait", "pfdd_cond_layers", "pfdd_gpu_cond_enable", "pfdd_gpu_cond_set_state",
     "pfdd_gpu_cond_get_state", "pfdd_gpu_cond_step",
 ]
 KERNELS = ["fwd_planes", "xpencil", "step_planes", "finalize"]
@@ -112,6 +112,7 @@ def load(path: str = LIB_PATH):
     lib.pfdd_gpu_energy.argtypes = [vp, ctypes.c_int, DP, DP, DP]
     lib.pfdd_gpu_strain_stress.argtypes = [vp, ctypes.c_int, DP, DP, DP, DP]
     lib.pfdd_gpu_core_profile.argtypes = [vp, ctypes.c_int, ctypes.c_int, DP, DP]
+    lib.pfdd_gpu_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.pfdd_gpu_snapshot_begin.argtypes = [vp, ctypes.c_int, DP, DP]
     lib.pfdd_gpu_snapshot_wait.argtypes = [vp, ctypes.c_int]
     lib.pfdd_cond_layers.argtypes = [ctypes.POINTER(CondMaterial), ctypes.POINTER(CondMaterial), ctypes.c_int,
@@ -272,6 +273,13 @@ class Stepper:
         e = np.empty(3)
         self._check(self._lib.pfdd_gpu_energy(self.h, inst, _dp(e[0:1]), _dp(e[1:2]), _dp(e[2:3])))
         return tuple(e)
+
+    def autotune(self, reps=5):
+        """Time every x-pencil tile width per group and keep the fastest;
+        returns the chosen width per instance."""
+        out = (ctypes.c_int * len(self.descs))()
+        self._check(self._lib.pfdd_gpu_autotune(self.h, int(reps), out))
+        return list(out)
 
     def snapshot_begin(self, inst, re, im=None):
         """Start copying the current state into re / im (float64 arrays of
