@@ -296,7 +296,9 @@ pfdd_status pfdd_gpu_cond_step(pfdd_gpu *h, int inst, int n_iters, pfdd_cond_sta
  * applied stress.  Forward pass with a state checkpoint every ckpt_every
  * steps; backward pass per segment (forward recompute, then adjoint steps
  *   lam_n = lam_{n+1} - CD dt (L lam_{n+1} + f''(xi_n) lam_{n+1}),
- * L the self-adjoint elastic operator, masked sites frozen).
+ * L the self-adjoint elastic operator, masked sites frozen).  ckpt_every >=
+ * n_steps keeps every Re xi_n of the forward pass (n_steps * S * N values in
+ * the compute precision on the device) and recomputes nothing. 
  *   xi_target  host [S*N] target for Re xi_N (reference site order)
  *   loss       receives J (may be NULL)
  *   dL_dparams [2]: sine / sine-field cores dJ/d(isf, usf); perfect / USFE

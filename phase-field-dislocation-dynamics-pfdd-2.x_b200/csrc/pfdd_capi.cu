@@ -1012,10 +1012,16 @@ pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const dou
   k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.an(), I.stress, 0, I.flags());
   PlaneArgs pa;
   fill_plane_args<T>(I, pa);
-  // forward with checkpoints: one opening transform, then fused steps
+  // forward with checkpoints: one opening transform, then fused steps.  With
+  // one segment (K >= n_steps) the forward pass keeps every state the
+  // backward steps read, and nothing is recomputed.
+  const bool store_all = K >= n_steps;
   launch_fwd<T>(I, st, I.xi[I.cur].as<T>(), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
   for (int n = 0; n < n_steps; ++n) {
     if (n % K == 0) CUDA_TRY(h, save(n / K));
+    if (store_all)
+      CUDA_TRY(h, cudaMemcpyAsync(seg.as<T>() + (size_t)n * n_re, I.xi[I.cur].p, n_re * sizeof(T),
+                                  cudaMemcpyDeviceToDevice, st));
     enqueue_step_fused<T>(I, st, n + 1 < n_steps);
     I.cur ^= 1;
   }
@@ -1034,10 +1040,11 @@ pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const dou
   // backward over segments
   for (int j = nck - 1; j >= 0; --j) {
     const int n0 = j * K, n1 = std::min(n_steps, n0 + K);
-    CUDA_TRY(h, restore(j));
+    if (!store_all) CUDA_TRY(h, restore(j));
     // recompute the segment's states (fused steps after one opening transform)
-    if (n1 - n0 > 1) launch_fwd<T>(I, st, I.xi[I.cur].as<T>(), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
-    for (int n = n0; n < n1; ++n) {
+    if (!store_all && n1 - n0 > 1)
+      launch_fwd<T>(I, st, I.xi[I.cur].as<T>(), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
+    for (int n = n0; n < n1 && !store_all; ++n) {
       CUDA_TRY(h, cudaMemcpyAsync(seg.as<T>() + (size_t)(n - n0) * n_re, I.xi[I.cur].p, n_re * sizeof(T),
                                   cudaMemcpyDeviceToDevice, st));
       if (n + 1 < n1) {

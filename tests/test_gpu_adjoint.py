@@ -116,3 +116,19 @@ def test_autograd_function_wrapper():
     _, dp, _, _ = _gpu_adjoint(w0, target)
     assert float(isf.grad) == pytest.approx(dp[0], rel=1e-12)
     assert float(usf.grad) == pytest.approx(dp[1], rel=1e-12)
+
+
+def test_store_all_equals_checkpointed():
+    """ckpt_every >= n_steps keeps every forward state (no recomputation) and
+    gives the checkpointed call's loss and gradients."""
+    w = _workload(False)
+    target = _target(w)
+    a = _gpu_adjoint(w, target)
+    with capi.Stepper.from_workloads([w], precision=capi.FP64) as st:
+        st.set_state(0, w.xi0)
+        loss, dp, ds = st.adjoint(0, N_STEPS, N_STEPS, target)
+        re, _ = st.get_state(0)
+    assert abs(loss - a[0]) <= 1e-12 * abs(a[0])
+    np.testing.assert_allclose(dp, a[1], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(ds, a[2], rtol=1e-12, atol=1e-12 * np.abs(a[2]).max())
+    assert np.abs(re - a[3]).max() == 0.0
