@@ -28,7 +28,9 @@ def _oracle(cc, eff, lay, c0, n):
     return c, np.array(out)
 
 
-@pytest.mark.parametrize("shape", [(8, 32, 8), (16, 24, 12)])
+# (8, 32, 8) and (16, 24, 12) run split planes (2-CTA clusters: too few planes
+# for the SMs), (384, 16, 8) whole-plane CTAs
+@pytest.mark.parametrize("shape", [(8, 32, 8), (16, 24, 12), (384, 16, 8)])
 def test_cond_step_matches_oracle(shape):
     cc, eff, lay, c0 = _case(*shape)
     ref, st_ref = _oracle(cc, eff, lay, c0, 3)
