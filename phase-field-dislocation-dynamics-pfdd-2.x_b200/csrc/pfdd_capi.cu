@@ -636,7 +636,6 @@ void launch_group_pencil(const Instance &L, const Group &G, cudaStream_t st) {
 
 template <typename T>
 void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol, bool fwd, cudaEvent_t *ev = nullptr) {
-  constexpr int NC = Threads<T>::pencil;
   const unsigned B = (unsigned)G.members.size();
   const InstPtrs *tab = static_cast<const InstPtrs *>(G.table.p);
   PlaneArgs pa;
