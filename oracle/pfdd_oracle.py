@@ -404,6 +404,8 @@ class CoreModel:
             return isf * np.sin(PI * xr) ** 2 + Cn * np.sin(2 * PI * xr) ** 2
         if f == 7:
             return self.site / s * np.sin(PI * xr) ** 2
+        if f == 5:   # usf' cof(theta) sin^2(pi xi), as core_energy_bcc_perfect accumulates it (:1119)
+            return self.usf / s * self._bcc_cof(xr) * np.sin(PI * xr) ** 2
         raise ValueError("energy of core model %d not restated" % f)
 
 

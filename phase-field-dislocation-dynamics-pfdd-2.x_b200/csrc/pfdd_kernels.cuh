@@ -1032,9 +1032,11 @@ __device__ __forceinline__ T core_derivative(const Core &cm, T x, int a, size_t 
 // accumulates E_core but never reduces it, fft_fftw_slab.cpp:1399).
 template <typename T>
 __device__ __forceinline__ T core_energy_density(const Core &cm, T x, int a, size_t r, size_t N,
-                                                 const T *__restrict__ site) {
+                                                 const T *__restrict__ site, const T *__restrict__ xin) {
   const T s1 = sinpi_t<T>(x), s2 = sinpi_t<T>((T)2 * x);
   switch (cm.flag) {
+    case 5:   // BCC perfect: usf' cof(theta) sin^2(pi x) (fft_fftw_slab.cpp:1119)
+      return core_k<T>(cm, 10) * bcc_cof<T>(cm, a, r, N, xin) * s1 * s1;
     case 1:
       return core_k<T>(cm, 10) * s1 * s1;
     case 6:
@@ -1250,7 +1252,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
         const double x = (double)xv[q];
         e_el += 0.5 * x * (double)(e[q] * invN);
         if (real_field) {
-          e_core += (double)core_energy_density<T>(u.core, xv[q], sys, rbase + idx + q, N, site);
+          e_core += (double)core_energy_density<T>(u.core, xv[q], sys, rbase + idx + q, N, site, xin);
           e_app -= tau * x;
         }
       }

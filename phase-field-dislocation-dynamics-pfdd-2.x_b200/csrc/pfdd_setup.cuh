@@ -240,6 +240,7 @@ inline bool build_core(const pfdd_instance_desc &d, Core &c) {
     }
     if (d.core_flag == PFDD_CORE_MPEA) c.k[10] = 1.0 / s;
   }
+  if (d.core_flag == PFDD_CORE_BCC_PERFECT) c.k[10] = d.usf / s;   // usf' of the energy density
   for (int i = 0; i < 12; ++i) c.kf[i] = (float)c.k[i];
   return true;
 }

@@ -161,3 +161,23 @@ def test_nyquist_rejects_mask():
     w.xo = np.zeros((w.S, 16, 16, 16))
     with pytest.raises(capi.PfddError):
         capi.Stepper.from_workloads([w], imag_mode=capi.IMAG_NYQUIST)
+
+
+@pytest.mark.parametrize("make", ["loop", "skew"])
+def test_bcc_perfect_energy(make):
+    """Energy with core model 5: usf' cof(theta) sin^2(pi xi) summed with the
+    elastic and applied terms, FP64, against the oracle."""
+    if make == "loop":
+        w = configs.loop_workload(n=16, nz=8, radius=4.0, seed=8, sigma_mpa=250.0)
+    else:
+        w = configs.frank_read_workload(nx=16, ny=16, nz=8, seg=4)
+    w.core_flag = capi.CORE_BCC_PERFECT
+    inst = oracle_instance(w)
+    xi, _, _ = O.run(inst, w.xi0, 5)
+    want = O.total_energy(inst, xi)
+    with capi.Stepper.from_workloads([w], precision=capi.FP64) as st:
+        st.set_state(0, w.xi0)
+        st.advance(5)
+        got = st.energy(0)
+    for g, e in zip(got, want):
+        assert abs(g - e) <= 1e-10 * max(1.0, abs(e)), (got, want)
