@@ -181,8 +181,9 @@ pfdd_status pfdd_gpu_step_history(pfdd_gpu *h, int inst, double *xinorm, double 
  * (src/fft_fftw_slab.cpp:1399); these are the terms whose gradient is the
  * drift of update_order_parameter (src/fft_fftw_slab.cpp:1773).  For core
  * model 5 the core term is sum usf' cof(theta) sin^2(pi xi) as
- * core_energy_bcc_perfect accumulates it (:1119), whose force holds cof fixed.
- * Core models 2 and 4 return PFDD_EUNSUPPORTED. */
+ * core_energy_bcc_perfect accumulates it (:1119), whose force holds cof fixed;
+ * for core model 2 it is the fcore of each plane of three systems (:1320).
+ * Core model 4 returns PFDD_EUNSUPPORTED. */
 pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_core,
                             double *e_applied);
 

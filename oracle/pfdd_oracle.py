@@ -406,6 +406,23 @@ class CoreModel:
             return self.site / s * np.sin(PI * xr) ** 2
         if f == 5:   # usf' cof(theta) sin^2(pi xi), as core_energy_bcc_perfect accumulates it (:1119)
             return self.usf / s * self._bcc_cof(xr) * np.sin(PI * xr) ** 2
+        if f == 2:   # fcore of each plane of three systems (:1320), on the plane's first system
+            c0, c1, c2, c3, c4, a1, a3 = (v / self.mu for v in self.c)
+            db = self.dslip * self.b
+            out = np.zeros_like(xr)
+            cos, sin, tp, fp = np.cos, np.sin, 2.0 * PI, 4.0 * PI
+            for p in range(xr.shape[0] // 3):
+                x1, x2, x3 = xr[3 * p], xr[3 * p + 1], xr[3 * p + 2]
+                out[3 * p] = (c0 + c1 * (cos(tp * (x1 - x2)) + cos(tp * (x2 - x3)) + cos(tp * (x3 - x1)))
+                              + c2 * (cos(tp * (2.0 * x1 - x2 - x3)) + cos(tp * (2.0 * x2 - x3 - x1))
+                                      + cos(tp * (2.0 * x3 - x1 - x2)))
+                              + c3 * (cos(fp * (x1 - x2)) + cos(fp * (x2 - x3)) + cos(fp * (x3 - x1)))
+                              + c4 * (cos(tp * (3.0 * x1 - x2 - 2.0 * x3)) + cos(tp * (3.0 * x1 - 2.0 * x2 - x3))
+                                      + cos(tp * (3.0 * x2 - x3 - 2.0 * x1)) + cos(tp * (3.0 * x2 - 2.0 * x3 - x1))
+                                      + cos(tp * (3.0 * x3 - x1 - 2.0 * x2)) + cos(tp * (3.0 * x3 - 2.0 * x1 - x2)))
+                              + a1 * (sin(tp * (x1 - x2)) + sin(tp * (x2 - x3)) + sin(tp * (x3 - x1)))
+                              + a3 * (sin(fp * (x1 - x2)) + sin(fp * (x2 - x3)) + sin(fp * (x3 - x1)))) / db
+            return out
         raise ValueError("energy of core model %d not restated" % f)
 
 

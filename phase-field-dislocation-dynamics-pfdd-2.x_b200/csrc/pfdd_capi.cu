@@ -1792,7 +1792,7 @@ pfdd_status pfdd_gpu_energy(pfdd_gpu *h, int inst, double *e_elastic, double *e_
   if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
   Instance &I = *h->inst[inst];
   const int f = I.d.core_flag;
-  if (f == PFDD_CORE_EXTENDED || f == PFDD_CORE_PYRII)
+  if (f == PFDD_CORE_PYRII)
     return fail(h, PFDD_EUNSUPPORTED, "no energy density for core model %d", f);
   cudaSetDevice(h->device);
   return h->precision == PFDD_FP64 ? energy_impl<double>(h, I, e_elastic, e_core, e_applied)

@@ -1037,6 +1037,27 @@ __device__ __forceinline__ T core_energy_density(const Core &cm, T x, int a, siz
   switch (cm.flag) {
     case 5:   // BCC perfect: usf' cof(theta) sin^2(pi x) (fft_fftw_slab.cpp:1119)
       return core_k<T>(cm, 10) * bcc_cof<T>(cm, a, r, N, xin) * s1 * s1;
+    case 2: { // extended: fcore of the plane of systems 3p..3p+2 (fft_fftw_slab.cpp:1320), on its first system
+      const int p = a / 3;
+      if (a != 3 * p) return (T)0;
+      const T x1 = xin[(size_t)(3 * p) * N + r], x2 = xin[(size_t)(3 * p + 1) * N + r],
+              x3 = xin[(size_t)(3 * p + 2) * N + r];
+      auto C2 = [](T t) { return cospi_t<T>((T)2 * t); };
+      auto C4 = [](T t) { return cospi_t<T>((T)4 * t); };
+      auto S2 = [](T t) { return sinpi_t<T>((T)2 * t); };
+      auto S4 = [](T t) { return sinpi_t<T>((T)4 * t); };
+      const T two = (T)2, three = (T)3;
+      const T e = core_k<T>(cm, 7) +
+                  core_k<T>(cm, 0) * (C2(x1 - x2) + C2(x2 - x3) + C2(x3 - x1)) +
+                  core_k<T>(cm, 1) * (C2(two * x1 - x2 - x3) + C2(two * x2 - x3 - x1) + C2(two * x3 - x1 - x2)) +
+                  core_k<T>(cm, 2) * (C4(x1 - x2) + C4(x2 - x3) + C4(x3 - x1)) +
+                  core_k<T>(cm, 3) * (C2(three * x1 - x2 - two * x3) + C2(three * x1 - two * x2 - x3) +
+                                      C2(three * x2 - x3 - two * x1) + C2(three * x2 - two * x3 - x1) +
+                                      C2(three * x3 - x1 - two * x2) + C2(three * x3 - two * x1 - x2)) +
+                  core_k<T>(cm, 4) * (S2(x1 - x2) + S2(x2 - x3) + S2(x3 - x1)) +
+                  core_k<T>(cm, 5) * (S4(x1 - x2) + S4(x2 - x3) + S4(x3 - x1));
+      return core_k<T>(cm, 8) * e;
+    }
     case 1:
       return core_k<T>(cm, 10) * s1 * s1;
     case 6:

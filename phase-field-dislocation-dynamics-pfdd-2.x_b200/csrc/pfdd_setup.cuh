@@ -223,6 +223,8 @@ inline bool build_core(const pfdd_instance_desc &d, Core &c) {
       c.k[0] = d.c[1] / mu; c.k[1] = d.c[2] / mu; c.k[2] = d.c[3] / mu; c.k[3] = d.c[4] / mu;
       c.k[4] = d.c[5] / mu; c.k[5] = d.c[6] / mu;
       c.k[6] = (2.0 * M_PI) / (d.dslip * d.b);
+      c.k[7] = d.c[0] / mu;                  // c0' and 1/(dslip b) of the energy fcore (:1280, :1320)
+      c.k[8] = 1.0 / (d.dslip * d.b);
       break;
     default:
       return false;

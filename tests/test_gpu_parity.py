@@ -181,3 +181,23 @@ def test_bcc_perfect_energy(make):
         got = st.energy(0)
     for g, e in zip(got, want):
         assert abs(g - e) <= 1e-10 * max(1.0, abs(e)), (got, want)
+
+
+def test_extended_core_energy():
+    """Energy with core model 2 (three-system Fourier GSFE, the Ni preset of
+    the reference-written fixture): the plane's fcore, FP64, against the oracle,
+    and its gradient is the update's drift (energy decreases per step)."""
+    from common import load_golden
+    w, fx = load_golden("fcc12_extended")
+    inst = oracle_instance(w)
+    xi, _, _ = O.run(inst, fx["xi0"], 3)
+    want = O.total_energy(inst, xi)
+    with capi.Stepper.from_workloads([w], precision=capi.FP64) as st:
+        st.set_state(0, np.real(fx["xi0"]), np.imag(fx["xi0"]))
+        st.advance(3)
+        got = st.energy(0)
+        st.advance(1)
+        later = st.energy(0)
+    for g, e in zip(got, want):
+        assert abs(g - e) <= 1e-10 * max(1.0, abs(e)), (got, want)
+    assert sum(later) < sum(got)
