@@ -14,6 +14,29 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("imag,pinned", [(capi.IMAG_FULL, True), (capi.IMAG_NYQUIST, True),
                                          (capi.IMAG_NYQUIST, False)])
 def test_snapshot_beside_the_next_steps(imag, pinned):
+    _snapshot_case(imag, pinned, capi.FP64, 1e-10)
+
+
+def test_snapshot_fp32_equals_get_state():
+    """FP32 handle: the snapshot holds exactly what get_state returns at the
+    same step (the same conversion to FP64)."""
+    import torch
+    w = small_loop(16)
+    n = w.S * w.N
+    re = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    im = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    with capi.Stepper.from_workloads([w], precision=capi.FP32) as st:
+        st.set_state(0, w.xi0)
+        st.advance(3)
+        r3, i3 = st.get_state(0)
+        st.snapshot_begin(0, re, im)
+        st.advance(2)
+        st.snapshot_wait(0)
+    assert np.array_equal(re, r3.reshape(-1))
+    assert np.array_equal(im, i3.reshape(-1))
+
+
+def _snapshot_case(imag, pinned, prec, tol):
     import torch
     w = small_loop(16)
     n = w.S * w.N
@@ -25,7 +48,7 @@ def test_snapshot_beside_the_next_steps(imag, pinned):
     inst = oracle_instance(w)
     ref3, _, _ = O.run(inst, w.xi0, 3)
     ref7, _, _ = O.run(inst, ref3, 4)
-    with capi.Stepper.from_workloads([w], precision=capi.FP64, imag_mode=imag) as st:
+    with capi.Stepper.from_workloads([w], precision=prec, imag_mode=imag) as st:
         st.set_state(0, w.xi0)
         st.advance(3)
         st.snapshot_begin(0, re, im)
@@ -38,9 +61,9 @@ def test_snapshot_beside_the_next_steps(imag, pinned):
         st.snapshot_wait(0)
         second = re.copy()
     shape = (w.S, w.nx, w.ny, w.nz)
-    assert np.abs(first.reshape(shape) - ref3.real).max() <= 1e-10
-    assert np.abs(second.reshape(shape) - ref7.real).max() <= 1e-10
-    assert np.abs(r7 - ref7.real).max() <= 1e-10
-    assert np.abs(i7 - ref7.imag).max() <= 1e-10
+    assert np.abs(first.reshape(shape) - ref3.real).max() <= tol
+    assert np.abs(second.reshape(shape) - ref7.real).max() <= tol
+    assert np.abs(r7 - ref7.real).max() <= tol
+    assert np.abs(i7 - ref7.imag).max() <= tol
     # the first snapshot's imaginary part was not overwritten by the second call
-    assert np.abs(im.reshape(shape) - ref3.imag).max() <= 1e-10
+    assert np.abs(im.reshape(shape) - ref3.imag).max() <= tol
