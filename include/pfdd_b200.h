@@ -312,6 +312,14 @@ pfdd_status pfdd_gpu_cond_step(pfdd_gpu *h, int inst, int n_iters, pfdd_cond_sta
 pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every, const double *xi_target,
                              double *loss, double *dL_dparams, double *dL_dsigma);
 
+/* Set instance `inst`'s current applied stress (units of mu), replacing the
+ * device's copy; dsigma is kept.  The host side of the reference owns sigma
+ * (App::sigma, src/app.cpp:325-381, incremented by SolveGL::iterate after each
+ * stress state, src/solve_GL.cpp:150-155): a binding that advances one stress
+ * state in several chunks (output steps in between) sets it before each chunk,
+ * since pfdd_gpu_advance adds dsigma when a stress state ends. */
+pfdd_status pfdd_gpu_set_stress(pfdd_gpu *h, int inst, const double sigma[3][3]);
+
 /* Resolved shear stresses tau[S] of instance `inst` at the current stress state. */
 pfdd_status pfdd_gpu_tau(pfdd_gpu *h, int inst, double *tau);
 
@@ -350,9 +358,11 @@ void pfdd_gpu_destroy(pfdd_gpu *h);
 
 /* No counterpart in the reference.  One FP64 GL iteration of one instance
  * (Re and Im carried as full fields, so the result is the reference's) that
- * allocates nothing, for callers that cannot call cudaMalloc: code running
- * while a CUDA graph is captured, runtimes that own all device memory through
- * their own pool, and hosts that must not allocate after start-up.
+ * allocates nothing, for callers that cannot call cudaMalloc: host codes whose
+ * runtime hands out all device memory through its own pool (a direct
+ * cudaMalloc would fragment it or exceed the pool's reservation), and
+ * long-running or real-time hosts that must not allocate after start-up
+ * (an allocation can block on the device or fail at an arbitrary time).
  *   d_xi_in, d_xi_out  caller-owned DEVICE arrays of 2*S*N doubles: the S Re
  *                      planes, then the S Im planes (reference site order);
  *                      they must not alias
@@ -360,15 +370,17 @@ void pfdd_gpu_destroy(pfdd_gpu *h);
  *                      given, the call waits for the step and reports
  *                      PFDD_EDIVERGED / PFDD_ETIMEOUT, otherwise it returns
  *                      after enqueueing on `stream` (a cudaStream_t, NULL =
- *                      legacy default stream)
+ *                      legacy default stream) and reports neither: the next
+ *                      call clears the device flags unread
  * All scratch (half spectrum, partial sums, tables) lives in one file-scope
  * device array of PFDD_STATIC_SCRATCH_BYTES that every GPU loading the library
  * holds until exit; a grid needing more (e.g. above 64^3 with 3 systems)
  * returns PFDD_EINVAL and computes nothing -- use pfdd_gpu_create for those.
  * The first call on a device (with that device current) looks up the array's
- * device address and sets kernel attributes, so make it before any stream
- * capture.  Calls share the array and it keeps the last call's contents;
- * calls whose GPU work overlaps race on it.  The descriptor's mask, per-site
+ * device address and caches it for the process, so make it before any stream
+ * capture; cudaDeviceReset between calls is not supported (the cached address
+ * would be stale).  Calls share the array and it keeps the last call's
+ * contents; calls whose GPU work overlaps race on it.  The descriptor's mask, per-site
  * GSFE field and dsigma are not used (xo and site_gsfe must be NULL); tau is
  * taken at `sigma`. */
 pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, const double *d_xi_in, double *d_xi_out,

@@ -1,22 +1,26 @@
 // pfdd_gl_step_noalloc: one FP64 Ginzburg-Landau iteration of one instance on
 // caller-owned device buffers, without allocating any memory.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
-// being captured, runtimes that hand out all device memory through their own
-// pool and forbid direct allocation, and real-time or embedded hosts that must
-// not allocate after start-up.  For them this entry point keeps every piece of
-// scratch the step needs -- the half spectrum, the per-plane partial sums,
-// the stress/flag words, the twiddle and slot tables -- in one file-scope
-// device array of PFDD_STATIC_SCRATCH_BYTES.  Every GPU that loads the
-// library holds that array until the process exits.
+// Some callers cannot call cudaMalloc: host codes whose runtime hands out all
+// device memory through its own pool and forbids direct allocation (a stray
+// cudaMalloc would fragment the pool or exceed its reservation), and
+// long-running or real-time hosts that must not allocate after start-up (an
+// allocation can block on the device or fail at an arbitrary time).  For them
+// this entry point keeps every piece of scratch the step needs -- the half
+// spectrum, the per-plane partial sums, the stress/flag words, the twiddle and
+// slot tables -- in one file-scope device array of PFDD_STATIC_SCRATCH_BYTES.
+// Every GPU that loads the library holds that array until the process exits.
 //
 // Host code only ever sees a stand-in for the array's name, so the first call
 // on each device (with that device current) looks its device address up with
-// cudaGetSymbolAddress and raises the kernels' shared-memory limits; that
-// first call should therefore come before any stream capture.  All calls share
-// the one array and it keeps the last call's contents: the flags are cleared
-// on every call, and calls whose work overlaps on the GPU (different streams,
-// or different host threads on one device) race on it.
+// cudaGetSymbolAddress and caches it for the life of the process; that first
+// call should therefore come before any stream capture, and cudaDeviceReset
+// between calls is not supported (the cached address would be stale).  All
+// calls share the one array and it keeps the last call's contents: the flags
+// are cleared on every call, and calls whose work overlaps on the GPU
+// (different streams, or different host threads on one device) race on it.
+// Without h_stats the call reports neither divergence nor a timeout (the next
+// call clears the flags unread).
 #include <cuda_runtime.h>
 
 #include <cmath>

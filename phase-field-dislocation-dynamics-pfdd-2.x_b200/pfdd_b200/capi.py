@@ -1,8 +1,8 @@
 """ctypes binding of libpfdd_b200.so (C ABI in include/pfdd_b200.h).
 
 This is the Python-side mirror of the boundary the reference's host code binds
-(its FFT style object replaced by the library): the same
-descriptors and calls a C++ FftStyle plugin makes.  The library is loaded from
+(its FFT style object replaced by the library): the same descriptors and calls
+a C++ FftStyle plugin makes.  The library is loaded from
 this package directory; when it is missing, or no sm_100 device exists, every
 call raises -- there is no CPU fallback.
 """
@@ -29,7 +29,7 @@ CORE_BCC_PERFECT = 5
 EXPORTS = [
     "pfdd_gpu_create", "pfdd_gpu_set_state", "pfdd_gpu_set_state_interleaved", "pfdd_gpu_get_state",
     "pfdd_gpu_get_state_interleaved", "pfdd_gpu_advance", "pfdd_gpu_step_history", "pfdd_gpu_energy",
-    "pfdd_gpu_tau", "pfdd_gpu_info", "pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version",
+    "pfdd_gpu_tau", "pfdd_gpu_set_stress", "pfdd_gpu_info", "pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version",
     "pfdd_gpu_set_stream", "pfdd_gpu_profile", "pfdd_gpu_adjoint", "pfdd_gpu_strain_stress",
     "pfdd_gpu_core_profile", "pfdd_gpu_autotune", "pfdd_gpu_snapshot_begin", "pfdd_gpu_snapshot_wait", "pfdd_cond_layers", "pfdd_gpu_cond_enable", "pfdd_gpu_cond_set_state",
     "pfdd_gpu_cond_get_state", "pfdd_gpu_cond_step",
@@ -122,6 +122,7 @@ def load(path: str = LIB_PATH):
     lib.pfdd_gpu_cond_get_state.argtypes = [vp, ctypes.c_int, DP, DP]
     lib.pfdd_gpu_cond_step.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(CondStats)]
     lib.pfdd_gpu_tau.argtypes = [vp, ctypes.c_int, DP]
+    lib.pfdd_gpu_set_stress.argtypes = [vp, ctypes.c_int, DP]
     lib.pfdd_gpu_adjoint.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, DP, DP, DP, DP]
     lib.pfdd_gpu_set_stream.argtypes = [vp, vp]
     lib.pfdd_gpu_profile.argtypes = [vp, ctypes.c_int, DP, ctypes.POINTER(ctypes.c_int)]
@@ -263,6 +264,11 @@ class Stepper:
         b = np.empty(max(n, 1))
         self._check(self._lib.pfdd_gpu_step_history(self.h, inst, _dp(a), _dp(b), n, ctypes.byref(cnt)))
         return a[:n], b[:n]
+
+    def set_stress(self, inst, sigma):
+        """Replace instance inst's current applied stress (3x3, units of mu)."""
+        s = np.ascontiguousarray(sigma, dtype=np.float64).reshape(9)
+        self._check(self._lib.pfdd_gpu_set_stress(self.h, inst, _dp(s)))
 
     def tau(self, inst):
         t = np.empty(self.descs[inst].n_slip)

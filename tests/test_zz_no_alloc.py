@@ -1,8 +1,8 @@
 """The allocation-free single-step entry point, pfdd_gl_step_noalloc.
 
-It exists for callers that cannot call cudaMalloc (code running under CUDA
-graph capture, runtimes owning all device memory through their own pool,
-hosts that must not allocate after start-up).  Its scratch is a fixed device
+It exists for callers that cannot call cudaMalloc (host codes whose runtime
+owns all device memory through its own pool, long-running or real-time hosts
+that must not allocate after start-up).  Its scratch is a fixed device
 array inside the library, so this test checks it the way such a caller uses
 it: device buffers owned by the caller, two steps in a row through the C ABI,
 each compared with the handle-based entry point (pfdd_gpu_advance) on the same
