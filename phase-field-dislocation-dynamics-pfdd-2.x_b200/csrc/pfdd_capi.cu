@@ -30,6 +30,14 @@ namespace {
 
 thread_local std::string g_create_error;
 
+// Test hook of the allocation-failure path: PFDD_FAIL_ALLOC_ABOVE=<bytes> in
+// the environment makes every device allocation of the library larger than
+// that fail as cudaMalloc does when memory runs out (nothing is allocated).
+bool alloc_refused(size_t n) {
+  const char *e = getenv("PFDD_FAIL_ALLOC_ABOVE");
+  return e && *e && n > (size_t)strtoull(e, nullptr, 10);
+}
+
 struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;
@@ -40,6 +48,10 @@ struct DevBuf {
     bytes = 0;
   }
   cudaError_t alloc(size_t n) {
+    if (n && alloc_refused(n)) {
+      bytes = 0;
+      return cudaErrorMemoryAllocation;
+    }
     bytes = n;
     return n ? cudaMalloc(&p, n) : cudaSuccess;
   }
@@ -152,6 +164,11 @@ struct pfdd_gpu {
   std::string err;
   size_t device_bytes = 0;
   int nsm = 148;                      // SMs of the device (grid sizing)
+  // a create that fails part-way still releases its stream (device buffers
+  // free themselves)
+  ~pfdd_gpu() {
+    if (own_stream) cudaStreamDestroy(own_stream);
+  }
 };
 
 namespace {
@@ -173,6 +190,25 @@ pfdd_status fail(pfdd_gpu *h, pfdd_status code, const char *fmt, ...) {
     if (e_ != cudaSuccess)                                                                  \
       return fail(h, e_ == cudaErrorMemoryAllocation ? PFDD_ENOMEM : PFDD_ECUDA, "%s: %s (%s:%d)", \
                   #call, cudaGetErrorString(e_), __FILE__, __LINE__);                       \
+  } while (0)
+
+// Error words of an instance, cleared where a call that steps or transforms
+// starts (a reported divergence or timeout does not stick to the handle), and
+// the stall test switch of the bounded-wait path (flags[5]): with
+// PFDD_STALL_BULK_WAITS=1 in the environment, every plane-pass CTA's copy
+// barrier withholds one arrival, so its first wait runs out after
+// kStallWaitNs, the CTA waits for its copies to land, sets the timeout word
+// and abandons the plane; the call returns PFDD_ETIMEOUT and the state is
+// undefined until the next set_state.  Read at each such call.
+int stall_requested() {
+  const char *e = getenv("PFDD_STALL_BULK_WAITS");
+  return (e && atoi(e) != 0) ? 1 : 0;
+}
+#define ARM_FLAGS(h, I)                                                                      \
+  do {                                                                                       \
+    CUDA_TRY(h, cudaMemsetAsync((I).flags() + 1, 0, sizeof(int), (h)->stream));             \
+    CUDA_TRY(h, cudaMemsetAsync((I).flags() + 3, 0, sizeof(int), (h)->stream));             \
+    CUDA_TRY(h, cudaMemsetAsync((I).flags() + 5, stall_requested(), sizeof(int), (h)->stream)); \
   } while (0)
 
 template <typename T> size_t csize() { return sizeof(cx<T>); }
@@ -729,6 +765,7 @@ pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *si
   using C = cx<T>;
   constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
   cudaStream_t st = h->stream;
+  ARM_FLAGS(h, I);
   const size_t N = I.N;
   const int S = I.S;
   // sigma_rot (rotate_stress, fft_fftw_slab.cpp:242-274) of the stress state
@@ -880,6 +917,7 @@ pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *si
 template <typename T>
 pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, double *e_app) {
   cudaStream_t st = h->stream;
+  ARM_FLAGS(h, I);
   DevBuf gpart;
   CUDA_TRY(h, gpart.alloc(4 * (size_t)I.F * I.nx * sizeof(double)));
   k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.an(), I.stress, 0, nullptr);
@@ -930,6 +968,11 @@ pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, 
   }
   CUDA_TRY(h, cudaStreamSynchronize(st));
   CUDA_TRY(h, cudaGetLastError());
+  {
+    int fl[4];
+    CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+    if (fl[3]) return fail(h, PFDD_ETIMEOUT, "a bounded device wait ran out");
+  }
   // compensated (Neumaier) sums in FP64
   auto sum = [](const double *v, size_t n, size_t stride, double scale) {
     double s = 0.0, c = 0.0;
@@ -958,6 +1001,7 @@ template <typename T>
 pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const double *target, double *loss,
                          double *dparams, double *dsigma) {
   cudaStream_t st = h->stream;
+  ARM_FLAGS(h, I);
   const size_t n_re = (size_t)I.S * I.N;
   const size_t n_all = (size_t)I.F * I.N;
   const size_t aux_bytes = I.aux.bytes;
@@ -1177,9 +1221,9 @@ pfdd_status collect(pfdd_gpu *h, pfdd_step_stats *stats) {
     Instance &I = *h->inst[i];
     int fl[5];
     CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+    I.cur = fl[4];   // the device's buffer selector, also after an error
     if (fl[3]) return fail(h, PFDD_ETIMEOUT, "instance %zu: a bounded device wait ran out", i);
     if (fl[1]) return fail(h, PFDD_EDIVERGED, "instance %zu: non-finite order parameter", i);
-    I.cur = fl[4];
     const int did = std::min(fl[2], I.stats_cap);
     I.hist.resize(2 * (size_t)did);
     if (did)
@@ -1196,7 +1240,10 @@ pfdd_status collect(pfdd_gpu *h, pfdd_step_stats *stats) {
 }
 
 pfdd_status reset_counters(pfdd_gpu *h) {
-  for (auto &ip : h->inst) CUDA_TRY(h, cudaMemsetAsync(ip->flags() + 2, 0, sizeof(int), h->stream));
+  for (auto &ip : h->inst) {
+    CUDA_TRY(h, cudaMemsetAsync(ip->flags() + 2, 0, sizeof(int), h->stream));
+    ARM_FLAGS(h, *ip);
+  }
   return PFDD_OK;
 }
 
@@ -1340,8 +1387,10 @@ pfdd_status get_state_impl(pfdd_gpu *h, Instance &I, double *re, double *im, dou
   DevBuf &tmp = h->staging;
   const T *dre = I.xi[I.cur].as<T>();
   const T *dim = I.F > I.S ? dre + n : nullptr;
-  if (I.imag == IMAG_NYQ && (inter || im)) {
+  const bool synth = I.imag == IMAG_NYQ && (inter || im);
+  if (synth) {
     // the other ping-pong buffer is free between steps
+    ARM_FLAGS(h, I);
     T *scratch = I.xi[I.cur ^ 1].as<T>();
     synth_imag<T>(I, h->stream, scratch);
     dim = scratch;
@@ -1366,6 +1415,11 @@ pfdd_status get_state_impl(pfdd_gpu *h, Instance &I, double *re, double *im, dou
   }
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   CUDA_TRY(h, cudaGetLastError());
+  if (synth) {
+    int fl[4];
+    CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+    if (fl[3]) return fail(h, PFDD_ETIMEOUT, "a bounded device wait ran out");
+  }
   return PFDD_OK;
 }
 
@@ -1486,6 +1540,7 @@ pfdd_status snapshot_begin_impl(pfdd_gpu *h, Instance &I, double *re, double *im
   const T *dre = I.xi[I.cur].as<T>();
   const T *dim = I.F > I.S ? dre + n : nullptr;
   if (I.imag == IMAG_NYQ && im) {
+    ARM_FLAGS(h, I);
     T *scratch = I.xi[I.cur ^ 1].as<T>();   // free between steps
     synth_imag<T>(I, h->stream, scratch);
     dim = scratch;
@@ -1511,6 +1566,7 @@ pfdd_status cond_step_impl(pfdd_gpu *h, Instance &I, int n_iters, pfdd_cond_stat
   using C = cx<T>;
   constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
   cudaStream_t st = h->stream;
+  ARM_FLAGS(h, I);
   const size_t N = I.N, ncols = (size_t)I.ny * I.nzp;
   const int nb = 2 * h->nsm;
   if (I.cond_part.bytes < (size_t)n_iters * nb * 3 * sizeof(double)) {
@@ -1776,6 +1832,23 @@ pfdd_status pfdd_gpu_step_history(pfdd_gpu *h, int inst, double *xinorm, double 
   return PFDD_OK;
 }
 
+pfdd_status pfdd_gpu_set_stress(pfdd_gpu *h, int inst, const double sigma[3][3]) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size() || !sigma) return fail(h, PFDD_EINVAL, "bad arguments");
+  Instance &I = *h->inst[inst];
+  cudaSetDevice(h->device);
+  double s[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      if (!std::isfinite(sigma[i][j])) return fail(h, PFDD_EINVAL, "non-finite sigma");
+      s[3 * i + j] = sigma[i][j];
+    }
+  CUDA_TRY(h, cudaMemcpyAsync(I.sigma(), s, sizeof s, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  I.advanced = false;   // the device sigma is the current stress state again
+  return PFDD_OK;
+}
+
 pfdd_status pfdd_gpu_tau(pfdd_gpu *h, int inst, double *tau) {
   if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
   if (inst < 0 || inst >= (int)h->inst.size() || !tau) return fail(h, PFDD_EINVAL, "bad arguments");
@@ -1983,6 +2056,9 @@ pfdd_status pfdd_gpu_snapshot_wait(pfdd_gpu *h, int inst) {
   CUDA_TRY(h, cudaEventSynchronize(I.snap_done));
   I.snap_pending = false;
   CUDA_TRY(h, cudaGetLastError());
+  int fl[4];
+  CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+  if (fl[3]) return fail(h, PFDD_ETIMEOUT, "a bounded device wait ran out");
   return PFDD_OK;
 }
 
@@ -2054,6 +2130,7 @@ void pfdd_gpu_destroy(pfdd_gpu *h) {
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   h->staging.release();
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  h->own_stream = nullptr;
   delete h;
 }
 

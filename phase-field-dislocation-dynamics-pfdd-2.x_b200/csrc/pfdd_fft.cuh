@@ -382,21 +382,61 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
 }
-// Returns false if the phase did not complete within the iteration limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Time limits of the bulk-copy waits: kWaitNs in normal operation (a copy of
+// a few hundred KB lands within microseconds, so a second means the copy
+// engine is gone), kStallWaitNs for the first wait when the stall test switch
+// is on (a barrier that nothing completes; see plane_wait below).
+constexpr uint64_t kWaitNs = 1000000000ull;
+constexpr uint64_t kStallWaitNs = 200000ull;
+// Returns false if the phase did not complete within limit_ns of %globaltimer.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns = kWaitNs) {
   const uint32_t a = smem_u32(bar);
-  for (int it = 0; it < (1 << 22); ++it) {
+  const uint32_t hint = limit_ns < 1000000ull ? (uint32_t)limit_ns : 1000000u;
+  const uint64_t t0 = globaltimer_ns();
+  for (;;) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(a), "r"(parity), "r"(1000000)
+        : "r"(a), "r"(parity), "r"(hint)
         : "memory");
     if (done) return true;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
   }
-  return false;
+}
+// Arrivals the plane passes' copy barrier expects: one (thread 0's
+// arrive.expect_tx), plus one that nothing delivers while the stall test
+// switch (err[2], an instance's flags[5]) is on.
+__device__ __forceinline__ int stall_switch(const int *err) {
+  return err ? *reinterpret_cast<const volatile int *>(err + 2) : 0;
+}
+// Wait of a plane-pass CTA for its bulk copies (phase 0 of bar).  Returns
+// false after a timeout, with err[0] set; before returning it waits (bounded
+// again) until the copies into this CTA's shared memory have landed: with the
+// stall switch on, thread 0 delivers the withheld arrival so the phase
+// completes exactly when the copies have.  Every thread of the CTA calls it.
+__device__ __forceinline__ bool plane_wait(uint64_t *bar, int stall, int *err) {
+  const bool ok = __syncthreads_and(mbar_wait(bar, 0, stall ? kStallWaitNs : kWaitNs));
+  if (!ok) {
+    if (threadIdx.x == 0) {
+      if (stall) mbar_arrive(bar);
+      if (err) atomicExch(err, 1);
+    }
+    __syncthreads();
+    mbar_wait(bar, 0, kWaitNs);
+    __syncthreads();
+  }
+  return ok;
 }
 __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, uint32_t bytes, uint64_t *bar) {
   asm volatile(

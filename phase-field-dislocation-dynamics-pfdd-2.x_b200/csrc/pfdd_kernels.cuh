@@ -439,7 +439,8 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
   const int rows = SPLIT ? ny / 2 : ny;
   const int row0 = row0_of_block<SPLIT>(ny);
   const PlaneSmem<C> sm(smem_raw, a, rows);
-  if (threadIdx.x == 0) mbar_init(sm.bar, 1);
+  const int stall = stall_switch(err);
+  if (threadIdx.x == 0) mbar_init(sm.bar, 1 + stall);
   __syncthreads();
   // rows of the real plane -> shared rows of stride 2*nzs reals (bulk copies)
   if (threadIdx.x < 32) {
@@ -451,12 +452,9 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
       bulk_g2s(bufr + (size_t)y * 2 * nzs, src + (size_t)y * nz, (uint32_t)(nz * sizeof(T)), sm.bar);
   }
   load_plane_tables(sm, a);
-  const bool ok = __syncthreads_and(mbar_wait(sm.bar, 0));
-  if (!ok) {
-    if (threadIdx.x == 0) atomicExch(err, 1);
-    // a split CTA carries on without storing: its peer waits at the cluster barriers
-    if constexpr (!SPLIT) return;
-  }
+  const bool ok = plane_wait(sm.bar, stall, err);
+  // after a timeout a split CTA carries on without storing: its peer waits at the cluster barriers
+  if (!ok && !SPLIT) return;
   fwd_planes_compute<T, NT, SPLIT>(sm, a, spec, plane, rows, row0, ok);
 }
 
@@ -1160,8 +1158,9 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
   const int rows = SPLIT ? ny / 2 : ny;
   const int row0 = row0_of_block<SPLIT>(ny);
   const PlaneSmem<C> sm(smem_raw, a, rows);
+  const int stall = stall_switch(err);
   if (threadIdx.x == 0) {
-    mbar_init(sm.bar, 1);
+    mbar_init(sm.bar, 1 + stall);
     // the update reads this CTA's xi rows after the transforms: start them towards L2 now
     if (u.mode != PASS_SYNTH) prefetch_l2_bulk(xin + (plane * ny + row0) * nz, (uint32_t)(rows * nz * sizeof(T)));
   }
@@ -1180,12 +1179,9 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
   }
   load_plane_tables(sm, a);
   __syncthreads();
-  const bool ok = __syncthreads_and(mbar_wait(sm.bar, 0));
-  if (!ok) {
-    if (threadIdx.x == 0) atomicExch(err, 1);
-    // a split CTA carries on without storing: its peer waits at the cluster barriers
-    if constexpr (!SPLIT) return;
-  }
+  const bool ok = plane_wait(sm.bar, stall, err);
+  // after a timeout a split CTA carries on without storing: its peer waits at the cluster barriers
+  if (!ok && !SPLIT) return;
   C *buf = sm.buf;
   const C *twr = sm.twr;
   const int *pos = sm.pos;
