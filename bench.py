@@ -25,8 +25,8 @@ by timing (pfdd_gpu_autotune, outside the timed region, like a planner);
 
 Multi-GPU (torchrun): every rank advances its own replica (no data-path
 collective; scaling "weak"); the time is the max over ranks.
---impl reference times the reference's own CPU code on this host's cores
-(independent processes, aggregate throughput) and prints the same line.
+--impl reference times the reference's own CPU code on this host's cores on
+the same workload (see reference_arm) and prints the same line.
 """
 import argparse
 import json
@@ -196,35 +196,112 @@ def cpu_baseline_reference(K=10, procs=1, nx=64, ny=64, nz=32):
     return rate, sample
 
 
-def reference_arm(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return 0
-    ncpu = os.cpu_count() or 1
-    mem_gb = 8.0
+def mem_available_gb():
     try:
         for line in open("/proc/meminfo"):
             if line.startswith("MemAvailable"):
-                mem_gb = int(line.split()[1]) / 1e6
+                return int(line.split()[1]) / 1e6
     except Exception:
         pass
-    procs = max(1, min(ncpu, int(mem_gb * 0.5 / 1.0), 64))
-    K = max(1, args.steps)
-    t0 = time.time()
-    rate, sample = cpu_baseline_reference(K=K, procs=procs)
-    if rate is None:
-        print(json.dumps({"impl": "reference", "unavailable": sample}))
+    return None
+
+
+def reference_host_bytes(w):
+    """Resident host bytes of the reference on workload w (FFTW_Slab::allocate,
+    fft_fftw_slab.cpp:140-237, as Bmatrix/Fmatrix and the GL loop touch them):
+    BB (S^2 N), FF and DD (9 S N each), data_fftw/data_real/temp_data/data_core
+    (complex S N each), xi, dE_core, f, xo, fx/fy/fz and the strain/stress
+    fields, in doubles."""
+    S, N = w.S, w.N
+    doubles = S * S * N + 18 * S * N + 8 * S * N + 2 * S * N + 3 * S * N + 3 * N + 4 * 18 * N
+    return 8 * doubles
+
+
+def reference_arm(args):
+    """The reference's own CPU implementation (its sources compiled in
+    oracle/_ref) on this host, on the same workload as the GPU arm: the full
+    grid for one-instance workloads, K' <= 3 GL iterations timed as the
+    reference's loop time (Finish, finish.cpp:42-55), set-up excluded.  Its
+    per-wavevector set-up runs on forked one-plane slabs and its FFTW-2
+    stand-in on threads, over every host core (bit-identical to one process,
+    tests/test_oracle_parallel_cpu.py); the reference's own loops
+    (internal_energy, core force, update) run on one core, as on one MPI rank.
+    Multi-instance workloads run independent single-thread processes, one per
+    instance, up to the core count.  Rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
         return 0
-    wall = time.time() - t0
-    w_desc = workload_config(args.workload)[1]
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner
+    ncpu = os.cpu_count() or 1
+    ws, w_desc, _ = workload_config(args.workload)
+    if not ref_runner.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference oracle not built (make -C oracle/ref_build)"}))
+        return 0
+    t0 = time.time()
+    mem = mem_available_gb()
+    iters = max(1, min(args.steps, 3))
+    if len(ws) == 1:
+        w = ws[0]
+        need_gb = reference_host_bytes(w) / 1e9
+        if mem is not None and mem < 1.25 * need_gb:
+            # not enough host memory for the full grid: a labelled sample of the same deck instead
+            from pfdd_b200 import configs
+            w = configs.fcc_workload(64, 64, 32, n_loops=4)
+            w_desc = ("SAMPLE fcc 64x64x32 (12 FCC systems, 4 loops): the host has %.0f GB available, the "
+                      "reference needs ~%.0f GB for %s" % (mem, need_gb, args.workload))
+        env_old = {k: os.environ.get(k) for k in ("PFDD_ORACLE_SETUP_PROCS", "PFDD_SHIM_THREADS")}
+        os.environ["PFDD_ORACLE_SETUP_PROCS"] = str(ncpu)
+        os.environ["PFDD_SHIM_THREADS"] = str(ncpu)
+        try:
+            r = ref_runner.run_reference(w, iters, timing=True, timeout=3000)
+        finally:
+            for k, v in env_old.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
+        tm = r["timing"]
+        rate = tm["site_slip_updates_per_s"]
+        cores = ncpu
+        sample = ("reference src/*.cpp built -O3 with a single-rank MPI stub and an FP64 FFTW-2 API stand-in "
+                  "(transforms on %d threads, %.2f GFLOP/s of FFT work per loop second); %dx%dx%d grid x %d systems, "
+                  "%d GL iterations, loop time %.2f s (set-up on %d forked processes, not timed); the reference's "
+                  "own loops run on one core as on one MPI rank"
+                  % (ncpu, tm["fft_gflops"], w.nx, w.ny, w.nz, w.S, tm["iterations"], tm["loop_s"], ncpu))
+        parallelism = "1 process, FFT on %d threads" % ncpu
+    else:
+        import concurrent.futures as cf
+        sub = ws[:max(1, min(len(ws), ncpu))]
+
+        def one(w):
+            # the per-site-multiplier sine core has no reference counterpart: the
+            # reference's per-site-amplitude core (core_energy_mpea, flag 7) stands in
+            import copy
+            wr = copy.copy(w)
+            mpea = None
+            if w.core_flag == 103:
+                wr.core_flag = 7
+                mpea = w.site * w.material.usf
+            return ref_runner.run_reference(wr, iters, mpea=mpea, timing=True)["timing"]
+
+        with cf.ThreadPoolExecutor(len(sub)) as ex:
+            res = list(ex.map(one, sub))
+        rate = sum(r["site_slip_updates_per_s"] for r in res)
+        cores = len(sub)
+        sample = ("reference src/*.cpp built -O3 with a single-rank MPI stub and an FP64 FFTW-2 API stand-in; "
+                  "%d of the %d instances as concurrent single-thread processes, %d GL iterations each, loop time "
+                  "only, aggregate throughput; the per-site GSFE field runs through the reference's per-site "
+                  "amplitude core (core_energy_mpea)" % (len(sub), len(ws), iters))
+        parallelism = "%d independent CPU processes" % len(sub)
     line = {
-        "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": K, "warmup": args.warmup,
+        "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": iters, "warmup": args.warmup,
         "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": w_desc, "parallelism": "%d independent CPU processes" % procs},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample},
+        "config": {"workload": w_desc, "parallelism": parallelism},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "wall_s": wall,
+        "host_mem_available_gb": mem, "wall_s": time.time() - t0,
     }
     print(json.dumps(line))
     return 0
@@ -260,8 +337,10 @@ def timed_events(stream, fn):
 
 
 def fp32_vs_fp64(ws, K, stream, local, steps=2000):
-    """Plain-FP64 workload: FP32 speed (same timed profile pass) and the FP32
-    error against the FP64 GPU path after `steps` steps (relative L2 of Re xi)."""
+    """FP32 and FP64 speed of the same grid (the same timed profile pass of K
+    steps) and the FP32 error against the FP64 GPU path after `steps` steps
+    (relative L2 of Re xi).  The FP64 path equals the oracle to 1e-10 per step
+    (tests/test_gpu_config_sizes.py, which also bounds this error at 1e-5)."""
     import numpy as np
     from pfdd_b200 import capi
     w = ws[0]
@@ -279,7 +358,12 @@ def fp32_vs_fp64(ws, K, stream, local, steps=2000):
             out[name + "_state"] = st.get_state(0)[0]
     a, b = out.pop("fp32_state"), out.pop("fp64_state")
     out["rel_l2_fp32_vs_fp64_after_%d" % steps] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out["max_abs_fp32_vs_fp64_after_%d" % steps] = float(np.abs(a - b).max())
+    out["steps_compared"] = steps
     out["fp32_speedup"] = out["fp64_ms_per_step"] / out["fp32_ms_per_step"]
+    units = w.S * w.N
+    out["fp64_site_slip_updates_per_s"] = units / (out["fp64_ms_per_step"] / 1e3)
+    out["fp32_site_slip_updates_per_s"] = units / (out["fp32_ms_per_step"] / 1e3)
     return out
 
 
@@ -313,9 +397,15 @@ def cufft_comparison(w, F, prec, stream, reps=10):
 def adjoint_ratio(st, w, prec, stream, local, steps=500, ckpt=50):
     """Adjoint call over forward time for `steps` steps, keeping every state
     and with checkpoints; the target state comes from a forward run with
-    isf 40 / usf 160 mJ/m^2 and 250 MPa."""
+    isf 40 / usf 160 mJ/m^2 and 250 MPa.  st = None: a stepper of w of its own."""
     import copy
     from pfdd_b200 import capi, configs
+    if st is None:
+        with capi.Stepper.from_workloads([w], precision=prec, device=local) as own:
+            own.set_stream(stream.cuda_stream)
+            own.set_state(0, w.xi0)
+            own.autotune(reps=5)
+            return adjoint_ratio(own, w, prec, stream, local, steps, ckpt)
     wt = copy.deepcopy(w)
     wt.material.isf, wt.material.usf = 0.040, 0.160
     wt.sigma = configs._sigma("xz", 250e6 / wt.material.mu)
@@ -482,10 +572,18 @@ def main():
         dms = [timed_events(stream, lambda: st.strain_stress(0, fields=False))[0] for _ in range(3)]
         extras["strain_stress_ms"] = statistics.median(dms)
     if not args.no_extras and rank == 0:
-        if args.workload == "loop64":
+        if args.workload in ("loop64", "fcc256"):
+            # the metric's "FP32 vs FP64 at stated err" on the timed grid itself
             extras["fp32_vs_fp64"] = fp32_vs_fp64(ws, args.steps, stream, local)
-        if args.workload == "edge128":
-            extras["adjoint"] = adjoint_ratio(st, ws[0], prec, stream, local)
+        if args.workload in ("edge128", "fcc256"):
+            # the metric's "adjoint/fwd ratio" on its own configuration: 128x128x32,
+            # 500 steps, a checkpoint every 50
+            from pfdd_b200 import configs
+            if args.workload == "edge128":
+                extras["adjoint"] = adjoint_ratio(st, ws[0], prec, stream, local)
+            else:
+                extras["adjoint"] = dict(adjoint_ratio(None, configs.edge_workload(), capi.FP32, stream, local),
+                                         workload="edge128: 128x128x32, 3 systems, FP32")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <algorithm>
 #include <map>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -78,8 +79,9 @@ Plan1D *get_plan(int n, int sign) {
   return pl;
 }
 
-// One Stockham stage on V-vectors: x -> y.
-void run_stage(const Stage &st, int sign, const double *x, double *y, int V) {
+// One Stockham stage on V-vectors: x -> y, vector components [v0, v1) only
+// (components are independent, so disjoint ranges can run on separate threads).
+void run_stage(const Stage &st, int sign, const double *x, double *y, int V, int v0, int v1) {
   const int p = st.p, m = st.m, s = st.s;
   const size_t sv = (size_t)s * V;  // doubles per "q-run" is 2*sv
   const double c3 = -0.5, s3 = sign * std::sqrt(3.0) * 0.5;
@@ -89,7 +91,8 @@ void run_stage(const Stage &st, int sign, const double *x, double *y, int V) {
   if (p > 5) { ar.resize(p); ai.resize(p); }
   for (int j = 0; j < m; ++j) {
     const double *tw = &st.tw[2 * (size_t)j * p];
-    for (size_t qv = 0; qv < sv; ++qv) {
+    for (size_t q0 = 0; q0 < sv; q0 += V)
+    for (size_t qv = q0 + v0; qv < q0 + v1; ++qv) {
       // input r: index (j + r*m) * s  (+q) ; vector offset folded into qv
       const double *in0 = x + 2 * ((size_t)j * sv + qv);
       const size_t istep = 2 * (size_t)m * sv;
@@ -175,20 +178,60 @@ void run_stage(const Stage &st, int sign, const double *x, double *y, int V) {
   }
 }
 
-// Transform `count` independent transforms of length n whose elements are
-// V-vectors: element (t, i, v) at data[(t*n + i)*V + v].
+// Worker threads of one transform: PFDD_SHIM_THREADS (default 1).  The
+// reference's FFTW-MPI build spreads its transforms over the MPI ranks; this
+// single-rank stand-in spreads them over threads instead.  Every element is
+// computed by the same operations in the same order whatever the count, so
+// the results are bit-identical.
+int shim_threads() {
+  static int t = -1;
+  if (t < 0) {
+    const char *e = getenv("PFDD_SHIM_THREADS");
+    t = e ? std::max(1, atoi(e)) : 1;
+  }
+  return t;
+}
+
+template <class F>
+void parallel_for(int count, F body) {
+  const int T = std::min(shim_threads(), count);
+  if (T <= 1) {
+    body(0, count, 0);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int k = 0; k < T; ++k) {
+    const int a = (int)((long long)count * k / T), b = (int)((long long)count * (k + 1) / T);
+    th.emplace_back([=] { body(a, b, k); });
+  }
+  for (auto &x : th) x.join();
+}
+
+// `count` independent transforms of length n whose elements are V-vectors:
+// element (t, i, v) at data[(t*n + i)*V + v]; scratch holds count*n*V complex.
+// Threads take whole transforms when there are several, else ranges of v.
 void fft_lines(double *data, double *scratch, int count, int n, int V, int sign) {
   if (n <= 1) return;
   Plan1D *pl = get_plan(n, sign);
   const size_t tsz = 2 * (size_t)n * V;
-  for (int t = 0; t < count; ++t) {
-    double *a = data + t * tsz, *b = scratch;
+  auto one = [&](int t, int v0, int v1) {
+    double *a = data + t * tsz, *b = scratch + t * tsz;
     for (const Stage &st : pl->stages) {
-      run_stage(st, sign, a, b, V);
+      run_stage(st, sign, a, b, V, v0, v1);
       std::swap(a, b);
     }
-    if (a != data + t * tsz) std::memcpy(data + t * tsz, a, tsz * sizeof(double));
-  }
+    if (a != data + t * tsz)
+      for (int i = 0; i < n; ++i)
+        std::memcpy(data + t * tsz + 2 * ((size_t)i * V + v0), a + 2 * ((size_t)i * V + v0),
+                    2 * (size_t)(v1 - v0) * sizeof(double));
+  };
+  if (count >= shim_threads())
+    parallel_for(count, [&](int t0, int t1, int) {
+      for (int t = t0; t < t1; ++t) one(t, 0, V);
+    });
+  else
+    for (int t = 0; t < count; ++t)
+      parallel_for(V, [&](int v0, int v1, int) { one(t, v0, v1); });
   g_flops += 5.0 * n * std::log2((double)n) * (double)count * V;
 }
 
@@ -228,26 +271,38 @@ void fftwnd_mpi(fftwnd_mpi_plan p, int n_fields, fftw_complex *local_data,
   // vectors, then scattered back.
   const int lines = nx * ny;
   const int B = 8;
-  std::vector<double> blk(2 * (size_t)nz * B * h), bsc(2 * (size_t)nz * B * h);
-  for (int l0 = 0; l0 < lines; l0 += B) {
-    const int nb = std::min(B, lines - l0);
-    const int V = nb * h;
-    for (int b = 0; b < nb; ++b)
-      for (int i = 0; i < nz; ++i)
-        for (int f = 0; f < h; ++f) {
-          const double *src = d + 2 * (((size_t)(l0 + b) * nz + i) * h + f);
-          double *dst = blk.data() + 2 * ((size_t)i * V + b * h + f);
-          dst[0] = src[0]; dst[1] = src[1];
+  const int groups = (lines + B - 1) / B;
+  Plan1D *pl = nz > 1 ? get_plan(nz, p->sign) : nullptr;   // plans are built outside the threads
+  parallel_for(groups, [&](int g0, int g1, int) {
+    std::vector<double> blk(2 * (size_t)nz * B * h), bsc(2 * (size_t)nz * B * h);
+    for (int l0 = g0 * B; l0 < std::min(lines, g1 * B); l0 += B) {
+      const int nb = std::min(B, lines - l0);
+      const int V = nb * h;
+      for (int b = 0; b < nb; ++b)
+        for (int i = 0; i < nz; ++i)
+          for (int f = 0; f < h; ++f) {
+            const double *src = d + 2 * (((size_t)(l0 + b) * nz + i) * h + f);
+            double *dst = blk.data() + 2 * ((size_t)i * V + b * h + f);
+            dst[0] = src[0]; dst[1] = src[1];
+          }
+      if (nz > 1) {
+        double *a = blk.data(), *c = bsc.data();
+        for (const Stage &st : pl->stages) {
+          run_stage(st, p->sign, a, c, V, 0, V);
+          std::swap(a, c);
         }
-    fft_lines(blk.data(), bsc.data(), 1, nz, V, p->sign);
-    for (int b = 0; b < nb; ++b)
-      for (int i = 0; i < nz; ++i)
-        for (int f = 0; f < h; ++f) {
-          double *dst = d + 2 * (((size_t)(l0 + b) * nz + i) * h + f);
-          const double *src = blk.data() + 2 * ((size_t)i * V + b * h + f);
-          dst[0] = src[0]; dst[1] = src[1];
-        }
-  }
+        if (a != blk.data()) std::memcpy(blk.data(), a, 2 * (size_t)nz * V * sizeof(double));
+      }
+      for (int b = 0; b < nb; ++b)
+        for (int i = 0; i < nz; ++i)
+          for (int f = 0; f < h; ++f) {
+            double *dst = d + 2 * (((size_t)(l0 + b) * nz + i) * h + f);
+            const double *src = blk.data() + 2 * ((size_t)i * V + b * h + f);
+            dst[0] = src[0]; dst[1] = src[1];
+          }
+    }
+  });
+  if (nz > 1) g_flops += 5.0 * nz * std::log2((double)nz) * (double)lines * h;
   // y: nx transforms of ny elements, vector = nz*fields
   fft_lines(d, scratch.data(), nx, ny, nz * h, p->sign);
   // x: one transform of nx elements, vector = ny*nz*fields

@@ -25,6 +25,10 @@
 // (material.h).  Uninitialised reference members that change control flow are
 // set explicitly: FFT::ximin (fft.h:51, read at solve_GL.cpp:108,142) = 0 and
 // App::num_planes (app.h) = S, or S/3 for core_energy 2.
+#include <sys/mman.h>
+#include <sys/wait.h>
+#include <unistd.h>
+
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -62,6 +66,90 @@ void OracleSlab::update_order_parameter() {
   FFTW_Slab::update_order_parameter();
   step_xinorm.push_back(xinorm);
   step_xiave.push_back(xiave);
+}
+
+static int setup_procs() {
+  const char *e = getenv("PFDD_ORACLE_SETUP_PROCS");
+  return e ? atoi(e) : 1;
+}
+
+// Bmatrix / Fmatrix on forked one-x-plane slabs (see oracle_slab.h).  Each
+// table is [comps][local_x*ny*nz] (BB: ka + kb*S; FF, DD: ka + i*S + j*3S);
+// a slab call lays out its plane as [comps][ny*nz], copied into place here.
+void OracleSlab::slab_call(int which) {
+  if (which == 0) FFTW_Slab::Bmatrix();
+  else FFTW_Slab::Fmatrix();
+}
+
+void OracleSlab::forked_setup(int which, SlabOut *outs, int nouts) {
+  const int lx = local_x, lx0 = local_x_start;
+  const size_t plane = (size_t)local_y * local_z, n = (size_t)lx * plane;
+  int P = setup_procs();
+  if (P > lx) P = lx;
+  // the scalars and small tables the call also sets (material mu/ll/young/xnu,
+  // eps): one plane in this process, into scratch
+  std::vector<std::vector<double>> scratch(nouts);
+  std::vector<double *> saved(nouts);
+  for (int o = 0; o < nouts; ++o) {
+    saved[o] = *outs[o].member;
+    scratch[o].resize((size_t)outs[o].comps * plane);
+    *outs[o].member = scratch[o].data();
+  }
+  local_x = 1;
+  slab_call(which);
+  local_x = lx;
+  // shared mappings replace the tables (the reference never frees them)
+  std::vector<double *> shared(nouts);
+  for (int o = 0; o < nouts; ++o) {
+    size_t bytes = (size_t)outs[o].comps * n * sizeof(double);
+    void *m = mmap(nullptr, bytes, PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
+    if (m == MAP_FAILED) { fprintf(stderr, "harness: mmap of %zu bytes failed\n", bytes); exit(2); }
+    shared[o] = static_cast<double *>(m);
+    if (saved[o]) memory->destroy(saved[o]);
+  }
+  std::vector<pid_t> kids;
+  for (int r = 0; r < P; ++r) {
+    pid_t pid = fork();
+    if (pid < 0) { fprintf(stderr, "harness: fork failed\n"); exit(2); }
+    if (pid == 0) {
+      if (!freopen("/dev/null", "w", stdout)) _exit(3);   // the set-up's per-call prints
+      for (int x = r; x < lx; x += P) {
+        local_x = 1;
+        local_x_start = lx0 + x;
+        frec();
+        for (int o = 0; o < nouts; ++o) *outs[o].member = scratch[o].data();
+        slab_call(which);
+        for (int o = 0; o < nouts; ++o)
+          for (int c = 0; c < outs[o].comps; ++c)
+            memcpy(shared[o] + (size_t)c * n + (size_t)x * plane, scratch[o].data() + (size_t)c * plane,
+                   plane * sizeof(double));
+      }
+      _exit(0);
+    }
+    kids.push_back(pid);
+  }
+  for (pid_t k : kids) {
+    int status = 0;
+    if (waitpid(k, &status, 0) < 0 || !WIFEXITED(status) || WEXITSTATUS(status) != 0) {
+      fprintf(stderr, "harness: a set-up process failed\n");
+      exit(2);
+    }
+  }
+  local_x = lx;
+  local_x_start = lx0;
+  for (int o = 0; o < nouts; ++o) *outs[o].member = shared[o];
+}
+
+void OracleSlab::Bmatrix() {
+  if (setup_procs() <= 1 || local_x < 2) { FFTW_Slab::Bmatrix(); return; }
+  SlabOut o[1] = {{&BB, slip_systems * slip_systems}};
+  forked_setup(0, o, 1);
+}
+
+void OracleSlab::Fmatrix() {
+  if (setup_procs() <= 1 || local_x < 2) { FFTW_Slab::Fmatrix(); return; }
+  SlabOut o[2] = {{&FF, 9 * slip_systems}, {&DD, 9 * slip_systems}};
+  forked_setup(1, o, 2);
 }
 
 #ifndef PFDD_ORACLE_SLAB_ONLY
