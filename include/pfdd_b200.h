@@ -294,23 +294,36 @@ pfdd_status pfdd_gpu_cond_get_state(pfdd_gpu *h, int inst, double *re, double *i
 pfdd_status pfdd_gpu_cond_step(pfdd_gpu *h, int inst, int n_iters, pfdd_cond_stats *stats);
 
 /* No counterpart in the reference (a hand-written adjoint of the GL step).
- * Gradient of J = sum over sites and systems of (Re xi_N - target)^2, where
- * xi_N is instance `inst` after n_steps GL iterations from its current state
- * at the current stress state, with respect to the GSFE parameters and the
- * applied stress.  Forward pass with a state checkpoint every ckpt_every
- * steps; backward pass per segment (forward recompute, then adjoint steps
+ * Gradients of a loss L(Re xi_N), xi_N = instance `inst` after n_steps GL
+ * iterations from its current state at the current stress state, with
+ * respect to the GSFE parameters and the applied stress, seeded with
+ * dL/dRe xi_N; any final-state loss has that seed.
+ *
+ * pfdd_gpu_adjoint_forward runs the n_steps and keeps them as a tape: the
+ * state every ckpt_every steps (with the Nyquist carrier of Im xi) and every
+ * state of the last segment, on the device in the compute precision; the
+ * instance ends at xi_N, as after pfdd_gpu_advance(h, n_steps, 1, 0, .), so
+ * the caller can read xi_N (pfdd_gpu_get_state) to form its seed.
+ * pfdd_gpu_adjoint_backward then recomputes each earlier segment from its
+ * checkpoint and runs the adjoint steps
  *   lam_n = lam_{n+1} - CD dt (L lam_{n+1} + f''(xi_n) lam_{n+1}),
- * L the self-adjoint elastic operator, masked sites frozen).  ckpt_every >=
- * n_steps keeps every Re xi_n of the forward pass (n_steps * S * N values in
- * the compute precision on the device) and recomputes nothing. 
- *   xi_target  host [S*N] target for Re xi_N (reference site order)
- *   loss       receives J (may be NULL)
- *   dL_dparams [2]: sine / sine-field cores dJ/d(isf, usf); perfect / USFE
- *              dJ/d(An, -); MPEA (0, 0)  (J/m^2)
- *   dL_dsigma  [6]: dJ/d(sigma xx yy zz xy xz yz), deck units (stress / mu)
- * The instance ends at xi_N, as after pfdd_gpu_advance(h, n_steps, 1, 0, .). */
-pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every, const double *xi_target,
-                             double *loss, double *dL_dparams, double *dL_dsigma);
+ * L the self-adjoint elastic operator, masked sites frozen, from
+ * lam_N = dL_dxiN.  It may run several seeds on one tape; the tape is
+ * dropped when the instance's state changes (advance, set_state, load)
+ * (PFDD_ESTATE without one).  ckpt_every >= n_steps keeps every state and
+ * recomputes nothing.
+ *   dL_dxiN     host [S*N] dL/dRe xi_N (reference site order)
+ *   dL_dparams  [2] or NULL: sine / sine-field cores dL/d(isf, usf); perfect
+ *               / USFE dL/d(An, -); MPEA (0, 0)  (J/m^2)
+ *   dL_dsigma   [6] or NULL: dL/d(sigma xx yy zz xy xz yz), deck units (stress / mu)
+ * A non-finite gradient returns PFDD_EDIVERGED.  Core models 2, 4 and 5 have
+ * no adjoint (PFDD_EUNSUPPORTED).  pfdd_gpu_adjoint is both calls in one,
+ * for a seed known beforehand. */
+pfdd_status pfdd_gpu_adjoint_forward(pfdd_gpu *h, int inst, int n_steps, int ckpt_every);
+pfdd_status pfdd_gpu_adjoint_backward(pfdd_gpu *h, int inst, const double *dL_dxiN, double *dL_dparams,
+                                      double *dL_dsigma);
+pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every, const double *dL_dxiN,
+                             double *dL_dparams, double *dL_dsigma);
 
 /* Set instance `inst`'s current applied stress (units of mu), replacing the
  * device's copy; dsigma is kept.  The host side of the reference owns sigma
@@ -319,6 +332,41 @@ pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every,
  * state in several chunks (output steps in between) sets it before each chunk,
  * since pfdd_gpu_advance adds dsigma when a stress state ends. */
 pfdd_status pfdd_gpu_set_stress(pfdd_gpu *h, int inst, const double sigma[3][3]);
+
+/* ---- Binary checkpoints for resume ----
+ * No counterpart in the reference, which keeps no resumable state (its only
+ * copies are the in-memory temp_stor_data / reset_data pair,
+ * src/fft_fftw_slab.cpp:1891-1925, and the six-digit text dumps,
+ * src/dump_text.cpp:361-400).  A checkpoint holds one instance's device state
+ * as it is stepped (fields in the compute precision, the Nyquist carrier of
+ * Im xi, the device's sigma and dsigma), so a handle created from the same
+ * descriptor and options that loads it continues bit for bit as the writer
+ * would have.  The file is a 256-byte little-endian header with FNV-1a 64
+ * checksums of itself and of the payload, then the payload; reading refuses a
+ * file whose magic, version, sizes or checksums do not match (PFDD_EINVAL). */
+typedef struct {
+  int nx, ny, nz, n_slip;
+  int fields;                  /* real fields carried: n_slip, or 2 n_slip with the full Im carrier */
+  int precision;               /* PFDD_FP64 / PFDD_FP32 of the stored values */
+  int imag_mode;               /* PFDD_IMAG_FULL or PFDD_IMAG_NYQUIST */
+  int advanced;                /* 1: sigma is one dsigma past the last stress state stepped */
+  size_t field_bytes, carrier_bytes;
+  double sigma[3][3], dsigma[3][3];
+  unsigned long long steps;    /* GL iterations the writer had run (informational) */
+} pfdd_checkpoint_info;
+
+/* The file format alone (host only, no device): write a checkpoint from
+ * host buffers, or read one (fields == carrier == NULL: the header only). */
+pfdd_status pfdd_checkpoint_write(const char *path, const pfdd_checkpoint_info *info, const void *fields,
+                                  const void *carrier);
+pfdd_status pfdd_checkpoint_read(const char *path, pfdd_checkpoint_info *info, void *fields, size_t field_cap,
+                                 void *carrier, size_t carrier_cap);
+
+/* Save instance `inst`'s state to `path`; load it back into an instance of
+ * the same grid, slip systems, precision and carrier mode (PFDD_EINVAL
+ * otherwise, the instance unchanged). */
+pfdd_status pfdd_gpu_checkpoint_save(pfdd_gpu *h, int inst, const char *path);
+pfdd_status pfdd_gpu_checkpoint_load(pfdd_gpu *h, int inst, const char *path);
 
 /* Resolved shear stresses tau[S] of instance `inst` at the current stress state. */
 pfdd_status pfdd_gpu_tau(pfdd_gpu *h, int inst, double *tau);

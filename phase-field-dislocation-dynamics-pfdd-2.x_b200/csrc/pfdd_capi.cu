@@ -87,6 +87,7 @@ struct Instance {
   int ccols, fstride, ntiles;
   int sx_n, sy_n;
   bool split = false;  // P1/P3 planes on 2-CTA clusters, half the rows per CTA
+  bool merged = false; // in a mixed-size batch: its group runs in the merge class's launches
   size_t smem_plane, smem_update, smem_pencil;
   DevBuf aux;          // Nyquist spectrum of Im xi (IMAG_NYQ)
   DevBuf ppart;        // per-tile partial sums of P2
@@ -108,9 +109,16 @@ struct Instance {
   int hist_count = 0;
   int group = -1;       // index of the batched group this instance belongs to
   bool advanced = false;  // an advance ran: the device sigma is one increment past its last stress state
-  // adjoint scratch, kept between calls (checkpoints, segment states,
-  // lambda pair, target, Nyquist carrier of lambda, partial sums, final state)
-  DevBuf adj_ck, adj_seg, adj_lam[2], adj_tgt, adj_aux, adj_gpart, adj_acc, adj_lpart, adj_fin, adj_finaux;
+  unsigned long long steps_total = 0;  // GL iterations run by advances (checkpoint header)
+  // adjoint tape and scratch, kept between calls (checkpoints, segment states,
+  // lambda pair, Nyquist carrier of lambda, per-plane gradient sums, their
+  // total, final state and carrier); tape_steps > 0 while the tape describes
+  // the run that ended at the current state
+  DevBuf adj_ck, adj_seg, adj_last, adj_lam[2], adj_aux, adj_gpart, adj_acc, adj_fin, adj_finaux;
+  // strain / stress diagnostics scratch, kept between calls (per-system sums,
+  // six strain spectra, six strain fields, FP64 field copies, partial sums)
+  DevBuf ss_part, ss_spec6, ss_strain6, ss_e9, ss_s9, ss_fpart;
+  int tape_steps = 0, tape_K = 1;
   double *tau() const { return small.as<double>(); }
   double *sigma() const { return small.as<double>() + PFDD_MAXS; }   // sigma[9] then dsigma[9]
   int *flags() const { return reinterpret_cast<int *>(small.as<double>() + PFDD_MAXS + 18); }
@@ -139,6 +147,18 @@ struct Group {
   DevBuf table;   // InstPtrs[members.size()]
 };
 
+// Groups of one merge class (everything equal but the grid size) that run
+// in one launch per pass (k_*_multi); the device tables hold each group's
+// arguments, MultiLaunch the CTA prefix of each group.
+struct MergeClass {
+  std::vector<int> groups;
+  DevBuf ptab, pentab, ftab;   // MultiPlaneGroup[], MultiPencilGroup[], MultiFinalGroup[]
+  MultiLaunch mp{}, mpe{}, mf{};
+  unsigned plane_ctas = 0, pencil_ctas = 0, insts = 0;
+  size_t smem_plane = 0, smem_pencil = 0;
+  int S = 0;
+};
+
 struct GraphKey {
   int steps;
   int states;   // 0: steps of the current stress state; k > 0: k whole stress states of `steps` steps
@@ -156,6 +176,8 @@ struct pfdd_gpu {
   pfdd_options opt{};
   std::vector<std::unique_ptr<Instance>> inst;
   std::vector<Group> groups;
+  std::vector<MergeClass> merges;  // mixed-size batches
+  std::vector<int> group_merge;    // per group: its merge class, or -1 (own launches)
   std::map<GraphKey, cudaGraphExec_t> graphs;   // K-step launch sequences, replayed by advance
   cudaStream_t stream = nullptr;      // stream in use
   cudaStream_t own_stream = nullptr;  // stream created by the handle
@@ -212,6 +234,15 @@ int stall_requested() {
   } while (0)
 
 template <typename T> size_t csize() { return sizeof(cx<T>); }
+
+// Grow a kept scratch buffer to `bytes` (after the stream's earlier work).
+cudaError_t grow(cudaStream_t st, DevBuf &b, size_t bytes) {
+  if (b.p && b.bytes >= bytes) return cudaSuccess;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return e;
+  b.release();
+  return b.alloc(bytes);
+}
 
 template <typename T>
 pfdd_status upload_table(pfdd_gpu *h, DevBuf &dst, const std::vector<double> &tw) {
@@ -409,7 +440,7 @@ pfdd_status set_smem_attrs(pfdd_gpu *h, size_t plane, size_t upd, size_t pencil)
   CUDA_TRY(h, raise_smem_limit(k_inv_update<T, NP, false>, upd));
   CUDA_TRY(h, raise_smem_limit(k_inv_update<T, NH, true>, upd));
   cudaError_t pe_err = cudaSuccess;
-  for (int sc : {0, 2, 3})
+  for (int sc : {0, 2, 3, 12})
     with_pencil_sc(sc, [&](auto SCc) {
       constexpr int SC = decltype(SCc)::value;
       if (pe_err == cudaSuccess) pe_err = raise_smem_limit(k_xpencil<T, NC, SC>, pencil);
@@ -511,14 +542,18 @@ struct AdjointPass {
 // spectrum is current, i.e. opened by launch_fwd or left by the previous fused
 // plane pass: P2, the fused plane pass (fwd: also the next iteration's
 // spectrum) and, for forward steps, the reduction.
+// Forward steps may read and write explicit state buffers (fin/fout, the
+// adjoint's tape) and leave out the reduction (stats = false).
 template <typename T>
-void enqueue_step_fused(Instance &I, cudaStream_t st, bool fwd, const AdjointPass *adj = nullptr) {
+void enqueue_step_fused(Instance &I, cudaStream_t st, bool fwd, const AdjointPass *adj = nullptr,
+                        const void *fin = nullptr, void *fout = nullptr, bool stats = true) {
   constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
   PlaneArgs pa;
   fill_plane_args<T>(I, pa);
   int *flags = I.flags();
-  const T *xin = adj ? static_cast<const T *>(adj->lam_in) : I.xi[I.cur].as<T>();
-  T *xout = adj ? static_cast<T *>(adj->lam_out) : I.xi[I.cur ^ 1].as<T>();
+  const T *xin = adj ? static_cast<const T *>(adj->lam_in)
+                     : (fin ? static_cast<const T *>(fin) : I.xi[I.cur].as<T>());
+  T *xout = adj ? static_cast<T *>(adj->lam_out) : (fout ? static_cast<T *>(fout) : I.xi[I.cur ^ 1].as<T>());
   cx<T> *spec = I.spec.as<cx<T>>();
   const int planes = I.F * I.nx;
   PencilArgs pe{};
@@ -564,6 +599,7 @@ void enqueue_step_fused(Instance &I, cudaStream_t st, bool fwd, const AdjointPas
     launch_pair(k_step_planes<T, NH, true>, dim3(2 * planes), NH, I.smem_update, st, spec, xin, xout, pa, ua,
                 partials, (int)fwd);
   else k_step_planes<T, NP, false><<<planes, NP, I.smem_update, st>>>(spec, xin, xout, pa, ua, partials, (int)fwd);
+  if (!stats) return;
   const bool nyq = I.imag == IMAG_NYQ;
   k_finalize<<<1, 1024, 0, st>>>(partials, planes, I.stats.as<double>(), 0, 0.0, flags, flags + 1, flags + 2,
                                  nyq ? I.ppart.as<double>() : nullptr, nyq ? I.ntiles : 0, 1.0 / (double)I.N);
@@ -586,6 +622,142 @@ bool same_group(const Instance &a, const Instance &b) {
     return false;
   if ((a.mask.p == nullptr) != (b.mask.p == nullptr) || (a.site.p == nullptr) != (b.site.p == nullptr)) return false;
   return true;
+}
+
+// Instances that differ in nothing but the grid size (slip systems, carrier,
+// material, core model, stress projections, mask and GSFE-field presence):
+// their groups can share the mixed-size launches.
+bool same_class(const Instance &a, const Instance &b) {
+  if (a.S != b.S || a.F != b.F || a.imag != b.imag || a.split || b.split) return false;
+  const pfdd_instance_desc &x = a.d, &y = b.d;
+  if (x.core_flag != y.core_flag || x.C44 != y.C44 || x.C12 != y.C12 || x.C11 != y.C11 || x.dslip != y.dslip ||
+      x.b != y.b || x.cd_dt != y.cd_dt || x.isf != y.isf || x.usf != y.usf || x.An != y.An)
+    return false;
+  if (memcmp(x.four, y.four, sizeof x.four) || memcmp(x.prim, y.prim, sizeof x.prim) ||
+      memcmp(x.xn, y.xn, sizeof(double) * 3 * a.S) || memcmp(x.xb, y.xb, sizeof(double) * 3 * a.S) ||
+      memcmp(x.c, y.c, sizeof x.c) || memcmp(x.aa, y.aa, sizeof x.aa) || memcmp(x.bb, y.bb, sizeof x.bb))
+    return false;
+  if ((x.non_schmid != 0) != (y.non_schmid != 0) || x.angle_to_110 != y.angle_to_110 || x.w1 != y.w1 ||
+      x.w2 != y.w2 || x.w3 != y.w3 || memcmp(x.usfe_fit, y.usfe_fit, sizeof x.usfe_fit))
+    return false;
+  return (a.mask.p == nullptr) == (b.mask.p == nullptr) && (a.site.p == nullptr) == (b.site.p == nullptr);
+}
+
+template <typename T> const GreenT<T> &green_host(const Green &g);
+template <> const GreenT<double> &green_host<double>(const Green &g) { return g.d; }
+template <> const GreenT<float> &green_host<float>(const Green &g) { return g.f; }
+
+// x-pencil arguments of instance L's group (the tile width is the group's)
+template <typename T>
+void group_pencil_args(const Instance &L, PencilArgs &pe) {
+  pe = PencilArgs{};
+  pe.px = L.px;
+  pe.nx = L.nx; pe.ny = L.ny; pe.nz = L.nz; pe.nzh = L.nzh; pe.nzp = L.nzp; pe.M = L.M;
+  pe.S = L.S; pe.F = L.F; pe.imag = L.imag;
+  pe.ncols = L.ny * L.nzp;
+  pe.ccols = L.ccols;
+  pe.tw_x = L.tw_x.p;
+  pe.kx_of = L.kx_of; pe.ky_of = L.ky_of; pe.kz_of = L.kz_of;
+  pe.mode = PASS_STEP;
+  pe.fstride = L.fstride;
+  pe.sx_n = L.sx_n; pe.sy_n = L.sy_n;
+  pe.cd = L.d.cd_dt;
+  pe.g = L.green;
+  set_pencil_divisors<T>(pe);
+}
+
+// update arguments of instance L's group stepping (per-instance pointers come
+// from the group table)
+void group_update_args(const Instance &L, UpdateArgs &ua) {
+  memset(&ua, 0, sizeof ua);
+  ua.nx = L.nx; ua.ny = L.ny; ua.nz = L.nz; ua.nzh = L.nzh; ua.nzp = L.nzp; ua.S = L.S; ua.F = L.F;
+  ua.cd = L.d.cd_dt;
+  ua.invN = 1.0 / (double)L.N;
+  ua.core = L.core;
+  ua.mode = PASS_STEP;
+}
+
+template <typename T>
+pfdd_status build_merges_t(pfdd_gpu *h) {
+  constexpr int NC = Threads<T>::pencil;
+  h->merges.clear();
+  h->group_merge.assign(h->groups.size(), -1);
+  std::vector<std::vector<int>> cls;
+  for (size_t gi = 0; gi < h->groups.size(); ++gi) {
+    const Instance &L = *h->inst[h->groups[gi].members[0]];
+    if (!L.merged || L.split) continue;
+    int c = -1;
+    for (size_t k = 0; k < cls.size() && c < 0; ++k)
+      if ((int)cls[k].size() < kMaxMerged && same_class(*h->inst[h->groups[cls[k][0]].members[0]], L)) c = (int)k;
+    if (c < 0) {
+      cls.emplace_back();
+      c = (int)cls.size() - 1;
+    }
+    cls[c].push_back((int)gi);
+  }
+  for (auto &gl : cls) {
+    if (gl.size() < 2) continue;
+    h->merges.emplace_back();
+    MergeClass &mc = h->merges.back();
+    mc.groups = gl;
+    const int n = (int)gl.size();
+    std::vector<MultiPlaneGroup> pg(n);
+    std::vector<MultiPencilGroup> peg(n);
+    std::vector<MultiFinalGroup> fg(n);
+    mc.mp.ngroups = mc.mpe.ngroups = mc.mf.ngroups = n;
+    unsigned pc = 0, pec = 0, ic = 0;
+    for (int k = 0; k < n; ++k) {
+      const Group &G = h->groups[gl[k]];
+      const Instance &L = *h->inst[G.members[0]];
+      const unsigned B = (unsigned)G.members.size();
+      fill_plane_args<T>(L, pg[k].a);
+      group_update_args(L, pg[k].u);
+      pg[k].tab = static_cast<const InstPtrs *>(G.table.p);
+      pg[k].per_member = L.F * L.nx;
+      group_pencil_args<T>(L, peg[k].a);
+      peg[k].tab = pg[k].tab;
+      peg[k].per_member = L.ntiles;
+      fg[k].tab = pg[k].tab;
+      fg[k].nparts = L.F * L.nx;
+      fg[k].nparts2 = L.imag == IMAG_NYQ ? L.ntiles : 0;
+      fg[k].scale2 = 1.0 / (double)L.N;
+      mc.mp.starts[k] = (int)pc;
+      mc.mpe.starts[k] = (int)pec;
+      mc.mf.starts[k] = (int)ic;
+      pc += B * (unsigned)pg[k].per_member;
+      pec += B * (unsigned)L.ntiles;
+      ic += B;
+      mc.smem_plane = std::max(mc.smem_plane, L.smem_update);
+      mc.smem_pencil = std::max(mc.smem_pencil, L.smem_pencil);
+      mc.S = L.S;
+    }
+    mc.mp.starts[n] = (int)pc;
+    mc.mpe.starts[n] = (int)pec;
+    mc.mf.starts[n] = (int)ic;
+    mc.plane_ctas = pc;
+    mc.pencil_ctas = pec;
+    mc.insts = ic;
+    CUDA_TRY(h, mc.ptab.alloc(n * sizeof(MultiPlaneGroup)));
+    CUDA_TRY(h, cudaMemcpy(mc.ptab.p, pg.data(), n * sizeof(MultiPlaneGroup), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, mc.pentab.alloc(n * sizeof(MultiPencilGroup)));
+    CUDA_TRY(h, cudaMemcpy(mc.pentab.p, peg.data(), n * sizeof(MultiPencilGroup), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, mc.ftab.alloc(n * sizeof(MultiFinalGroup)));
+    CUDA_TRY(h, cudaMemcpy(mc.ftab.p, fg.data(), n * sizeof(MultiFinalGroup), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, raise_smem_limit(k_step_planes_multi<T, 256>, mc.smem_plane));
+    CUDA_TRY(h, raise_smem_limit(k_fwd_planes_multi<T, 256>, mc.smem_plane));
+    cudaError_t e = cudaSuccess;
+    with_pencil_sc(mc.S, [&](auto SCc) {
+      constexpr int SC = decltype(SCc)::value;
+      e = raise_smem_limit(k_xpencil_multi<T, NC, SC>, mc.smem_pencil);
+    });
+    CUDA_TRY(h, e);
+    for (int g : gl) h->group_merge[g] = (int)h->merges.size() - 1;
+  }
+  return PFDD_OK;
+}
+
+pfdd_status build_merges(pfdd_gpu *h) {
+  return h->precision == PFDD_FP64 ? build_merges_t<double>(h) : build_merges_t<float>(h);
 }
 
 // Write every group's InstPtrs table (after any per-instance buffer changes).
@@ -613,7 +785,8 @@ pfdd_status refresh_tables(pfdd_gpu *h) {
     if (!G.table.p) CUDA_TRY(h, G.table.alloc(t.size() * sizeof(InstPtrs)));
     CUDA_TRY(h, cudaMemcpy(G.table.p, t.data(), t.size() * sizeof(InstPtrs), cudaMemcpyHostToDevice));
   }
-  return PFDD_OK;
+  // the mixed-size launches read tile widths and buffer sizes from their tables
+  return build_merges(h);
 }
 
 void build_groups(pfdd_gpu *h) {
@@ -651,20 +824,7 @@ void launch_group_pencil(const Instance &L, const Group &G, cudaStream_t st) {
   const unsigned B = (unsigned)G.members.size();
   const InstPtrs *tab = static_cast<const InstPtrs *>(G.table.p);
   PencilArgs pe;
-  pe = PencilArgs{};
-  pe.px = L.px;
-  pe.nx = L.nx; pe.ny = L.ny; pe.nz = L.nz; pe.nzh = L.nzh; pe.nzp = L.nzp; pe.M = L.M;
-  pe.S = L.S; pe.F = L.F; pe.imag = L.imag;
-  pe.ncols = L.ny * L.nzp;
-  pe.ccols = L.ccols;
-  pe.tw_x = L.tw_x.p;
-  pe.kx_of = L.kx_of; pe.ky_of = L.ky_of; pe.kz_of = L.kz_of;
-  pe.mode = PASS_STEP;
-  pe.fstride = L.fstride;
-  pe.sx_n = L.sx_n; pe.sy_n = L.sy_n;
-  pe.cd = L.d.cd_dt;
-  pe.g = L.green;
-  set_pencil_divisors<T>(pe);
+  group_pencil_args<T>(L, pe);
   with_pencil_sc(L.S, [&](auto SCc) {
     k_xpencil_tab<T, NC, decltype(SCc)::value><<<dim3(L.ntiles, B), NC, L.smem_pencil, st>>>(tab, pe);
   });
@@ -681,12 +841,7 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   launch_group_pencil<T>(L, G, st);
   if (ev) cudaEventRecord(ev[1], st);
   UpdateArgs ua;
-  memset(&ua, 0, sizeof ua);
-  ua.nx = L.nx; ua.ny = L.ny; ua.nz = L.nz; ua.nzh = L.nzh; ua.nzp = L.nzp; ua.S = L.S; ua.F = L.F;
-  ua.cd = L.d.cd_dt;
-  ua.invN = 1.0 / (double)L.N;
-  ua.core = L.core;
-  ua.mode = PASS_STEP;
+  group_update_args(L, ua);
   launch_step_tab<T>(L, B, st, tab, pa, ua, fwd);
   if (ev) cudaEventRecord(ev[2], st);
   const bool nyq = L.imag == IMAG_NYQ;
@@ -694,14 +849,52 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   if (ev) cudaEventRecord(ev[3], st);
 }
 
+// One step of a merge class: three launches for all of its groups.
 template <typename T>
-void enqueue_open_all(pfdd_gpu *h, cudaStream_t st) {
-  for (auto &G : h->groups) enqueue_group_open<T>(*h->inst[G.members[0]], G, st);
+void enqueue_merge_step(pfdd_gpu *h, const MergeClass &mc, cudaStream_t st, double tol, bool fwd,
+                        cudaEvent_t *ev = nullptr) {
+  constexpr int NC = Threads<T>::pencil;
+  const Instance &L = *h->inst[h->groups[mc.groups[0]].members[0]];
+  if (ev) cudaEventRecord(ev[0], st);
+  with_pencil_sc(mc.S, [&](auto SCc) {
+    k_xpencil_multi<T, NC, decltype(SCc)::value><<<mc.pencil_ctas, NC, mc.smem_pencil, st>>>(
+        mc.pentab.as<MultiPencilGroup>(), mc.mpe, green_host<T>(L.green));
+  });
+  if (ev) cudaEventRecord(ev[1], st);
+  k_step_planes_multi<T, 256><<<mc.plane_ctas, 256, mc.smem_plane, st>>>(mc.ptab.as<MultiPlaneGroup>(), mc.mp,
+                                                                         (int)fwd);
+  if (ev) cudaEventRecord(ev[2], st);
+  k_finalize_multi<<<mc.insts, 1024, 0, st>>>(mc.ftab.as<MultiFinalGroup>(), mc.mf, tol);
+  if (ev) cudaEventRecord(ev[3], st);
 }
 
 template <typename T>
-void enqueue_all_groups(pfdd_gpu *h, cudaStream_t st, double tol, bool fwd) {
-  for (auto &G : h->groups) enqueue_group_step<T>(*h->inst[G.members[0]], G, st, tol, fwd);
+void enqueue_open_all(pfdd_gpu *h, cudaStream_t st) {
+  for (size_t gi = 0; gi < h->groups.size(); ++gi)
+    if (h->group_merge[gi] < 0) enqueue_group_open<T>(*h->inst[h->groups[gi].members[0]], h->groups[gi], st);
+  for (auto &mc : h->merges)
+    k_fwd_planes_multi<T, 256><<<mc.plane_ctas, 256, mc.smem_plane, st>>>(mc.ptab.as<MultiPlaneGroup>(), mc.mp);
+}
+
+// Launch units of one step: merge classes and groups outside them.
+inline int n_units(const pfdd_gpu *h) {
+  int n = (int)h->merges.size();
+  for (int m : h->group_merge) n += m < 0;
+  return n;
+}
+
+// ev: 4 events per unit (n_units of them), in unit order
+template <typename T>
+void enqueue_all_groups(pfdd_gpu *h, cudaStream_t st, double tol, bool fwd, cudaEvent_t *ev = nullptr) {
+  for (size_t gi = 0; gi < h->groups.size(); ++gi)
+    if (h->group_merge[gi] < 0) {
+      enqueue_group_step<T>(*h->inst[h->groups[gi].members[0]], h->groups[gi], st, tol, fwd, ev);
+      if (ev) ev += 4;
+    }
+  for (auto &mc : h->merges) {
+    enqueue_merge_step<T>(h, mc, st, tol, fwd, ev);
+    if (ev) ev += 4;
+  }
 }
 
 constexpr int kLaunchesPerStep = 3;   // per group, plus one opening P1 per run
@@ -719,18 +912,17 @@ pfdd_status profile_impl(pfdd_gpu *h, int n_steps, double *kernel_ms) {
   if ((ps = ensure_stats(h, n_steps))) return ps;
   if ((ps = reset_counters(h))) return ps;
   stress_all<T>(h, 0);
-  const size_t ng = h->groups.size();
+  const size_t ng = (size_t)n_units(h);
   std::vector<cudaEvent_t> ev(4 * (size_t)n_steps * ng + 2);
   for (auto &e : ev) CUDA_TRY(h, cudaEventCreate(&e));
   cudaEventRecord(ev[0], st);
   enqueue_open_all<T>(h, st);
   cudaEventRecord(ev[1], st);
   size_t q = 2;
-  for (int it = 0; it < n_steps; ++it)
-    for (auto &G : h->groups) {
-      enqueue_group_step<T>(*h->inst[G.members[0]], G, st, 0.0, it + 1 < n_steps, &ev[q]);
-      q += 4;
-    }
+  for (int it = 0; it < n_steps; ++it) {
+    enqueue_all_groups<T>(h, st, 0.0, it + 1 < n_steps, &ev[q]);
+    q += 4 * ng;
+  }
   cudaError_t e = cudaStreamSynchronize(st);
   if (e == cudaSuccess) {
     float ms = 0.f;
@@ -773,11 +965,69 @@ pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *si
   // before sigma += dsigma (solve_GL.cpp:110-155), while pfdd_gpu_advance has
   // already added the increment when it returns
   double sig[9], sr[3][3];
-  CUDA_TRY(h, cudaMemcpyAsync(sig, I.sigma(), sizeof sig, cudaMemcpyDeviceToHost, st));
-  // per-system sums of Re xi of the current state
   const int nb = 296;
-  DevBuf part, spec6, strain6, e9, s9, fpart;
-  CUDA_TRY(h, part.alloc((size_t)nb * S * sizeof(double)));
+  DevBuf &part = I.ss_part, &spec6 = I.ss_spec6, &strain6 = I.ss_strain6, &e9 = I.ss_e9, &s9 = I.ss_s9,
+         &fpart = I.ss_fpart;
+  const size_t ncols = (size_t)I.ny * I.nzp;
+  CUDA_TRY(h, grow(st, part, (size_t)nb * S * sizeof(double)));
+  CUDA_TRY(h, grow(st, spec6, 6 * (size_t)I.nx * ncols * sizeof(C)));
+  CUDA_TRY(h, grow(st, strain6, 6 * N * sizeof(T)));
+  CUDA_TRY(h, grow(st, fpart, (size_t)nb * 18 * sizeof(double)));
+  if (eps) CUDA_TRY(h, grow(st, e9, 9 * N * sizeof(double)));
+  if (sigma) CUDA_TRY(h, grow(st, s9, 9 * N * sizeof(double)));
+  CUDA_TRY(h, cudaMemcpyAsync(sig, I.sigma(), sizeof sig, cudaMemcpyDeviceToHost, st));
+
+  // forward planes of the current state into the spectrum buffer
+  PlaneArgs pa;
+  fill_plane_args<T>(I, pa);
+  launch_fwd<T>(I, st, I.xi[I.cur].as<T>(), I.spec.as<C>(), pa, nullptr, I.flags() + 3);
+  const double C44 = I.d.C44, C12 = I.d.C12, C11 = I.d.C11;
+  const double mu = C44 - (2.0 * C44 + C12 - C11) / 5.0, ll = C12 - (2.0 * C44 + C12 - C11) / 5.0;
+  // strain pencils: tile width reduced until max(F, 6) fields fit
+  const int FB = std::max(I.F, 6);
+  int cc = I.ccols;
+  auto bytes = [&](int c) { return ((size_t)FB * I.nx * c + I.nx) * sizeof(C); };
+  while (cc > 1 && bytes(cc) > 227 * 1024) cc >>= 1;
+  if (bytes(cc) > 227 * 1024 || ncols % cc)
+    return fail(h, PFDD_EUNSUPPORTED, "strain pencil of %d x %d fields does not fit shared memory", I.nx, FB);
+  CUDA_TRY(h, raise_smem_limit(k_strain_pencil<T, 256>, bytes(cc)));
+  PencilArgs pe{};
+  pe.px = I.px;
+  pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.nzp = I.nzp; pe.M = I.M;
+  pe.S = I.S; pe.F = I.F; pe.imag = I.imag;
+  pe.ncols = (int)ncols;
+  pe.ccols = cc;
+  pe.tw_x = I.tw_x.p;
+  pe.kx_of = I.kx_of; pe.ky_of = I.ky_of; pe.kz_of = I.kz_of;
+  pe.mode = PASS_STEP;
+  pe.fstride = I.nx * cc;
+  pe.aux = I.aux.p;
+  pe.sx_n = I.sx_n; pe.sy_n = I.sy_n;
+  pe.g = I.green;
+  set_pencil_divisors<T>(pe);
+  pe.fd_6cc = FastDiv(6 * cc);
+  pe.inv2mu = 0.5 / mu;
+  k_strain_pencil<T, 256><<<(unsigned)(ncols / cc), 256, bytes(cc), st>>>(I.spec.as<C>(), spec6.as<C>(), pe);
+  // inverse planes of the six strain spectra (the Im-synthesis pass: IFFT / N)
+  {
+    UpdateArgs ua;
+    memset(&ua, 0, sizeof ua);
+    ua.nx = I.nx; ua.ny = I.ny; ua.nz = I.nz; ua.nzh = I.nzh; ua.nzp = I.nzp; ua.S = I.S; ua.F = 6;
+    ua.invN = 1.0 / (double)N;
+    ua.core = I.core;
+    ua.err = I.flags() + 3;
+    ua.mode = PASS_SYNTH;
+    const unsigned planes6 = (unsigned)(6 * I.nx);
+    if (I.split)
+      launch_pair(k_inv_update<T, NH, true>, dim3(2 * planes6), NH, I.smem_update, st, spec6.as<C>(),
+                  I.xi[I.cur].as<T>(), strain6.as<T>(), pa, ua, I.partials.as<double>());
+    else
+      k_inv_update<T, NP, false><<<planes6, NP, I.smem_update, st>>>(spec6.as<C>(), I.xi[I.cur].as<T>(),
+                                                                       strain6.as<T>(), pa, ua,
+                                                                       I.partials.as<double>());
+  }
+  // per-system sums of Re xi of the current state, read back once the
+  // transforms are queued (the host forms the stress constants from them)
   k_field_sums<T><<<nb, 256, 0, st>>>(I.xi[I.cur].as<T>(), S, N, part.as<double>());
   std::vector<double> hp((size_t)nb * S);
   CUDA_TRY(h, cudaMemcpyAsync(hp.data(), part.p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -796,8 +1046,6 @@ pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *si
       }
       sr[i][j] = v;
     }
-  const double C44 = I.d.C44, C12 = I.d.C12, C11 = I.d.C11;
-  const double mu = C44 - (2.0 * C44 + C12 - C11) / 5.0, ll = C12 - (2.0 * C44 + C12 - C11) / 5.0;
   const double young = mu * (3 * ll + 2 * mu) / (ll + mu), xnu = young / 2.0 / mu - 1.0;
   const double S11 = 1.0 / young, S12 = -xnu / young, S44 = 2.0 * (S11 - S12);
   double epsm[PFDD_MAXS][3][3], mean[PFDD_MAXS];
@@ -837,59 +1085,10 @@ pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *si
   sp.C12 = C12;
   sp.S = S;
 
-  // forward planes of the current state into the spectrum buffer
-  PlaneArgs pa;
-  fill_plane_args<T>(I, pa);
-  launch_fwd<T>(I, st, I.xi[I.cur].as<T>(), I.spec.as<C>(), pa, nullptr, I.flags() + 3);
-  // strain pencils: tile width reduced until max(F, 6) fields fit
-  const size_t ncols = (size_t)I.ny * I.nzp;
-  const int FB = std::max(I.F, 6);
-  int cc = I.ccols;
-  auto bytes = [&](int c) { return ((size_t)FB * I.nx * c + I.nx) * sizeof(C); };
-  while (cc > 1 && bytes(cc) > 227 * 1024) cc >>= 1;
-  if (bytes(cc) > 227 * 1024 || ncols % cc)
-    return fail(h, PFDD_EUNSUPPORTED, "strain pencil of %d x %d fields does not fit shared memory", I.nx, FB);
-  CUDA_TRY(h, raise_smem_limit(k_strain_pencil<T, 256>, bytes(cc)));
-  PencilArgs pe{};
-  pe.px = I.px;
-  pe.nx = I.nx; pe.ny = I.ny; pe.nz = I.nz; pe.nzh = I.nzh; pe.nzp = I.nzp; pe.M = I.M;
-  pe.S = I.S; pe.F = I.F; pe.imag = I.imag;
-  pe.ncols = (int)ncols;
-  pe.ccols = cc;
-  pe.tw_x = I.tw_x.p;
-  pe.kx_of = I.kx_of; pe.ky_of = I.ky_of; pe.kz_of = I.kz_of;
-  pe.mode = PASS_STEP;
-  pe.fstride = I.nx * cc;
-  pe.aux = I.aux.p;
-  pe.sx_n = I.sx_n; pe.sy_n = I.sy_n;
-  pe.g = I.green;
-  set_pencil_divisors<T>(pe);
-  pe.fd_6cc = FastDiv(6 * cc);
-  pe.inv2mu = 0.5 / mu;
-  CUDA_TRY(h, spec6.alloc(6 * (size_t)I.nx * ncols * sizeof(C)));
-  k_strain_pencil<T, 256><<<(unsigned)(ncols / cc), 256, bytes(cc), st>>>(I.spec.as<C>(), spec6.as<C>(), pe);
-  // inverse planes of the six strain spectra (the Im-synthesis pass: IFFT / N)
-  CUDA_TRY(h, strain6.alloc(6 * N * sizeof(T)));
-  UpdateArgs ua;
-  memset(&ua, 0, sizeof ua);
-  ua.nx = I.nx; ua.ny = I.ny; ua.nz = I.nz; ua.nzh = I.nzh; ua.nzp = I.nzp; ua.S = I.S; ua.F = 6;
-  ua.invN = 1.0 / (double)N;
-  ua.core = I.core;
-  ua.err = I.flags() + 3;
-  ua.mode = PASS_SYNTH;
-  const unsigned planes6 = (unsigned)(6 * I.nx);
-  if (I.split)
-    launch_pair(k_inv_update<T, NH, true>, dim3(2 * planes6), NH, I.smem_update, st, spec6.as<C>(),
-                I.xi[I.cur].as<T>(), strain6.as<T>(), pa, ua, I.partials.as<double>());
-  else
-    k_inv_update<T, NP, false><<<planes6, NP, I.smem_update, st>>>(spec6.as<C>(), I.xi[I.cur].as<T>(),
-                                                                     strain6.as<T>(), pa, ua, I.partials.as<double>());
   // pointwise strain and stress, FP64 sums of both
-  if (eps) CUDA_TRY(h, e9.alloc(9 * N * sizeof(double)));
-  if (sigma) CUDA_TRY(h, s9.alloc(9 * N * sizeof(double)));
-  CUDA_TRY(h, fpart.alloc((size_t)nb * 18 * sizeof(double)));
-  k_stress_fields<T><<<nb, 256, 0, st>>>(strain6.as<T>(), I.xi[I.cur].as<T>(), N, sp, e9.as<double>(),
-                                          s9.as<double>(), fpart.as<double>());
+  k_stress_fields<T><<<nb, 256, 0, st>>>(strain6.as<T>(), I.xi[I.cur].as<T>(), N, sp,
+                                          eps ? e9.as<double>() : nullptr, sigma ? s9.as<double>() : nullptr,
+                                          fpart.as<double>());
   std::vector<double> hf((size_t)nb * 18);
   CUDA_TRY(h, cudaMemcpyAsync(hf.data(), fpart.p, hf.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
   if (eps) CUDA_TRY(h, cudaMemcpyAsync(eps, e9.p, 9 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -992,21 +1191,29 @@ pfdd_status energy_impl(pfdd_gpu *h, Instance &I, double *e_el, double *e_core, 
 }
 
 // ------------------------------------------------------------ adjoint
-// Gradient of J = sum (Re xi_N - target)^2 over the S real fields, N = n_steps
-// GL iterations from the current state (one stress state), with respect to
-// the GSFE parameters and the applied stress.  Checkpoints every K steps;
-// each segment is recomputed forward (storing Re xi_n) and then stepped
-// backward.  The instance ends at xi_N, as after pfdd_gpu_advance.
+// Reverse-mode gradient of a loss L(Re xi_N), xi_N = n_steps GL iterations
+// from the current state at the current stress state, in two calls:
+//   adjoint_forward_impl  the forward run, kept as a tape: the state every K
+//                         steps (with the Nyquist carrier of Im xi), and every
+//                         state of the last segment; the instance ends at xi_N;
+//   adjoint_backward_impl seeded with dL/dRe xi_N, each segment's states
+//                         recomputed from its checkpoint (the last segment's
+//                         are on the tape already), then the adjoint steps
+//   lam_n = lam_{n+1} - cd (L lam_{n+1} + f''(xi_n) lam_{n+1}),
+// whose plane passes add their per-plane gradient sums into one accumulator;
+// one reduction at the end.  The tape stays valid (several seeds may be
+// run) until the instance's state changes.  Tape steps leave out the per-step
+// reduction (no xinorm is needed); a non-finite gradient reports divergence.
 template <typename T>
-pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const double *target, double *loss,
-                         double *dparams, double *dsigma) {
+pfdd_status adjoint_forward_impl(pfdd_gpu *h, Instance &I, int n_steps, int K) {
   cudaStream_t st = h->stream;
   ARM_FLAGS(h, I);
-  const size_t n_re = (size_t)I.S * I.N;
-  const size_t n_all = (size_t)I.F * I.N;
+  I.tape_steps = 0;
+  const size_t n_all = (size_t)I.F * I.N, sb = n_all * sizeof(T);
   const size_t aux_bytes = I.aux.bytes;
   const int nck = (n_steps + K - 1) / K;
-  // scratch kept in the instance and grown on demand (no allocation per call)
+  const int last0 = (nck - 1) * K;            // first step of the last segment
+  const int seg_slots = n_steps - last0;      // states n = last0 .. n_steps-1
   auto need = [&](DevBuf &b, size_t bytes) -> cudaError_t {
     if (b.bytes >= bytes && b.p) return cudaSuccess;
     cudaError_t e = cudaStreamSynchronize(st);
@@ -1014,113 +1221,137 @@ pfdd_status adjoint_impl(pfdd_gpu *h, Instance &I, int n_steps, int K, const dou
     b.release();
     return b.alloc(bytes);
   };
-  DevBuf &ck = I.adj_ck, &seg = I.adj_seg, &tgt = I.adj_tgt, &auxa = I.adj_aux, &gpart = I.adj_gpart,
-         &acc = I.adj_acc, &lpart = I.adj_lpart;
-  DevBuf *lam = I.adj_lam;
-  CUDA_TRY(h, need(ck, (size_t)nck * (n_all * sizeof(T) + aux_bytes)));
-  CUDA_TRY(h, need(seg, (size_t)K * n_re * sizeof(T)));
-  for (int b = 0; b < 2; ++b) CUDA_TRY(h, need(lam[b], n_all * sizeof(T)));
-  CUDA_TRY(h, need(tgt, n_re * sizeof(T)));
-  if (aux_bytes) CUDA_TRY(h, need(auxa, aux_bytes));
-  CUDA_TRY(h, need(gpart, 4 * (size_t)I.F * I.nx * sizeof(double)));
-  CUDA_TRY(h, need(acc, 2 * (2 + PFDD_MAXS) * sizeof(double)));
-  CUDA_TRY(h, need(lpart, 2 * 1184 * sizeof(double)));
-  CUDA_TRY(h, cudaMemsetAsync(acc.p, 0, acc.bytes, st));
-  if (I.stats_cap < 1) {  // the forward steps record their stats at index 0
-    CUDA_TRY(h, I.stats.alloc(2 * sizeof(double)));
-    I.stats_cap = 1;
-  }
-  {  // target in compute precision, through the staging buffer
-    if (h->staging.bytes < 2 * n_re * sizeof(double)) {
-      CUDA_TRY(h, cudaStreamSynchronize(st));
-      h->staging.release();
-      CUDA_TRY(h, h->staging.alloc(2 * n_re * sizeof(double)));
-    }
-    CUDA_TRY(h, cudaMemcpyAsync(h->staging.p, target, n_re * sizeof(double), cudaMemcpyHostToDevice, st));
-    k_from_planar<T><<<1184, 256, 0, st>>>(h->staging.as<double>(), tgt.as<T>(), n_re);
-  }
-  auto ck_state = [&](int j) { return ck.as<char>() + (size_t)j * (n_all * sizeof(T) + aux_bytes); };
-  auto save = [&](int j) -> cudaError_t {
-    cudaError_t e = cudaMemcpyAsync(ck_state(j), I.xi[I.cur].p, n_all * sizeof(T), cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess && aux_bytes)
-      e = cudaMemcpyAsync(ck_state(j) + n_all * sizeof(T), I.aux.p, aux_bytes, cudaMemcpyDeviceToDevice, st);
-    return e;
-  };
-  auto restore = [&](int j) -> cudaError_t {
-    cudaError_t e = cudaMemcpyAsync(I.xi[I.cur].p, ck_state(j), n_all * sizeof(T), cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess && aux_bytes)
-      e = cudaMemcpyAsync(I.aux.p, ck_state(j) + n_all * sizeof(T), aux_bytes, cudaMemcpyDeviceToDevice, st);
-    return e;
-  };
+  // the last segment's states stay on the tape (adj_last); earlier segments
+  // are recomputed into adj_seg during the backward pass
+  CUDA_TRY(h, need(I.adj_ck, (size_t)nck * (sb + aux_bytes)));
+  CUDA_TRY(h, need(I.adj_last, (size_t)seg_slots * sb));
+  if (nck > 1) CUDA_TRY(h, need(I.adj_seg, (size_t)K * sb));
+  CUDA_TRY(h, need(I.adj_fin, sb));
+  if (aux_bytes) CUDA_TRY(h, need(I.adj_finaux, aux_bytes));
+  auto ck_state = [&](int j) { return I.adj_ck.as<char>() + (size_t)j * (sb + aux_bytes); };
+  auto slot = [&](int n) { return I.adj_last.as<char>() + (size_t)(n - last0) * sb; };
   k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.an(), I.stress, 0, I.flags());
   PlaneArgs pa;
   fill_plane_args<T>(I, pa);
-  // forward with checkpoints: one opening transform, then fused steps.  With
-  // one segment (K >= n_steps) the forward pass keeps every state the
-  // backward steps read, and nothing is recomputed.
-  const bool store_all = K >= n_steps;
-  launch_fwd<T>(I, st, I.xi[I.cur].as<T>(), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
+  // the opening transform, then fused steps; state n lives in I.xi (n < last0)
+  // or in its tape slot (n >= last0)
+  const void *cur = I.xi[I.cur].p;
+  launch_fwd<T>(I, st, static_cast<const T *>(cur), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
+  int pp = I.cur;   // ping-pong index of the state in I.xi while n < last0
   for (int n = 0; n < n_steps; ++n) {
-    if (n % K == 0) CUDA_TRY(h, save(n / K));
-    if (store_all)
-      CUDA_TRY(h, cudaMemcpyAsync(seg.as<T>() + (size_t)n * n_re, I.xi[I.cur].p, n_re * sizeof(T),
-                                  cudaMemcpyDeviceToDevice, st));
-    enqueue_step_fused<T>(I, st, n + 1 < n_steps);
-    I.cur ^= 1;
-  }
-  // keep the final state to hand back; seed lambda = 2 (Re xi_N - target), mu = 0
-  DevBuf &fin = I.adj_fin, &finaux = I.adj_finaux;
-  CUDA_TRY(h, need(fin, n_all * sizeof(T)));
-  CUDA_TRY(h, cudaMemcpyAsync(fin.p, I.xi[I.cur].p, n_all * sizeof(T), cudaMemcpyDeviceToDevice, st));
-  if (aux_bytes) {
-    CUDA_TRY(h, need(finaux, aux_bytes));
-    CUDA_TRY(h, cudaMemcpyAsync(finaux.p, I.aux.p, aux_bytes, cudaMemcpyDeviceToDevice, st));
-    CUDA_TRY(h, cudaMemsetAsync(auxa.p, 0, aux_bytes, st));
-  }
-  CUDA_TRY(h, cudaMemsetAsync(lam[0].p, 0, n_all * sizeof(T), st));
-  k_loss_seed<T><<<1184, 256, 0, st>>>(I.xi[I.cur].as<T>(), tgt.as<T>(), lam[0].as<T>(), n_re, lpart.as<double>());
-  int lc = 0;
-  // backward over segments
-  for (int j = nck - 1; j >= 0; --j) {
-    const int n0 = j * K, n1 = std::min(n_steps, n0 + K);
-    if (!store_all) CUDA_TRY(h, restore(j));
-    // recompute the segment's states (fused steps after one opening transform)
-    if (!store_all && n1 - n0 > 1)
-      launch_fwd<T>(I, st, I.xi[I.cur].as<T>(), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
-    for (int n = n0; n < n1 && !store_all; ++n) {
-      CUDA_TRY(h, cudaMemcpyAsync(seg.as<T>() + (size_t)(n - n0) * n_re, I.xi[I.cur].p, n_re * sizeof(T),
-                                  cudaMemcpyDeviceToDevice, st));
-      if (n + 1 < n1) {
-        enqueue_step_fused<T>(I, st, n + 2 < n1);
-        I.cur ^= 1;
-      }
+    if (n % K == 0) {
+      CUDA_TRY(h, cudaMemcpyAsync(ck_state(n / K), cur, sb, cudaMemcpyDeviceToDevice, st));
+      if (aux_bytes)
+        CUDA_TRY(h, cudaMemcpyAsync(ck_state(n / K) + sb, I.aux.p, aux_bytes, cudaMemcpyDeviceToDevice, st));
     }
-    // backward steps: the plane pass of each also transforms the new lambda
-    launch_fwd<T>(I, st, lam[lc].as<T>(), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
-    for (int n = n1 - 1; n >= n0; --n) {
-      AdjointPass ap{lam[lc].p, lam[lc ^ 1].p, seg.as<T>() + (size_t)(n - n0) * n_re, auxa.p, gpart.as<double>()};
-      enqueue_step_fused<T>(I, st, n > n0, &ap);
-      lc ^= 1;
-      k_grad_accum<<<1, 32, 0, st>>>(gpart.as<double>(), I.S, I.nx, acc.as<double>(), acc.as<double>() + 2 + PFDD_MAXS);
+    if (n == last0 && cur != slot(n)) {   // the last segment's first state onto the tape
+      CUDA_TRY(h, cudaMemcpyAsync(slot(n), cur, sb, cudaMemcpyDeviceToDevice, st));
+      cur = slot(n);
     }
+    void *out;
+    if (n + 1 == n_steps) out = I.xi[I.cur ^ 1].p;      // xi_N where the instance keeps its state
+    else if (n + 1 >= last0) out = slot(n + 1);
+    else {
+      pp ^= 1;
+      out = I.xi[pp].p;
+    }
+    enqueue_step_fused<T>(I, st, n + 1 < n_steps, nullptr, cur, out, false);
+    cur = out;
   }
-  // hand back xi_N (and make the device's buffer selector agree with the host's)
-  CUDA_TRY(h, cudaMemcpyAsync(I.xi[I.cur].p, fin.p, n_all * sizeof(T), cudaMemcpyDeviceToDevice, st));
+  I.cur ^= 1;
   CUDA_TRY(h, cudaMemcpyAsync(I.flags() + 4, &I.cur, sizeof(int), cudaMemcpyHostToDevice, st));
-  if (aux_bytes) CUDA_TRY(h, cudaMemcpyAsync(I.aux.p, finaux.p, aux_bytes, cudaMemcpyDeviceToDevice, st));
-  double hacc[2 * (2 + PFDD_MAXS)], hl[2 * 1184];
-  CUDA_TRY(h, cudaMemcpyAsync(hacc, acc.p, sizeof hacc, cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(h, cudaMemcpyAsync(hl, lpart.p, sizeof hl, cudaMemcpyDeviceToHost, st));
+  // xi_N and its carrier, restored after the backward pass reuses the buffers
+  CUDA_TRY(h, cudaMemcpyAsync(I.adj_fin.p, I.xi[I.cur].p, sb, cudaMemcpyDeviceToDevice, st));
+  if (aux_bytes) CUDA_TRY(h, cudaMemcpyAsync(I.adj_finaux.p, I.aux.p, aux_bytes, cudaMemcpyDeviceToDevice, st));
   CUDA_TRY(h, cudaStreamSynchronize(st));
+  CUDA_TRY(h, cudaGetLastError());
   int fl[4];
   CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
   if (fl[3]) return fail(h, PFDD_ETIMEOUT, "a bounded device wait ran out");
-  double L = 0.0;
-  for (int b = 0; b < 1184; ++b) L += hl[2 * b];
+  I.tape_steps = n_steps;
+  I.tape_K = K;
+  return PFDD_OK;
+}
+
+template <typename T>
+pfdd_status adjoint_backward_impl(pfdd_gpu *h, Instance &I, const double *seed, double *dparams, double *dsigma) {
+  cudaStream_t st = h->stream;
+  if (I.tape_steps < 1) return fail(h, PFDD_ESTATE, "no adjoint tape: call pfdd_gpu_adjoint_forward first");
+  ARM_FLAGS(h, I);
+  const int n_steps = I.tape_steps, K = I.tape_K;
+  const size_t n_re = (size_t)I.S * I.N, n_all = (size_t)I.F * I.N, sb = n_all * sizeof(T);
+  const size_t aux_bytes = I.aux.bytes;
+  const int nck = (n_steps + K - 1) / K, last0 = (nck - 1) * K;
+  auto need = [&](DevBuf &b, size_t bytes) -> cudaError_t {
+    if (b.bytes >= bytes && b.p) return cudaSuccess;
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    b.release();
+    return b.alloc(bytes);
+  };
+  DevBuf *lam = I.adj_lam;
+  for (int b = 0; b < 2; ++b) CUDA_TRY(h, need(lam[b], sb));
+  if (aux_bytes) CUDA_TRY(h, need(I.adj_aux, aux_bytes));
+  CUDA_TRY(h, need(I.adj_gpart, 4 * (size_t)I.F * I.nx * sizeof(double)));
+  CUDA_TRY(h, need(I.adj_acc, 2 * (2 + PFDD_MAXS) * sizeof(double)));
+  CUDA_TRY(h, cudaMemsetAsync(I.adj_acc.p, 0, I.adj_acc.bytes, st));
+  CUDA_TRY(h, cudaMemsetAsync(I.adj_gpart.p, 0, I.adj_gpart.bytes, st));
+  // seed: lam_N = dL/dRe xi_N on the real fields, 0 on Im (and its carrier)
+  if (h->staging.bytes < 2 * n_re * sizeof(double)) {
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    h->staging.release();
+    CUDA_TRY(h, h->staging.alloc(2 * n_re * sizeof(double)));
+  }
+  CUDA_TRY(h, cudaMemcpyAsync(h->staging.p, seed, n_re * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(h, cudaMemsetAsync(lam[0].p, 0, sb, st));
+  k_from_planar<T><<<1184, 256, 0, st>>>(h->staging.as<double>(), lam[0].as<T>(), n_re);
+  if (aux_bytes) CUDA_TRY(h, cudaMemsetAsync(I.adj_aux.p, 0, aux_bytes, st));
+  auto ck_state = [&](int j) { return I.adj_ck.as<char>() + (size_t)j * (sb + aux_bytes); };
+  k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.an(), I.stress, 0, I.flags());
+  PlaneArgs pa;
+  fill_plane_args<T>(I, pa);
+  int lc = 0;
+  for (int j = nck - 1; j >= 0; --j) {
+    const int n0 = j * K, n1 = std::min(n_steps, n0 + K);
+    // the last segment's states are on the tape; earlier ones are recomputed
+    char *states = (n0 == last0 ? I.adj_last : I.adj_seg).as<char>();
+    auto slot = [&](int i) { return states + (size_t)i * sb; };
+    if (n0 != last0) {
+      // recompute the segment's states into the tape slots from its checkpoint
+      CUDA_TRY(h, cudaMemcpyAsync(slot(0), ck_state(j), sb, cudaMemcpyDeviceToDevice, st));
+      if (aux_bytes)
+        CUDA_TRY(h, cudaMemcpyAsync(I.aux.p, ck_state(j) + sb, aux_bytes, cudaMemcpyDeviceToDevice, st));
+      if (n1 - n0 > 1)
+        launch_fwd<T>(I, st, reinterpret_cast<const T *>(slot(0)), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
+      for (int n = n0; n + 1 < n1; ++n)
+        enqueue_step_fused<T>(I, st, n + 2 < n1, nullptr, slot(n - n0), slot(n + 1 - n0), false);
+    }
+    // backward steps: each plane pass also transforms the new lambda
+    launch_fwd<T>(I, st, lam[lc].as<T>(), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
+    for (int n = n1 - 1; n >= n0; --n) {
+      AdjointPass ap{lam[lc].p, lam[lc ^ 1].p, slot(n - n0), I.adj_aux.p, I.adj_gpart.as<double>()};
+      enqueue_step_fused<T>(I, st, n > n0, &ap);
+      lc ^= 1;
+    }
+  }
+  k_grad_accum<<<1, 32, 0, st>>>(I.adj_gpart.as<double>(), I.S, I.nx, I.adj_acc.as<double>(),
+                                  I.adj_acc.as<double>() + 2 + PFDD_MAXS);
+  // hand back xi_N (the recomputation reused the carrier)
+  CUDA_TRY(h, cudaMemcpyAsync(I.xi[I.cur].p, I.adj_fin.p, sb, cudaMemcpyDeviceToDevice, st));
+  if (aux_bytes) CUDA_TRY(h, cudaMemcpyAsync(I.aux.p, I.adj_finaux.p, aux_bytes, cudaMemcpyDeviceToDevice, st));
+  double hacc[2 * (2 + PFDD_MAXS)];
+  CUDA_TRY(h, cudaMemcpyAsync(hacc, I.adj_acc.p, sizeof hacc, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  CUDA_TRY(h, cudaGetLastError());
+  int fl[4];
+  CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+  if (fl[3]) return fail(h, PFDD_ETIMEOUT, "a bounded device wait ran out");
   const double cd = I.d.cd_dt;
   double A[2 + PFDD_MAXS];
-  for (int t = 0; t < 2 + I.S; ++t) A[t] = hacc[t] + hacc[2 + PFDD_MAXS + t];
-  if (loss) *loss = L;
+  for (int t = 0; t < 2 + I.S; ++t) {
+    A[t] = hacc[t] + hacc[2 + PFDD_MAXS + t];
+    if (!std::isfinite(A[t])) return fail(h, PFDD_EDIVERGED, "non-finite adjoint sums");
+  }
   if (dparams) {
     dparams[0] = -cd * A[0];
     dparams[1] = -cd * A[1];
@@ -1229,6 +1460,7 @@ pfdd_status collect(pfdd_gpu *h, pfdd_step_stats *stats) {
     if (did)
       CUDA_TRY(h, cudaMemcpy(I.hist.data(), I.stats.p, 2 * (size_t)did * sizeof(double), cudaMemcpyDeviceToHost));
     I.hist_count = did;
+    I.steps_total += (unsigned long long)fl[2];
     if (stats) {
       stats[i].steps_done = fl[2];
       stats[i].converged = fl[0];
@@ -1241,6 +1473,7 @@ pfdd_status collect(pfdd_gpu *h, pfdd_step_stats *stats) {
 
 pfdd_status reset_counters(pfdd_gpu *h) {
   for (auto &ip : h->inst) {
+    ip->tape_steps = 0;   // the state moves on: the adjoint tape no longer describes it
     CUDA_TRY(h, cudaMemsetAsync(ip->flags() + 2, 0, sizeof(int), h->stream));
     ARM_FLAGS(h, *ip);
   }
@@ -1301,6 +1534,7 @@ pfdd_status advance_impl(pfdd_gpu *h, int n_steps, int stress_states, double tol
 template <typename T>
 pfdd_status set_state_impl(pfdd_gpu *h, Instance &I, const double *re, const double *im, bool interleaved) {
   const size_t n = (size_t)I.S * I.N;
+  I.tape_steps = 0;
   if (h->staging.bytes < 2 * n * sizeof(double)) {
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     h->staging.release();
@@ -1561,6 +1795,63 @@ pfdd_status snapshot_begin_impl(pfdd_gpu *h, Instance &I, double *re, double *im
   return PFDD_OK;
 }
 
+// ------------------------------------------------------------ checkpoints
+template <typename T>
+pfdd_status checkpoint_save_impl(pfdd_gpu *h, Instance &I, const char *path) {
+  pfdd_checkpoint_info in;
+  memset(&in, 0, sizeof in);
+  in.nx = I.nx; in.ny = I.ny; in.nz = I.nz; in.n_slip = I.S; in.fields = I.F;
+  in.precision = sizeof(T) == 8 ? PFDD_FP64 : PFDD_FP32;
+  in.imag_mode = I.imag == IMAG_FULL ? PFDD_IMAG_FULL : PFDD_IMAG_NYQUIST;
+  in.advanced = I.advanced ? 1 : 0;
+  in.field_bytes = (size_t)I.F * I.N * sizeof(T);
+  in.carrier_bytes = I.imag == IMAG_NYQ ? I.aux.bytes : 0;
+  in.steps = I.steps_total;
+  std::vector<unsigned char> f(in.field_bytes), c(in.carrier_bytes);
+  double sig[18];
+  CUDA_TRY(h, cudaMemcpyAsync(f.data(), I.xi[I.cur].p, in.field_bytes, cudaMemcpyDeviceToHost, h->stream));
+  if (in.carrier_bytes)
+    CUDA_TRY(h, cudaMemcpyAsync(c.data(), I.aux.p, in.carrier_bytes, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(sig, I.sigma(), sizeof sig, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  for (int i = 0; i < 9; ++i) {
+    in.sigma[i / 3][i % 3] = sig[i];
+    in.dsigma[i / 3][i % 3] = sig[9 + i];
+  }
+  const pfdd_status st = pfdd_checkpoint_write(path, &in, f.data(), c.empty() ? nullptr : c.data());
+  if (st != PFDD_OK) return fail(h, st, "cannot write checkpoint %s", path);
+  return PFDD_OK;
+}
+
+template <typename T>
+pfdd_status checkpoint_load_impl(pfdd_gpu *h, Instance &I, const char *path) {
+  pfdd_checkpoint_info in;
+  if (pfdd_checkpoint_read(path, &in, nullptr, 0, nullptr, 0) != PFDD_OK)
+    return fail(h, PFDD_EINVAL, "%s is not a readable checkpoint", path);
+  const int want_imag = I.imag == IMAG_FULL ? PFDD_IMAG_FULL : PFDD_IMAG_NYQUIST;
+  const size_t fb = (size_t)I.F * I.N * sizeof(T), cb = I.imag == IMAG_NYQ ? I.aux.bytes : 0;
+  if (in.nx != I.nx || in.ny != I.ny || in.nz != I.nz || in.n_slip != I.S || in.fields != I.F ||
+      in.precision != (sizeof(T) == 8 ? PFDD_FP64 : PFDD_FP32) || in.imag_mode != want_imag ||
+      in.field_bytes != fb || in.carrier_bytes != cb)
+    return fail(h, PFDD_EINVAL, "checkpoint %s was written for another grid, precision or carrier", path);
+  std::vector<unsigned char> f(fb), c(cb);
+  if (pfdd_checkpoint_read(path, &in, f.data(), fb, c.empty() ? nullptr : c.data(), cb) != PFDD_OK)
+    return fail(h, PFDD_EINVAL, "checkpoint %s is truncated or corrupted (checksum)", path);
+  double sig[18];
+  for (int i = 0; i < 9; ++i) {
+    sig[i] = in.sigma[i / 3][i % 3];
+    sig[9 + i] = in.dsigma[i / 3][i % 3];
+  }
+  CUDA_TRY(h, cudaMemcpyAsync(I.xi[I.cur].p, f.data(), fb, cudaMemcpyHostToDevice, h->stream));
+  if (cb) CUDA_TRY(h, cudaMemcpyAsync(I.aux.p, c.data(), cb, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(I.sigma(), sig, sizeof sig, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  I.advanced = in.advanced != 0;
+  I.steps_total = in.steps;
+  I.tape_steps = 0;
+  return PFDD_OK;
+}
+
 template <typename T>
 pfdd_status cond_step_impl(pfdd_gpu *h, Instance &I, int n_iters, pfdd_cond_stats *stats) {
   using C = cx<T>;
@@ -1701,6 +1992,31 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(nullptr, PFDD_ECUDA, "stream creation failed");
   h->stream = h->own_stream;
+  // Mixed-size batches: instances whose descriptors differ only in the grid
+  // size, when the batch holds two sizes or more, run their groups in one
+  // launch per pass (whole planes; PFDD_MERGE=0 in the environment keeps one
+  // launch per group).
+  auto same_but_size = [&](const pfdd_instance_desc &x, const pfdd_instance_desc &y) {
+    const int S = x.n_slip;
+    return S == y.n_slip && x.core_flag == y.core_flag && x.C44 == y.C44 && x.C12 == y.C12 && x.C11 == y.C11 &&
+           x.dslip == y.dslip && x.b == y.b && x.cd_dt == y.cd_dt && x.isf == y.isf && x.usf == y.usf &&
+           x.An == y.An && !memcmp(x.four, y.four, sizeof x.four) && !memcmp(x.prim, y.prim, sizeof x.prim) &&
+           !memcmp(x.xn, y.xn, sizeof(double) * 3 * S) && !memcmp(x.xb, y.xb, sizeof(double) * 3 * S) &&
+           !memcmp(x.c, y.c, sizeof x.c) && !memcmp(x.aa, y.aa, sizeof x.aa) && !memcmp(x.bb, y.bb, sizeof x.bb) &&
+           (x.non_schmid != 0) == (y.non_schmid != 0) && x.angle_to_110 == y.angle_to_110 && x.w1 == y.w1 &&
+           x.w2 == y.w2 && x.w3 == y.w3 && !memcmp(x.usfe_fit, y.usfe_fit, sizeof x.usfe_fit) &&
+           (x.xo == nullptr) == (y.xo == nullptr) && (x.site_gsfe == nullptr) == (y.site_gsfe == nullptr);
+  };
+  std::vector<char> batch_mixed(n_instances, 0);
+  {
+    const char *env = getenv("PFDD_MERGE");
+    if (!(env && !strcmp(env, "0")))
+      for (int i = 0; i < n_instances; ++i)
+        for (int j = 0; j < n_instances && !batch_mixed[i]; ++j)
+          if (same_but_size(descs[i], descs[j]) &&
+              (descs[i].nx != descs[j].nx || descs[i].ny != descs[j].ny || descs[i].nz != descs[j].nz))
+            batch_mixed[i] = 1;
+  }
   size_t max_plane = 0, max_upd = 0, max_pen = 0;
   for (int i = 0; i < n_instances; ++i) {
     std::unique_ptr<Instance> I(new Instance);
@@ -1738,6 +2054,10 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
                                                     : PlaneSmem<cx<double>>::bytes(I->ny, I->ny, I->nzs, I->M);
     // (small grids split too, so the plane passes fill the SMs twice over)
     I->split = whole > kSplitAbove || I->F * I->nx < 2 * h->nsm;
+    if (batch_mixed[i] && whole <= kSplitAbove) {   // a batch fills the SMs by instance count
+      I->split = false;
+      I->merged = true;
+    }
     if (const char *env = getenv("PFDD_PLANE_SPLIT")) {
       if (!strcmp(env, "0")) I->split = false;
       else if (!strcmp(env, "1")) I->split = true;
@@ -1830,6 +2150,22 @@ pfdd_status pfdd_gpu_step_history(pfdd_gpu *h, int inst, double *xinorm, double 
   }
   if (count) *count = I.hist_count;
   return PFDD_OK;
+}
+
+pfdd_status pfdd_gpu_checkpoint_save(pfdd_gpu *h, int inst, const char *path) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size() || !path) return fail(h, PFDD_EINVAL, "bad arguments");
+  cudaSetDevice(h->device);
+  return h->precision == PFDD_FP64 ? checkpoint_save_impl<double>(h, *h->inst[inst], path)
+                                   : checkpoint_save_impl<float>(h, *h->inst[inst], path);
+}
+
+pfdd_status pfdd_gpu_checkpoint_load(pfdd_gpu *h, int inst, const char *path) {
+  if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
+  if (inst < 0 || inst >= (int)h->inst.size() || !path) return fail(h, PFDD_EINVAL, "bad arguments");
+  cudaSetDevice(h->device);
+  return h->precision == PFDD_FP64 ? checkpoint_load_impl<double>(h, *h->inst[inst], path)
+                                   : checkpoint_load_impl<float>(h, *h->inst[inst], path);
 }
 
 pfdd_status pfdd_gpu_set_stress(pfdd_gpu *h, int inst, const double sigma[3][3]) {
@@ -2073,19 +2409,41 @@ pfdd_status pfdd_gpu_cond_step(pfdd_gpu *h, int inst, int n_iters, pfdd_cond_sta
                                    : cond_step_impl<float>(h, I, n_iters, stats);
 }
 
-pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every, const double *xi_target,
-                             double *loss, double *dL_dparams, double *dL_dsigma) {
+static pfdd_status adjoint_check(pfdd_gpu *h, int inst) {
   if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
   if (inst < 0 || inst >= (int)h->inst.size()) return fail(h, PFDD_EINVAL, "instance %d out of range", inst);
-  if (n_steps < 1 || ckpt_every < 1 || !xi_target) return fail(h, PFDD_EINVAL, "need n_steps, ckpt_every >= 1, target");
-  Instance &I = *h->inst[inst];
-  const int f = I.d.core_flag;
+  const int f = h->inst[inst]->d.core_flag;
   if (f == PFDD_CORE_EXTENDED || f == PFDD_CORE_PYRII || f == PFDD_CORE_BCC_PERFECT)
     return fail(h, PFDD_EUNSUPPORTED, "no adjoint for core model %d", f);
   cudaSetDevice(h->device);
-  return h->precision == PFDD_FP64
-             ? adjoint_impl<double>(h, I, n_steps, ckpt_every, xi_target, loss, dL_dparams, dL_dsigma)
-             : adjoint_impl<float>(h, I, n_steps, ckpt_every, xi_target, loss, dL_dparams, dL_dsigma);
+  return PFDD_OK;
+}
+
+pfdd_status pfdd_gpu_adjoint_forward(pfdd_gpu *h, int inst, int n_steps, int ckpt_every) {
+  pfdd_status st = adjoint_check(h, inst);
+  if (st != PFDD_OK) return st;
+  if (n_steps < 1 || ckpt_every < 1) return fail(h, PFDD_EINVAL, "need n_steps, ckpt_every >= 1");
+  Instance &I = *h->inst[inst];
+  return h->precision == PFDD_FP64 ? adjoint_forward_impl<double>(h, I, n_steps, ckpt_every)
+                                   : adjoint_forward_impl<float>(h, I, n_steps, ckpt_every);
+}
+
+pfdd_status pfdd_gpu_adjoint_backward(pfdd_gpu *h, int inst, const double *dL_dxiN, double *dL_dparams,
+                                      double *dL_dsigma) {
+  pfdd_status st = adjoint_check(h, inst);
+  if (st != PFDD_OK) return st;
+  if (!dL_dxiN) return fail(h, PFDD_EINVAL, "dL_dxiN is NULL");
+  Instance &I = *h->inst[inst];
+  return h->precision == PFDD_FP64 ? adjoint_backward_impl<double>(h, I, dL_dxiN, dL_dparams, dL_dsigma)
+                                   : adjoint_backward_impl<float>(h, I, dL_dxiN, dL_dparams, dL_dsigma);
+}
+
+pfdd_status pfdd_gpu_adjoint(pfdd_gpu *h, int inst, int n_steps, int ckpt_every, const double *dL_dxiN,
+                             double *dL_dparams, double *dL_dsigma) {
+  if (h && !dL_dxiN) return fail(h, PFDD_EINVAL, "dL_dxiN is NULL");
+  pfdd_status st = pfdd_gpu_adjoint_forward(h, inst, n_steps, ckpt_every);
+  if (st != PFDD_OK) return st;
+  return pfdd_gpu_adjoint_backward(h, inst, dL_dxiN, dL_dparams, dL_dsigma);
 }
 
 pfdd_status pfdd_gpu_set_stream(pfdd_gpu *h, void *stream) {
@@ -2100,7 +2458,7 @@ pfdd_status pfdd_gpu_profile(pfdd_gpu *h, int n_steps, double *kernel_ms, int *l
   if (!h) return fail(nullptr, PFDD_EINVAL, "NULL handle");
   if (n_steps < 1 || !kernel_ms) return fail(h, PFDD_EINVAL, "need n_steps >= 1 and kernel_ms");
   cudaSetDevice(h->device);
-  if (launches_per_step) *launches_per_step = kLaunchesPerStep * (int)h->groups.size();
+  if (launches_per_step) *launches_per_step = kLaunchesPerStep * n_units(h);
   return h->precision == PFDD_FP64 ? profile_impl<double>(h, n_steps, kernel_ms)
                                    : profile_impl<float>(h, n_steps, kernel_ms);
 }

@@ -38,6 +38,7 @@
 // of the ny/2-point plan, which the host's ky slot table encodes.
 #pragma once
 #include <cooperative_groups.h>
+#include <cstddef>
 
 #include <type_traits>
 
@@ -292,13 +293,15 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], double *scratch) {
 // cluster, rank 1 handing its totals to rank 0 through distributed shared
 // memory) written to out[0..NV-1] by one thread.  scratch: NV*32 + NV doubles.
 // Every thread of both CTAs must call it.
-template <bool SPLIT, int NV>
+// ACCUM: added to out[] instead of stored (a running sum over launches; one
+// CTA or CTA pair owns each plane's out[], so no other thread writes it).
+template <bool SPLIT, int NV, bool ACCUM = false>
 __device__ __forceinline__ void plane_sum(double (&v)[NV], double *scratch, double *out) {
   block_reduce<NV>(v, scratch);
   if constexpr (!SPLIT) {
     if (threadIdx.x == 0) {
 #pragma unroll
-      for (int q = 0; q < NV; ++q) out[q] = v[q];
+      for (int q = 0; q < NV; ++q) out[q] = ACCUM ? out[q] + v[q] : v[q];
     }
   } else {
     namespace cg = cooperative_groups;
@@ -313,7 +316,7 @@ __device__ __forceinline__ void plane_sum(double (&v)[NV], double *scratch, doub
     cl.sync();
     if (rank == 0 && threadIdx.x == 0) {
 #pragma unroll
-      for (int q = 0; q < NV; ++q) out[q] = v[q] + slot[q];
+      for (int q = 0; q < NV; ++q) out[q] = ACCUM ? out[q] + (v[q] + slot[q]) : v[q] + slot[q];
     }
   }
 }
@@ -652,9 +655,11 @@ __device__ __forceinline__ size_t nyq_index(const PencilArgs &a, int f, int sx, 
 // SC > 0: the slip-system count is the constant SC (contraction loops
 // unrolled, the per-system constants read as immediates of the parameter
 // block); 0: a.S at run time.
+// gt: the contraction's constant tables (green_t<T>(a.g), or one copy shared
+// by the groups of a mixed-size launch); tile: this CTA's column tile.
 template <typename T, int NT, int SC>
-__device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const PencilArgs &a, void *aux_ptr,
-                                             double *ppart) {
+__device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const PencilArgs &a, const GreenT<T> &gt,
+                                             void *aux_ptr, double *ppart, int tile) {
   using C = cx<T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nx = a.nx, F = a.F, cc = a.ccols, S = SC > 0 ? SC : a.S, fst = a.fstride;
@@ -670,7 +675,7 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
   // read once at CTA start: those few points would otherwise make one warp
   // wait on S dependent global loads while the CTA waits for it
   C *nqs = reinterpret_cast<C *>(csz + ((cc + 3) & ~3));
-  const size_t col0 = (size_t)blockIdx.x * cc;
+  const size_t col0 = (size_t)tile * cc;
   const size_t ncols = a.ncols;
   const int cpr = (int)(cc * sizeof(C) / 16);    // 16-byte chunks per (field, x) row
   const int nchunks = F * nx * cpr;
@@ -688,7 +693,7 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
   }
   load_table(twx, a.tw_x, nx);
   {
-    const GreenT<T> &g = green_t<T>(a.g);
+    const GreenT<T> &g = gt;
     for (int i = threadIdx.x; i < nx + cc; i += blockDim.x) {
       if (i < nx) {
         const int ix = a.kx_of[i];
@@ -723,7 +728,7 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
   if (a.mode != PASS_SYNTH) fft_forward<MaxRadix<NT>::value, GeomPencil>(buf, twx, a.px, gx);
 
   double dsq = 0.0;
-  const GreenT<T> &g = green_t<T>(a.g);
+  const GreenT<T> &g = gt;
   const size_t fs = (size_t)fst;
   for (int w = threadIdx.x; w < nx * cc; w += blockDim.x) {
     const int sx = a.fd_cc.div(w), c = w - sx * cc;
@@ -860,7 +865,7 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
       if (aa < S) pk[aa * fs] = green_out<T>(g, aa, sr, Tp, zp);
     }
   }
-  if (ppart) block_sum2(dsq, 0.0, red, ppart + 2 * blockIdx.x);
+  if (ppart) block_sum2(dsq, 0.0, red, ppart + 2 * tile);
   __syncthreads();
 
   fft_inverse<MaxRadix<NT>::value, GeomPencil>(buf, twx, a.px, gx);
@@ -879,7 +884,7 @@ template <typename T, int NT, int SC = 0>
 __global__ void __launch_bounds__(NT, (PencilMinBlocks<T>::value)) k_xpencil(cx<T> *__restrict__ spec, PencilArgs a,
                                                 const int *__restrict__ stop) {
   if (stop && *stop) return;
-  xpencil_body<T, NT, SC>(spec, a, a.aux, a.partials);
+  xpencil_body<T, NT, SC>(spec, a, green_t<T>(a.g), a.aux, a.partials, blockIdx.x);
 }
 
 // grid = (tiles, instances of the group)
@@ -887,16 +892,22 @@ template <typename T, int NT, int SC = 0>
 __global__ void __launch_bounds__(NT, (PencilMinBlocks<T>::value)) k_xpencil_tab(const InstPtrs *__restrict__ tab, PencilArgs a) {
   const InstPtrs &ip = tab[blockIdx.y];
   if (ip.flags[0]) return;
-  xpencil_body<T, NT, SC>(static_cast<cx<T> *>(ip.spec), a, ip.aux, ip.ppart);
+  xpencil_body<T, NT, SC>(static_cast<cx<T> *>(ip.spec), a, green_t<T>(a.g), ip.aux, ip.ppart, blockIdx.x);
 }
 
 // Slip-system counts with an unrolled contraction (basal / {111} triples 3,
 // BCC pairs 2); others, FCC's 12 among them (fully unrolled it spills),
 // run the generic loop.
+#ifndef PFDD_UNROLL_S12
+#define PFDD_UNROLL_S12 0
+#endif
 template <typename Fn> __host__ inline void with_pencil_sc(int S, Fn f) {
   switch (S) {
     case 3: f(std::integral_constant<int, 3>()); break;
     case 2: f(std::integral_constant<int, 2>()); break;
+#if PFDD_UNROLL_S12
+    case 12: f(std::integral_constant<int, 12>()); break;
+#endif
     default: f(std::integral_constant<int, 0>()); break;
   }
 }
@@ -1315,7 +1326,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
             *reinterpret_cast<V *>(nv);
     }
     double v[4] = {g0, g1, gl, 0.0};
-    plane_sum<SPLIT>(v, sm.red, u.gpart + 4 * plane);
+    plane_sum<SPLIT, 4, true>(v, sm.red, u.gpart + 4 * plane);   // summed over the backward steps
     if constexpr (FUSE == 2) {
       if (fwd) {   // the next backward step's spectrum of the new lambda
         __syncthreads();
@@ -1452,6 +1463,104 @@ __global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, SPLIT>::value)) k_inv_u
                                 ip.tau, ip.mask, ip.site, ip.flags + 3);
 }
 
+// ------------------------------------------------------------ mixed-size batches
+// Groups of one merge class (the same slip systems, material, core model and
+// carrier, any grid size) advance in one launch per pass: blockIdx.x maps to
+// (group, instance, plane or column tile) through the prefix table
+// MultiLaunch::starts (CTAs before each group), and each CTA copies its group's
+// geometry (plans, sizes, tables, divisors) into shared memory at its start.
+// The planes run whole (no 2-CTA clusters): a batch fills the SMs by count.
+constexpr int kMaxMerged = 16;
+struct MultiLaunch {
+  int ngroups;
+  int starts[kMaxMerged + 1];
+};
+struct MultiPlaneGroup {
+  PlaneArgs a;
+  UpdateArgs u;
+  const InstPtrs *tab;
+  int per_member;       // CTAs per instance: F * nx planes
+};
+struct MultiPencilGroup {
+  PencilArgs a;         // only the geometry before `g` is read (one Green table per launch)
+  const InstPtrs *tab;
+  int per_member;       // column tiles per instance
+};
+struct MultiFinalGroup {
+  const InstPtrs *tab;
+  int nparts, nparts2;
+  double scale2;
+};
+
+__device__ __forceinline__ int group_of_block(const MultiLaunch &m) {
+  int g = 0;
+  while (g + 1 < m.ngroups && (int)blockIdx.x >= m.starts[g + 1]) ++g;
+  return g;
+}
+// bytes (a multiple of 4) from global to shared memory by the CTA's threads
+__device__ __forceinline__ void copy_words(void *dst, const void *src, int bytes) {
+  const int *sp = static_cast<const int *>(src);
+  int *dp = static_cast<int *>(dst);
+  for (int i = threadIdx.x; i < bytes / 4; i += blockDim.x) dp[i] = sp[i];
+}
+
+// The fused plane pass of every group of a merge class (P3 of this step and,
+// when fwd, P1 of the next).  Static shared memory holds the group's
+// arguments; the dynamic part is the plane buffer of the largest group.
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, true>::value))
+    k_step_planes_multi(const MultiPlaneGroup *__restrict__ groups, MultiLaunch m, int fwd) {
+  __shared__ __align__(16) unsigned char graw[sizeof(MultiPlaneGroup)];
+  const MultiPlaneGroup &G = *reinterpret_cast<const MultiPlaneGroup *>(graw);
+  const int gi = group_of_block(m);
+  copy_words(graw, groups + gi, (int)sizeof(MultiPlaneGroup));
+  __syncthreads();
+  const int local = (int)blockIdx.x - m.starts[gi];
+  const int member = local / G.per_member, plane = local - member * G.per_member;
+  const InstPtrs &ip = G.tab[member];
+  if (ip.flags[0]) return;
+  const int cur = ip.flags[4];
+  inv_update_body<T, NT, false, 1>(static_cast<const cx<T> *>(ip.spec), static_cast<const T *>(ip.xi[cur]),
+                                   static_cast<T *>(ip.xi[cur ^ 1]), G.a, G.u, ip.partials, (size_t)plane,
+                                   ip.tau, ip.mask, ip.site, ip.flags + 3, fwd != 0);
+}
+
+// The forward plane pass that opens a run, for every group of a merge class.
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, (PlaneMinBlocks<T, true>::value))
+    k_fwd_planes_multi(const MultiPlaneGroup *__restrict__ groups, MultiLaunch m) {
+  __shared__ __align__(16) unsigned char graw[sizeof(MultiPlaneGroup)];
+  const MultiPlaneGroup &G = *reinterpret_cast<const MultiPlaneGroup *>(graw);
+  const int gi = group_of_block(m);
+  copy_words(graw, groups + gi, (int)sizeof(MultiPlaneGroup));
+  __syncthreads();
+  const int local = (int)blockIdx.x - m.starts[gi];
+  const int member = local / G.per_member, plane = local - member * G.per_member;
+  const InstPtrs &ip = G.tab[member];
+  if (ip.flags[0]) return;
+  fwd_planes_body<T, NT, false>(static_cast<const T *>(ip.xi[ip.flags[4]]), static_cast<cx<T> *>(ip.spec), G.a,
+                                ip.flags + 3, (size_t)plane);
+}
+
+// The x-pencil pass of every group of a merge class; gt: the contraction's
+// constants, equal across the class.
+template <typename T, int NT, int SC>
+__global__ void __launch_bounds__(NT, (PencilMinBlocks<T>::value))
+    k_xpencil_multi(const MultiPencilGroup *__restrict__ groups, MultiLaunch m, const __grid_constant__ GreenT<T> gt) {
+  constexpr int kGeom = (int)offsetof(PencilArgs, g);
+  __shared__ __align__(16) unsigned char araw[(kGeom + 15) & ~15];
+  const PencilArgs &A = *reinterpret_cast<const PencilArgs *>(araw);
+  const int gi = group_of_block(m);
+  copy_words(araw, &groups[gi].a, kGeom & ~3);
+  __syncthreads();
+  const int local = (int)blockIdx.x - m.starts[gi];
+  const int per = groups[gi].per_member;
+  const int member = local / per, tile = local - member * per;
+  const InstPtrs &ip = groups[gi].tab[member];
+  if (ip.flags[0]) return;
+  xpencil_body<T, NT, SC>(static_cast<cx<T> *>(ip.spec), A, gt, ip.aux, ip.ppart, tile);
+}
+
 // ------------------------------------------------------------ reduction
 // Neumaier-compensated FP64 sums: each thread folds a strided share of the
 // partials into (sum, compensation) pairs; the pairs are merged by a fixed
@@ -1539,6 +1648,38 @@ static __global__ void k_finalize_tab(const InstPtrs *__restrict__ tab, int npar
   }
   if (partials2)
     for (int i = threadIdx.x; i < nparts2; i += blockDim.x) neu_add(s0, c0, partials2[2 * i] * scale2);
+  block_neumaier2(s0, c0, s1, c1, sh);
+  if (threadIdx.x == 0) {
+    const double xinorm = sqrt(s0 + c0), xiave = s1 + c1;
+    const int k = flags[2];
+    if (k < ip.stats_cap) {
+      ip.stats[2 * k] = xinorm;
+      ip.stats[2 * k + 1] = xiave;
+    }
+    flags[2] = k + 1;
+    flags[4] ^= 1;
+    if (!isfinite(xinorm) || !isfinite(xiave)) flags[1] = 1;
+    if (tol > 0.0 && xinorm < tol) flags[0] = 1;
+  }
+}
+
+// k_finalize_tab for every instance of a merge class: blockIdx.x runs over
+// the instances of the groups in order (MultiLaunch::starts counts instances).
+static __global__ void k_finalize_multi(const MultiFinalGroup *__restrict__ groups, MultiLaunch m, double tol) {
+  const int gi = group_of_block(m);
+  const MultiFinalGroup &G = groups[gi];
+  const InstPtrs &ip = G.tab[blockIdx.x - m.starts[gi]];
+  int *flags = ip.flags;
+  if (flags[0]) return;
+  __shared__ double sh[128];
+  const double *partials = ip.partials, *partials2 = ip.ppart;
+  double s0 = 0, c0 = 0, s1 = 0, c1 = 0;
+  for (int i = threadIdx.x; i < G.nparts; i += blockDim.x) {
+    neu_add(s0, c0, partials[2 * i]);
+    neu_add(s1, c1, partials[2 * i + 1]);
+  }
+  if (partials2)
+    for (int i = threadIdx.x; i < G.nparts2; i += blockDim.x) neu_add(s0, c0, partials2[2 * i] * G.scale2);
   block_neumaier2(s0, c0, s1, c1, sh);
   if (threadIdx.x == 0) {
     const double xinorm = sqrt(s0 + c0), xiave = s1 + c1;
@@ -1680,8 +1821,9 @@ static __global__ void k_stress_state_tab(const InstPtrs *__restrict__ tab, Stre
 
 // ------------------------------------------------------------ adjoint reductions
 // acc[0..1] += sums of the per-plane parameter partials over the real-field
-// planes, acc[2 + a] += sum of lambda over system a's planes; comp[] holds
-// the Neumaier compensation terms across calls.
+// planes, acc[2 + a] += sum of lambda over system a's planes (each partial
+// already summed over the backward steps by the plane passes); comp[] holds
+// the Neumaier compensation terms.
 static __global__ void k_grad_accum(const double *__restrict__ gpart, int S, int nx, double *acc, double *comp) {
   const int t = threadIdx.x;
   if (t >= 2 + S) return;
@@ -1696,21 +1838,6 @@ static __global__ void k_grad_accum(const double *__restrict__ gpart, int S, int
   const double v = s + c, u = acc[t] + v;
   comp[t] += (fabs(acc[t]) >= fabs(v)) ? (acc[t] - u) + v : (v - u) + acc[t];
   acc[t] = u;
-}
-
-// lam = 2 (Re xi - target) on the S real fields; FP64 partial sums of the
-// squared residual per block.
-template <typename T>
-__global__ void k_loss_seed(const T *__restrict__ xr, const T *__restrict__ target, T *__restrict__ lam, size_t n,
-                            double *__restrict__ partial) {
-  __shared__ double red[64];
-  double acc = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const T d = xr[i] - target[i];
-    lam[i] = (T)2 * d;
-    acc += (double)d * (double)d;
-  }
-  block_sum2(acc, 0.0, red, partial + 2 * blockIdx.x);
 }
 
 // ------------------------------------------------------------ strain / stress diagnostics
@@ -1753,7 +1880,7 @@ __device__ __forceinline__ void strain_of(const C (&sig)[6], T kx, T ky, T kz, T
 // symmetric strain components (xx yy zz xy xz yz) after the inverse x FFT.
 // grid.x = ncols / ccols; smem = (max(F, 6) * fstride + nx) * sizeof(C).
 template <typename T, int NT>
-__global__ void __launch_bounds__(NT, 1) k_strain_pencil(const cx<T> *__restrict__ spec, cx<T> *__restrict__ out6,
+__global__ void __launch_bounds__(NT, 2) k_strain_pencil(const cx<T> *__restrict__ spec, cx<T> *__restrict__ out6,
                                                          PencilArgs a) {
   using C = cx<T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];

@@ -30,9 +30,11 @@ EXPORTS = [
     "pfdd_gpu_create", "pfdd_gpu_set_state", "pfdd_gpu_set_state_interleaved", "pfdd_gpu_get_state",
     "pfdd_gpu_get_state_interleaved", "pfdd_gpu_advance", "pfdd_gpu_step_history", "pfdd_gpu_energy",
     "pfdd_gpu_tau", "pfdd_gpu_set_stress", "pfdd_gpu_info", "pfdd_gpu_last_error", "pfdd_gpu_destroy", "pfdd_gpu_version",
-    "pfdd_gpu_set_stream", "pfdd_gpu_profile", "pfdd_gpu_adjoint", "pfdd_gpu_strain_stress",
+    "pfdd_gpu_set_stream", "pfdd_gpu_profile", "pfdd_gpu_adjoint", "pfdd_gpu_adjoint_forward",
+    "pfdd_gpu_adjoint_backward", "pfdd_gpu_strain_stress",
     "pfdd_gpu_core_profile", "pfdd_gpu_autotune", "pfdd_gpu_snapshot_begin", "pfdd_gpu_snapshot_wait", "pfdd_cond_layers", "pfdd_gpu_cond_enable", "pfdd_gpu_cond_set_state",
-    "pfdd_gpu_cond_get_state", "pfdd_gpu_cond_step",
+    "pfdd_gpu_cond_get_state", "pfdd_gpu_cond_step", "pfdd_checkpoint_write", "pfdd_checkpoint_read",
+    "pfdd_gpu_checkpoint_save", "pfdd_gpu_checkpoint_load", "pfdd_gl_step_noalloc",
 ]
 KERNELS = ["fwd_planes", "xpencil", "step_planes", "finalize"]
 
@@ -71,6 +73,13 @@ class CondDesc(ctypes.Structure):
 
 class CondStats(ctypes.Structure):
     _fields_ = [("condxinorm", ctypes.c_double), ("condxiave", ctypes.c_double), ("conductivity", ctypes.c_double)]
+
+
+class CheckpointInfo(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("n_slip", ctypes.c_int),
+                ("fields", ctypes.c_int), ("precision", ctypes.c_int), ("imag_mode", ctypes.c_int),
+                ("advanced", ctypes.c_int), ("field_bytes", ctypes.c_size_t), ("carrier_bytes", ctypes.c_size_t),
+                ("sigma", D33), ("dsigma", D33), ("steps", ctypes.c_ulonglong)]
 
 
 class Options(ctypes.Structure):
@@ -122,8 +131,16 @@ def load(path: str = LIB_PATH):
     lib.pfdd_gpu_cond_get_state.argtypes = [vp, ctypes.c_int, DP, DP]
     lib.pfdd_gpu_cond_step.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(CondStats)]
     lib.pfdd_gpu_tau.argtypes = [vp, ctypes.c_int, DP]
+    lib.pfdd_checkpoint_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(CheckpointInfo), vp, vp]
+    lib.pfdd_checkpoint_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(CheckpointInfo), vp, ctypes.c_size_t, vp,
+                                         ctypes.c_size_t]
+    lib.pfdd_gpu_checkpoint_save.argtypes = [vp, ctypes.c_int, ctypes.c_char_p]
+    lib.pfdd_gpu_checkpoint_load.argtypes = [vp, ctypes.c_int, ctypes.c_char_p]
+    lib.pfdd_gl_step_noalloc.argtypes = [ctypes.POINTER(InstanceDesc), vp, vp, DP, vp]
     lib.pfdd_gpu_set_stress.argtypes = [vp, ctypes.c_int, DP]
-    lib.pfdd_gpu_adjoint.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, DP, DP, DP, DP]
+    lib.pfdd_gpu_adjoint.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, DP, DP, DP]
+    lib.pfdd_gpu_adjoint_forward.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.pfdd_gpu_adjoint_backward.argtypes = [vp, ctypes.c_int, DP, DP, DP]
     lib.pfdd_gpu_set_stream.argtypes = [vp, vp]
     lib.pfdd_gpu_profile.argtypes = [vp, ctypes.c_int, DP, ctypes.POINTER(ctypes.c_int)]
     lib.pfdd_gpu_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_size_t)]
@@ -242,14 +259,15 @@ class Stepper:
         im = None if im is None else np.ascontiguousarray(im, dtype=np.float64).reshape(-1)
         self._check(self._lib.pfdd_gpu_set_state(self.h, inst, _dp(re), _dp(im)))
 
-    def get_state(self, inst):
+    def get_state(self, inst, imag=True):
+        """(Re xi, Im xi) as [S, nx, ny, nz] arrays; imag=False: Im is None."""
         d = self.descs[inst]
         n = d.n_slip * d.nx * d.ny * d.nz
         re = np.empty(n)
-        im = np.empty(n)
+        im = np.empty(n) if imag else None
         self._check(self._lib.pfdd_gpu_get_state(self.h, inst, _dp(re), _dp(im)))
         shape = (d.n_slip, d.nx, d.ny, d.nz)
-        return re.reshape(shape), im.reshape(shape)
+        return re.reshape(shape), (im.reshape(shape) if imag else None)
 
     def advance(self, n_steps, stress_states=1, tol=0.0):
         stats = (StepStats * self.n)()
@@ -269,6 +287,12 @@ class Stepper:
         """Replace instance inst's current applied stress (3x3, units of mu)."""
         s = np.ascontiguousarray(sigma, dtype=np.float64).reshape(9)
         self._check(self._lib.pfdd_gpu_set_stress(self.h, inst, _dp(s)))
+
+    def checkpoint_save(self, inst, path):
+        self._check(self._lib.pfdd_gpu_checkpoint_save(self.h, inst, os.fsencode(path)))
+
+    def checkpoint_load(self, inst, path):
+        self._check(self._lib.pfdd_gpu_checkpoint_load(self.h, inst, os.fsencode(path)))
 
     def tau(self, inst):
         t = np.empty(self.descs[inst].n_slip)
@@ -349,15 +373,26 @@ class Stepper:
         return (e.reshape(shape) if fields else None, s.reshape(shape) if fields else None,
                 ae.reshape(3, 3), asg.reshape(3, 3))
 
-    def adjoint(self, inst, n_steps, ckpt_every, target):
-        """(loss, dJ/d(p0, p1), dJ/dsigma[6]) of J = sum (Re xi_N - target)^2."""
-        t = np.ascontiguousarray(target, dtype=np.float64).reshape(-1)
-        loss = np.zeros(1)
+    def adjoint_forward(self, inst, n_steps, ckpt_every):
+        """Forward run of n_steps kept as the adjoint's tape (checkpoints every
+        ckpt_every steps); the instance ends at xi_N as after advance."""
+        self._check(self._lib.pfdd_gpu_adjoint_forward(self.h, inst, n_steps, ckpt_every))
+
+    def adjoint_backward(self, inst, dL_dxiN):
+        """(dL/d(p0, p1), dL/dsigma[6]) for the seed dL/dRe xi_N [S, nx, ny, nz]."""
+        g = np.ascontiguousarray(dL_dxiN, dtype=np.float64).reshape(-1)
         dp = np.zeros(2)
         ds = np.zeros(6)
-        self._check(self._lib.pfdd_gpu_adjoint(self.h, inst, n_steps, ckpt_every, _dp(t), _dp(loss), _dp(dp),
-                                               _dp(ds)))
-        return float(loss[0]), dp, ds
+        self._check(self._lib.pfdd_gpu_adjoint_backward(self.h, inst, _dp(g), _dp(dp), _dp(ds)))
+        return dp, ds
+
+    def adjoint(self, inst, n_steps, ckpt_every, dL_dxiN):
+        """Forward tape and backward pass in one call, for a seed known beforehand."""
+        g = np.ascontiguousarray(dL_dxiN, dtype=np.float64).reshape(-1)
+        dp = np.zeros(2)
+        ds = np.zeros(6)
+        self._check(self._lib.pfdd_gpu_adjoint(self.h, inst, n_steps, ckpt_every, _dp(g), _dp(dp), _dp(ds)))
+        return dp, ds
 
     def set_stream(self, stream_handle):
         """Run on a caller stream (an int cudaStream_t, e.g. torch.cuda.current_stream().cuda_stream)."""

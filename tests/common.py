@@ -73,3 +73,14 @@ def oracle_run_golden(w, fx):
         aves += list(a)
         sig = sig + np.asarray(fx["dsigma"])
     return xi, np.array(norms), np.array(aves)
+
+
+def adjoint_l2(st, inst, n_steps, ckpt_every, target):
+    """J = sum (Re xi_N - target)^2 and its gradients through the general-seed
+    adjoint (test-harness loss): the forward tape, then the seed
+    dJ/dRe xi_N = 2 (Re xi_N - target).  Returns (J, dJ/dparams, dJ/dsigma)."""
+    st.adjoint_forward(inst, n_steps, ckpt_every)
+    xr, _ = st.get_state(inst, imag=False)
+    r = xr - np.asarray(target)
+    dp, ds = st.adjoint_backward(inst, 2.0 * r)
+    return float(np.sum(r * r)), dp, ds

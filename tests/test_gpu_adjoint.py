@@ -1,6 +1,8 @@
-"""Adjoint of the GL step through the C ABI (pfdd_gpu_adjoint).
+"""Adjoint of the GL step through the C ABI (pfdd_gpu_adjoint_forward /
+_backward, pfdd_gpu_adjoint), seeded with dL/dRe xi_N.
 
-J = sum (Re xi_N - target)^2 after N steps; gradients with respect to
+The test-harness loss J = sum (Re xi_N - target)^2 after N steps
+(common.adjoint_l2) and a linear loss; gradients with respect to
 (isf, usf) and sigma are checked against FP64 central finite differences of
 J computed with the numpy oracle (an independent restatement of the
 reference step).  Tolerance: 2e-6 relative (FP64), 2e-3 (FP32 vs FP64).
@@ -9,7 +11,7 @@ import numpy as np
 import pytest
 
 import pfdd_oracle as O
-from common import oracle_instance
+from common import adjoint_l2, oracle_instance
 from pfdd_b200 import capi, configs
 
 pytestmark = pytest.mark.gpu
@@ -52,7 +54,7 @@ def _loss_oracle(w, target, isf=None, usf=None, dsig=0.0):
 def _gpu_adjoint(w, target, prec=capi.FP64):
     with capi.Stepper.from_workloads([w], precision=prec) as st:
         st.set_state(0, w.xi0)
-        loss, dp, ds = st.adjoint(0, N_STEPS, CKPT, target)
+        loss, dp, ds = adjoint_l2(st, 0, N_STEPS, CKPT, target)
         re, _ = st.get_state(0)
     return loss, dp, ds, re
 
@@ -126,9 +128,54 @@ def test_store_all_equals_checkpointed():
     a = _gpu_adjoint(w, target)
     with capi.Stepper.from_workloads([w], precision=capi.FP64) as st:
         st.set_state(0, w.xi0)
-        loss, dp, ds = st.adjoint(0, N_STEPS, N_STEPS, target)
+        loss, dp, ds = adjoint_l2(st, 0, N_STEPS, N_STEPS, target)
         re, _ = st.get_state(0)
     assert abs(loss - a[0]) <= 1e-12 * abs(a[0])
     np.testing.assert_allclose(dp, a[1], rtol=1e-12, atol=0)
     np.testing.assert_allclose(ds, a[2], rtol=1e-12, atol=1e-12 * np.abs(a[2]).max())
     assert np.abs(re - a[3]).max() == 0.0
+
+
+def test_general_seed_linear_loss_and_reused_tape():
+    """A seed that is not an L2 residual: L = sum W * Re xi_N with a fixed
+    random weight W (dL/dRe xi_N = W), checked against FP64 central finite
+    differences of the oracle's L; a second backward pass on the same tape
+    with another seed equals a fresh one-call adjoint with that seed."""
+    w = _workload()
+    W = np.random.default_rng(4).standard_normal((w.S, w.nx, w.ny, w.nz))
+
+    def L(isf=None, usf=None, dsig=0.0):
+        m = configs.Material(**{k: getattr(w.material, k) for k in ("preset", "mu", "young", "b", "isf", "usf",
+                                                                     "An", "dslip")})
+        m.isf = w.material.isf if isf is None else isf
+        m.usf = w.material.usf if usf is None else usf
+        sig = w.sigma.copy()
+        sig[0, 2] += dsig
+        sig[2, 0] += dsig
+        w2 = configs.Workload(w.name, w.nx, w.ny, w.nz, w.app, w.xn, w.xb, w.four, w.prim, m, w.core_flag, sig,
+                              w.cd_dt, w.xi0)
+        xi, _, _ = O.run(oracle_instance(w2), w.xi0, N_STEPS)
+        return float(np.sum(W * xi.real))
+
+    W2 = np.random.default_rng(5).standard_normal(W.shape)
+    with capi.Stepper.from_workloads([w], precision=capi.FP64) as st:
+        st.set_state(0, w.xi0)
+        st.adjoint_forward(0, N_STEPS, CKPT)
+        dp, ds = st.adjoint_backward(0, W)
+        dp2, ds2 = st.adjoint_backward(0, W2)
+        st.set_state(0, w.xi0)
+        dp2b, ds2b = st.adjoint(0, N_STEPS, CKPT, W2)
+        # the tape is gone once the state changes
+        st.set_state(0, w.xi0)
+        with pytest.raises(capi.PfddError) as e:
+            st.adjoint_backward(0, W)
+        assert e.value.code == -7
+    h_isf, h_usf, h_sig = 1e-6 * w.material.isf, 1e-6 * w.material.usf, 1e-9
+    fd_isf = (L(isf=w.material.isf + h_isf) - L(isf=w.material.isf - h_isf)) / (2 * h_isf)
+    fd_usf = (L(usf=w.material.usf + h_usf) - L(usf=w.material.usf - h_usf)) / (2 * h_usf)
+    fd_sxz = (L(dsig=h_sig) - L(dsig=-h_sig)) / (2 * h_sig)
+    assert abs(dp[0] - fd_isf) <= 2e-6 * abs(fd_isf), (dp[0], fd_isf)
+    assert abs(dp[1] - fd_usf) <= 2e-6 * abs(fd_usf), (dp[1], fd_usf)
+    assert abs(ds[4] - fd_sxz) <= 2e-6 * abs(fd_sxz), (ds[4], fd_sxz)
+    np.testing.assert_array_equal(dp2, dp2b)
+    np.testing.assert_array_equal(ds2, ds2b)

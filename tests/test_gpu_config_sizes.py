@@ -15,9 +15,12 @@ passes and the FP32 compile-time plans are all checked where they run:
                                   the 256^2 x 128 grid)
   Frank-Read 512 x 512 x 64 x 2   FP64 <= 1e-10, FP32 rel. L2 <= 2e-5 (2 steps),
   (60-degree grid, mask)          full complex carrier
-  FCC 256 x 256 x 128 x 12        FP32 vs the FP64 GPU path (equal to the oracle
+  loop 64^3 x 3                   FP32 vs the FP64 GPU path (equal to the oracle
                                   per step above) after 2000 steps: rel. L2 of
                                   Re xi <= 1e-5
+  FCC 256 x 256 x 128 x 12        FP32 vs FP64 <= 1e-5 after 10 steps; after 2000
+                                  steps no further than an FP64 run perturbed by
+                                  1e-7 (this trajectory amplifies perturbations)
 
 The reference's counterparts are the update and transforms these grids run
 through: update_order_parameter and forward/backward_mode1
@@ -129,14 +132,41 @@ def test_frank_read_512x512x64_fp64_and_fp32():
     assert _rel_l2(got32[2], ref[2]) <= TOL32
 
 
-def test_fcc256_fp32_against_fp64_after_2000_steps():
-    w = configs.fcc_workload()
+def _fp_runs(w, runs, checkpoints):
+    """{name: {step: Re xi}} for runs = {name: (precision, initial state)}."""
     out = {}
-    for prec in (capi.FP64, capi.FP32):
+    for name, (prec, x0) in runs.items():
+        out[name] = {}
         with capi.Stepper.from_workloads([w], precision=prec) as st:
-            st.set_state(0, w.xi0)
-            st.advance(2000)
-            out[prec] = st.get_state(0)[0]
-    a, b = out[capi.FP32], out[capi.FP64]
-    rel = np.linalg.norm(a - b) / np.linalg.norm(b)
-    assert rel <= 1e-5, rel
+            st.set_state(0, x0)
+            done = 0
+            for c in checkpoints:
+                st.advance(c - done)
+                done = c
+                out[name][c] = st.get_state(0, imag=False)[0]
+    return out
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_loop64_fp32_against_fp64_after_2000_steps():
+    w = configs.loop_workload()
+    r = _fp_runs(w, {"fp64": (capi.FP64, w.xi0), "fp32": (capi.FP32, w.xi0)}, (2000,))
+    assert _rel(r["fp32"][2000], r["fp64"][2000]) <= 1e-5
+
+
+def test_fcc256_fp32_error_bounded_by_the_dynamics():
+    """On the 256x256x128, 12-system FCC deck the trajectory itself amplifies
+    any perturbation: an FP64 run started 1e-7 (normal, seeded) away ends 0.16
+    (relative L2) away after 2000 steps, as far as the FP32 run does.  So the
+    FP32 path is checked where the dynamics have not amplified its rounding,
+    <= 1e-5 relative L2 after 10 steps, and after 2000 steps against that
+    FP64 control: no further from the FP64 run than the perturbed FP64 run."""
+    w = configs.fcc_workload()
+    pert = 1e-7 * np.random.default_rng(1).standard_normal(w.xi0.shape)
+    r = _fp_runs(w, {"fp64": (capi.FP64, w.xi0), "fp32": (capi.FP32, w.xi0),
+                     "fp64_pert": (capi.FP64, w.xi0 + pert)}, (10, 2000))
+    assert _rel(r["fp32"][10], r["fp64"][10]) <= 1e-5
+    assert _rel(r["fp32"][2000], r["fp64"][2000]) <= _rel(r["fp64_pert"][2000], r["fp64"][2000])

@@ -23,7 +23,7 @@ import numpy as np
 import pytest
 
 import pfdd_oracle as O
-from common import oracle_instance, small_loop
+from common import adjoint_l2, oracle_instance, small_loop
 from pfdd_b200 import capi
 
 pytestmark = pytest.mark.gpu
@@ -103,7 +103,7 @@ def test_stalled_wait_in_strain_stress_and_adjoint():
         st.advance(2)
         with _env(PFDD_STALL_BULK_WAITS=1):
             assert _code(lambda: st.strain_stress(0, fields=False)) == -8
-            assert _code(lambda: st.adjoint(0, 3, 2, np.zeros_like(w.xi0))) == -8
+            assert _code(lambda: adjoint_l2(st, 0, 3, 2, np.zeros_like(w.xi0))) == -8
         _check_steps(st, w)
         _, _, ae, asg = st.strain_stress(0, fields=False)
         assert np.isfinite(ae).all() and np.isfinite(asg).all()
@@ -117,7 +117,7 @@ def test_failed_allocation_reports_enomem():
         st.set_state(0, w.xi0)
         # the adjoint's checkpoint buffers are allocated on its first call
         with _env(PFDD_FAIL_ALLOC_ABOVE=1 << 16):
-            assert _code(lambda: st.adjoint(0, 4, 2, np.zeros_like(w.xi0))) == -2
+            assert _code(lambda: adjoint_l2(st, 0, 4, 2, np.zeros_like(w.xi0))) == -2
         _check_steps(st, w)
-        loss, dp, ds = st.adjoint(0, 4, 2, np.zeros_like(w.xi0))
+        loss, dp, ds = adjoint_l2(st, 0, 4, 2, np.zeros_like(w.xi0))
         assert np.isfinite(loss) and np.isfinite(dp).all() and np.isfinite(ds).all()

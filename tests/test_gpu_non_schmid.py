@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import pfdd_oracle as O
-from common import oracle_instance, oracle_run_golden
+from common import adjoint_l2, oracle_instance, oracle_run_golden
 from pfdd_b200 import capi, configs
 
 pytestmark = pytest.mark.gpu
@@ -88,7 +88,7 @@ def test_adjoint_stress_gradient_non_schmid_usfe():
     target = target.real
     with capi.Stepper.from_workloads([w], precision=capi.FP64) as st:
         st.set_state(0, w.xi0)
-        loss, dp, ds = st.adjoint(0, N_STEPS, CKPT, target)
+        loss, dp, ds = adjoint_l2(st, 0, N_STEPS, CKPT, target)
     assert abs(loss - _loss_oracle(w, target, 0, 0.0)) <= 1e-10 * max(1.0, loss)
     h = 1e-9
     for c in (4, 5):   # sigma_xz, sigma_yz (sigma_yz moves the amplitude)
