@@ -23,8 +23,10 @@ Before the warm-up the x-pencil tile width of every batched group is chosen
 by timing (pfdd_gpu_autotune, outside the timed region, like a planner);
 --no-autotune keeps the set-up's rule.
 
-Multi-GPU (torchrun): every rank advances its own replica (no data-path
-collective; scaling "weak"); the time is the max over ranks.
+Multi-GPU (torchrun): a multi-instance workload (alloy64) is split over the
+ranks, each instance on one GPU (scaling "strong"); a one-grid workload runs
+one replica per rank (scaling "weak").  No data-path collective; the time is
+the max over ranks, the value every rank's units over it.
 --impl reference times the reference's own CPU code on this host's cores on
 the same workload (see reference_arm) and prints the same line.
 """
@@ -190,8 +192,8 @@ def cpu_baseline_reference(K=10, procs=1, nx=64, ny=64, nz=32):
     rate = sum(r["site_slip_updates_per_s"] for r in res)
     fft = statistics.mean(r["fft_gflops"] for r in res)
     sample = ("reference src/*.cpp built -O3 with a single-rank MPI stub and an FP64 FFTW-2 API stand-in "
-              "(%.2f GFLOP/s FFT); FCC 12 systems on %dx%dx%d, %d GL steps x %d process(es), loop time only "
-              "(the 256x256x128 grid needs ~20 GB and ~10 min of B(k) set-up in the reference)"
+              "(%.2f GFLOP/s FFT); a bounded sample of the FCC 12-system deck on %dx%dx%d, %d GL steps x %d "
+              "process(es), loop time only (the full 256x256x128 grid is timed by bench.py --impl reference)"
               % (fft, nx, ny, nz, K, procs))
     return rate, sample
 
@@ -324,6 +326,28 @@ def aggregate_rate(units_per_rank, world, ms):
     return units_per_rank * world / (ms / 1e3)
 
 
+def shard_instances(ws, rank, world):
+    """The instances rank `rank` advances: a multi-instance workload is split
+    round robin over the ranks (each instance on one GPU, no data-path
+    collective; the total work is fixed, so scaling is strong); a one-grid
+    workload runs as one replica per rank (weak scaling)."""
+    if world > 1 and len(ws) > 1:
+        if len(ws) < world:
+            raise SystemExit("%d instances cannot be split over %d ranks" % (len(ws), world))
+        return ws[rank::world], "strong"
+    return ws, "weak"
+
+
+def sum_over_ranks(x, dist, device="cuda"):
+    """Sum of each rank's x (every rank calls it at the same point)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def timed_events(stream, fn):
     import torch
     torch.cuda.synchronize()
@@ -336,35 +360,64 @@ def timed_events(stream, fn):
     return e0.elapsed_time(e1), out
 
 
-def fp32_vs_fp64(ws, K, stream, local, steps=2000):
+def fp32_vs_fp64(ws, K, stream, local, steps=2000, early=10):
     """FP32 and FP64 speed of the same grid (the same timed profile pass of K
-    steps) and the FP32 error against the FP64 GPU path after `steps` steps
-    (relative L2 of Re xi).  The FP64 path equals the oracle to 1e-10 per step
-    (tests/test_gpu_config_sizes.py, which also bounds this error at 1e-5)."""
+    steps), and the FP32 error against the FP64 GPU path (relative L2 of Re
+    xi) after `early` and `steps` steps.  The FP64 path equals the oracle to
+    1e-10 per step (tests/test_gpu_config_sizes.py).  An FP64 run started 1e-7
+    (seeded normal) away is the control: where it drifts as far as FP32 does,
+    the trajectory amplifies perturbations and the long-horizon figure
+    measures the dynamics, not the arithmetic."""
     import numpy as np
     from pfdd_b200 import capi
     w = ws[0]
-    out = {}
-    for name, prec in (("fp32", capi.FP32), ("fp64", capi.FP64)):
+    pert = 1e-7 * np.random.default_rng(1).standard_normal(w.xi0.shape)
+    out, states = {}, {}
+    for name, prec, x0 in (("fp32", capi.FP32, w.xi0), ("fp64", capi.FP64, w.xi0),
+                           ("fp64_perturbed", capi.FP64, w.xi0 + pert)):
         with capi.Stepper.from_workloads([w], precision=prec, device=local) as st:
             st.set_stream(stream.cuda_stream)
             st.set_state(0, w.xi0)
-            st.autotune(reps=5)
-            st.advance(5)
-            ms, _ = timed_events(stream, lambda: st.profile(K))
-            out[name + "_ms_per_step"] = ms / K
-            st.set_state(0, w.xi0)
-            st.advance(steps)
-            out[name + "_state"] = st.get_state(0)[0]
-    a, b = out.pop("fp32_state"), out.pop("fp64_state")
-    out["rel_l2_fp32_vs_fp64_after_%d" % steps] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
-    out["max_abs_fp32_vs_fp64_after_%d" % steps] = float(np.abs(a - b).max())
-    out["steps_compared"] = steps
+            if name != "fp64_perturbed":
+                st.autotune(reps=5)
+                st.advance(5)
+                ms, _ = timed_events(stream, lambda: st.profile(K))
+                out[name + "_ms_per_step"] = ms / K
+            st.set_state(0, x0)
+            st.advance(early)
+            states[(name, early)] = st.get_state(0, imag=False)[0]
+            st.advance(steps - early)
+            states[(name, steps)] = st.get_state(0, imag=False)[0]
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    for n in (early, steps):
+        b = states[("fp64", n)]
+        out["rel_l2_fp32_vs_fp64_after_%d" % n] = rel(states[("fp32", n)], b)
+        out["rel_l2_fp64_perturbed_1e-7_vs_fp64_after_%d" % n] = rel(states[("fp64_perturbed", n)], b)
+    out["max_abs_fp32_vs_fp64_after_%d" % steps] = float(np.abs(states[("fp32", steps)] - states[("fp64", steps)]).max())
+    out["steps_compared"] = [early, steps]
     out["fp32_speedup"] = out["fp64_ms_per_step"] / out["fp32_ms_per_step"]
     units = w.S * w.N
     out["fp64_site_slip_updates_per_s"] = units / (out["fp64_ms_per_step"] / 1e3)
     out["fp32_site_slip_updates_per_s"] = units / (out["fp32_ms_per_step"] / 1e3)
     return out
+
+
+def fp64_plain_batch(ws, K, stream, local):
+    """The plain FP64 path on a batch: each instance on its own handle, one
+    after the other (no batching, no merged launches), K steps each timed
+    with CUDA events; site-slip updates/s over the whole batch."""
+    from pfdd_b200 import capi
+    total_ms, units = 0.0, 0
+    for w in ws:
+        with capi.Stepper.from_workloads([w], precision=capi.FP64, device=local) as st:
+            st.set_stream(stream.cuda_stream)
+            st.set_state(0, w.xi0)
+            st.advance(3)
+            ms, _ = timed_events(stream, lambda: st.advance(K))
+            total_ms += ms / K
+            units += w.S * w.N
+    return {"fp64_plain_ms_per_step": total_ms, "fp64_plain_site_slip_updates_per_s": units / (total_ms / 1e3),
+            "note": "each of the %d instances advanced alone in FP64 (graph replay), %d steps each" % (len(ws), K)}
 
 
 def cufft_comparison(w, F, prec, stream, reps=10):
@@ -396,9 +449,12 @@ def cufft_comparison(w, F, prec, stream, reps=10):
 
 def adjoint_ratio(st, w, prec, stream, local, steps=500, ckpt=50):
     """Adjoint call over forward time for `steps` steps, keeping every state
-    and with checkpoints; the target state comes from a forward run with
-    isf 40 / usf 160 mJ/m^2 and 250 MPa.  st = None: a stepper of w of its own."""
+    and with checkpoints: pfdd_gpu_adjoint (forward tape + backward) seeded
+    with dJ/dRe xi_N of J = sum (Re xi_N - target)^2, the target state from a
+    forward run with isf 40 / usf 160 mJ/m^2 and 250 MPa.  st = None: a
+    stepper of w of its own."""
     import copy
+    import numpy as np
     from pfdd_b200 import capi, configs
     if st is None:
         with capi.Stepper.from_workloads([w], precision=prec, device=local) as own:
@@ -415,10 +471,14 @@ def adjoint_ratio(st, w, prec, stream, local, steps=500, ckpt=50):
         target = tg.get_state(0)[0]
     st.set_state(0, w.xi0)
     fwd_ms, _ = timed_events(stream, lambda: st.advance(steps))
-    out = {"steps": steps, "forward_ms": fwd_ms}
-    # every Re xi_n of the run kept on the device (no recomputation) when it
+    # the seed of J = sum (Re xi_N - target)^2 at this run's end state
+    xN, _ = st.get_state(0, imag=False)
+    seed = 2.0 * (xN - target)
+    loss = float(np.sum((xN - target) ** 2))
+    out = {"steps": steps, "forward_ms": fwd_ms, "loss": loss}
+    # every state of the run kept on the device (no recomputation) when it
     # takes under 16 GB, and checkpoints every `ckpt` steps with one forward
-    # re-run per segment
+    # re-run per segment but the last
     state_bytes = w.S * w.N * (4 if prec == capi.FP32 else 8)
     modes = [("checkpointed", ckpt)]
     if steps * state_bytes <= 16e9:
@@ -427,12 +487,12 @@ def adjoint_ratio(st, w, prec, stream, local, steps=500, ckpt=50):
         # one untimed call of the same length first: its scratch buffers (kept
         # by the instance between calls) and first kernel loads
         st.set_state(0, w.xi0)
-        st.adjoint(0, steps, k, target)
+        st.adjoint(0, steps, k, seed)
         st.set_state(0, w.xi0)
-        adj_ms, res = timed_events(stream, lambda: st.adjoint(0, steps, k, target))
-        loss, dp, ds = res
+        adj_ms, res = timed_events(stream, lambda: st.adjoint(0, steps, k, seed))
+        dp, ds = res
         out[name] = {"checkpoint_every": k, "adjoint_call_ms": adj_ms, "adjoint_call_over_forward": adj_ms / fwd_ms,
-                     "backward_over_forward": (adj_ms - fwd_ms) / fwd_ms, "loss": float(loss),
+                     "backward_over_forward": (adj_ms - fwd_ms) / fwd_ms,
                      "dL_dparams": [float(x) for x in dp], "dL_dsigma": [float(x) for x in ds]}
     return out
 
@@ -471,7 +531,8 @@ def main():
         dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = dist_mod
 
-    ws, w_desc, prec_name = workload_config(args.workload)
+    ws_all, w_desc, prec_name = workload_config(args.workload)
+    ws, scaling = shard_instances(ws_all, rank, world)
     prec_name = args.precision or prec_name
     prec = capi.FP32 if prec_name == "fp32" else capi.FP64
     ramp = args.workload == "frank512"   # one GL step per stress state
@@ -503,7 +564,9 @@ def main():
     clocks = parse_clocks(clk_proc, clk_path)
     ms = max_over_ranks(e0.elapsed_time(e1), dist)
     units_per_step = sum(w.S * w.N for w in ws)
-    value = aggregate_rate(units_per_step * args.steps, world, ms)
+    # units of the whole job: every rank's own (sharded or replicated)
+    job_units_per_step = sum_over_ranks(units_per_step, dist)
+    value = job_units_per_step * args.steps / (ms / 1e3)
 
     # roofline of the dominant kernel (bytes summed over the instances of every group)
     n_inst, dev_bytes = st.info()
@@ -559,7 +622,7 @@ def main():
             raise RuntimeError(lib.pfdd_gpu_last_error(st.h))
         ems = max_over_ranks(ems, dist)
         nbytes = sum(16 * w.S * w.N for w in ws)
-        e2e = {"value": aggregate_rate(units_per_step * E, world, ems), "unit": UNIT, "steps": E,
+        e2e = {"value": job_units_per_step * E / (ems / 1e3), "unit": UNIT, "steps": E,
                "h2d_bytes_per_step": nbytes / E, "d2h_bytes_per_step": nbytes / E + 16 * len(ws),
                "note": ("set_state_interleaved + advance(%s) + get_state_interleaved per instance, pinned host "
                         "buffers" % ("1 step x %d stress states" % E if ramp else "%d" % E))}
@@ -572,6 +635,11 @@ def main():
         dms = [timed_events(stream, lambda: st.strain_stress(0, fields=False))[0] for _ in range(3)]
         extras["strain_stress_ms"] = statistics.median(dms)
     if not args.no_extras and rank == 0:
+        if args.workload == "alloy64":
+            # the FP32 batched path against the plain FP64 path on the same instances
+            pl = fp64_plain_batch(ws, 20, stream, local)
+            pl["fp32_batched_over_fp64_plain"] = value / pl["fp64_plain_site_slip_updates_per_s"]
+            extras["fp64_plain"] = pl
         if args.workload in ("loop64", "fcc256"):
             # the metric's "FP32 vs FP64 at stated err" on the timed grid itself
             extras["fp32_vs_fp64"] = fp32_vs_fp64(ws, args.steps, stream, local)
@@ -597,14 +665,15 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == capi.FP32 else "f64",
+            "scaling": scaling, "vs_baseline": None, "dtype": "f32" if prec == capi.FP32 else "f64",
             "data": "synthetic",
             "config": {"workload": w_desc, "instances": len(ws),
                        "grid": [ws[0].nx, ws[0].ny, ws[0].nz] if len(ws) == 1 else "mixed",
                        "slip_systems": ws[0].S, "precision": prec_name,
                        "imag_part": ("full complex carrier (obstacle mask)" if ws[0].xo is not None else
                                      "Nyquist-plane spectrum carried in the x-pencil pass"),
-                       "parallelism": "replicas x%d" % world,
+                       "parallelism": ("%d instances split over %d ranks" % (len(ws_all), world)
+                                       if scaling == "strong" else "replicas x%d" % world),
                        "pencil_tile_widths": tile_widths if tile_widths is not None else "set-up rule",
                        "l2": "working set %.2f GB > 126 MB L2 (no flush)" % (dev_bytes / 1e9)},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
