@@ -114,7 +114,8 @@ struct Instance {
   // lambda pair, Nyquist carrier of lambda, per-plane gradient sums, their
   // total, final state and carrier); tape_steps > 0 while the tape describes
   // the run that ended at the current state
-  DevBuf adj_ck, adj_seg, adj_last, adj_lam[2], adj_aux, adj_gpart, adj_acc, adj_fin, adj_finaux;
+  DevBuf adj_ck, adj_seg[2], adj_last, adj_lam[2], adj_aux, adj_gpart, adj_acc, adj_fin, adj_finaux;
+  DevBuf adj_rspec, adj_raux;   // spectrum and carrier of the segment recomputation
   // strain / stress diagnostics scratch, kept between calls (per-system sums,
   // six strain spectra, six strain fields, FP64 field copies, partial sums)
   DevBuf ss_part, ss_spec6, ss_strain6, ss_e9, ss_s9, ss_fpart;
@@ -183,6 +184,7 @@ struct pfdd_gpu {
   cudaStream_t own_stream = nullptr;  // stream created by the handle
   DevBuf staging;                     // FP64 host<->device staging, kept across calls
   cudaStream_t copy_stream = nullptr; // device-to-host snapshots, beside the stepping stream
+  cudaStream_t side_stream = nullptr; // the adjoint's segment recomputation, beside its backward steps
   std::string err;
   size_t device_bytes = 0;
   int nsm = 148;                      // SMs of the device (grid sizing)
@@ -544,9 +546,12 @@ struct AdjointPass {
 // spectrum) and, for forward steps, the reduction.
 // Forward steps may read and write explicit state buffers (fin/fout, the
 // adjoint's tape) and leave out the reduction (stats = false).
+// spec_buf / aux_buf: another spectrum and Nyquist carrier than the
+// instance's (the adjoint recomputes segments beside its backward steps).
 template <typename T>
 void enqueue_step_fused(Instance &I, cudaStream_t st, bool fwd, const AdjointPass *adj = nullptr,
-                        const void *fin = nullptr, void *fout = nullptr, bool stats = true) {
+                        const void *fin = nullptr, void *fout = nullptr, bool stats = true,
+                        void *spec_buf = nullptr, void *aux_buf = nullptr) {
   constexpr int NP = Threads<T>::plane, NH = Threads<T>::half;
   PlaneArgs pa;
   fill_plane_args<T>(I, pa);
@@ -554,7 +559,7 @@ void enqueue_step_fused(Instance &I, cudaStream_t st, bool fwd, const AdjointPas
   const T *xin = adj ? static_cast<const T *>(adj->lam_in)
                      : (fin ? static_cast<const T *>(fin) : I.xi[I.cur].as<T>());
   T *xout = adj ? static_cast<T *>(adj->lam_out) : (fout ? static_cast<T *>(fout) : I.xi[I.cur ^ 1].as<T>());
-  cx<T> *spec = I.spec.as<cx<T>>();
+  cx<T> *spec = spec_buf ? static_cast<cx<T> *>(spec_buf) : I.spec.as<cx<T>>();
   const int planes = I.F * I.nx;
   PencilArgs pe{};
   pe.px = I.px;
@@ -566,10 +571,10 @@ void enqueue_step_fused(Instance &I, cudaStream_t st, bool fwd, const AdjointPas
   pe.kx_of = I.kx_of; pe.ky_of = I.ky_of; pe.kz_of = I.kz_of;
   pe.mode = PASS_STEP;
   pe.fstride = I.fstride;
-  pe.aux = adj ? adj->aux : I.aux.p;
+  pe.aux = adj ? adj->aux : (aux_buf ? aux_buf : I.aux.p);
   pe.sx_n = I.sx_n; pe.sy_n = I.sy_n;
   pe.cd = I.d.cd_dt;
-  pe.partials = (I.imag == IMAG_NYQ && !adj) ? I.ppart.as<double>() : nullptr;
+  pe.partials = (I.imag == IMAG_NYQ && !adj && stats) ? I.ppart.as<double>() : nullptr;
   pe.g = I.green;
   set_pencil_divisors<T>(pe);
   launch_pencil<T>(I, st, spec, pe, flags);
@@ -1222,10 +1227,10 @@ pfdd_status adjoint_forward_impl(pfdd_gpu *h, Instance &I, int n_steps, int K) {
     return b.alloc(bytes);
   };
   // the last segment's states stay on the tape (adj_last); earlier segments
-  // are recomputed into adj_seg during the backward pass
+  // are recomputed into adj_seg[j & 1] during the backward pass
   CUDA_TRY(h, need(I.adj_ck, (size_t)nck * (sb + aux_bytes)));
   CUDA_TRY(h, need(I.adj_last, (size_t)seg_slots * sb));
-  if (nck > 1) CUDA_TRY(h, need(I.adj_seg, (size_t)K * sb));
+  for (int b = 0; b < std::min(2, nck - 1); ++b) CUDA_TRY(h, need(I.adj_seg[b], (size_t)K * sb));
   CUDA_TRY(h, need(I.adj_fin, sb));
   if (aux_bytes) CUDA_TRY(h, need(I.adj_finaux, aux_bytes));
   auto ck_state = [&](int j) { return I.adj_ck.as<char>() + (size_t)j * (sb + aux_bytes); };
@@ -1281,7 +1286,7 @@ pfdd_status adjoint_backward_impl(pfdd_gpu *h, Instance &I, const double *seed, 
   const int n_steps = I.tape_steps, K = I.tape_K;
   const size_t n_re = (size_t)I.S * I.N, n_all = (size_t)I.F * I.N, sb = n_all * sizeof(T);
   const size_t aux_bytes = I.aux.bytes;
-  const int nck = (n_steps + K - 1) / K, last0 = (nck - 1) * K;
+  const int nck = (n_steps + K - 1) / K;
   auto need = [&](DevBuf &b, size_t bytes) -> cudaError_t {
     if (b.bytes >= bytes && b.p) return cudaSuccess;
     cudaError_t e = cudaStreamSynchronize(st);
@@ -1310,22 +1315,69 @@ pfdd_status adjoint_backward_impl(pfdd_gpu *h, Instance &I, const double *seed, 
   k_stress_state<<<1, 32, 0, st>>>(I.sigma(), I.tau(), I.an(), I.stress, 0, I.flags());
   PlaneArgs pa;
   fill_plane_args<T>(I, pa);
+  // Segment j - 1 is recomputed on a second stream while segment j runs
+  // backwards (the two chains share no buffer: the recomputation has its own
+  // spectrum, carrier and one of two state buffers), so small grids keep the
+  // SMs busy with two independent chains.
+  if (nck > 1) {
+    CUDA_TRY(h, need(I.adj_rspec, I.spec.bytes));
+    if (aux_bytes) CUDA_TRY(h, need(I.adj_raux, aux_bytes));
+    if (!h->side_stream) CUDA_TRY(h, cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
+  }
+  cudaStream_t rs = h->side_stream;
+  std::vector<cudaEvent_t> evs;
+  auto event = [&](cudaEvent_t *e) -> cudaError_t {
+    cudaError_t r = cudaEventCreateWithFlags(e, cudaEventDisableTiming);
+    if (r == cudaSuccess) evs.push_back(*e);
+    return r;
+  };
+  struct EvGuard {
+    std::vector<cudaEvent_t> &v;
+    ~EvGuard() {
+      for (auto e : v) cudaEventDestroy(e);
+    }
+  } guard{evs};
+  std::vector<cudaEvent_t> rec_done(nck, nullptr), bwd_done(nck, nullptr);
+  auto seg_states = [&](int j) { return (j == nck - 1 ? I.adj_last : I.adj_seg[j & 1]).as<char>(); };
+  // recompute segment j's states (from its checkpoint) on the side stream
+  auto recompute = [&](int j) -> pfdd_status {
+    const int n0 = j * K, n1 = std::min(n_steps, n0 + K);
+    char *states = seg_states(j);
+    auto slot = [&](int i) { return states + (size_t)i * sb; };
+    CUDA_TRY(h, cudaMemcpyAsync(slot(0), ck_state(j), sb, cudaMemcpyDeviceToDevice, rs));
+    if (aux_bytes)
+      CUDA_TRY(h, cudaMemcpyAsync(I.adj_raux.p, ck_state(j) + sb, aux_bytes, cudaMemcpyDeviceToDevice, rs));
+    if (n1 - n0 > 1)
+      launch_fwd<T>(I, rs, reinterpret_cast<const T *>(slot(0)), I.adj_rspec.as<cx<T>>(), pa, I.flags(),
+                    I.flags() + 3);
+    for (int n = n0; n + 1 < n1; ++n)
+      enqueue_step_fused<T>(I, rs, n + 2 < n1, nullptr, slot(n - n0), slot(n + 1 - n0), false, I.adj_rspec.p,
+                            aux_bytes ? I.adj_raux.p : nullptr);
+    CUDA_TRY(h, event(&rec_done[j]));
+    CUDA_TRY(h, cudaEventRecord(rec_done[j], rs));
+    return PFDD_OK;
+  };
+  if (nck > 1) {
+    cudaEvent_t start;
+    CUDA_TRY(h, event(&start));
+    CUDA_TRY(h, cudaEventRecord(start, st));   // tau and flags are set
+    CUDA_TRY(h, cudaStreamWaitEvent(rs, start, 0));
+    pfdd_status ps = recompute(nck - 2);
+    if (ps != PFDD_OK) return ps;
+  }
   int lc = 0;
   for (int j = nck - 1; j >= 0; --j) {
     const int n0 = j * K, n1 = std::min(n_steps, n0 + K);
-    // the last segment's states are on the tape; earlier ones are recomputed
-    char *states = (n0 == last0 ? I.adj_last : I.adj_seg).as<char>();
-    auto slot = [&](int i) { return states + (size_t)i * sb; };
-    if (n0 != last0) {
-      // recompute the segment's states into the tape slots from its checkpoint
-      CUDA_TRY(h, cudaMemcpyAsync(slot(0), ck_state(j), sb, cudaMemcpyDeviceToDevice, st));
-      if (aux_bytes)
-        CUDA_TRY(h, cudaMemcpyAsync(I.aux.p, ck_state(j) + sb, aux_bytes, cudaMemcpyDeviceToDevice, st));
-      if (n1 - n0 > 1)
-        launch_fwd<T>(I, st, reinterpret_cast<const T *>(slot(0)), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
-      for (int n = n0; n + 1 < n1; ++n)
-        enqueue_step_fused<T>(I, st, n + 2 < n1, nullptr, slot(n - n0), slot(n + 1 - n0), false);
+    // the next segment down is recomputed beside this one's backward steps,
+    // into the state buffer the segment above used (free once it is done)
+    if (j - 1 >= 0 && j - 1 != nck - 2) {
+      if (j + 1 <= nck - 2) CUDA_TRY(h, cudaStreamWaitEvent(rs, bwd_done[j + 1], 0));
+      pfdd_status ps = recompute(j - 1);
+      if (ps != PFDD_OK) return ps;
     }
+    if (j != nck - 1) CUDA_TRY(h, cudaStreamWaitEvent(st, rec_done[j], 0));
+    char *states = seg_states(j);
+    auto slot = [&](int i) { return states + (size_t)i * sb; };
     // backward steps: each plane pass also transforms the new lambda
     launch_fwd<T>(I, st, lam[lc].as<T>(), I.spec.as<cx<T>>(), pa, I.flags(), I.flags() + 3);
     for (int n = n1 - 1; n >= n0; --n) {
@@ -1333,6 +1385,8 @@ pfdd_status adjoint_backward_impl(pfdd_gpu *h, Instance &I, const double *seed, 
       enqueue_step_fused<T>(I, st, n > n0, &ap);
       lc ^= 1;
     }
+    CUDA_TRY(h, event(&bwd_done[j]));
+    CUDA_TRY(h, cudaEventRecord(bwd_done[j], st));
   }
   k_grad_accum<<<1, 32, 0, st>>>(I.adj_gpart.as<double>(), I.S, I.nx, I.adj_acc.as<double>(),
                                   I.adj_acc.as<double>() + 2 + PFDD_MAXS);
@@ -2486,6 +2540,10 @@ void pfdd_gpu_destroy(pfdd_gpu *h) {
   }
   h->inst.clear();
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  if (h->side_stream) {
+    cudaStreamSynchronize(h->side_stream);
+    cudaStreamDestroy(h->side_stream);
+  }
   h->staging.release();
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   h->own_stream = nullptr;

@@ -64,6 +64,11 @@ template <typename T, bool SPLIT> struct PlaneMinBlocks {
 #ifndef PFDD_PENCIL_MINB_F32
 #define PFDD_PENCIL_MINB_F32 2
 #endif
+// 1: with a run-time slip count the x-pencil contraction reads its constants
+// from a shared-memory stage as vectors (0: scalar constant-bank loads)
+#ifndef PFDD_PENCIL_SMEM_CONST
+#define PFDD_PENCIL_SMEM_CONST 0
+#endif
 template <typename T> struct PencilMinBlocks {
   static constexpr int value = sizeof(T) == 4 ? PFDD_PENCIL_MINB_F32 : 1;
 };
@@ -627,6 +632,45 @@ __device__ __forceinline__ void green_accumulate(const GreenT<T> &g, int b, C x,
   for (int q = 0; q < 6; ++q) { sig[q].x += s[q] * x.x; sig[q].y += s[q] * x.y; }
 }
 
+// The same two operations with one system's constants read from a
+// shared-memory stage as pairs (cs: sig[6] per system; co: epso[6], sigo[6]
+// per system): 3 and 6 vector loads instead of 6 and 12 scalar constant loads
+// when the system index is only known at run time.
+template <typename T> struct Pair;
+template <> struct Pair<float> { using type = float2; };
+template <> struct Pair<double> { using type = double2; };
+template <typename T, typename C>
+__device__ __forceinline__ void green_accumulate_s(const T *__restrict__ cs, int b, C x, C (&sig)[6]) {
+  using P = typename Pair<T>::type;
+  const P *p = reinterpret_cast<const P *>(cs + 6 * b);
+  const P a0 = p[0], a1 = p[1], a2 = p[2];
+  const T v[6] = {a0.x, a0.y, a1.x, a1.y, a2.x, a2.y};
+#pragma unroll
+  for (int q = 0; q < 6; ++q) { sig[q].x += v[q] * x.x; sig[q].y += v[q] * x.y; }
+}
+template <typename T, typename C>
+__device__ __forceinline__ C green_out_s(const T *__restrict__ co, int a, const C (&sig)[6], const C (&Tq)[6], bool nz) {
+  if (!nz) return mk<C>((T)0, (T)0);
+  using P = typename Pair<T>::type;
+  const P *p = reinterpret_cast<const P *>(co + 12 * a);
+  T e[6], o[6];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const P pe = p[i], po = p[3 + i];
+    e[2 * i] = pe.x; e[2 * i + 1] = pe.y;
+    o[2 * i] = po.x; o[2 * i + 1] = po.y;
+  }
+  T ex = (T)0, ey = (T)0, ox = (T)0, oy = (T)0;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    ex = fma_t(e[q], sig[q].x, ex);
+    ey = fma_t(e[q], sig[q].y, ey);
+    ox = fma_t(o[q], Tq[q].x, ox);
+    oy = fma_t(o[q], Tq[q].y, oy);
+  }
+  return mk<C>(ex + ox, ey + oy);
+}
+
 // frequency of index i on an axis of length n (frec, fft_fftw_slab.cpp:295-330)
 template <typename T> __device__ __forceinline__ T freq_of(int i, int n) {
   return (i >= n / 2) ? (T)(i - n) / (T)n : (T)i / (T)n;
@@ -721,6 +765,18 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
         nqs[i] = nq ? caux[ai] : mk<C>((T)0, (T)0);
       }
   }
+  // run-time slip count: the contraction's constants staged for vector loads
+  constexpr bool STAGED = SC == 0 && PFDD_PENCIL_SMEM_CONST;
+  __shared__ __align__(16) T cst_sig[STAGED ? PFDD_MAXS * 6 : 1];
+  __shared__ __align__(16) T cst_out[STAGED ? PFDD_MAXS * 12 : 1];
+  if constexpr (STAGED) {
+    for (int i = threadIdx.x; i < S * 6; i += blockDim.x) {
+      const int b = i / 6, q = i - 6 * b;
+      cst_sig[i] = gt.sig[b][q];
+      cst_out[12 * b + q] = gt.epso[b][q];
+      cst_out[12 * b + 6 + q] = gt.sigo[b][q];
+    }
+  }
   if (a.mode != PASS_SYNTH) cp_async_wait_all();
   __syncthreads();
 
@@ -730,6 +786,14 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
   double dsq = 0.0;
   const GreenT<T> &g = gt;
   const size_t fs = (size_t)fst;
+  auto gacc = [&](int b, C x, C (&acc)[6]) {
+    if constexpr (STAGED) green_accumulate_s<T>(cst_sig, b, x, acc);
+    else green_accumulate<T>(g, b, x, acc);
+  };
+  auto gout = [&](int aa, const C (&sv)[6], const C (&Tq)[6], bool nzk) -> C {
+    if constexpr (STAGED) return green_out_s<T>(cst_out, aa, sv, Tq, nzk);
+    else return green_out<T>(g, aa, sv, Tq, nzk);
+  };
   for (int w = threadIdx.x; w < nx * cc; w += blockDim.x) {
     const int sx = a.fd_cc.div(w), c = w - sx * cc;
     const int sy = csy[c], sz = csz[c];
@@ -757,10 +821,10 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
 #pragma unroll(SC > 0 ? SC / 2 : 1)
       for (; b + 1 < S; b += 2) {
         const C y0 = pk[b * fs], y1 = pk[(b + 1) * fs];
-        green_accumulate<T>(g, b, y0, sr);
-        green_accumulate<T>(g, b + 1, y1, s2);
+        gacc(b, y0, sr);
+        gacc(b + 1, y1, s2);
       }
-      if (b < S) green_accumulate<T>(g, b, pk[b * fs], sr);
+      if (b < S) gacc(b, pk[b * fs], sr);
 #pragma unroll
       for (int q = 0; q < 6; ++q) sr[q] = mk<C>(sr[q].x + s2[q].x, sr[q].y + s2[q].y);
     }
@@ -783,7 +847,7 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
         const bool zq = green_tensor<T>(g, sr, mx, my, mz, Tm);
 #pragma unroll(SC > 0 ? SC : 1)
         for (int aa = 0; aa < S; ++aa) {
-          const C P = green_out<T>(g, aa, sr, Tp, zp), Q = green_out<T>(g, aa, sr, Tm, zq);
+          const C P = gout(aa, sr, Tp, zp), Q = gout(aa, sr, Tm, zq);
           pk[aa * fs] = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
         }
         continue;
@@ -812,7 +876,7 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-          if (b0 + q < S) green_accumulate<T>(g, b0 + q, xv[q], si);
+          if (b0 + q < S) gacc(b0 + q, xv[q], si);
       }
       C sp[6], sq[6];
 #pragma unroll
@@ -827,8 +891,8 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
       const double wgt = (sz == 0 || sz == a.M) ? 1.0 : 2.0;   // k and its unstored partner -k
 #pragma unroll 1
       for (int aa = 0; aa < S; ++aa) {
-        const C P = green_out<T>(g, aa, sp, Tp, zp);
-        const C Q = green_out<T>(g, aa, sq, Tm, zq);
+        const C P = gout(aa, sp, Tp, zp);
+        const C Q = gout(aa, sq, Tm, zq);
         pk[aa * fs] = mk<C>((T)0.5 * (P.x + Q.x), (T)0.5 * (P.y + Q.y));
         // (P - Q)/(2i) = -i (P - Q)/2
         const C ei = mk<C>((T)0.5 * (P.y - Q.y), (T)-0.5 * (P.x - Q.x));
@@ -858,11 +922,11 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
       int aa = 0;
 #pragma unroll(SC > 0 ? SC / 2 : 1)
       for (; aa + 1 < S; aa += 2) {   // two outputs in flight
-        const C o0 = green_out<T>(g, aa, sr, Tp, zp), o1 = green_out<T>(g, aa + 1, sr, Tp, zp);
+        const C o0 = gout(aa, sr, Tp, zp), o1 = gout(aa + 1, sr, Tp, zp);
         pk[aa * fs] = o0;
         pk[(aa + 1) * fs] = o1;
       }
-      if (aa < S) pk[aa * fs] = green_out<T>(g, aa, sr, Tp, zp);
+      if (aa < S) pk[aa * fs] = gout(aa, sr, Tp, zp);
     }
   }
   if (ppart) block_sum2(dsq, 0.0, red, ppart + 2 * tile);
@@ -1300,26 +1364,32 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
       const int y = dv.div(i), zq = i - y * nvec;
       const int idx = y * nz + zq * VN;
-      T lam[VN], e[VN], nv[VN];
+      T lam[VN], e[VN], nv[VN], xv[VN];
       *reinterpret_cast<V *>(lam) = *reinterpret_cast<const V *>(xin + off + idx);
       *reinterpret_cast<V *>(e) = *reinterpret_cast<const V *>(bufr + (size_t)y * 2 * nzs + zq * VN);
+      if (real_field) *reinterpret_cast<V *>(xv) = *reinterpret_cast<const V *>(xf + (size_t)sys * N + rbase + idx);
+      // the vector's gradient terms summed in the compute precision, then added in FP64
+      T v0 = (T)0, v1 = (T)0, vl = (T)0;
 #pragma unroll
       for (int q = 0; q < VN; ++q) {
         const size_t r = rbase + idx + q;
         const bool frozen = mask && mask[(size_t)sys * N + r];
         if (real_field) {
           T d2, dp0, dp1;
-          core_adjoint_terms<T>(u.core, xf[(size_t)sys * N + r], sys, r, N, site, d2, dp0, dp1);
+          core_adjoint_terms<T>(u.core, xv[q], sys, r, N, site, d2, dp0, dp1);
           nv[q] = frozen ? lam[q] : lam[q] - cd * (e[q] * invN + d2 * lam[q]);
           if (!frozen) {
-            g0 += (double)lam[q] * (double)dp0;
-            g1 += (double)lam[q] * (double)dp1;
-            gl += (double)lam[q];
+            v0 = fma_t(lam[q], dp0, v0);
+            v1 = fma_t(lam[q], dp1, v1);
+            vl += lam[q];
           }
         } else {
           nv[q] = frozen ? lam[q] : lam[q] - cd * e[q] * invN;
         }
       }
+      g0 += (double)v0;
+      g1 += (double)v1;
+      gl += (double)vl;
       if (ok) *reinterpret_cast<V *>(xout + off + idx) = *reinterpret_cast<V *>(nv);
       if (FUSE == 2 && fwd)
         *reinterpret_cast<V *>(reinterpret_cast<T *>(buf) + (size_t)y * 2 * nzs + zq * VN) =
