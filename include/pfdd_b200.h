@@ -339,7 +339,7 @@ pfdd_status pfdd_gpu_set_stress(pfdd_gpu *h, int inst, const double sigma[3][3])
  * src/fft_fftw_slab.cpp:1891-1925, and the six-digit text dumps,
  * src/dump_text.cpp:361-400).  A checkpoint holds one instance's device state
  * as it is stepped (fields in the compute precision, the Nyquist carrier of
- * Im xi, the device's sigma and dsigma), so a handle created from the same
+ * Im xi in frequency order, the device's sigma and dsigma), so a handle created from the same
  * descriptor and options that loads it continues bit for bit as the writer
  * would have.  The file is a 256-byte little-endian header with FNV-1a 64
  * checksums of itself and of the payload, then the payload; reading refuses a

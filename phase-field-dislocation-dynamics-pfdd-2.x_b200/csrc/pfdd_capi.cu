@@ -1850,6 +1850,39 @@ pfdd_status snapshot_begin_impl(pfdd_gpu *h, Instance &I, double *re, double *im
 }
 
 // ------------------------------------------------------------ checkpoints
+// Index in the frequency-ordered carrier of a checkpoint file (kz = nz/2
+// plane [S][kx][ky], ky = ny/2 plane [S][kx][kz], kx = nx/2 plane [S][ky][kz])
+// of every complex value of the device's carrier, which is stored in
+// transform-slot coordinates (the digit-reversed slots of this instance's
+// plans; a split plane's rank r holds ky = r + 2k).
+std::vector<size_t> carrier_file_order(const Instance &I) {
+  const int nx = I.nx, ny = I.ny, M = I.M, S = I.S;
+  std::vector<int> fx(nx), fy(ny), fz(M);
+  const std::vector<int> px = positions(I.px), py = positions(I.py), pz = positions(I.pz);
+  for (int k = 0; k < nx; ++k) fx[px[k]] = k;
+  if (I.split) {
+    const int nyh = ny / 2;
+    for (int r = 0; r < 2; ++r)
+      for (int k = 0; k < nyh; ++k) fy[r * nyh + py[k]] = r + 2 * k;
+  } else {
+    for (int k = 0; k < ny; ++k) fy[py[k]] = k;
+  }
+  for (int k = 0; k < M; ++k) fz[pz[k]] = k;
+  std::vector<size_t> out;
+  out.reserve((size_t)S * ((size_t)nx * ny + (size_t)nx * M + (size_t)ny * M));
+  const size_t oZ = 0, oY = (size_t)S * nx * ny, oX = oY + (size_t)S * nx * M;
+  for (int f = 0; f < S; ++f)
+    for (int sx = 0; sx < nx; ++sx)
+      for (int sy = 0; sy < ny; ++sy) out.push_back(oZ + ((size_t)f * nx + fx[sx]) * ny + fy[sy]);
+  for (int f = 0; f < S; ++f)
+    for (int sx = 0; sx < nx; ++sx)
+      for (int sz = 0; sz < M; ++sz) out.push_back(oY + ((size_t)f * nx + fx[sx]) * M + fz[sz]);
+  for (int f = 0; f < S; ++f)
+    for (int sy = 0; sy < ny; ++sy)
+      for (int sz = 0; sz < M; ++sz) out.push_back(oX + ((size_t)f * ny + fy[sy]) * M + fz[sz]);
+  return out;
+}
+
 template <typename T>
 pfdd_status checkpoint_save_impl(pfdd_gpu *h, Instance &I, const char *path) {
   pfdd_checkpoint_info in;
@@ -1871,6 +1904,13 @@ pfdd_status checkpoint_save_impl(pfdd_gpu *h, Instance &I, const char *path) {
   for (int i = 0; i < 9; ++i) {
     in.sigma[i / 3][i % 3] = sig[i];
     in.dsigma[i / 3][i % 3] = sig[9 + i];
+  }
+  if (!c.empty()) {   // slot order -> the file's frequency order
+    const std::vector<size_t> ord = carrier_file_order(I);
+    if (ord.size() * sizeof(cx<T>) != c.size()) return fail(h, PFDD_EINVAL, "carrier size mismatch");
+    std::vector<unsigned char> cf(c.size());
+    for (size_t i = 0; i < ord.size(); ++i) memcpy(&cf[ord[i] * sizeof(cx<T>)], &c[i * sizeof(cx<T>)], sizeof(cx<T>));
+    c.swap(cf);
   }
   const pfdd_status st = pfdd_checkpoint_write(path, &in, f.data(), c.empty() ? nullptr : c.data());
   if (st != PFDD_OK) return fail(h, st, "cannot write checkpoint %s", path);
@@ -1895,6 +1935,13 @@ pfdd_status checkpoint_load_impl(pfdd_gpu *h, Instance &I, const char *path) {
   for (int i = 0; i < 9; ++i) {
     sig[i] = in.sigma[i / 3][i % 3];
     sig[9 + i] = in.dsigma[i / 3][i % 3];
+  }
+  if (cb) {   // the file's frequency order -> this instance's slot order
+    const std::vector<size_t> ord = carrier_file_order(I);
+    if (ord.size() * sizeof(cx<T>) != cb) return fail(h, PFDD_EINVAL, "carrier size mismatch");
+    std::vector<unsigned char> cs(cb);
+    for (size_t i = 0; i < ord.size(); ++i) memcpy(&cs[i * sizeof(cx<T>)], &c[ord[i] * sizeof(cx<T>)], sizeof(cx<T>));
+    c.swap(cs);
   }
   CUDA_TRY(h, cudaMemcpyAsync(I.xi[I.cur].p, f.data(), fb, cudaMemcpyHostToDevice, h->stream));
   if (cb) CUDA_TRY(h, cudaMemcpyAsync(I.aux.p, c.data(), cb, cudaMemcpyHostToDevice, h->stream));
@@ -2091,11 +2138,12 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
     I->nzh = I->M + 1;
     // spectrum rows padded to whole 16-byte units so a plane moves in one bulk copy
     I->nzp = (o.precision == PFDD_FP32) ? ((I->nzh + 1) & ~1) : I->nzh;
-    // shared-memory row stride: consecutive rows start 8 words apart in the
-    // 32 banks (FP32: 2*nzs = 8 mod 32; FP64: nzs = 4 mod 8 16-byte units)
+    // shared-memory row stride: FP32 rows start 4 words apart in the 32 banks
+    // (2*nzs = 4 mod 32), which the register-resident z passes' thread order
+    // turns into conflict-free block loads; FP64: nzs = 4 mod 8 16-byte units
     I->nzs = I->nzp;
     if (o.precision == PFDD_FP32)
-      while ((2 * I->nzs) % 32 != 8) I->nzs += 2;
+      while ((2 * I->nzs) % 32 != 4) I->nzs += 2;
     else
       while (I->nzs % 8 != 4) ++I->nzs;
     // store spectrum rows with the same stride, so a plane moves in one bulk copy
@@ -2121,7 +2169,7 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
                          : std::min(MaxRadix<Threads<double>::plane>::value, MaxRadix<Threads<double>::half>::value);
     make_plan(I->nx, I->px, maxr);
     make_plan(I->split ? I->ny / 2 : I->ny, I->py, maxr);
-    make_plan(I->M, I->pz, maxr);
+    make_zplan(I->M, I->pz, maxr);
     pfdd_instance_desc d = descs[i];
     I->d.xo = d.xo;               // used during set-up only
     I->d.site_gsfe = d.site_gsfe;

@@ -7,7 +7,7 @@
 //
 //   header (256 bytes, little-endian)
 //     0   char[8]   "PFDDCKP1"
-//     8   u32       format version (1)
+//     8   u32       format version (2)
 //     12  u32       header size (256)
 //     16  i32[8]    nx, ny, nz, n_slip, fields carried, precision, imag mode, advanced
 //     48  u64       field bytes, 56 u64 carrier bytes
@@ -18,7 +18,10 @@
 //     232 ...       zero
 //   payload: the fields (fields carried x N values of the compute precision,
 //   reference site order), then the Nyquist carrier of Im xi (complex values
-//   of the compute precision; empty with the full carrier).
+//   of the compute precision; empty with the full carrier) in frequency order:
+//   the kz = nz/2 plane [S][kx][ky], the ky = ny/2 plane [S][kx][kz < nz/2],
+//   the kx = nx/2 plane [S][ky][kz < nz/2], each index the FFT index of its
+//   axis (format 1 stored the device's transform-slot order instead).
 //
 // Reading checks the magic, version, header checksum, payload size and
 // payload checksum before anything is returned, so a truncated or altered
@@ -33,7 +36,7 @@
 namespace {
 
 constexpr char kMagic[8] = {'P', 'F', 'D', 'D', 'C', 'K', 'P', '1'};
-constexpr uint32_t kVersion = 1, kHeaderBytes = 256;
+constexpr uint32_t kVersion = 2, kHeaderBytes = 256;
 
 uint64_t fnv1a(const void *p, size_t n, uint64_t h = 1469598103934665603ull) {
   const unsigned char *b = static_cast<const unsigned char *>(p);

@@ -54,12 +54,16 @@ namespace pfdd {
 template <int NT> struct MaxRadix { static constexpr int value = NT >= 1024 ? 8 : 16; };
 
 // Resident CTAs per SM a plane kernel is compiled for (register cap): FP32
-// split planes (half a plane of shared memory each) fit three to an SM.
+// split planes (half a plane of shared memory each) fit three to an SM; FP64
+// planes are held to 128 registers so that small planes run two to an SM.
 #ifndef PFDD_SPLIT_MINB_F32
 #define PFDD_SPLIT_MINB_F32 3
 #endif
+#ifndef PFDD_PLANE_MINB_F64
+#define PFDD_PLANE_MINB_F64 1
+#endif
 template <typename T, bool SPLIT> struct PlaneMinBlocks {
-  static constexpr int value = (SPLIT && sizeof(T) == 4) ? PFDD_SPLIT_MINB_F32 : 1;
+  static constexpr int value = sizeof(T) == 4 ? (SPLIT ? PFDD_SPLIT_MINB_F32 : 1) : PFDD_PLANE_MINB_F64;
 };
 #ifndef PFDD_PENCIL_MINB_F32
 #define PFDD_PENCIL_MINB_F32 2
@@ -466,6 +470,13 @@ __device__ __forceinline__ void fwd_planes_body(const T *__restrict__ xi, cx<T> 
   fwd_planes_compute<T, NT, SPLIT>(sm, a, spec, plane, rows, row0, ok);
 }
 
+template <typename T, int NT, bool SPLIT>
+__device__ __forceinline__ void fwd_planes_tail(const PlaneSmem<cx<T>> &sm, const PlaneArgs &a,
+                                                cx<T> *__restrict__ spec, size_t plane, int rows, int row0,
+                                                bool ok);
+template <typename T, int NT>
+__device__ __forceinline__ void fwd_planes_z(const PlaneSmem<cx<T>> &sm, const PlaneArgs &a, int rows);
+
 // The forward part of P1 on the real rows already in shared memory (row
 // stride 2*nzs reals): z real-to-complex, y, DC/Nyquist split, bulk store of
 // the half-spectrum rows.  `ok` false: compute (a split peer waits at the
@@ -474,8 +485,16 @@ template <typename T, int NT, bool SPLIT>
 __device__ __forceinline__ void fwd_planes_compute(const PlaneSmem<cx<T>> &sm, const PlaneArgs &a,
                                                    cx<T> *__restrict__ spec, size_t plane, int rows, int row0,
                                                    bool ok) {
+  fwd_planes_z<T, NT>(sm, a, rows);
+  fwd_planes_tail<T, NT, SPLIT>(sm, a, spec, plane, rows, row0, ok);
+}
+
+// The z side of the forward part: the M-point transforms of the packed real
+// rows and the real-to-complex unpacking (no barrier at the end).
+template <typename T, int NT>
+__device__ __forceinline__ void fwd_planes_z(const PlaneSmem<cx<T>> &sm, const PlaneArgs &a, int rows) {
   using C = cx<T>;
-  const int ny = a.ny, nzh = a.nzh, nzp = a.nzp, nzs = a.nzs, M = a.M;
+  const int nzh = a.nzh, nzp = a.nzp, nzs = a.nzs, M = a.M;
   C *buf = sm.buf;
   const C *twr = sm.twr;
   const int *pos = sm.pos;
@@ -510,6 +529,18 @@ __device__ __forceinline__ void fwd_planes_compute(const PlaneSmem<cx<T>> &sm, c
       if (pm != pk) row[pm] = cconj(csub(e, wo));
     }
   }
+}
+
+// The y side of the forward part, after the z transforms and the
+// real-to-complex unpacking of every row: the cross-CTA stage (SPLIT) or a
+// barrier, the y transforms, the DC/Nyquist split and the bulk store.
+template <typename T, int NT, bool SPLIT>
+__device__ __forceinline__ void fwd_planes_tail(const PlaneSmem<cx<T>> &sm, const PlaneArgs &a,
+                                                cx<T> *__restrict__ spec, size_t plane, int rows, int row0,
+                                                bool ok) {
+  using C = cx<T>;
+  const int ny = a.ny, nzp = a.nzp, nzs = a.nzs, M = a.M;
+  C *buf = sm.buf;
   if constexpr (SPLIT) cross_stage<false>(buf, sm.twy, rows, a.fd_m, nzs);
   else __syncthreads();
 
@@ -1213,6 +1244,205 @@ __device__ __forceinline__ T update_one(const UpdateArgs &u, bool real_field, in
   return old - cd * el;
 }
 
+// ------------------------------------------------------------ register-resident z passes
+// The z side of the fused plane pass for a two-stage z plan M = R1 * R2
+// (stage A: radix R1 over the whole row, elements j + R2 r; stage B: radix
+// R2 over contiguous blocks of R2 slots).  Three passes over shared memory
+// replace seven (complex-to-real pairs, two inverse stages, the update's
+// read and write, two forward stages, real-to-complex pairs):
+//   A  per (row, mirrored block pair): complex-to-real pairs, inverse stage B
+//   B  per (row, j): inverse stage A, the per-site update of the 2 R1 real
+//      sites the thread then holds (z = 2 (j + R2 r) and + 1), forward stage A
+//   C  per (row, mirrored block pair): forward stage B, real-to-complex pairs
+// Frequency k = k0 + R1 k1 sits at slot k0 R2 + k1, so the partner M - k of
+// block k0 lies in block R1 - k0 (element R2 - 1 - k1), and blocks 0 and
+// R1/2 pair with themselves: one work unit holds both blocks of a pair.
+template <int M> struct ZPlan {   // the host's make_zplan for the lengths this path compiles
+  static constexpr int R1 = (M == 16 || M == 32 || M == 64) ? 8 : (M % 16 == 0) ? 16 : (M % 8 == 0) ? 8 : 4;
+  static constexpr int R2 = M / R1;
+};
+// Calls f(integral_constant<M>) for the z lengths with a register-resident
+// path whose host plan is [R1, R2]; returns false otherwise (generic path).
+template <typename Fn> __device__ __forceinline__ bool with_zfused(const FftPlan &pz, Fn &&f) {
+  auto run = [&](auto Mc) -> bool {
+    constexpr int M = decltype(Mc)::value, R1 = ZPlan<M>::R1, R2 = ZPlan<M>::R2;
+    if (pz.radix[0] != R1 || pz.nst != (R2 > 1 ? 2 : 1) || (R2 > 1 && pz.radix[1] != R2)) return false;
+    f(Mc);
+    return true;
+  };
+  switch (pz.n) {
+    case 64: return run(std::integral_constant<int, 64>());
+    case 32: return run(std::integral_constant<int, 32>());
+    case 16: return run(std::integral_constant<int, 16>());
+    case 48: return run(std::integral_constant<int, 48>());
+    case 24: return run(std::integral_constant<int, 24>());
+    default: return false;
+  }
+}
+
+// Core models whose force is m (A sin 2 pi x + B sin 4 pi x), A and B
+// constant and m = 1 or the per-site field (1 perfect, 3 sine, 6 USFE, 7 MPEA,
+// 103 sine with a per-site multiplier): the register-resident z passes inline
+// these; the others keep the generic passes.  Adjoint terms in the same form:
+// f'' = m (P cos 2 pi x + Q cos 4 pi x), df'/dp0 = m (R sin 2 pi x - S sin 4 pi x),
+// df'/dp1 = m U sin 4 pi x (core_adjoint_terms).
+__device__ __forceinline__ bool core_sine_family(int flag) {
+  return flag == 1 || flag == 3 || flag == 6 || flag == 7 || flag == 103;
+}
+template <typename T> struct SineCore {
+  T A, B, P, Q, R, S, U;
+  bool per_site;
+};
+template <typename T> __device__ __forceinline__ SineCore<T> sine_core(const Core &cm, const T *__restrict__ site) {
+  const T pi = (T)PFDD_PI_T;
+  SineCore<T> c{(T)0, (T)0, (T)0, (T)0, (T)0, (T)0, (T)0, false};
+  const T k0 = core_k<T>(cm, 0), k1 = core_k<T>(cm, 1), k7 = core_k<T>(cm, 7);
+  switch (cm.flag) {
+    case 1: c.A = k0; c.P = k0 * (T)2 * pi; c.R = k7; break;
+    case 6: c.A = site[0]; c.P = site[0] * (T)2 * pi; c.R = k7; break;
+    case 3:
+      c.A = k0; c.B = k1; c.P = k0 * (T)2 * pi; c.Q = k1 * (T)4 * pi;
+      c.R = k7; c.S = core_k<T>(cm, 8); c.U = core_k<T>(cm, 9);
+      break;
+    case 7: c.per_site = true; c.A = k0; c.P = k0 * (T)2 * pi; break;
+    case 103: {
+      const T k2 = core_k<T>(cm, 2), cn = core_k<T>(cm, 3) - k2 * core_k<T>(cm, 4);
+      c.per_site = true;
+      c.A = pi * k2; c.B = (T)2 * pi * cn; c.P = (T)2 * pi * pi * k2; c.Q = (T)8 * pi * pi * cn;
+      c.R = k7; c.S = core_k<T>(cm, 8); c.U = core_k<T>(cm, 9);
+      break;
+    }
+    default: break;
+  }
+  return c;
+}
+
+// Thread orders of the z passes.  FP32 rows are 4 words apart in the 32 banks
+// (row stride 2 mod 16 complex), so rows y and y + d start 4 d words apart.
+// Pass B item w -> (row y, j): in blocks of 8 rows, each half-warp takes
+// 16 / R2 rows spaced R2 / 2 apart, whose 2 R2-word runs then tile the banks.
+template <int R2> __device__ __forceinline__ void zb_item(int w, int rows, int &y, int &j) {
+  if constexpr (R2 == 2 || R2 == 4 || R2 == 8) {
+    if ((rows & 7) == 0) {
+      constexpr int h = 16 / R2, sp = R2 / 2;
+      const int b8 = w / (8 * R2), t = w - b8 * (8 * R2);
+      const int rr = t / R2;
+      j = t - rr * R2;
+      y = 8 * b8 + (rr % h) * sp + rr / h;
+      return;
+    }
+  }
+  y = w / R2;
+  j = w - y * R2;
+}
+// Pass A / C unit w -> (row y, unit u), U = R1/2 units per row, each loading
+// two blocks of R2 slots as 16-byte chunks: each quarter-warp takes R2 / 2
+// consecutive rows x 16 / R2 consecutive units, whose first chunks
+// (4 y + 2 R2 u words) then cover the 32 banks once.
+template <int R2, int U> __device__ __forceinline__ void zac_item(int w, int rows, int &y, int &u) {
+  if constexpr ((R2 == 4 || R2 == 8) && U % (16 / R2) == 0) {
+    constexpr int Y = R2 / 2, V = 16 / R2;
+    if (rows % Y == 0) {
+      const int blk = w / (Y * U), t = w - blk * (Y * U);
+      const int inner = t & 7, qi = t >> 3;
+      y = blk * Y + inner % Y;
+      u = qi * V + inner / Y;
+      return;
+    }
+  }
+  y = w / U;
+  u = w - y * U;
+}
+
+template <int R2, typename C> __device__ __forceinline__ void zload_block(const C *p, C (&v)[R2]) {
+  if constexpr (sizeof(C) == 8 && R2 % 2 == 0) {
+#pragma unroll
+    for (int r = 0; r < R2; r += 2) {
+      const float4 q = reinterpret_cast<const float4 *>(p)[r / 2];
+      v[r] = mk<C>(q.x, q.y);
+      v[r + 1] = mk<C>(q.z, q.w);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < R2; ++r) v[r] = p[r];
+  }
+}
+template <int R2, typename C> __device__ __forceinline__ void zstore_block(C *p, const C (&v)[R2]) {
+  if constexpr (sizeof(C) == 8 && R2 % 2 == 0) {
+#pragma unroll
+    for (int r = 0; r < R2; r += 2)
+      reinterpret_cast<float4 *>(p)[r / 2] = make_float4(v[r].x, v[r].y, v[r + 1].x, v[r + 1].y);
+  } else {
+#pragma unroll
+    for (int r = 0; r < R2; ++r) p[r] = v[r];
+  }
+}
+
+// complex-to-real pair (k, M-k) before the inverse z transform:
+// A = X[k] + conj X[M-k], D = X[k] - conj X[M-k], Zin[k] = A + i D conj(W^k),
+// Zin[M-k] = conj(A - i D conj(W^k)) (same formulas as the generic loop)
+template <typename C> __device__ __forceinline__ void c2r_pair(C &xk, C &xm, const C w, bool self) {
+  const C A = mk<C>(xk.x + xm.x, xk.y - xm.y);
+  const C D = mk<C>(xk.x - xm.x, xk.y + xm.y);
+  const C wd = cmulc(D, w);
+  const C iwd = mk<C>(-wd.y, wd.x);
+  const C nk = cadd(A, iwd);
+  if (!self) xm = cconj(csub(A, iwd));
+  xk = nk;
+}
+// real-to-complex pair (k, M-k) after the forward z transform:
+// E = (Zk + conj Zm)/2, O = (Zk - conj Zm)/(2i), X[k] = E + W^k O, X[M-k] = conj(E - W^k O)
+template <typename C> __device__ __forceinline__ void r2c_pair(C &zk, C &zm, const C w, bool self) {
+  using T = decltype(C::x);
+  const C e = mk<C>((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y - zm.y));
+  const C o = mk<C>((T)0.5 * (zk.y + zm.y), (T)-0.5 * (zk.x - zm.x));
+  const C wo = cmul(w, o);
+  const C nk = cadd(e, wo);
+  if (!self) zm = cconj(csub(e, wo));
+  zk = nk;
+}
+
+// Pass A (INV) or C (!INV) over the rows of this CTA; ends with no barrier.
+template <bool INV, int M, typename C>
+__device__ __forceinline__ void zpass_pairs(C *buf, const C *__restrict__ twr, int rows, int nzs) {
+  constexpr int R1 = ZPlan<M>::R1, R2 = ZPlan<M>::R2, U = R1 / 2;
+  for (int w = threadIdx.x; w < rows * U; w += blockDim.x) {
+    int y, u;
+    zac_item<R2, U>(w, rows, y, u);
+    C *row = buf + (size_t)y * nzs;
+    const int ba = u, bb = u == 0 ? R1 / 2 : R1 - u;
+    C a[R2], b[R2];
+    zload_block<R2>(row + ba * R2, a);
+    zload_block<R2>(row + bb * R2, b);
+    if constexpr (!INV) {
+      dft<R2, -1>(a);
+      dft<R2, -1>(b);
+    }
+    auto pair = [&](C &p, C &q, int k, bool self) {
+      if constexpr (INV) c2r_pair(p, q, twr[k], self);
+      else r2c_pair(p, q, twr[k], self);
+    };
+    if (u == 0) {
+      // block 0 (k = R1 k1): k1 = 0 holds x0 + i xM (DC and Nyquist), k1 pairs with R2 - k1
+      a[0] = mk<C>(a[0].x + a[0].y, a[0].x - a[0].y);
+#pragma unroll
+      for (int k1 = 1; 2 * k1 <= R2; ++k1) pair(a[k1], a[R2 - k1], R1 * k1, 2 * k1 == R2);
+      // block R1/2 (k = R1/2 + R1 k1): k1 pairs with R2 - 1 - k1
+#pragma unroll
+      for (int k1 = 0; 2 * k1 <= R2 - 1; ++k1) pair(b[k1], b[R2 - 1 - k1], R1 / 2 + R1 * k1, 2 * k1 == R2 - 1);
+    } else {
+#pragma unroll
+      for (int k1 = 0; k1 < R2; ++k1) pair(a[k1], b[R2 - 1 - k1], u + R1 * k1, false);
+    }
+    if constexpr (INV) {
+      dft<R2, 1>(a);
+      dft<R2, 1>(b);
+    }
+    zstore_block<R2>(row + ba * R2, a);
+    zstore_block<R2>(row + bb * R2, b);
+  }
+}
+
 // Per-instance pointers travel as arguments so the constant parameter block
 // (PlaneArgs, UpdateArgs) is read in place and never copied.
 // FUSE 1 (PASS_STEP) / 2 (PASS_ADJOINT): only that pass is compiled, and the
@@ -1272,6 +1502,142 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
   fft_inverse<MaxRadix<NT>::value, GeomCols>(buf, SPLIT ? sm.twy + rows : sm.twy, a.py, gy);
   if constexpr (SPLIT) cross_stage<true>(buf, sm.twy, rows, a.fd_m, nzs);
 
+  const int f = (int)(plane / a.nx);
+  const int x = (int)(plane - (size_t)f * a.nx);
+  const bool real_field = f < u.S;
+  const int sys = real_field ? f : f - u.S;
+  const size_t N = (size_t)a.nx * ny * nz;
+  const size_t off = (plane * (size_t)ny + row0) * nz;   // first site of this CTA's rows
+  const size_t rbase = ((size_t)x * ny + row0) * nz;
+  const T invN = (T)u.invN;
+
+  // Update (FUSE 1) and adjoint (FUSE 2) passes of a two-stage z plan: the
+  // register-resident z passes A, B, C (see zpass_pairs).
+  bool zdone = false;
+  if constexpr (FUSE != 0) {
+    // (only when pass B, rows x R2 work items, keeps every thread busy in FP64
+    // or half of them in FP32: measured on 64^3 FP64 and 128x128x32 FP32)
+    const bool done = (FUSE == 1 || u.mode == PASS_ADJOINT) && core_sine_family(u.core.flag) &&
+                      (sizeof(T) == 4 ? 2 : 1) * rows * (a.pz.n / a.pz.radix[0]) >= (int)blockDim.x &&
+                      with_zfused(a.pz, [&](auto Mc) {
+      constexpr int MM = decltype(Mc)::value, R1 = ZPlan<MM>::R1, R2 = ZPlan<MM>::R2;
+      zpass_pairs<true, MM>(buf, twr, rows, nzs);
+      __syncthreads();
+      const C *twz = sm.twz;
+      const T *site = reinterpret_cast<const T *>(site_p);
+      const SineCore<T> sc = sine_core<T>(u.core, site);
+      const T *srow = sc.per_site ? site + (size_t)sys * N + rbase : nullptr;
+      const uint8_t *mrow = mask ? mask + (size_t)sys * N + rbase : nullptr;
+      const T cdt = (T)u.cd;
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};   // FUSE 1: |dxi|^2, sum xi; FUSE 2: the gradient sums
+      // B: inverse stage A, the per-site pass on the 2 R1 sites z = 2 (j + R2 r) + {0, 1}, forward stage A
+      for (int w = threadIdx.x; w < rows * R2; w += blockDim.x) {
+        int y, j;
+        zb_item<R2>(w, rows, y, j);
+        C *row = buf + (size_t)y * nzs;
+        const int base = y * nz + 2 * j;   // site of element j in this CTA's rows
+        // the item's old values first: their global loads are in flight during the transform
+        C ol[R1];
+#pragma unroll
+        for (int r = 0; r < R1; ++r) ol[r] = *reinterpret_cast<const C *>(xin + off + base + 2 * R2 * r);
+        C v[R1];
+#pragma unroll
+        for (int r = 0; r < R1; ++r) v[r] = row[j + R2 * r];
+        apply_twiddles<R1, true>(v, twz, j);
+        dft<R1, 1>(v);
+        T s0 = (T)0, s1 = (T)0, s2 = (T)0;   // four sites' sums in the compute precision, then FP64
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+          const int idx = base + 2 * R2 * r;
+          const C o = ol[r];
+          C m2 = mk<C>((T)1, (T)1);
+          if (real_field && srow) m2 = *reinterpret_cast<const C *>(srow + idx);
+          const T ov[2] = {o.x, o.y}, ev[2] = {v[r].x * invN, v[r].y * invN}, mv[2] = {m2.x, m2.y};
+          T nv[2];
+          if constexpr (FUSE == 1) {
+            const T tau = real_field ? (T)tau_p[sys] : (T)0;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+              if (real_field) {
+                T sv, cv;
+                sincospi_t<T>((T)2 * ov[q], &sv, &cv);
+                T force = sc.A * sv + sc.B * ((T)2 * sv * cv);
+                if (srow) force *= mv[q];
+                nv[q] = ov[q] - cdt * (ev[q] - tau + force);
+              } else {
+                nv[q] = ov[q] - cdt * ev[q];
+              }
+              if (mrow && mrow[idx + q]) nv[q] = ov[q];
+              const T d = nv[q] - ov[q];
+              s0 = fma_t(d, d, s0);
+              s1 += nv[q];
+            }
+          } else {
+            // lam_n = lam_{n+1} - cd (L lam + f''(xi_n) lam_{n+1}) on unmasked sites;
+            // the parameter gradients use lam_{n+1} and xi_n on the same sites
+            C xv2 = mk<C>((T)0, (T)0);
+            if (real_field) xv2 = *reinterpret_cast<const C *>(reinterpret_cast<const T *>(u.xfwd) +
+                                                                (size_t)sys * N + rbase + idx);
+            const T xv[2] = {xv2.x, xv2.y};
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+              const bool frozen = mrow && mrow[idx + q];
+              if (real_field) {
+                T sa, ca;
+                sincospi_t<T>((T)2 * xv[q], &sa, &ca);
+                const T s4 = (T)2 * sa * ca, c4 = (T)1 - (T)2 * sa * sa;
+                T d2 = sc.P * ca + sc.Q * c4, dp0 = sc.R * sa - sc.S * s4, dp1 = sc.U * s4;
+                if (srow) {
+                  d2 *= mv[q];
+                  dp0 *= mv[q];
+                  dp1 *= mv[q];
+                }
+                nv[q] = frozen ? ov[q] : ov[q] - cdt * (ev[q] + d2 * ov[q]);
+                if (!frozen) {
+                  s0 = fma_t(ov[q], dp0, s0);
+                  s1 = fma_t(ov[q], dp1, s1);
+                  s2 += ov[q];
+                }
+              } else {
+                nv[q] = frozen ? ov[q] : ov[q] - cdt * ev[q];
+              }
+            }
+          }
+          if (r & 1) {
+            acc[0] += (double)s0;
+            acc[1] += (double)s1;
+            acc[2] += (double)s2;
+            s0 = s1 = s2 = (T)0;
+          }
+          v[r] = mk<C>(nv[0], nv[1]);
+          if (ok) *reinterpret_cast<C *>(xout + off + idx) = v[r];
+        }
+        if (fwd) {
+          dft<R1, -1>(v);
+          apply_twiddles<R1, false>(v, twz, j);
+#pragma unroll
+          for (int r = 0; r < R1; ++r) row[j + R2 * r] = v[r];
+        }
+      }
+      if constexpr (FUSE == 1) {
+        double vv[2] = {acc[0], real_field ? acc[1] : 0.0};
+        plane_sum<SPLIT>(vv, sm.red, partials + 2 * plane);
+      } else {
+        plane_sum<SPLIT, 4, true>(acc, sm.red, u.gpart + 4 * plane);   // summed over the backward steps
+      }
+      if (fwd) {
+        // C: forward stage B and the real-to-complex pairs; zero row padding
+        __syncthreads();
+        zpass_pairs<false, MM>(buf, twr, rows, nzs);
+        for (int y = threadIdx.x; y < rows; y += blockDim.x)
+          for (int q = a.nzh; q < a.nzp; ++q) buf[(size_t)y * nzs + q] = mk<C>((T)0, (T)0);
+      }
+    });
+    zdone = done;
+  }
+
+  // the generic passes; returns whether the forward y side follows
+  auto generic = [&]() -> bool {
   // complex-to-real packing: Zin[k] = A + i w D, Zin[M-k] = conj(A - i w D),
   // A = X[k] + conj X[M-k], D = X[k] - conj X[M-k], w = exp(+2 pi i k / nz)
   // k = 0, one row per thread: slot 0 holds x0 + i xM (the real kz = 0 and
@@ -1305,15 +1671,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
 
   // fused GSFE force + applied stress + masked explicit Euler update,
   // VN consecutive z per thread, two vectors in flight per iteration
-  const int f = (int)(plane / a.nx);
-  const int x = (int)(plane - (size_t)f * a.nx);
-  const bool real_field = f < u.S;
-  const int sys = real_field ? f : f - u.S;
-  const size_t N = (size_t)a.nx * ny * nz;
-  const size_t off = (plane * (size_t)ny + row0) * nz;   // first site of this CTA's rows
-  const size_t rbase = ((size_t)x * ny + row0) * nz;
   const T *bufr = reinterpret_cast<const T *>(buf);
-  const T invN = (T)u.invN;
   const int nvec = nz / VN;
   const int total = rows * nvec;
   const FastDiv &dv = a.fd_nvec;
@@ -1326,7 +1684,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
       for (int q = 0; q < VN; ++q) e[q] *= invN;
       if (ok) *reinterpret_cast<V *>(xout + off + y * nz + zq * VN) = *reinterpret_cast<V *>(e);
     }
-    return;
+    return false;
   }
   if (FUSE == 0 && u.mode == PASS_ENERGY) {
     // 1/2 xi . (L xi), f(Re xi) and -tau Re xi, summed over the plane (FP64)
@@ -1351,7 +1709,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
     }
     double v[4] = {e_el, e_core, e_app, 0.0};
     plane_sum<SPLIT>(v, sm.red, u.gpart + 4 * plane);
-    return;
+    return false;
   }
   if (FUSE != 1 && u.mode == PASS_ADJOINT) {
     // lam_n = lam_{n+1} - cd (L lam + f''(xi_n) lam_{n+1}) on unmasked sites
@@ -1400,12 +1758,13 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
     if constexpr (FUSE == 2) {
       if (fwd) {   // the next backward step's spectrum of the new lambda
         __syncthreads();
-        fwd_planes_compute<T, NT, SPLIT>(sm, a, const_cast<cx<T> *>(spec), plane, rows, row0, ok);
+        fwd_planes_z<T, NT>(sm, a, rows);
       }
+      return fwd;
     }
-    return;
+    return false;
   }
-  if constexpr (FUSE == 2) return;
+  if constexpr (FUSE == 2) return false;
   else {
   // update pass only: tau, mask and per-site GSFE are read from here on
   const T tau = real_field ? (T)tau_p[sys] : (T)0;
@@ -1470,9 +1829,17 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
   if constexpr (FUSE == 1) {
     if (fwd) {
       __syncthreads();
-      fwd_planes_compute<T, NT, SPLIT>(sm, a, const_cast<cx<T> *>(spec), plane, rows, row0, ok);
+      fwd_planes_z<T, NT>(sm, a, rows);
     }
+    return fwd;
   }
+  return false;
+  }
+  };
+  const bool tail = zdone ? fwd : generic();
+  // the forward y side of the next step's spectrum (one call site per kernel)
+  if constexpr (FUSE != 0) {
+    if (tail) fwd_planes_tail<T, NT, SPLIT>(sm, a, const_cast<cx<T> *>(spec), plane, rows, row0, ok);
   }
 }
 

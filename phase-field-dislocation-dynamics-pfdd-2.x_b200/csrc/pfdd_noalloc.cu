@@ -93,7 +93,7 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   FftPlan px, py, pz;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   if (nx < 2 || ny < 2 || nz < 4 || nx > 1024 || ny > 1024 || nz > 1024 || (nx & 1) || (ny & 1) || (nz % 4) ||
-      !make_plan(nx, px) || !make_plan(ny, py) || !make_plan(nz / 2, pz))
+      !make_plan(nx, px) || !make_plan(ny, py) || !make_zplan(nz / 2, pz))
     return nerr(PFDD_EUNSUPPORTED, "grid extents must be even, 2^a 3^b, <= 1024, nz a multiple of 4");
   const int M = nz / 2, nzh = M + 1, nzp = nzh;  // FP64 rows are whole 16-byte units
   const int F = 2 * S;                           // Re and Im fields

@@ -54,6 +54,20 @@ inline bool make_plan(int n, FftPlan &p, int maxr = 16) {
   return true;
 }
 
+// z plans (length M = nz/2 of the packed real rows): radix 8 then M/8 for
+// M = 16, 32, 64, so that the register-resident z passes hold 8 complex
+// values per thread in their middle pass; the greedy plan otherwise.  The
+// kernels' ZPlan<M> follows the same rule.
+inline bool make_zplan(int M, FftPlan &p, int maxr = 16) {
+  if (!((M == 16 || M == 32 || M == 64) && maxr >= 8)) return make_plan(M, p, maxr);
+  const int r2 = M / 8;
+  p.n = M;
+  p.nst = 2;
+  p.radix[0] = 8;  p.L[0] = M;  p.twstep[0] = 1; p.per[0] = FastDiv(M / 8); p.lr[0] = FastDiv(M / 8);
+  p.radix[1] = r2; p.L[1] = r2; p.twstep[1] = 8; p.per[1] = FastDiv(8);     p.lr[1] = FastDiv(1);
+  return true;
+}
+
 // Host-built divisors of the plane and pencil kernels (after the integer
 // fields of the argument block are set).
 template <typename T> inline void set_plane_divisors(PlaneArgs &pa, int rows) {

@@ -63,3 +63,29 @@ def test_refused_checkpoints_leave_the_state(tmp_path):
             assert e.value.code == -1
         after = st.get_state(0)
         assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
+
+
+def test_carrier_is_layout_independent(tmp_path, monkeypatch):
+    """The file holds the Nyquist carrier of Im xi in frequency order, so a
+    checkpoint written by a handle whose planes run split over 2-CTA
+    clusters (its y transforms then keep a different slot order) resumes in
+    a handle with whole planes: the continued run matches the writer's own
+    continuation to FP64 round-off (the two layouts sum in different orders)."""
+    w = small_loop(16)
+    path = str(tmp_path / "split.ckp")
+    monkeypatch.setenv("PFDD_PLANE_SPLIT", "1")
+    with capi.Stepper.from_workloads([w], precision=capi.FP64, imag_mode=capi.IMAG_NYQUIST) as a:
+        a.set_state(0, w.xi0)
+        a.advance(6)
+        a.checkpoint_save(0, path)
+        a.advance(6)
+        want = a.get_state(0)
+    monkeypatch.setenv("PFDD_PLANE_SPLIT", "0")
+    with capi.Stepper.from_workloads([w], precision=capi.FP64, imag_mode=capi.IMAG_NYQUIST) as b:
+        b.checkpoint_load(0, path)
+        b.advance(6)
+        got = b.get_state(0)
+    scale = max(np.abs(want[0]).max(), np.abs(want[1]).max())
+    assert np.abs(got[0] - want[0]).max() <= 1e-10 * scale
+    assert np.abs(got[1] - want[1]).max() <= 1e-10 * scale
+    assert np.abs(want[1]).max() > 1e-6   # the carrier is not trivially zero
