@@ -97,7 +97,7 @@ struct Instance {
   DevBuf xi[2];        // ping-pong real fields [F][N]
   int cur = 0;
   DevBuf spec;         // [F][nx][ny][nzh] complex
-  DevBuf partials;     // 2 * F * nx doubles
+  DevBuf partials;     // 2 sums x F * nx planes (x 2 CTAs of a split plane)
   DevBuf stats;        // 2 * cap doubles
   int stats_cap = 0;
   DevBuf small;        // tau[12], sigma[9], dsigma[9], flags[8]
@@ -351,7 +351,7 @@ pfdd_status setup_instance(pfdd_gpu *h, Instance &I) {
   }
   CUDA_TRY(h, I.spec.alloc((size_t)I.F * I.nx * I.ny * I.nzp * sizeof(C)));
   h->device_bytes += I.spec.bytes;
-  CUDA_TRY(h, I.partials.alloc(2 * (size_t)I.F * I.nx * sizeof(double)));
+  CUDA_TRY(h, I.partials.alloc(4 * (size_t)I.F * I.nx * sizeof(double)));   // 2 sums x 2 CTAs of a split plane
   h->device_bytes += I.partials.bytes;
   CUDA_TRY(h, I.small.alloc((PFDD_MAXS + 26) * sizeof(double)));
   CUDA_TRY(h, cudaMemset(I.small.p, 0, (PFDD_MAXS + 26) * sizeof(double)));
@@ -606,8 +606,10 @@ void enqueue_step_fused(Instance &I, cudaStream_t st, bool fwd, const AdjointPas
   else k_step_planes<T, NP, false><<<planes, NP, I.smem_update, st>>>(spec, xin, xout, pa, ua, partials, (int)fwd);
   if (!stats) return;
   const bool nyq = I.imag == IMAG_NYQ;
-  k_finalize<<<1, 1024, 0, st>>>(partials, planes, I.stats.as<double>(), 0, 0.0, flags, flags + 1, flags + 2,
-                                 nyq ? I.ppart.as<double>() : nullptr, nyq ? I.ntiles : 0, 1.0 / (double)I.N);
+  // a split plane's CTAs write a partial each (plane_sum_slots)
+  k_finalize<<<1, 1024, 0, st>>>(partials, I.split ? 2 * planes : planes, I.stats.as<double>(), 0, 0.0, flags,
+                                 flags + 1, flags + 2, nyq ? I.ppart.as<double>() : nullptr, nyq ? I.ntiles : 0,
+                                 1.0 / (double)I.N);
 }
 
 // ------------------------------------------------------------ batched groups
@@ -850,7 +852,8 @@ void enqueue_group_step(Instance &L, const Group &G, cudaStream_t st, double tol
   launch_step_tab<T>(L, B, st, tab, pa, ua, fwd);
   if (ev) cudaEventRecord(ev[2], st);
   const bool nyq = L.imag == IMAG_NYQ;
-  k_finalize_tab<<<B, 1024, 0, st>>>(tab, planes, nyq ? L.ntiles : 0, 1.0 / (double)L.N, tol);
+  k_finalize_tab<<<B, 1024, 0, st>>>(tab, L.split ? 2 * planes : planes, nyq ? L.ntiles : 0, 1.0 / (double)L.N,
+                                     tol);
   if (ev) cudaEventRecord(ev[3], st);
 }
 

@@ -330,6 +330,21 @@ __device__ __forceinline__ void plane_sum(double (&v)[NV], double *scratch, doub
   }
 }
 
+// The same sums written without a cluster barrier (whose release fence would
+// wait for the plane pass's global stores): slot `plane`, or for a split
+// plane each CTA its own slot 2 plane + rank, which the reduction kernel adds
+// in order.  out: NV doubles per slot.
+template <bool SPLIT, int NV>
+__device__ __forceinline__ void plane_sum_slots(double (&v)[NV], double *scratch, double *out, size_t plane) {
+  block_reduce<NV>(v, scratch);
+  if (threadIdx.x == 0) {
+    size_t slot = plane;
+    if constexpr (SPLIT) slot = 2 * plane + cooperative_groups::this_cluster().block_rank();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) out[NV * slot + q] = v[q];
+  }
+}
+
 // The cross-CTA radix-2 stage of a split plane, over the nzh slot columns of
 // the ny/2 local rows.  Forward (decimation in frequency): lo = a + b,
 // hi = (a - b) W_ny^y with a, b rows y and y + ny/2; inverse (decimation in
@@ -1621,7 +1636,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
       }
       if constexpr (FUSE == 1) {
         double vv[2] = {acc[0], real_field ? acc[1] : 0.0};
-        plane_sum<SPLIT>(vv, sm.red, partials + 2 * plane);
+        plane_sum_slots<SPLIT>(vv, sm.red, partials, plane);
       } else {
         plane_sum<SPLIT, 4, true>(acc, sm.red, u.gpart + 4 * plane);   // summed over the backward steps
       }
@@ -1825,7 +1840,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
   if (u.core.flag == 3) update_loop(std::integral_constant<int, 3>());
   else update_loop(std::integral_constant<int, 0>());
   double v[2] = {dsq, sum};
-  plane_sum<SPLIT>(v, sm.red, partials + 2 * plane);
+  plane_sum_slots<SPLIT>(v, sm.red, partials, plane);
   if constexpr (FUSE == 1) {
     if (fwd) {
       __syncthreads();
