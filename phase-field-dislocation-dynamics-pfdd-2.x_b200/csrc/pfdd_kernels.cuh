@@ -87,6 +87,12 @@ template <typename T> struct GreenT {
   T epso[PFDD_MAXS][6];   // eps^a / mu: xx yy zz, xy+yx, xz+zx, yz+zy (contracts Sig)
   T c2;                   // 1 / (2 C44), Green's function prefactor, fft_fftw_slab.cpp:597
   T c1nu;                 // 1 / (1 - nu) (Voigt nu)
+  // tf = 1 when sigo[a] = lam o epso[a] for every system (glide systems,
+  // b . n = 0, so sigma^a = C44 (eps^a + eps^a^T)): lam = 2 C44 on the
+  // diagonal, C44 off it, and each output off the Nyquist planes is the one
+  // contraction eps^a : Z with Z = Sig + lam o Tq (green_z)
+  T lam[6];
+  int tf;
 };
 struct Green {
   double four[3][3];
@@ -678,6 +684,28 @@ __device__ __forceinline__ void green_accumulate(const GreenT<T> &g, int b, C x,
   for (int q = 0; q < 6; ++q) { sig[q].x += s[q] * x.x; sig[q].y += s[q] * x.y; }
 }
 
+// Z = Sig + lam o Tq (zero at k = 0) for GreenT::tf, and the output
+// eps^a : Z / mu of system a: 12 multiply-adds per output instead of 24
+template <typename T, typename C>
+__device__ __forceinline__ void green_z(const GreenT<T> &g, const C (&sig)[6], const C (&Tq)[6], bool nz, C (&Z)[6]) {
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+    Z[q] = nz ? mk<C>(fma_t(g.lam[q], Tq[q].x, sig[q].x), fma_t(g.lam[q], Tq[q].y, sig[q].y)) : mk<C>((T)0, (T)0);
+}
+template <typename T, typename C>
+__device__ __forceinline__ C green_out_z(const GreenT<T> &g, int a, const C (&Z)[6]) {
+  const T *e = g.epso[a];
+  T ex = (T)0, ey = (T)0, fx = (T)0, fy = (T)0;   // two chains
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    ex = fma_t(e[q], Z[q].x, ex);
+    ey = fma_t(e[q], Z[q].y, ey);
+    fx = fma_t(e[3 + q], Z[3 + q].x, fx);
+    fy = fma_t(e[3 + q], Z[3 + q].y, fy);
+  }
+  return mk<C>(ex + fx, ey + fy);
+}
+
 // The same two operations with one system's constants read from a
 // shared-memory stage as pairs (cs: sig[6] per system; co: epso[6], sigo[6]
 // per system): 3 and 6 vector loads instead of 6 and 12 scalar constant loads
@@ -964,6 +992,19 @@ __device__ __forceinline__ void xpencil_body(cx<T> *__restrict__ spec, const Pen
     // B(k) = B(index -k) off the Nyquist planes: Er = B Xr
     C Tp[6];
     const bool zp = green_tensor<T>(g, sr, kx, ky, kz, Tp);
+    if (SC == 0 && !STAGED && g.tf) {   // (with S unrolled the two-term form's constants are immediates)
+      C Z[6];
+      green_z<T>(g, sr, Tp, zp, Z);
+      int aa = 0;
+#pragma unroll(SC > 0 ? SC / 2 : 1)
+      for (; aa + 1 < S; aa += 2) {   // two outputs in flight
+        const C o0 = green_out_z<T>(g, aa, Z), o1 = green_out_z<T>(g, aa + 1, Z);
+        pk[aa * fs] = o0;
+        pk[(aa + 1) * fs] = o1;
+      }
+      if (aa < S) pk[aa * fs] = green_out_z<T>(g, aa, Z);
+      continue;
+    }
     {
       int aa = 0;
 #pragma unroll(SC > 0 ? SC / 2 : 1)

@@ -4,6 +4,7 @@
 // the stress state (what FFTW_Slab::setup computes in the reference,
 // fft_fftw_slab.cpp:111-119).
 #pragma once
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <type_traits>
@@ -181,6 +182,16 @@ inline void build_green(const pfdd_instance_desc &d, Green &g) {
       }
     t.c2 = (T)g.c2;
     t.c1nu = (T)g.c1nu;
+    // trace-free systems: sigma^a/mu = lam o (eps^a/mu) with lam = (2 C44 x3, C44 x3)
+    const double lam[6] = {2 * C44, 2 * C44, 2 * C44, C44, C44, C44};
+    double dev = 0.0, scale = 0.0;
+    for (int a = 0; a < d.n_slip; ++a)
+      for (int q = 0; q < 6; ++q) {
+        dev = std::max(dev, std::fabs(g.sig[a][q] - lam[q] * g.eps[a][q]));
+        scale = std::max(scale, std::fabs(g.sig[a][q]));
+      }
+    for (int q = 0; q < 6; ++q) t.lam[q] = (T)lam[q];
+    t.tf = dev <= 1e-13 * scale ? 1 : 0;
   };
   fill(g.d);
   fill(g.f);
