@@ -82,6 +82,7 @@ struct Instance {
   pfdd_instance_desc d;
   int S, F, imag;
   int nx, ny, nz, nzh, nzp, nzs, M;
+  int zfused = 1;      // register-resident z passes allowed (PFDD_ZFUSED=0 at creation: off)
   size_t N;
   FftPlan px, py, pz;
   int ccols, fstride, ntiles;
@@ -432,6 +433,7 @@ void fill_plane_args(const Instance &I, PlaneArgs &pa) {
   pa.negy = I.negy;
   pa.kord = I.kord;
   set_plane_divisors<T>(pa, I.split ? I.ny / 2 : I.ny);
+  pa.zfused = I.zfused;
 }
 
 template <typename T>
@@ -2167,6 +2169,9 @@ pfdd_status pfdd_gpu_create(const pfdd_instance_desc *descs, int n_instances, co
       if (!strcmp(env, "0")) I->split = false;
       else if (!strcmp(env, "1")) I->split = true;
     }
+    // PFDD_ZFUSED=0: the update and adjoint passes keep the generic staged z
+    // passes (same results to round-off; the tests compare the two)
+    if (const char *env = getenv("PFDD_ZFUSED")) I->zfused = strcmp(env, "0") ? 1 : 0;
     const int maxr = (o.precision == PFDD_FP32)
                          ? std::min(MaxRadix<Threads<float>::plane>::value, MaxRadix<Threads<float>::half>::value)
                          : std::min(MaxRadix<Threads<double>::plane>::value, MaxRadix<Threads<double>::half>::value);

@@ -141,6 +141,7 @@ struct PlaneArgs {
   // divisors built on the host: rows per CTA (ny, or ny/2 when split),
   // nz / vector width, M, M/2 (real-to-complex pairs per row)
   FastDiv fd_rows, fd_nvec, fd_m, fd_mh;
+  int zfused;                 // 1: update and adjoint passes may take the register-resident z passes
 };
 
 struct PencilArgs {
@@ -1573,7 +1574,7 @@ __device__ __forceinline__ void inv_update_body(const cx<T> *spec, const T *__re
   if constexpr (FUSE != 0) {
     // (only when pass B, rows x R2 work items, keeps every thread busy in FP64
     // or half of them in FP32: measured on 64^3 FP64 and 128x128x32 FP32)
-    const bool done = (FUSE == 1 || u.mode == PASS_ADJOINT) && core_sine_family(u.core.flag) &&
+    const bool done = a.zfused && (FUSE == 1 || u.mode == PASS_ADJOINT) && core_sine_family(u.core.flag) &&
                       (sizeof(T) == 4 ? 2 : 1) * rows * (a.pz.n / a.pz.radix[0]) >= (int)blockDim.x &&
                       with_zfused(a.pz, [&](auto Mc) {
       constexpr int MM = decltype(Mc)::value, R1 = ZPlan<MM>::R1, R2 = ZPlan<MM>::R2;

@@ -202,6 +202,7 @@ extern "C" pfdd_status pfdd_gl_step_noalloc(const pfdd_instance_desc *desc, cons
   pa.py = py; pa.pz = pz;
   pa.nx = nx; pa.ny = ny; pa.nz = nz; pa.nzh = nzh; pa.nzp = nzp; pa.nzs = nzp; pa.M = M;
   pa.S = S; pa.F = F;
+  pa.zfused = 1;
   pa.tw_y = tw_y; pa.tw_z = tw_z; pa.tw_r = tw_r;
   pa.posM = t_posM - htab + tab;
   pa.negy = t_neg - htab + tab;
