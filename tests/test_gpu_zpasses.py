@@ -65,6 +65,8 @@ def test_register_resident_z_passes_match_generic(monkeypatch, prec, tol, name, 
     np.testing.assert_allclose(a[3], b[3], rtol=10 * tol, atol=10 * tol * np.abs(b[3]).max())
     # the dynamics moved the state: the comparison is not of two unchanged inputs
     assert np.abs(b[0] - w.xi0).max() > 1e-4
+    # and the two forms did run: their plane sums add the sites in other orders
+    assert not np.array_equal(a[2], b[2])
 
 
 @pytest.mark.parametrize("split", [None, True])
