@@ -975,7 +975,7 @@ pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *si
   // before sigma += dsigma (solve_GL.cpp:110-155), while pfdd_gpu_advance has
   // already added the increment when it returns
   double sig[9], sr[3][3];
-  const int nb = 296;
+  const int nb = 4 * h->nsm;   // reduction blocks of the field sums
   DevBuf &part = I.ss_part, &spec6 = I.ss_spec6, &strain6 = I.ss_strain6, &e9 = I.ss_e9, &s9 = I.ss_s9,
          &fpart = I.ss_fpart;
   const size_t ncols = (size_t)I.ny * I.nzp;
@@ -996,7 +996,8 @@ pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *si
   // strain pencils: tile width reduced until max(F, 6) fields fit
   const int FB = std::max(I.F, 6);
   int cc = I.ccols;
-  auto bytes = [&](int c) { return ((size_t)FB * I.nx * c + I.nx) * sizeof(C); };
+  // field stride padded against bank conflicts, as the x-pencil pass's
+  auto bytes = [&](int c) { return ((size_t)FB * pencil_fstride<T>(I, c) + I.nx) * sizeof(C); };
   while (cc > 1 && bytes(cc) > 227 * 1024) cc >>= 1;
   if (bytes(cc) > 227 * 1024 || ncols % cc)
     return fail(h, PFDD_EUNSUPPORTED, "strain pencil of %d x %d fields does not fit shared memory", I.nx, FB);
@@ -1010,7 +1011,7 @@ pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *si
   pe.tw_x = I.tw_x.p;
   pe.kx_of = I.kx_of; pe.ky_of = I.ky_of; pe.kz_of = I.kz_of;
   pe.mode = PASS_STEP;
-  pe.fstride = I.nx * cc;
+  pe.fstride = pencil_fstride<T>(I, cc);
   pe.aux = I.aux.p;
   pe.sx_n = I.sx_n; pe.sy_n = I.sy_n;
   pe.g = I.green;
@@ -1039,8 +1040,14 @@ pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *si
   // per-system sums of Re xi of the current state, read back once the
   // transforms are queued (the host forms the stress constants from them)
   k_field_sums<T><<<nb, 256, 0, st>>>(I.xi[I.cur].as<T>(), S, N, part.as<double>());
-  std::vector<double> hp((size_t)nb * S);
+  // averages only: the six strain sums are all the device still has to add
+  // (the stress average is linear in them and in the sums of Re xi above)
+  const bool ave_only = !eps && !sigma;
+  if (ave_only) k_field_sums<T><<<nb, 256, 0, st>>>(strain6.as<T>(), 6, N, fpart.as<double>());
+  std::vector<double> hp((size_t)nb * S), h6(ave_only ? (size_t)nb * 6 : 0);
   CUDA_TRY(h, cudaMemcpyAsync(hp.data(), part.p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (ave_only)
+    CUDA_TRY(h, cudaMemcpyAsync(h6.data(), fpart.p, h6.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(h, cudaStreamSynchronize(st));
   const StressArgs &sa = I.stress;
   if (I.advanced)
@@ -1095,6 +1102,38 @@ pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *si
   sp.C12 = C12;
   sp.S = S;
 
+  auto neumaier = [](const double *v, int n, int stride) {
+    double t = 0.0, c = 0.0;
+    for (int b = 0; b < n; ++b) {
+      const double x = v[(size_t)b * stride], u = t + x;
+      c += (std::fabs(t) >= std::fabs(x)) ? (t - u) + x : (x - u) + t;
+      t = u;
+    }
+    return t + c;
+  };
+  if (ave_only) {
+    // <eps_q> = <strain_q> + avepst_q; <X_q> = <eps_q> - sum_s e6[s][q] <Re xi_s> - avepsts_q;
+    // <sigma_ij> = 2 C44 <X_q> + C12 tr<X> delta_ij + sigma_rot mu (k_stress_fields, averaged)
+    int fl[4];
+    CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
+    if (fl[3]) return fail(h, PFDD_ETIMEOUT, "a bounded device wait ran out");
+    double em[6], xm[6];
+    for (int q = 0; q < 6; ++q) {
+      em[q] = neumaier(h6.data() + q, nb, 6) / (double)N + sp.avepst6[q];
+      double d = 0.0;
+      for (int a = 0; a < S; ++a) d += sp.e6[a][q] * mean[a];
+      xm[q] = em[q] - d - sp.avepsts6[q];
+    }
+    const int map[9] = {0, 3, 4, 3, 1, 5, 4, 5, 2};
+    const double tr = xm[0] + xm[1] + xm[2];
+    for (int ij = 0; ij < 9; ++ij) {
+      const int i = ij / 3, j = ij - 3 * i, q = map[ij];
+      if (ave_eps) ave_eps[ij] = em[q];
+      if (ave_sigma) ave_sigma[ij] = 2.0 * C44 * xm[q] + (i == j ? C12 * tr : 0.0) + sp.sigmu[ij];
+    }
+    return PFDD_OK;
+  }
+
   // pointwise strain and stress, FP64 sums of both
   k_stress_fields<T><<<nb, 256, 0, st>>>(strain6.as<T>(), I.xi[I.cur].as<T>(), N, sp,
                                           eps ? e9.as<double>() : nullptr, sigma ? s9.as<double>() : nullptr,
@@ -1108,13 +1147,7 @@ pfdd_status strain_stress_impl(pfdd_gpu *h, Instance &I, double *eps, double *si
   CUDA_TRY(h, cudaMemcpy(fl, I.flags(), sizeof fl, cudaMemcpyDeviceToHost));
   if (fl[3]) return fail(h, PFDD_ETIMEOUT, "a bounded device wait ran out");
   for (int q = 0; q < 18; ++q) {
-    double t = 0.0, c = 0.0;
-    for (int b = 0; b < nb; ++b) {   // Neumaier-compensated
-      const double v = hf[(size_t)b * 18 + q], u = t + v;
-      c += (std::fabs(t) >= std::fabs(v)) ? (t - u) + v : (v - u) + t;
-      t = u;
-    }
-    const double m = (t + c) / (double)N;
+    const double m = neumaier(hf.data() + q, nb, 18) / (double)N;   // Neumaier-compensated
     if (q < 9 && ave_eps) ave_eps[q] = m;
     if (q >= 9 && ave_sigma) ave_sigma[q - 9] = m;
   }

@@ -2384,11 +2384,26 @@ __global__ void __launch_bounds__(NT, 2) k_strain_pencil(const cx<T> *__restrict
   C *twx = buf + (size_t)FB * fst;
   const size_t col0 = (size_t)blockIdx.x * cc, ncols = a.ncols;
   const int per = nx * cc;
-  for (int i = threadIdx.x; i < F * per; i += blockDim.x) {
-    const int f = i / per, rem = i - f * per, x = rem / cc, c = rem - x * cc;
-    buf[(size_t)f * fst + rem] = spec[((size_t)f * nx + x) * ncols + col0 + c];
+  // (field, x) rows of the tile in 16-byte chunks (cp.async, as the x-pencil
+  // pass) when a row is whole chunks; element by element otherwise
+  const int cpr = (int)(cc * sizeof(C) / 16);
+  const bool chunks = cpr > 0 && (cc * sizeof(C)) % 16 == 0;
+  if (chunks) {
+    for (int q = threadIdx.x; q < F * nx * cpr; q += blockDim.x) {
+      const int fx = a.fd_cpr.div(q), ch = q - fx * cpr;
+      const int f = a.fd_nx.div(fx), x = fx - f * nx;
+      cp_async16(reinterpret_cast<char *>(buf + (size_t)f * fst + (size_t)x * cc) + 16 * ch,
+                 reinterpret_cast<const char *>(spec + (size_t)fx * ncols + col0) + 16 * ch);
+    }
+  } else {
+    for (int f = 0; f < F; ++f)
+      for (int rem = threadIdx.x; rem < per; rem += blockDim.x) {
+        const int x = a.fd_cc.div(rem), c = rem - x * cc;
+        buf[(size_t)f * fst + (size_t)x * cc + c] = spec[((size_t)f * nx + x) * ncols + col0 + c];
+      }
   }
   load_table(twx, a.tw_x, nx);
+  if (chunks) cp_async_wait_all();
   __syncthreads();
   Batch gx{F * cc, cc, 1, fst, cc, true, a.fd_fcc, a.fd_cc};
   fft_forward<MaxRadix<NT>::value, GeomPencil>(buf, twx, a.px, gx);
@@ -2399,7 +2414,7 @@ __global__ void __launch_bounds__(NT, 2) k_strain_pencil(const cx<T> *__restrict
     const int sx = a.fd_cc.div(w), c = w - sx * cc;
     const int col = (int)(col0 + c);
     const int sy = a.fd_nzp.div(col), sz = col - sy * a.nzp;
-    C *pk = buf + sx * cc + c;
+    C *pk = buf + (size_t)sx * cc + c;
     C o[6];
 #pragma unroll
     for (int q = 0; q < 6; ++q) o[q] = mk<C>((T)0, (T)0);
@@ -2454,10 +2469,21 @@ __global__ void __launch_bounds__(NT, 2) k_strain_pencil(const cx<T> *__restrict
   __syncthreads();
   Batch g6{6 * cc, cc, 1, fst, cc, true, a.fd_6cc, a.fd_cc};
   fft_inverse<MaxRadix<NT>::value, GeomPencil>(buf, twx, a.px, g6);
-  for (int i = threadIdx.x; i < 6 * per; i += blockDim.x) {
-    const int f = i / per, rem = i - f * per, x = rem / cc, c = rem - x * cc;
-    out6[((size_t)f * nx + x) * ncols + col0 + c] = buf[(size_t)f * fst + rem];
+  if (chunks) {
+    for (int q = threadIdx.x; q < 6 * nx * cpr; q += blockDim.x) {
+      const int fx = a.fd_cpr.div(q), ch = q - fx * cpr;
+      const int f = a.fd_nx.div(fx), x = fx - f * nx;
+      *reinterpret_cast<float4 *>(reinterpret_cast<char *>(out6 + (size_t)fx * ncols + col0) + 16 * ch) =
+          *reinterpret_cast<const float4 *>(reinterpret_cast<const char *>(buf + (size_t)f * fst + (size_t)x * cc) +
+                                            16 * ch);
+    }
+    return;
   }
+  for (int f = 0; f < 6; ++f)
+    for (int rem = threadIdx.x; rem < per; rem += blockDim.x) {
+      const int x = a.fd_cc.div(rem), c = rem - x * cc;
+      out6[((size_t)f * nx + x) * ncols + col0 + c] = buf[(size_t)f * fst + (size_t)x * cc + c];
+    }
 }
 
 // ------------------------------------------------------------ conductivity
@@ -2585,11 +2611,27 @@ __global__ void k_cond_update(T *__restrict__ cxi, const T *__restrict__ fr, con
 // Per-system sums of Re xi ([S][N], compute precision) in FP64: part[blk * S + s].
 template <typename T>
 __global__ void k_field_sums(const T *__restrict__ xr, int S, size_t N, double *__restrict__ part) {
+  // 16-byte loads (N is a multiple of 4: nx and ny are even), one FP64
+  // accumulator per vector lane, several loads in flight per thread
+  using V = typename Vec<T>::type;
+  constexpr int VN = Vec<T>::n;
   __shared__ double red[64];
+  const size_t nv = N / VN, stride = (size_t)gridDim.x * blockDim.x;
   for (int s0 = 0; s0 < S; ++s0) {
-    double acc = 0.0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x)
-      acc += (double)xr[(size_t)s0 * N + i];
+    const V *p = reinterpret_cast<const V *>(xr + (size_t)s0 * N);
+    double a[VN];
+#pragma unroll
+    for (int q = 0; q < VN; ++q) a[q] = 0.0;
+#pragma unroll 4
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nv; i += stride) {
+      T t[VN];
+      *reinterpret_cast<V *>(t) = p[i];
+#pragma unroll
+      for (int q = 0; q < VN; ++q) a[q] += (double)t[q];
+    }
+    double acc = a[0];
+#pragma unroll
+    for (int q = 1; q < VN; ++q) acc += a[q];
     double out[2];
     block_sum2(acc, 0.0, red, out);
     if (threadIdx.x == 0) part[(size_t)blockIdx.x * S + s0] = out[0];

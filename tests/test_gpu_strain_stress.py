@@ -46,5 +46,7 @@ def test_strain_stress_matches_oracle(make, prec):
     assert np.abs(sig - so).max() <= tol * ss
     assert np.abs(ave_eps - aeo).max() <= tol * se
     assert np.abs(ave_sig - aso).max() <= tol * ss
-    np.testing.assert_array_equal(ave_eps, ave_eps2)
-    np.testing.assert_array_equal(ave_sig, ave_sig2)
+    # without fields the stress average is formed from the sums it is linear in
+    # (<strain> and <Re xi>): the same averages to round-off
+    np.testing.assert_allclose(ave_eps2, ave_eps, rtol=0, atol=1e-12 * se)
+    np.testing.assert_allclose(ave_sig2, ave_sig, rtol=0, atol=1e-12 * ss)
