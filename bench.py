@@ -9,7 +9,9 @@ reductions; synthetic seeded input.  A "step" is one GL iteration over the
 whole grid; the metric is site-slip updates per second (S * N per step).
 
   value     device time of K steps (CUDA events on the stepper's stream,
-            inputs resident in HBM; working set > L2, no flush needed)
+            inputs resident in HBM; the default workload's working set > L2, no
+            flush needed; smaller workloads say in config.l2 that they stay
+            L2-resident)
   e2e       the same metric through the C ABI from pinned host memory:
             set_state (H2D) + advance(E steps) + get_state (D2H), E =
             --e2e-steps (default 5000, the run length of this configuration)
@@ -675,7 +677,10 @@ def main():
                        "parallelism": ("%d instances split over %d ranks" % (len(ws_all), world)
                                        if scaling == "strong" else "replicas x%d" % world),
                        "pencil_tile_widths": tile_widths if tile_widths is not None else "set-up rule",
-                       "l2": "working set %.2f GB > 126 MB L2 (no flush)" % (dev_bytes / 1e9)},
+                       "l2": (("working set %.2f GB > 126 MB L2 (no flush)" % (dev_bytes / 1e9))
+                              if dev_bytes > 126e6 else
+                              ("working set %.3f GB < 126 MB L2: stays L2-resident from step to step (not "
+                               "flushed; the default fcc256 line exceeds L2)" % (dev_bytes / 1e9)))},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches_per_step * args.steps + 2 * (launches_per_step // 3),
         }
