@@ -499,6 +499,28 @@ def adjoint_ratio(st, w, prec, stream, local, steps=500, ckpt=50):
     return out
 
 
+def diagnostic_only(args):
+    """pfdd_gpu_strain_stress (averages only, as DiagStress reads them between
+    dumps) on the first instance of the workload: one untimed call, then four
+    event-timed calls; prints one JSON line (not a bench line)."""
+    import statistics
+    import torch
+    from pfdd_b200 import capi
+    ws, w_desc, prec_name = workload_config(args.workload)
+    prec = capi.FP32 if (args.precision or prec_name) == "fp32" else capi.FP64
+    w = ws[0]
+    with capi.Stepper.from_workloads([w], precision=prec) as st:
+        stream = torch.cuda.current_stream()
+        st.set_stream(stream.cuda_stream)
+        st.set_state(0, w.xi0)
+        st.advance(2)
+        st.strain_stress(0, fields=False)
+        ms = [timed_events(stream, lambda: st.strain_stress(0, fields=False))[0] for _ in range(4)]
+    print(json.dumps({"diagnostic": "strain_stress (averages)", "workload": w_desc,
+                      "ms_median": statistics.median(ms), "ms": ms}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -512,11 +534,16 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the set-up's x-pencil tile widths instead of timing them (pfdd_gpu_autotune)")
+    ap.add_argument("--diagnostic-only", action="store_true",
+                    help="time only the strain/stress diagnostic (averages) on the workload's first instance, "
+                         "after two steps: a short run for profiling its kernels")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
     if args.impl == "reference":
         return reference_arm(args)
+    if args.diagnostic_only:
+        return diagnostic_only(args)
 
     import numpy as np
     import torch
